@@ -1,0 +1,173 @@
+"""Scenarios shared by the oracle tests and the CUDA-engine parity tests.
+
+Each function takes `api`: either the engine's `nestgpu` module or an
+`oracle.Oracle` instance; both expose the reference's nestgpu.py calling
+conventions.  The scenarios restate the reference's own tests
+(python/test/test_<model>.py, test_connect.py, test_brunel_list.py) and add
+seeded networks for bit-exact comparisons.
+"""
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden_traces():
+    return np.load(os.path.join(GOLDEN, "nest_traces.npz"))
+
+
+def trace_scenario(api, model):
+    """Single neuron driven by a two-spike spike_generator through every
+    receptor; returns the recorded V_m trace (mV, one row per 0.1 ms step).
+    Follows python/test/test_<model>.py of the reference."""
+    sg_times = [10.0, 400.0]
+    if model in ("aeif_cond_beta_multisynapse", "aeif_cond_alpha_multisynapse"):
+        neuron = api.Create(model, 1, 3)
+        st = {"V_peak": 0.0, "a": 4.0, "b": 80.5, "E_L": -70.6, "g_L": 300.0,
+              "E_rev": [20.0, 0.0, -85.0]}
+        if model == "aeif_cond_beta_multisynapse":
+            st["tau_decay"] = [40.0, 20.0, 30.0]
+            st["tau_rise"] = [20.0, 10.0, 5.0]
+        else:
+            st["tau_syn"] = [40.0, 20.0, 30.0]
+        api.SetStatus(neuron, st)
+        delay = [1.0, 100.0, 130.0]
+        weight = [0.1, 0.2, 0.5]
+        var = "V_m"
+    elif model in ("aeif_psc_exp_multisynapse", "aeif_psc_alpha_multisynapse"):
+        neuron = api.Create(model, 1, 2)
+        api.SetStatus(neuron, {"V_peak": 0.0, "a": 4.0, "b": 80.5, "E_L": -70.6, "g_L": 300.0,
+                               "tau_syn": [40.0, 20.0]})
+        delay = [1.0, 100.0]
+        weight = [1.0, -2.0]
+        var = "V_m"
+    elif model == "iaf_psc_exp":
+        neuron = api.Create("iaf_psc_exp")
+        delay = [1.0, 100.0]
+        weight = [1.0, -2.0]
+        var = "V_m_rel"
+    else:
+        raise ValueError(model)
+    spike = api.Create("spike_generator")
+    api.SetStatus(spike, {"spike_times": sg_times})
+    for syn in range(len(delay)):
+        api.Connect(spike, neuron, {"rule": "all_to_all"},
+                    {"receptor": syn, "weight": weight[syn], "delay": delay[syn]})
+    rec = api.CreateRecord("", [var], [neuron[0]], [0])
+    api.Simulate(800.0)
+    data = np.asarray(api.GetRecordData(rec), dtype=np.float64)
+    v = data[:, 1]
+    if model == "iaf_psc_exp":
+        v = -70.0 + v
+    return data[:, 0], v
+
+
+def trace_rmse(v, ref):
+    """The reference tests' metric: std of the difference at 1 ms sampling,
+    relative to |mean V_m| (python/test/test_aeif_cond_beta_multisynapse.py:45-50)."""
+    dv = np.array([v[i * 10 + 20] - ref[i, 1] for i in range(len(ref))])
+    return float(np.std(dv) / abs(np.mean(v)))
+
+
+def connect_scenario(api):
+    """python/test/test_connect.py: all_to_all with weight/delay arrays between even and
+    odd neurons; returns {section: [status dict | [weight, delay]]}."""
+    N = 5
+    neuron = api.Create("aeif_cond_beta_multisynapse", 2 * N)
+    even = [neuron[2 * i] for i in range(N)]
+    odd = [neuron[2 * i + 1] for i in range(N)]
+    e2o_d, e2o_w, o2e_d, o2e_w = [], [], [], []
+    for itgt in range(N):
+        ite, ito = 2 * itgt, 2 * itgt + 1
+        for isrc in range(N):
+            ise, iso = 2 * isrc, 2 * isrc + 1
+            e2o_d.append(2.0 * N * ise + ito)
+            e2o_w.append(100.0 * (2.0 * N * ise + ito))
+            o2e_d.append(2.0 * N * iso + ite)
+            o2e_w.append(100.0 * (2.0 * N * iso + ite))
+    api.Connect(even, odd, {"rule": "all_to_all"}, {"weight_array": e2o_w, "delay_array": e2o_d})
+    api.Connect(odd, even, {"rule": "all_to_all"}, {"weight_array": o2e_w, "delay_array": o2e_d})
+    out = {}
+    status = getattr(api, "GetConnectionStatus", None)
+
+    def st(ids, key=None):
+        if status is not None:
+            return status(ids, key)
+        return api.GetStatus(ids, key)
+
+    ids = api.GetConnections(even, neuron)
+    out["Even to all"] = st(ids)
+    out["Even to all weight, delat"] = st(ids, ["weight", "delay"])
+    out["All to odd"] = st(api.GetConnections(neuron, odd))
+    n36 = neuron[3:7]
+    out["Even to 3,4,5,6"] = st(api.GetConnections(even, n36))
+    out["3,4,5,6 to odd"] = st(api.GetConnections(n36, odd))
+    return out
+
+
+def fixed_train_network(api, n=60, n_in=20, seed=7, t_sim=300.0, model="aeif_cond_beta_multisynapse",
+                        record=True):
+    """Recurrent network driven by fixed spike_generator trains (no Poisson), for
+    bit-exact spike counts.  Connectivity comes from the engine's own RandomInt
+    stream (fixed_indegree / fixed_total_number with normal_clipped delays)."""
+    rng = np.random.RandomState(seed)
+    api.SetKernelStatus("rnd_seed", 1000 + seed)
+    if model == "iaf_psc_exp":
+        neuron = api.Create("iaf_psc_exp", n)
+        api.SetStatus(neuron, {"I_e": 370.0})
+        w_exc, w_inh, w_in = 35.0, -60.0, 90.0
+        rec_var = "V_m_rel"
+    else:
+        neuron = api.Create(model, n, 2)
+        api.SetStatus(neuron, {"E_rev": [0.0, -85.0], "I_e": 500.0})
+        w_exc, w_inh, w_in = 2.0, 4.0, 6.0
+        rec_var = "V_m"
+    n_exc = int(0.8 * n)
+    exc = neuron[0:n_exc]
+    inh = neuron[n_exc:n]
+    gens = api.Create("spike_generator", n_in)
+    for i in range(n_in):
+        t = np.cumsum(rng.exponential(8.0, size=64)) + 1.0
+        t = np.round(t[t < t_sim - 1.0], 1)
+        t = np.unique(t)
+        api.SetStatus([gens[i]], {"spike_times": [float(x) for x in t]})
+    api.Connect(exc, neuron, {"rule": "fixed_indegree", "indegree": 10},
+                {"weight": w_exc, "receptor": 0,
+                 "delay": {"distribution": "normal_clipped", "mu": 1.5, "low": 0.5, "high": 3.0,
+                           "sigma": 0.6}})
+    inh_port = 1
+    api.Connect(inh, neuron, {"rule": "fixed_total_number", "total_num": 4 * n},
+                {"weight": w_inh, "receptor": inh_port, "delay": 0.8})
+    api.Connect(gens, neuron, {"rule": "fixed_indegree", "indegree": 3},
+                {"weight": w_in, "receptor": 0, "delay": 1.0})
+    api.ActivateSpikeCount(neuron)
+    rec = None
+    if record:
+        rec = api.CreateRecord("", [rec_var] * 3 + ["spike"] * 2, [neuron[0], neuron[1], neuron[n - 1],
+                                                                  neuron[0], neuron[5]], [0] * 5)
+    api.Simulate(t_sim)
+    counts = np.asarray(api.GetStatus(neuron, "spike_count")).ravel().astype(np.int64)
+    data = np.asarray(api.GetRecordData(rec)) if record else None
+    return counts, data
+
+
+def poisson_network(api, n=200, rate=12000.0, t_sim=200.0, seed=3, model="aeif_cond_beta_multisynapse"):
+    """Neurons driven only by one poisson_generator (all_to_all) plus sparse recurrent
+    coupling; used for bit-exact comparison of the counter-based Poisson drive."""
+    api.SetKernelStatus("rnd_seed", seed)
+    pg = api.Create("poisson_generator")
+    api.SetStatus(pg, "rate", rate)
+    if model == "iaf_psc_exp":
+        neuron = api.Create("iaf_psc_exp", n)
+        w = 60.0
+    else:
+        neuron = api.Create(model, n, 2)
+        api.SetStatus(neuron, {"E_rev": [0.0, -85.0]})
+        w = 0.4
+    api.Connect(pg, neuron, {"rule": "all_to_all"}, {"weight": w, "delay": 0.2, "receptor": 0})
+    api.Connect(neuron, neuron, {"rule": "fixed_total_number", "total_num": 8 * n},
+                {"weight": w * 0.5, "delay": 1.3, "receptor": 0})
+    api.ActivateSpikeCount(neuron)
+    api.Simulate(t_sim)
+    return np.asarray(api.GetStatus(neuron, "spike_count")).ravel().astype(np.int64)

@@ -1,0 +1,139 @@
+"""The oracle pinned against the reference's own golden vectors (CPU only)."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle as orc
+from scenarios import GOLDEN, connect_scenario, golden_traces, trace_rmse, trace_scenario
+
+MODELS = ["aeif_cond_beta_multisynapse", "aeif_cond_alpha_multisynapse",
+          "aeif_psc_exp_multisynapse", "aeif_psc_alpha_multisynapse", "iaf_psc_exp"]
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+@pytest.mark.parametrize("model", MODELS)
+def test_trace_vs_nest_golden(model, fp64):
+    g = golden_traces()
+    ref = g[model]
+    tol = float(g[model + "__tolerance"])
+    t, v = trace_scenario(orc.Oracle(fp64=fp64), model)
+    assert len(t) == 8001
+    assert abs(t[0]) < 1e-6 and abs(t[-1] - 800.0) < 1e-3
+    rmse = trace_rmse(v, ref)
+    assert rmse < tol, (model, rmse, tol)
+
+
+def test_fp32_mirror_close_to_fp64():
+    """The FP32 arithmetic stays within 1e-5 relative of the FP64 oracle on the
+    non-chaotic single-neuron traces."""
+    for model in MODELS:
+        _, v32 = trace_scenario(orc.Oracle(fp64=False), model)
+        _, v64 = trace_scenario(orc.Oracle(fp64=True), model)
+        rel = np.max(np.abs(v32 - v64) / np.maximum(np.abs(v64), 1.0))
+        assert rel < 1e-5, (model, rel)
+
+
+def test_connect_log_golden():
+    """Connection order and status against python/test/logp3_connect.txt."""
+    gold = json.load(open(os.path.join(GOLDEN, "connect_log.json")))
+    got = connect_scenario(orc.Oracle())
+    assert list(gold) == list(got)
+    for sec in gold:
+        assert len(gold[sec]) == len(got[sec]), sec
+        for a, b in zip(gold[sec], got[sec]):
+            if isinstance(a, dict):
+                for k in ("source", "target", "port", "syn"):
+                    assert a[k] == b[k], (sec, a, b)
+                assert a["delay"] == pytest.approx(b["delay"], rel=1e-6)
+                assert a["weight"] == pytest.approx(b["weight"], rel=1e-6)
+            else:
+                assert a == pytest.approx(b, rel=1e-6)
+
+
+def test_exp_log_accuracy():
+    xs = np.concatenate([np.linspace(-103.0, 88.0, 20001), np.linspace(-1, 1, 2001),
+                         np.array([0.0, 1e-8, -1e-8, 88.72, -87.3])]).astype(np.float32)
+    worst = 0.0
+    for x in xs:
+        y = orc.exp_m(float(x))
+        ref = math.exp(float(x))
+        if ref < 1.2e-38:
+            continue
+        worst = max(worst, abs(y - ref) / ref)
+    assert worst < 2.5e-7, worst
+    assert orc.exp_m(100.0) == float("inf")
+    assert orc.exp_m(-200.0) == 0.0
+    ls = np.concatenate([np.logspace(-30, 30, 4001), np.linspace(0.5, 2.0, 2001)]).astype(np.float32)
+    worst = 0.0
+    for x in ls:
+        y = orc.log_m(float(x))
+        ref = math.log(float(x))
+        worst = max(worst, abs(y - ref) / max(abs(ref), 1e-3))
+    assert worst < 5e-7, worst
+
+
+def test_philox_known_answers():
+    """Philox4x32-10 known-answer vectors published with Random123 (kat_vectors)."""
+    assert orc.philox([0, 0, 0, 0], [0, 0]) == [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]
+    assert orc.philox([0xffffffff] * 4, [0xffffffff] * 2) == [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]
+    assert orc.philox([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344], [0xa4093822, 0x299f31d0]) == \
+        [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]
+
+
+@pytest.mark.parametrize("lam", [0.05, 0.8, 2.0, 9.5, 37.0])
+def test_poisson_sampler_moments(lam):
+    n = 20000
+    x = np.array([orc.poisson_draw(lam, 12345, e, 17) for e in range(n)], dtype=np.float64)
+    se = math.sqrt(lam / n)
+    assert abs(x.mean() - lam) < 5 * se
+    assert abs(x.var() - lam) < 6 * lam * math.sqrt(2.0 / n) + 5 * se
+
+
+def test_spike_buffer_delay_semantics():
+    """A spike emitted in step n reaches a delay-D target in step n+D and is
+    integrated from step n+D+1 on (src/spike_buffer.cu:247-317, nestgpu.cu:469-635)."""
+    o = orc.Oracle()
+    sg = o.Create("spike_generator")
+    nrn = o.Create("iaf_psc_exp")
+    o.SetStatus(sg, {"spike_times": [1.0]})
+    o.Connect(sg, nrn, {"rule": "all_to_all"}, {"weight": 100.0, "delay": 0.5, "receptor": 0})
+    o.CreateRecord("", ["I_syn_ex"], [nrn[0]], [0])
+    o.Simulate(3.0)
+    d = o.GetRecordData()
+    nz = np.nonzero(d[:, 1])[0]
+    # spike emitted in step 10 (t: 1.0 -> 1.1), D = 5 steps: collected and folded at the
+    # end of step 15; record row k is written after step k-1, before that step's fold,
+    # so the input first shows in row 17, already decayed by one step of P11ex.
+    assert nz[0] == 17, nz[:3]
+    assert d[17, 1] == pytest.approx(100.0 * math.exp(-0.1 / 2.0), rel=1e-6)
+
+
+def test_fixed_indegree_shares_source_draw():
+    """Reference quirk: one RandomInt draw per Connect call, identical source list for
+    every target (src/connect_rules.h:203-269)."""
+    o = orc.Oracle()
+    o.SetKernelStatus("rnd_seed", 77)
+    src = o.Create("iaf_psc_exp", 100)
+    tgt = o.Create("iaf_psc_exp", 7)
+    o.Connect(src, tgt, {"rule": "fixed_indegree", "indegree": 5}, {"weight": 1.0, "delay": 1.0})
+    a = o.ConnectionArrays()
+    per_target = {}
+    for s, t in zip(a["source"], a["target"]):
+        per_target.setdefault(int(t), set()).add(int(s))
+    sets = list(per_target.values())
+    assert len(sets) == 7 and all(len(s) == 5 for s in sets)
+    assert all(s == sets[0] for s in sets)
+
+
+def test_oracle_errors_like_reference():
+    o = orc.Oracle()
+    a = o.Create("iaf_psc_exp", 3)
+    with pytest.raises(ValueError, match="Delay must be >= time resolution"):
+        o.Connect(a, a, {"rule": "all_to_all"}, {"weight": 1.0, "delay": 0.05})
+    with pytest.raises(ValueError, match="Indegree larger than number of source nodes"):
+        o.Connect(a, a, {"rule": "fixed_indegree", "indegree": 4}, {"weight": 1.0, "delay": 1.0})
+    with pytest.raises(ValueError, match="one-to-one"):
+        o.Connect(a, a[0:2], {"rule": "one_to_one"}, {"weight": 1.0, "delay": 1.0})
