@@ -1,0 +1,238 @@
+/*
+ * nestgpu_b200.h -- C ABI of the B200 spiking engine (libnestgpu_b200.so).
+ *
+ * The NESTGPU_* entry points have exactly the names, argument types and
+ * meaning of the reference's C ABI (NEST GPU 1.08, src/nestgpu_C.h); the line
+ * cited beside each group is where the reference declares the function this
+ * one replaces.  A program bound to the reference library (pythonlib/nestgpu.py
+ * loads it with ctypes through NESTGPU_LIB) binds to this one unchanged.
+ *
+ * Conventions shared with the reference:
+ *  - every call first clears the error state; on failure it sets an error code
+ *    (2: engine error, 1: allocation failure, 255: other) and a message, read
+ *    with NESTGPU_GetErrorCode / NESTGPU_GetErrorMessage;
+ *  - NESTGPU_SetOnException(0) (the default) makes a failing call print the
+ *    message and exit the process with the code; 1 returns to the caller;
+ *  - getters return host arrays the caller owns (malloc'd), except
+ *    NESTGPU_GetRecordData and NESTGPU_GetRecSpikeTimes, which point into
+ *    engine-owned storage valid until the next call of the same function.
+ *  - MPI entry points exist for binary compatibility: one process, rank 0.
+ *
+ * Entry points prefixed NGPU_ are engine extensions with no counterpart in
+ * the reference; each says so.
+ */
+#ifndef NESTGPU_B200_H
+#define NESTGPU_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* errors, seeds, kernel settings: src/nestgpu_C.h:34-52 */
+char *NESTGPU_GetErrorMessage();
+unsigned char NESTGPU_GetErrorCode();
+void NESTGPU_SetOnException(int on_exception);
+int NESTGPU_SetRandomSeed(unsigned long long seed);
+int NESTGPU_SetTimeResolution(float time_res);
+float NESTGPU_GetTimeResolution();
+int NESTGPU_SetMaxSpikeBufferSize(int max_size);
+int NESTGPU_GetMaxSpikeBufferSize();
+int NESTGPU_SetSimTime(float sim_time);
+int NESTGPU_SetVerbosityLevel(int verbosity_level);
+
+/* node creation and records: src/nestgpu_C.h:54-66 */
+int NESTGPU_Create(char *model_name, int n_neuron, int n_port);
+int NESTGPU_CreatePoissonGenerator(int n_node, float rate);
+int NESTGPU_CreateRecord(char *file_name, char *var_name_arr[], int *i_node_arr, int *port_arr,
+                         int n_node);
+int NESTGPU_GetRecordDataRows(int i_record);
+int NESTGPU_GetRecordDataColumns(int i_record);
+float **NESTGPU_GetRecordData(int i_record);
+
+/* parameters and variables: src/nestgpu_C.h:68-141 */
+int NESTGPU_SetNeuronScalParam(int i_node, int n_neuron, char *param_name, float val);
+int NESTGPU_SetNeuronArrayParam(int i_node, int n_neuron, char *param_name, float *param,
+                                int array_size);
+int NESTGPU_SetNeuronPtScalParam(int *i_node, int n_neuron, char *param_name, float val);
+int NESTGPU_SetNeuronPtArrayParam(int *i_node, int n_neuron, char *param_name, float *param,
+                                  int array_size);
+int NESTGPU_IsNeuronScalParam(int i_node, char *param_name);
+int NESTGPU_IsNeuronPortParam(int i_node, char *param_name);
+int NESTGPU_IsNeuronArrayParam(int i_node, char *param_name);
+int NESTGPU_SetNeuronIntVar(int i_node, int n_neuron, char *var_name, int val);
+int NESTGPU_SetNeuronScalVar(int i_node, int n_neuron, char *var_name, float val);
+int NESTGPU_SetNeuronArrayVar(int i_node, int n_neuron, char *var_name, float *var, int array_size);
+int NESTGPU_SetNeuronPtIntVar(int *i_node, int n_neuron, char *var_name, int val);
+int NESTGPU_SetNeuronPtScalVar(int *i_node, int n_neuron, char *var_name, float val);
+int NESTGPU_SetNeuronPtArrayVar(int *i_node, int n_neuron, char *var_name, float *var,
+                                int array_size);
+int NESTGPU_IsNeuronIntVar(int i_node, char *var_name);
+int NESTGPU_IsNeuronScalVar(int i_node, char *var_name);
+int NESTGPU_IsNeuronPortVar(int i_node, char *var_name);
+int NESTGPU_IsNeuronArrayVar(int i_node, char *var_name);
+int NESTGPU_GetNeuronParamSize(int i_node, char *param_name);
+int NESTGPU_GetNeuronVarSize(int i_node, char *var_name);
+float *NESTGPU_GetNeuronParam(int i_node, int n_neuron, char *param_name);
+float *NESTGPU_GetNeuronPtParam(int *i_node, int n_neuron, char *param_name);
+float *NESTGPU_GetArrayParam(int i_node, char *param_name);
+int *NESTGPU_GetNeuronIntVar(int i_node, int n_neuron, char *param_name);
+int *NESTGPU_GetNeuronPtIntVar(int *i_node, int n_neuron, char *param_name);
+float *NESTGPU_GetNeuronVar(int i_node, int n_neuron, char *param_name);
+float *NESTGPU_GetNeuronPtVar(int *i_node, int n_neuron, char *param_name);
+float *NESTGPU_GetArrayVar(int i_node, char *var_name);
+
+/* simulation control: src/nestgpu_C.h:143-151 */
+int NESTGPU_Calibrate();
+int NESTGPU_Simulate();
+int NESTGPU_StartSimulation();
+int NESTGPU_SimulationStep();
+int NESTGPU_EndSimulation();
+
+/* MPI (single process: rank 0 of 1): src/nestgpu_C.h:153-161 */
+int NESTGPU_ConnectMpiInit(int argc, char *argv[]);
+int NESTGPU_MpiId();
+int NESTGPU_MpiNp();
+int NESTGPU_ProcMaster();
+int NESTGPU_MpiFinalize();
+
+/* random numbers from the connection generator: src/nestgpu_C.h:163-170 */
+unsigned int *NESTGPU_RandomInt(size_t n);
+float *NESTGPU_RandomUniform(size_t n);
+float *NESTGPU_RandomNormal(size_t n, float mean, float stddev);
+float *NESTGPU_RandomNormalClipped(size_t n, float mean, float stddev, float vmin, float vmax,
+                                   float vstep);
+
+/* connections: src/nestgpu_C.h:172-222 */
+int NESTGPU_Connect(int i_source_node, int i_target_node, unsigned char port,
+                    unsigned char syn_group, float weight, float delay);
+int NESTGPU_ConnSpecInit();
+int NESTGPU_SetConnSpecParam(char *param_name, int value);
+int NESTGPU_ConnSpecIsParam(char *param_name);
+int NESTGPU_SynSpecInit();
+int NESTGPU_SetSynSpecIntParam(char *param_name, int value);
+int NESTGPU_SetSynSpecFloatParam(char *param_name, float value);
+int NESTGPU_SetSynSpecFloatPtParam(char *param_name, float *array_pt);
+int NESTGPU_SynSpecIsIntParam(char *param_name);
+int NESTGPU_SynSpecIsFloatParam(char *param_name);
+int NESTGPU_SynSpecIsFloatPtParam(char *param_name);
+int NESTGPU_ConnectSeqSeq(int i_source, int n_source, int i_target, int n_target);
+int NESTGPU_ConnectSeqGroup(int i_source, int n_source, int *i_target, int n_target);
+int NESTGPU_ConnectGroupSeq(int *i_source, int n_source, int i_target, int n_target);
+int NESTGPU_ConnectGroupGroup(int *i_source, int n_source, int *i_target, int n_target);
+int NESTGPU_RemoteConnectSeqSeq(int i_source_host, int i_source, int n_source, int i_target_host,
+                                int i_target, int n_target);
+int NESTGPU_RemoteConnectSeqGroup(int i_source_host, int i_source, int n_source,
+                                  int i_target_host, int *i_target, int n_target);
+int NESTGPU_RemoteConnectGroupSeq(int i_source_host, int *i_source, int n_source,
+                                  int i_target_host, int i_target, int n_target);
+int NESTGPU_RemoteConnectGroupGroup(int i_source_host, int *i_source, int n_source,
+                                    int i_target_host, int *i_target, int n_target);
+
+/* names: src/nestgpu_C.h:224-254 */
+char **NESTGPU_GetIntVarNames(int i_node);
+char **NESTGPU_GetScalVarNames(int i_node);
+int NESTGPU_GetNIntVar(int i_node);
+int NESTGPU_GetNScalVar(int i_node);
+char **NESTGPU_GetPortVarNames(int i_node);
+int NESTGPU_GetNPortVar(int i_node);
+char **NESTGPU_GetScalParamNames(int i_node);
+int NESTGPU_GetNScalParam(int i_node);
+char **NESTGPU_GetPortParamNames(int i_node);
+int NESTGPU_GetNGroupParam(int i_node);
+char **NESTGPU_GetGroupParamNames(int i_node);
+int NESTGPU_GetNPortParam(int i_node);
+char **NESTGPU_GetArrayParamNames(int i_node);
+int NESTGPU_GetNArrayParam(int i_node);
+char **NESTGPU_GetArrayVarNames(int i_node);
+int NESTGPU_GetNArrayVar(int i_node);
+
+/* connection queries: src/nestgpu_C.h:256-273 */
+int *NESTGPU_GetSeqSeqConnections(int i_source, int n_source, int i_target, int n_target,
+                                  int syn_group, int *n_conn);
+int *NESTGPU_GetSeqGroupConnections(int i_source, int n_source, int *i_target, int n_target,
+                                    int syn_group, int *n_conn);
+int *NESTGPU_GetGroupSeqConnections(int *i_source, int n_source, int i_target, int n_target,
+                                    int syn_group, int *n_conn);
+int *NESTGPU_GetGroupGroupConnections(int *i_source, int n_source, int *i_target, int n_target,
+                                      int syn_group, int *n_conn);
+int NESTGPU_GetConnectionStatus(int i_source, int i_group, int i_conn, int *i_target,
+                                unsigned char *port, unsigned char *syn_group, float *delay,
+                                float *weight);
+
+/* synapse groups (plasticity; not supported, error 2): src/nestgpu_C.h:275-287 */
+int NESTGPU_CreateSynGroup(char *model_name);
+int NESTGPU_GetSynGroupNParam(int i_syn_group);
+char **NESTGPU_GetSynGroupParamNames(int i_syn_group);
+int NESTGPU_IsSynGroupParam(int i_syn_group, char *param_name);
+int NESTGPU_GetSynGroupParamIdx(int i_syn_group, char *param_name);
+float NESTGPU_GetSynGroupParam(int i_syn_group, char *param_name);
+int NESTGPU_SetSynGroupParam(int i_syn_group, char *param_name, float val);
+
+/* spike counting and spike-time recording: src/nestgpu_C.h:289-301 */
+int NESTGPU_ActivateSpikeCount(int i_node, int n_node);
+int NESTGPU_ActivateRecSpikeTimes(int i_node, int n_node, int max_n_rec_spike_times);
+int NESTGPU_SetRecSpikeTimesStep(int i_node, int n_node, int rec_spike_times_step);
+int NESTGPU_GetNRecSpikeTimes(int i_node);
+int NESTGPU_GetRecSpikeTimes(int i_node, int n_node, int **n_spike_times_pt,
+                             float ***spike_times_pt);
+
+/* external neurons (not supported, error 2): src/nestgpu_C.h:303-307 */
+int NESTGPU_PushSpikesToNodes(int n_spikes, int *node_id);
+int NESTGPU_GetExtNeuronInputSpikes(int *n_spikes, int **node, int **port, float **spike_height,
+                                    int include_zeros);
+
+/* group parameters and kernel parameters: src/nestgpu_C.h:309-352 */
+int NESTGPU_SetNeuronGroupParam(int i_node, int n_node, char *param_name, float val);
+int NESTGPU_IsNeuronGroupParam(int i_node, char *param_name);
+float NESTGPU_GetNeuronGroupParam(int i_node, char *param_name);
+int NESTGPU_GetNBoolParam();
+char **NESTGPU_GetBoolParamNames();
+int NESTGPU_IsBoolParam(char *param_name);
+int NESTGPU_GetBoolParamIdx(char *param_name);
+bool NESTGPU_GetBoolParam(char *param_name);
+int NESTGPU_SetBoolParam(char *param_name, bool val);
+int NESTGPU_GetNFloatParam();
+char **NESTGPU_GetFloatParamNames();
+int NESTGPU_IsFloatParam(char *param_name);
+int NESTGPU_GetFloatParamIdx(char *param_name);
+float NESTGPU_GetFloatParam(char *param_name);
+int NESTGPU_SetFloatParam(char *param_name, float val);
+int NESTGPU_GetNIntParam();
+char **NESTGPU_GetIntParamNames();
+int NESTGPU_IsIntParam(char *param_name);
+int NESTGPU_GetIntParamIdx(char *param_name);
+int NESTGPU_GetIntParam(char *param_name);
+int NESTGPU_SetIntParam(char *param_name, int val);
+int NESTGPU_RemoteCreate(int i_host, char *model_name, int n_neuron, int n_port);
+
+/* ---- engine extensions (no counterpart in the reference) ---- */
+
+/* Release an array returned by a getter (the reference's Python front-end leaks them). */
+void NGPU_FreeArray(void *p);
+
+/* Destroy the engine instance so that the next call starts a new, empty network. */
+int NGPU_Reset();
+
+/* Counters since calibration: RK5 derivative evaluations, synaptic events delivered,
+   spikes emitted; wall time of the last Simulate step loop [s]; steps run; device status bits
+   (1 ring overflow, 2 RK5 iteration cap, 4 V_m/w guard reset, 8 spike-time buffer full). */
+int NGPU_GetStats(unsigned long long *n_derivs, unsigned long long *n_events,
+                  unsigned long long *n_spikes, double *sim_seconds, long long *steps,
+                  unsigned int *status);
+
+/* Bulk connection import: n edges with their own source, target, receptor, weight and
+   delay (ms).  Same validation and storage as n single connections, without per-call cost. */
+int NGPU_ConnectArrays(size_t n, int *source, int *target, unsigned char *port, float *weight,
+                       float *delay);
+
+/* Steps captured per CUDA graph (default 100). */
+int NGPU_SetGraphSteps(int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,268 @@
+// Host runtime of the spiking engine: node groups with structure-of-arrays
+// state, the connection store and rules, calibration into the device layout
+// (CSR by (source, delay), target-major poiss_gen edges, spike ring), and the
+// CUDA-graph step loop.  One process-wide instance sits behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <curand.h>
+
+#include <cstdint>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "ngpu_types.h"
+
+namespace ngpu {
+
+// Error with the reference's C-ABI code 2 (ngpu_exception).
+struct NgpuError : public std::runtime_error {
+  explicit NgpuError(const std::string &m) : std::runtime_error(m) {}
+};
+
+// Kinds of named quantities of a node group.
+enum Kind { K_NONE = -1, K_SCAL_VAR = 0, K_PORT_VAR, K_SCAL_PARAM, K_PORT_PARAM, K_GROUP_PARAM,
+            K_ARRAY_PARAM, K_INT_VAR };
+
+struct Group {
+  int model = 0;
+  int i0 = 0, n = 0, nport = 0;
+  // user-visible parameters [param][neuron] (scalar params then port params port-major)
+  std::vector<std::vector<float>> par;
+  // state variables [var][neuron]: authoritative on the host until calibration
+  std::vector<std::vector<float>> var;
+  float h_min_rel = 1.0e-3f, h0_rel = 1.0e-2f;
+  // spike_generator
+  std::vector<std::vector<float>> sg_times, sg_heights;
+  // recording options
+  bool spike_count_on = false;
+  int max_rec = 0;
+  int rec_times_step = 0;
+  std::vector<std::vector<float>> rec_times_host;   // drained, not yet handed out
+  std::vector<std::vector<float>> rec_export;       // handed out by the last query
+  std::vector<int> rec_n_host;                   // exported counts
+  std::vector<float *> rec_ptr_host;             // exported row pointers
+  // device state
+  float *d_var = nullptr;        // [nvar][n]
+  float *d_refr = nullptr;       // aeif refractory counter
+  double *d_x = nullptr;
+  float *d_h = nullptr;
+  size_t acc_off = 0;
+  std::vector<float *> d_der;    // derived-parameter arrays (null = uniform)
+  std::vector<float> der_val;    // derived-parameter uniform values
+  int *d_spike_count = nullptr;
+  int *d_n_rec = nullptr;
+  float *d_rec_times = nullptr;
+  int *d_pin_off = nullptr;
+  PoissonIn *d_pin = nullptr;
+  int *d_sg_off = nullptr, *d_sg_tidx = nullptr, *d_sg_next = nullptr;
+  float *d_sg_h = nullptr;
+  int gen0 = -1;                 // poiss_gen: first row in the generator table
+  bool dirty = true;             // parameters changed since last upload
+};
+
+struct RecordSpec {
+  std::string file;
+  std::vector<std::string> var;
+  std::vector<int> node, port;
+  std::vector<std::vector<float>> data;
+  std::vector<float *> row_ptr;
+  FILE *fp = nullptr;
+};
+
+struct EngineStats {
+  unsigned long long n_derivs = 0;      // RK5 derivative evaluations
+  unsigned long long n_events = 0;      // synaptic events delivered
+  unsigned long long n_spikes = 0;
+  double sim_seconds = 0.0;             // wall time inside the step loop of the last Simulate
+  long long steps = 0;
+  unsigned status = 0;
+};
+
+class Engine {
+ public:
+  Engine();
+  ~Engine();
+
+  // ---- kernel settings (src/nestgpu.cu:64-99, 1705-1947)
+  float dt = 0.1f;
+  unsigned long long seed = 54321ULL;
+  unsigned long long kernel_seed = 54321ULL + 12345ULL;
+  int max_spike_buffer_size = 20;
+  int verbosity = 4;
+  bool print_time = false;
+  float max_spike_num_fact = 1.0f;
+  float max_spike_per_host_fact = 1.0f;
+  int remote_spike_height = 0;
+  float sim_time = 1000.0f;
+  int graph_steps = 100;          // steps per captured CUDA graph
+  bool use_device_rng = true;     // cuRAND device generator (as the reference) if a GPU exists
+
+  void set_seed(unsigned long long s);
+  void set_time_resolution(float t);
+
+  // ---- nodes
+  int create(const std::string &model, int n, int nport);
+  int create_poisson_generator(int n, float rate);
+  Group &group_of(int node);
+  int group_index(int node);
+  int n_nodes() const { return (int)node_group_.size(); }
+  Kind locate(int node, const std::string &name, int *idx = nullptr);
+  std::vector<std::string> names(int node, Kind k);
+  int param_size(int node, const std::string &name);
+  int var_size(int node, const std::string &name);
+
+  void set_scalar(const std::vector<int> &nodes, const std::string &name, float v);
+  void set_port_or_array(const std::vector<int> &nodes, const std::string &name, const float *a, int sz);
+  void set_int_var(const std::vector<int> &nodes, const std::string &name, int v);
+  std::vector<float> get_values(const std::vector<int> &nodes, const std::string &name);   // node-major
+  std::vector<int> get_int_values(const std::vector<int> &nodes, const std::string &name);
+  std::vector<float> get_array_param(int node, const std::string &name);
+  void set_group_param(const std::vector<int> &nodes, const std::string &name, float v);
+  float get_group_param(int node, const std::string &name);
+
+  // ---- random numbers (cuRAND, as src/random.cu:8-76)
+  std::vector<unsigned> random_int(size_t n);
+  std::vector<float> random_uniform(size_t n);
+  std::vector<float> random_normal(size_t n, float mean, float sd);
+  std::vector<float> random_normal_clipped(size_t n, float mean, float sd, float vmin, float vmax,
+                                           float vstep);
+
+  // ---- connections
+  void connect1(int src, int tgt, int port, int syn_group, float w, float d);
+  void connect_rule(int rule, const int *src_arr, int src0, int ns, const int *tgt_arr, int tgt0,
+                    int nt, int degree, int port, int syn_group, float w, float d,
+                    const float *warr, const float *darr);
+  size_t n_connections() const { return c_src_.size(); }
+  // ids (source, group, index) in reference order, filtered
+  std::vector<int> get_connections(const int *src_arr, int src0, int ns, const int *tgt_arr,
+                                   int tgt0, int nt);
+  void connection_status(int src, int grp, int idx, int *tgt, unsigned char *port,
+                         unsigned char *syn, float *delay, float *w);
+  // Bulk import of a prebuilt edge list (engine extension, used by the large benchmarks).
+  void connect_arrays(size_t n, const int *src, const int *tgt, const unsigned char *port,
+                      const float *w, const float *d);
+  void connect_fixed_indegree_per_target(int src0, int ns, int tgt0, int nt, int k, int port,
+                                         float w, float dmin_ms, float dmax_ms, uint64_t seed);
+
+  // ---- recording
+  int create_record(const std::string &file, const std::vector<std::string> &vars,
+                    const std::vector<int> &nodes, const std::vector<int> &ports);
+  RecordSpec &record(int i);
+  void activate_spike_count(int i_node, int n);
+  void activate_rec_spike_times(int i_node, int n, int max_n);
+  void set_rec_spike_times_step(int i_node, int n, int step);
+  int n_rec_spike_times(int node);
+  void get_rec_spike_times(int i_node, int n, int **n_pt, float ***t_pt);
+
+  // ---- simulation
+  void calibrate();
+  void simulate(float t);
+  void start_simulation();
+  void simulation_step();
+  void end_simulation();
+  bool calibrated() const { return calibrated_; }
+  double neural_time() const { return neural_time_; }
+  EngineStats stats();
+
+  // device buffers exposed to the engine-level helpers
+  cudaStream_t stream() const { return stream_; }
+
+ private:
+  std::vector<Group> groups_;
+  std::vector<int> node_group_;
+  std::vector<RecordSpec> records_;
+  // connection store, insertion order
+  std::vector<int> c_src_, c_tgt_;
+  std::vector<unsigned char> c_port_;
+  std::vector<float> c_w_;
+  std::vector<int> c_d_;
+  // reference order cache: permutation, group index and index-in-group per edge
+  bool order_valid_ = false;
+  std::vector<long long> ord_;          // edge ids in reference order
+  std::vector<long long> src_first_;    // per source: first position in ord_
+  std::vector<int> ord_grp_, ord_idx_;  // per position
+  void build_order();
+
+  curandGenerator_t gen_ = nullptr;
+  bool gen_device_ = false;
+  void make_generator();
+
+  // simulation state
+  bool calibrated_ = false;
+  bool first_sim_ = true;
+  bool in_sim_ = false;
+  double neural_time_ = 0.0;
+  double neur_t0_ = 0.0;
+  long long it_ = 0, Nt_ = 0;
+  long long tidx_base_ = 0;
+
+  // device
+  cudaStream_t stream_ = nullptr;
+  Clock *d_clk_ = nullptr;
+  double *d_acc_ = nullptr;
+  size_t n_acc_ = 0;
+  int2 *d_ring_ = nullptr;
+  int *d_ring_cnt_ = nullptr;
+  int R_ = 0, cap_ = 0;
+  unsigned char *d_has_out_ = nullptr;
+  int *d_last_tidx_ = nullptr;
+  float *d_last_h_ = nullptr;
+  unsigned *d_status_ = nullptr;
+  long long *d_ev_off_ = nullptr;
+  EdgeW *d_edge_ = nullptr;
+  size_t n_edge_dev_ = 0;
+  int dmin_ = 0, dspan_ = 1;
+  GenPar *d_gen_ = nullptr;
+  int n_gen_ = 0;
+  unsigned long long *d_counters_ = nullptr;   // [0] derivs, [1] events
+  RecCol *d_cols_ = nullptr;
+  float *d_recbuf_ = nullptr;
+  int rec_ncol_ = 0, rec_rows_cap_ = 0;
+  std::vector<std::pair<int, int>> rec_cols_;  // (record, column)
+  int deliver_blocks_ = 148;
+  std::map<int, cudaGraphExec_t> graphs_;
+  std::vector<void *> allocs_;
+  double last_sim_seconds_ = 0.0;
+  long long total_steps_ = 0;
+  unsigned status_seen_ = 0;
+
+  template <class T> T *dalloc(size_t n);
+  void free_device();
+  void upload_params();
+  void build_records();
+  void launch_step(int k);
+  void launch_flush();
+  void run_steps(long long n);
+  void drain_records(long long rows);
+  void drain_rec_spike_times();
+  void invalidate_graphs();
+  SpikeOut spike_out() const;
+  AeifArgs aeif_args(Group &g);
+  IafArgs iaf_args(Group &g);
+  SpikeGenArgs sg_args(Group &g);
+  DeliverArgs deliver_args();
+  void check_status();
+};
+
+Engine &engine();
+void engine_reset();
+
+// launchers (ngpu_kernels.cu)
+void launch_aeif(int model, bool flush, const AeifArgs &A, const SpikeOut &so, Clock *clk, int k,
+                 cudaStream_t st);
+void launch_iaf(bool flush, const IafArgs &A, const SpikeOut &so, Clock *clk, int k, float dt,
+                cudaStream_t st);
+void launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, Clock *clk, int k, float dt,
+                      cudaStream_t st);
+void launch_deliver(const DeliverArgs &A, int n_blocks, Clock *clk, int k, float dt, cudaStream_t st);
+void launch_record(const RecCol *cols, int ncol, float *buf, const int *last_tidx,
+                   const float *last_height, const unsigned char *has_out, Clock *clk, int k,
+                   float dt, cudaStream_t st);
+void launch_clock_advance(Clock *clk, int K, cudaStream_t st);
+void launch_clock_clear_pending(Clock *clk, cudaStream_t st);
+int deliver_max_dspan();
+
+}  // namespace ngpu

@@ -1,0 +1,795 @@
+// Calibration into the device layout and the CUDA-graph step loop.
+//
+// Device layout (structure of arrays, one allocation per array):
+//   per group   state [nvar][n] float, aeif x [n] double, h [n] float, refractory [n] float;
+//               derived parameters: uniform -> kernel argument, else [n] float array;
+//               target-major poiss_gen in-edges (pin_off [n+1], PoissonIn [..]).
+//   global      acc [sum(n*nport)] double (spike input of the previous step);
+//               recurrent edges sorted by (source, delay): EdgeW {acc index, weight},
+//               ev_off [n_nodes*dspan + 1] int64 segment starts;
+//               spike ring [R][cap] (node, height) with counts [R], R = max delay + 3;
+//               per node has_out, last spike time index and height; clock; counters.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+
+#include "ngpu_engine.h"
+
+namespace ngpu {
+
+enum { A_V_th = 0, A_Delta_T, A_g_L, A_E_L, A_C_m, A_a, A_b, A_tau_w, A_I_e, A_V_peak,
+       A_V_reset, A_t_ref, A_refractory_step, A_den_delay, A_NSCAL };
+enum { I_tau_m = 0, I_C_m, I_E_L, I_I_e, I_Theta_rel, I_V_reset_rel, I_tau_ex, I_tau_in, I_t_ref,
+       I_den_delay, I_P20, I_P11ex, I_P11in, I_P21ex, I_P21in, I_P22, I_NPAR };
+enum { PG_rate = 0, PG_origin, PG_start, PG_stop };
+
+static bool is_aeif(int m) { return m <= M_AEIF_PSC_ALPHA; }
+static int n_port_par(int m) {
+  switch (m) {
+  case M_AEIF_COND_BETA: return 4;
+  case M_AEIF_COND_ALPHA: return 3;
+  case M_AEIF_PSC_EXP: return 1;
+  case M_AEIF_PSC_ALPHA: return 2;
+  default: return 0;
+  }
+}
+static int n_port_var(int m) { return m == M_AEIF_PSC_EXP ? 1 : 2; }
+
+static void cuda_check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess)
+    throw NgpuError(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+template <class T> T *Engine::dalloc(size_t n) {
+  T *p = nullptr;
+  if (n == 0) n = 1;
+  cuda_check(cudaMalloc((void **)&p, n * sizeof(T)), "cudaMalloc");
+  allocs_.push_back(p);
+  return p;
+}
+
+void Engine::free_device() {
+  for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+  graphs_.clear();
+  for (void *p : allocs_) cudaFree(p);
+  allocs_.clear();
+  if (stream_) cudaStreamDestroy(stream_);
+  stream_ = nullptr;
+}
+
+void Engine::invalidate_graphs() {
+  for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+  graphs_.clear();
+}
+
+// propagator_32 of src/propagator_stability.cu:31-52 (double precision)
+static double propagator_32(double tau_syn, double tau, double C, double h) {
+  const double P32_linear = 1.0 / (2.0 * C * tau * tau) * h * h * (tau_syn - tau) * std::exp(-h / tau);
+  const double P32_singular = h / C * std::exp(-h / tau);
+  const double P32 = -tau / (C * (1.0 - tau / tau_syn)) * std::exp(-h / tau_syn) *
+                     std::expm1(h * (1.0 / tau_syn - 1.0 / tau));
+  const double dev_P32 = std::fabs(P32 - P32_singular);
+  if (tau == tau_syn || (std::fabs(tau - tau_syn) < 0.1 && dev_P32 > 2.0 * std::fabs(P32_linear)))
+    return P32_singular;
+  return P32;
+}
+
+// ---------------------------------------------------------------------------
+// Calibrate (src/nestgpu.cu:294-352 and the models' Calibrate methods)
+// ---------------------------------------------------------------------------
+void Engine::calibrate() {
+  if (calibrated_) throw NgpuError("Calibration can be made only once");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    throw NgpuError("no CUDA device: the engine needs a GPU to calibrate and simulate");
+  }
+  if (verbosity >= 1) printf("Calibrating ...\n");
+  calibrated_ = true;
+  neural_time_ = 0.0;
+  cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+  const int N = n_nodes();
+
+  // ---- model-level calibration on the host parameter tables
+  size_t acc_total = 0;
+  for (auto &g : groups_) {
+    if (is_aeif(g.model)) {
+      const int npp = n_port_par(g.model);
+      for (int i = 0; i < g.n; i++) {
+        if (g.par[A_den_delay][i] != 0.0f) throw NgpuError("dendritic delay is not supported");
+        g.par[A_refractory_step][i] = 0.0f;
+        for (int p = 0; p < g.nport; p++) {
+          auto P = [&](int k) -> float & { return g.par[A_NSCAL + npp * p + k][i]; };
+          if (g.model == M_AEIF_COND_BETA) {
+            // g0 normalisation (src/aeif_cond_beta_multisynapse.cu:70-99)
+            float td = P(2), tr = P(1);
+            float denom1 = td - tr, denom2 = 0.0f;
+            if (denom1 != 0.0f) {
+              float t_p = td * tr * logf(td / tr) / denom1;
+              denom2 = expf(-t_p / td) - expf(-t_p / tr);
+            }
+            if (denom2 == 0.0f) P(3) = (float)(M_E / td);
+            else P(3) = (float)((1.0 / tr - 1.0 / td) / denom2);
+          } else if (g.model == M_AEIF_COND_ALPHA) {
+            P(2) = (float)(M_E / P(1));
+          } else if (g.model == M_AEIF_PSC_ALPHA) {
+            P(1) = (float)(M_E / P(0));
+          }
+        }
+        if ((g.model == M_AEIF_PSC_EXP || g.model == M_AEIF_PSC_ALPHA) && g.par[A_Delta_T][i] <= 0.0f)
+          g.par[A_V_peak][i] = g.par[A_V_th][i];
+      }
+    } else if (g.model == M_IAF_PSC_EXP) {
+      for (int i = 0; i < g.n; i++) {
+        if (g.par[I_den_delay][i] != 0.0f) throw NgpuError("dendritic delay is not supported");
+        // src/iaf_psc_exp.cu:68-82, propagators in double precision
+        const double h = dt, tau_m = g.par[I_tau_m][i], C_m = g.par[I_C_m][i];
+        const double tau_ex = g.par[I_tau_ex][i], tau_in = g.par[I_tau_in][i];
+        float P22 = (float)std::exp(-h / tau_m);
+        g.par[I_P11ex][i] = (float)std::exp(-h / tau_ex);
+        g.par[I_P11in][i] = (float)std::exp(-h / tau_in);
+        g.par[I_P22][i] = P22;
+        g.par[I_P21ex][i] = (float)propagator_32(tau_ex, tau_m, C_m, h);
+        g.par[I_P21in][i] = (float)propagator_32(tau_in, tau_m, C_m, h);
+        g.par[I_P20][i] = (float)(tau_m / C_m * (1.0 - (double)P22));
+      }
+    }
+    g.acc_off = acc_total;
+    acc_total += (size_t)g.n * g.nport;
+    g.dirty = true;
+  }
+  if (acc_total >= (1ULL << 32)) throw NgpuError("input accumulator exceeds 2^32 entries");
+  n_acc_ = acc_total;
+  d_acc_ = dalloc<double>(n_acc_);
+  cuda_check(cudaMemsetAsync(d_acc_, 0, std::max<size_t>(n_acc_, 1) * sizeof(double), stream_), "memset");
+
+  // ---- connections: recurrent edges into CSR by (source, delay); poiss_gen edges apart
+  build_order();   // reference order: the canonical numbering of poiss_gen edges
+  const size_t E = c_src_.size();
+  std::vector<unsigned char> is_pg(N, 0);
+  for (auto &g : groups_)
+    if (g.model == M_POISS_GEN)
+      for (int i = 0; i < g.n; i++) is_pg[g.i0 + i] = 1;
+  int dmin = INT32_MAX, dmax = INT32_MIN;
+  size_t n_rec_edges = 0;
+  for (size_t e = 0; e < E; e++) {
+    Group &tg = groups_[node_group_[c_tgt_[e]]];
+    if (c_port_[e] >= tg.nport)
+      throw NgpuError("receptor port " + std::to_string(c_port_[e]) + " out of range for target node " +
+                      std::to_string(c_tgt_[e]));
+    if (is_pg[c_src_[e]]) continue;
+    n_rec_edges++;
+    dmin = std::min(dmin, c_d_[e]);
+    dmax = std::max(dmax, c_d_[e]);
+  }
+  if (n_rec_edges == 0) { dmin = 0; dmax = 0; }
+  dmin_ = dmin;
+  dspan_ = dmax - dmin + 1;
+  if (dspan_ > deliver_max_dspan())
+    throw NgpuError("delay range exceeds " + std::to_string(deliver_max_dspan()) + " time steps");
+  std::vector<unsigned char> has_out(N, 0);
+  {
+    const size_t nkey = (size_t)N * dspan_;
+    std::vector<long long> off(nkey + 1, 0);
+    for (size_t e = 0; e < E; e++) {
+      if (is_pg[c_src_[e]]) continue;
+      off[(size_t)c_src_[e] * dspan_ + (c_d_[e] - dmin) + 1]++;
+      has_out[c_src_[e]] = 1;
+    }
+    for (size_t k = 0; k < nkey; k++) off[k + 1] += off[k];
+    std::vector<EdgeW> ew(n_rec_edges);
+    std::vector<long long> pos(off.begin(), off.end() - 1);
+    for (size_t e = 0; e < E; e++) {
+      if (is_pg[c_src_[e]]) continue;
+      const Group &tg = groups_[node_group_[c_tgt_[e]]];
+      size_t key = (size_t)c_src_[e] * dspan_ + (c_d_[e] - dmin);
+      EdgeW x;
+      x.acc = (uint32_t)(tg.acc_off + (size_t)c_port_[e] * tg.n + (c_tgt_[e] - tg.i0));
+      x.w = c_w_[e];
+      ew[pos[key]++] = x;
+    }
+    d_ev_off_ = dalloc<long long>(nkey + 1);
+    cuda_check(cudaMemcpy(d_ev_off_, off.data(), (nkey + 1) * sizeof(long long), cudaMemcpyHostToDevice), "ev_off");
+    d_edge_ = dalloc<EdgeW>(n_rec_edges);
+    if (n_rec_edges)
+      cuda_check(cudaMemcpy(d_edge_, ew.data(), n_rec_edges * sizeof(EdgeW), cudaMemcpyHostToDevice), "edges");
+    n_edge_dev_ = n_rec_edges;
+  }
+  d_has_out_ = dalloc<unsigned char>(N);
+  cuda_check(cudaMemcpy(d_has_out_, has_out.data(), N, cudaMemcpyHostToDevice), "has_out");
+  int n_src_out = 0;
+  for (int i = 0; i < N; i++) n_src_out += has_out[i];
+
+  // ---- poiss_gen: generator table and target-major in-edges with canonical ids
+  n_gen_ = 0;
+  for (auto &g : groups_)
+    if (g.model == M_POISS_GEN) { g.gen0 = n_gen_; n_gen_ += g.n; }
+  d_gen_ = dalloc<GenPar>(n_gen_);
+  {
+    struct DE { int tgt; PoissonIn pe; };
+    std::vector<DE> de;
+    uint32_t id = 0;
+    for (int s = 0; s < N; s++) {
+      if (!is_pg[s]) continue;
+      const Group &pg = groups_[node_group_[s]];
+      for (long long p = src_first_[s]; p < src_first_[s + 1]; p++) {
+        long long e = ord_[p];
+        DE x;
+        x.tgt = c_tgt_[e];
+        x.pe.edge_id = id++;
+        x.pe.gen = pg.gen0 + (s - pg.i0);
+        x.pe.weight = c_w_[e];
+        x.pe.delay = dt * (float)(c_d_[e] + 1);
+        x.pe.port = c_port_[e];
+        x.pe.pad = 0;
+        de.push_back(x);
+      }
+    }
+    std::stable_sort(de.begin(), de.end(), [](const DE &a, const DE &b) { return a.tgt < b.tgt; });
+    size_t k = 0;
+    for (auto &g : groups_) {
+      if (g.nport == 0) continue;
+      std::vector<int> off(g.n + 1, 0);
+      std::vector<PoissonIn> pin;
+      while (k < de.size() && de[k].tgt < g.i0) k++;
+      size_t k0 = k;
+      while (k < de.size() && de[k].tgt < g.i0 + g.n) {
+        off[de[k].tgt - g.i0 + 1]++;
+        pin.push_back(de[k].pe);
+        k++;
+      }
+      (void)k0;
+      if (pin.empty()) continue;
+      for (int i = 0; i < g.n; i++) off[i + 1] += off[i];
+      g.d_pin_off = dalloc<int>(g.n + 1);
+      g.d_pin = dalloc<PoissonIn>(pin.size());
+      cuda_check(cudaMemcpy(g.d_pin_off, off.data(), (g.n + 1) * sizeof(int), cudaMemcpyHostToDevice), "pin_off");
+      cuda_check(cudaMemcpy(g.d_pin, pin.data(), pin.size() * sizeof(PoissonIn), cudaMemcpyHostToDevice), "pin");
+    }
+  }
+
+  // ---- spike ring and per-node spike state
+  R_ = (dmin_ + dspan_ - 1) + 3;
+  cap_ = (int)std::min<long long>((long long)n_src_out * std::max(1.0f, max_spike_num_fact) + 1024, 1LL << 30);
+  d_ring_ = dalloc<int2>((size_t)R_ * cap_);
+  d_ring_cnt_ = dalloc<int>(R_);
+  cuda_check(cudaMemset(d_ring_cnt_, 0, R_ * sizeof(int)), "ring_cnt");
+  d_last_tidx_ = dalloc<int>(N);
+  cuda_check(cudaMemset(d_last_tidx_, 0xff, (size_t)N * sizeof(int)), "last_tidx");
+  d_last_h_ = dalloc<float>(N);
+  cuda_check(cudaMemset(d_last_h_, 0, (size_t)N * sizeof(float)), "last_h");
+  d_status_ = dalloc<unsigned>(1);
+  cuda_check(cudaMemset(d_status_, 0, sizeof(unsigned)), "status");
+  d_counters_ = dalloc<unsigned long long>(4);
+  cuda_check(cudaMemset(d_counters_, 0, 4 * sizeof(unsigned long long)), "counters");
+  d_clk_ = dalloc<Clock>(1);
+  cuda_check(cudaMemset(d_clk_, 0, sizeof(Clock)), "clock");
+  deliver_blocks_ = std::max(1, std::min(148 * 2, (n_src_out + 63) / 64));
+
+  // ---- per-group device state
+  for (auto &g : groups_) {
+    if (is_aeif(g.model) || g.model == M_IAF_PSC_EXP) {
+      const int nvar = (int)g.var.size();
+      g.d_var = dalloc<float>((size_t)nvar * g.n);
+      for (int v = 0; v < nvar; v++)
+        cuda_check(cudaMemcpy(g.d_var + (size_t)v * g.n, g.var[v].data(), g.n * sizeof(float),
+                              cudaMemcpyHostToDevice), "var");
+    }
+    if (is_aeif(g.model)) {
+      g.d_refr = dalloc<float>(g.n);
+      cuda_check(cudaMemcpy(g.d_refr, g.par[A_refractory_step].data(), g.n * sizeof(float),
+                            cudaMemcpyHostToDevice), "refr");
+      std::vector<double> x(g.n, 0.0);
+      std::vector<float> h(g.n, g.h0_rel * dt);
+      g.d_x = dalloc<double>(g.n);
+      g.d_h = dalloc<float>(g.n);
+      cuda_check(cudaMemcpy(g.d_x, x.data(), g.n * sizeof(double), cudaMemcpyHostToDevice), "x");
+      cuda_check(cudaMemcpy(g.d_h, h.data(), g.n * sizeof(float), cudaMemcpyHostToDevice), "h");
+    }
+    if (g.spike_count_on) {
+      g.d_spike_count = dalloc<int>(g.n);
+      cuda_check(cudaMemset(g.d_spike_count, 0, g.n * sizeof(int)), "spike_count");
+    }
+    if (g.max_rec > 0) {
+      g.d_n_rec = dalloc<int>(g.n);
+      g.d_rec_times = dalloc<float>((size_t)g.n * g.max_rec);
+      cuda_check(cudaMemset(g.d_n_rec, 0, g.n * sizeof(int)), "n_rec");
+    }
+    if (g.model == M_SPIKE_GEN) {
+      // src/spike_generator.cu:230-290: time indices round((t - t_min)/dt), strictly increasing
+      std::vector<int> off(g.n + 1, 0), tix;
+      std::vector<float> hh;
+      for (int i = 0; i < g.n; i++) {
+        const auto &t = g.sg_times[i];
+        std::vector<float> hs = g.sg_heights[i];
+        if (!t.empty()) {
+          if (hs.empty()) hs.assign(t.size(), 1.0f);
+          else if (hs.size() != t.size())
+            throw NgpuError("spike time array and spike height array must have the same size in spike generator");
+        }
+        for (size_t k = 0; k < t.size(); k++) {
+          int ti = (int)std::round((t[k] - 0.0f) / dt);
+          if (k > 0 && ti <= tix.back())
+            throw NgpuError("Spike times must be ordered, and the difference between\nconsecutive spikes must be >= the time resolution");
+          tix.push_back(ti);
+          hh.push_back(hs[k]);
+        }
+        off[i + 1] = (int)tix.size();
+      }
+      g.d_sg_off = dalloc<int>(g.n + 1);
+      g.d_sg_tidx = dalloc<int>(tix.size());
+      g.d_sg_h = dalloc<float>(hh.size());
+      g.d_sg_next = dalloc<int>(g.n);
+      cuda_check(cudaMemcpy(g.d_sg_off, off.data(), (g.n + 1) * sizeof(int), cudaMemcpyHostToDevice), "sg");
+      if (!tix.empty()) {
+        cuda_check(cudaMemcpy(g.d_sg_tidx, tix.data(), tix.size() * sizeof(int), cudaMemcpyHostToDevice), "sg");
+        cuda_check(cudaMemcpy(g.d_sg_h, hh.data(), hh.size() * sizeof(float), cudaMemcpyHostToDevice), "sg");
+      }
+      cuda_check(cudaMemset(g.d_sg_next, 0, g.n * sizeof(int)), "sg");
+    }
+  }
+  build_records();
+  cuda_check(cudaDeviceSynchronize(), "calibrate");
+}
+
+// Derived parameters: uniform over the group -> kernel argument, else device array.
+void Engine::upload_params() {
+  bool any = false;
+  auto put = [&](Group &g, int slot, const std::vector<float> &v) {
+    bool uni = true;
+    for (int i = 1; i < g.n && uni; i++) uni = (std::memcmp(&v[i], &v[0], 4) == 0);
+    if (uni) {
+      g.der_val[slot] = v[0];
+      g.d_der[slot] = nullptr;
+    } else {
+      float *d = dalloc<float>(g.n);
+      cuda_check(cudaMemcpy(d, v.data(), g.n * sizeof(float), cudaMemcpyHostToDevice), "param");
+      g.der_val[slot] = 0.0f;
+      g.d_der[slot] = d;
+    }
+  };
+  std::vector<GenPar> gp(n_gen_);
+  bool gen_dirty = false;
+  for (auto &g : groups_) {
+    if (!g.dirty) continue;
+    any = true;
+    g.dirty = false;
+    const int n = g.n;
+    std::vector<float> v(n);
+    if (is_aeif(g.model)) {
+      g.der_val.assign(AEIF_NPAR, 0.0f);
+      g.d_der.assign(AEIF_NPAR, nullptr);
+      auto cp = [&](int slot, int src) { put(g, slot, g.par[src]); };
+      cp(AP_V_th, A_V_th);
+      cp(AP_Delta_T, A_Delta_T);
+      for (int i = 0; i < n; i++) v[i] = 1.0f / g.par[A_Delta_T][i];
+      put(g, AP_inv_Delta_T, v);
+      cp(AP_g_L, A_g_L);
+      cp(AP_E_L, A_E_L);
+      for (int i = 0; i < n; i++) v[i] = 1.0f / g.par[A_C_m][i];
+      put(g, AP_inv_C_m, v);
+      cp(AP_a, A_a);
+      cp(AP_b, A_b);
+      for (int i = 0; i < n; i++) v[i] = 1.0f / g.par[A_tau_w][i];
+      put(g, AP_inv_tau_w, v);
+      cp(AP_I_e, A_I_e);
+      cp(AP_V_peak, A_V_peak);
+      cp(AP_V_reset, A_V_reset);
+      for (int i = 0; i < n; i++) {
+        float rs = (float)(int)roundf(g.par[A_t_ref][i] / dt);
+        v[i] = rs < 0.0f ? 0.0f : rs;
+      }
+      put(g, AP_refr_steps, v);
+      const int npp = n_port_par(g.model);
+      for (int p = 0; p < g.nport; p++) {
+        const int b = AEIF_NSCAL + AEIF_NPORTPAR * p, hb = A_NSCAL + npp * p;
+        std::vector<float> er(n, 0.0f), t1(n), t2(n), pw(n, 1.0f);
+        for (int i = 0; i < n; i++) {
+          switch (g.model) {
+          case M_AEIF_COND_BETA:
+            er[i] = g.par[hb + 0][i]; t1[i] = 1.0f / g.par[hb + 1][i]; t2[i] = 1.0f / g.par[hb + 2][i];
+            pw[i] = g.par[hb + 3][i];
+            break;
+          case M_AEIF_COND_ALPHA:
+            er[i] = g.par[hb + 0][i]; t1[i] = 1.0f / g.par[hb + 1][i]; t2[i] = t1[i]; pw[i] = g.par[hb + 2][i];
+            break;
+          case M_AEIF_PSC_EXP:
+            t1[i] = 1.0f / g.par[hb + 0][i]; t2[i] = t1[i];
+            break;
+          default:
+            t1[i] = 1.0f / g.par[hb + 0][i]; t2[i] = t1[i]; pw[i] = g.par[hb + 1][i];
+            break;
+          }
+        }
+        put(g, b + 0, er);
+        put(g, b + 1, t1);
+        put(g, b + 2, t2);
+        put(g, b + 3, pw);
+      }
+    } else if (g.model == M_IAF_PSC_EXP) {
+      g.der_val.assign(IP_NPAR, 0.0f);
+      g.d_der.assign(IP_NPAR, nullptr);
+      put(g, IP_I_e, g.par[I_I_e]);
+      put(g, IP_Theta_rel, g.par[I_Theta_rel]);
+      put(g, IP_V_reset_rel, g.par[I_V_reset_rel]);
+      for (int i = 0; i < n; i++) v[i] = (float)(int)roundf(g.par[I_t_ref][i] / dt);
+      put(g, IP_refr_steps, v);
+      put(g, IP_P20, g.par[I_P20]);
+      put(g, IP_P11ex, g.par[I_P11ex]);
+      put(g, IP_P11in, g.par[I_P11in]);
+      put(g, IP_P21ex, g.par[I_P21ex]);
+      put(g, IP_P21in, g.par[I_P21in]);
+      put(g, IP_P22, g.par[I_P22]);
+    } else if (g.model == M_POISS_GEN) {
+      gen_dirty = true;
+    }
+  }
+  if (gen_dirty && n_gen_ > 0) {
+    for (auto &g : groups_) {
+      if (g.model != M_POISS_GEN) continue;
+      for (int i = 0; i < g.n; i++)
+        gp[g.gen0 + i] = {g.par[PG_rate][i], g.par[PG_origin][i], g.par[PG_start][i], g.par[PG_stop][i]};
+    }
+    cuda_check(cudaMemcpy(d_gen_, gp.data(), n_gen_ * sizeof(GenPar), cudaMemcpyHostToDevice), "gen");
+  }
+  if (any) invalidate_graphs();
+}
+
+void Engine::build_records() {
+  std::vector<RecCol> cols;
+  rec_cols_.clear();
+  for (size_t r = 0; r < records_.size(); r++) {
+    RecordSpec &rs = records_[r];
+    for (size_t c = 0; c < rs.var.size(); c++) {
+      RecCol rc{nullptr, rs.node[c], 0};
+      if (rs.var[c] != "spike") {
+        Group &g = group_of(rs.node[c]);
+        int idx;
+        Kind k = locate(rs.node[c], rs.var[c], &idx);
+        int rel = rs.node[c] - g.i0;
+        if (is_aeif(g.model)) {
+          if (k == K_SCAL_VAR) rc.ptr = g.d_var + (size_t)idx * g.n + rel;
+          else if (k == K_PORT_VAR)
+            rc.ptr = g.d_var + (size_t)(2 + n_port_var(g.model) * rs.port[c] + idx) * g.n + rel;
+          else rc.ptr = g.d_refr + rel;
+        } else {
+          rc.ptr = g.d_var + (size_t)idx * g.n + rel;
+        }
+      }
+      cols.push_back(rc);
+      rec_cols_.push_back({(int)r, (int)c});
+    }
+    if (!rs.file.empty()) {
+      rs.fp = fopen(rs.file.c_str(), "w");
+      if (!rs.fp) throw NgpuError("cannot open record file " + rs.file);
+    }
+  }
+  rec_ncol_ = (int)cols.size();
+  if (rec_ncol_) {
+    d_cols_ = dalloc<RecCol>(cols.size());
+    cuda_check(cudaMemcpy(d_cols_, cols.data(), cols.size() * sizeof(RecCol), cudaMemcpyHostToDevice), "rec");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Kernel argument blocks
+// ---------------------------------------------------------------------------
+SpikeOut Engine::spike_out() const {
+  SpikeOut so;
+  so.ring = d_ring_;
+  so.ring_cnt = d_ring_cnt_;
+  so.R = R_;
+  so.cap = cap_;
+  so.has_out = d_has_out_;
+  so.last_tidx = d_last_tidx_;
+  so.last_height = d_last_h_;
+  so.status = d_status_;
+  so.n_spikes = d_counters_ + 2;
+  return so;
+}
+
+static GroupSpikeRec spike_rec(Group &g) {
+  GroupSpikeRec r;
+  r.spike_count = g.d_spike_count;
+  r.n_rec = g.d_n_rec;
+  r.rec_times = g.d_rec_times;
+  r.max_rec = g.max_rec;
+  return r;
+}
+
+AeifArgs Engine::aeif_args(Group &g) {
+  AeifArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.n = g.n;
+  A.i0 = g.i0;
+  A.nport = g.nport;
+  A.nvar = 2 + n_port_var(g.model) * g.nport;
+  A.var = g.d_var;
+  A.refr = g.d_refr;
+  A.x = g.d_x;
+  A.h = g.d_h;
+  A.acc = d_acc_ + g.acc_off;
+  A.pin_off = g.d_pin_off;
+  A.pin = g.d_pin;
+  A.gen = d_gen_;
+  A.lam_scale = (float)(dt / 1000.0);
+  A.dt = dt;
+  A.hmin = g.h_min_rel * dt;
+  A.hmin_acc = A.hmin * 1.00001f;
+  A.seed = kernel_seed;
+  A.nderiv = d_counters_;
+  A.rec = spike_rec(g);
+  for (int j = 0; j < AEIF_NPAR; j++) {
+    A.pval[j] = g.der_val[j];
+    A.parr[j] = g.d_der[j];
+  }
+  return A;
+}
+
+IafArgs Engine::iaf_args(Group &g) {
+  IafArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.n = g.n;
+  A.i0 = g.i0;
+  A.var = g.d_var;
+  A.acc = d_acc_ + g.acc_off;
+  A.pin_off = g.d_pin_off;
+  A.pin = g.d_pin;
+  A.gen = d_gen_;
+  A.lam_scale = (float)(dt / 1000.0);
+  A.seed = kernel_seed;
+  A.rec = spike_rec(g);
+  for (int j = 0; j < IP_NPAR; j++) {
+    A.pval[j] = g.der_val[j];
+    A.parr[j] = g.d_der[j];
+  }
+  return A;
+}
+
+SpikeGenArgs Engine::sg_args(Group &g) {
+  SpikeGenArgs A;
+  A.n = g.n;
+  A.i0 = g.i0;
+  A.off = g.d_sg_off;
+  A.tidx = g.d_sg_tidx;
+  A.height = g.d_sg_h;
+  A.next = g.d_sg_next;
+  A.rec = spike_rec(g);
+  return A;
+}
+
+DeliverArgs Engine::deliver_args() {
+  DeliverArgs A;
+  A.ring = d_ring_;
+  A.ring_cnt = d_ring_cnt_;
+  A.R = R_;
+  A.cap = cap_;
+  A.dmin = dmin_;
+  A.dspan = dspan_;
+  A.ev_off = d_ev_off_;
+  A.edge = d_edge_;
+  A.acc = d_acc_;
+  A.n_events = d_counters_ + 1;
+  return A;
+}
+
+// ---------------------------------------------------------------------------
+// Step loop
+// ---------------------------------------------------------------------------
+void Engine::launch_step(int k) {
+  SpikeOut so = spike_out();
+  for (auto &g : groups_) {
+    if (is_aeif(g.model)) launch_aeif(g.model, false, aeif_args(g), so, d_clk_, k, stream_);
+    else if (g.model == M_IAF_PSC_EXP) launch_iaf(false, iaf_args(g), so, d_clk_, k, dt, stream_);
+    else if (g.model == M_SPIKE_GEN) launch_spike_gen(sg_args(g), so, d_clk_, k, dt, stream_);
+  }
+  if (rec_ncol_)
+    launch_record(d_cols_, rec_ncol_, d_recbuf_, d_last_tidx_, d_last_h_, d_has_out_, d_clk_, k, dt,
+                  stream_);
+  launch_deliver(deliver_args(), deliver_blocks_, d_clk_, k, dt, stream_);
+}
+
+void Engine::launch_flush() {
+  SpikeOut so = spike_out();
+  for (auto &g : groups_) {
+    if (is_aeif(g.model)) launch_aeif(g.model, true, aeif_args(g), so, d_clk_, 0, stream_);
+    else if (g.model == M_IAF_PSC_EXP) launch_iaf(true, iaf_args(g), so, d_clk_, 0, dt, stream_);
+  }
+  launch_clock_clear_pending(d_clk_, stream_);
+}
+
+void Engine::run_steps(long long n) {
+  const int K = std::max(1, graph_steps);
+  long long window = n;
+  const long long REC_WINDOW = 10000;
+  if (rec_ncol_) {
+    window = std::min<long long>(n, REC_WINDOW);
+    if (window > rec_rows_cap_) {
+      d_recbuf_ = dalloc<float>((size_t)window * (rec_ncol_ + 1));
+      rec_rows_cap_ = (int)window;
+      invalidate_graphs();
+    }
+  }
+  long long done = 0;
+  while (done < n) {
+    long long w = std::min(window, n - done);
+    long long full = w / K, rem = w % K;
+    auto run = [&](int steps) {
+      auto itg = graphs_.find(steps);
+      if (itg == graphs_.end()) {
+        cudaGraph_t graph;
+        cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+        for (int k = 0; k < steps; k++) launch_step(k);
+        launch_clock_advance(d_clk_, steps, stream_);
+        cuda_check(cudaStreamEndCapture(stream_, &graph), "capture");
+        cudaGraphExec_t exec;
+        cuda_check(cudaGraphInstantiate(&exec, graph, 0), "instantiate");
+        cudaGraphDestroy(graph);
+        itg = graphs_.emplace(steps, exec).first;
+      }
+      cuda_check(cudaGraphLaunch(itg->second, stream_), "graph launch");
+    };
+    for (long long i = 0; i < full; i++) run(K);
+    if (rem) run((int)rem);
+    if (rec_ncol_) drain_records(w);
+    done += w;
+  }
+}
+
+void Engine::drain_records(long long rows) {
+  std::vector<float> buf((size_t)rows * (rec_ncol_ + 1));
+  cuda_check(cudaMemcpyAsync(buf.data(), d_recbuf_, buf.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                             stream_), "record copy");
+  cuda_check(cudaStreamSynchronize(stream_), "record sync");
+  // next window starts where this one ended
+  Clock c;
+  cuda_check(cudaMemcpy(&c, d_clk_, sizeof(Clock), cudaMemcpyDeviceToHost), "clock");
+  c.rec_it0 = c.it0;
+  cuda_check(cudaMemcpy(d_clk_, &c, sizeof(Clock), cudaMemcpyHostToDevice), "clock");
+  for (long long r = 0; r < rows; r++) {
+    const float *row = &buf[(size_t)r * (rec_ncol_ + 1)];
+    size_t c0 = 0;
+    for (auto &rs : records_) {
+      std::vector<float> v;
+      v.push_back(row[0]);
+      for (size_t c2 = 0; c2 < rs.var.size(); c2++) v.push_back(row[1 + c0 + c2]);
+      c0 += rs.var.size();
+      if (rs.fp) {
+        fprintf(rs.fp, "%f", v[0]);
+        for (size_t j = 1; j < v.size(); j++) fprintf(rs.fp, "\t%f", v[j]);
+        fprintf(rs.fp, "\n");
+      }
+      rs.data.push_back(std::move(v));
+    }
+  }
+}
+
+void Engine::drain_rec_spike_times() {
+  if (!calibrated_) return;
+  cuda_check(cudaStreamSynchronize(stream_), "sync");
+  for (auto &g : groups_) {
+    if (g.max_rec <= 0 || !g.d_n_rec) continue;
+    std::vector<int> nr(g.n);
+    cuda_check(cudaMemcpy(nr.data(), g.d_n_rec, g.n * sizeof(int), cudaMemcpyDeviceToHost), "n_rec");
+    int any = 0;
+    for (int v : nr) any |= v;
+    if (!any) continue;
+    std::vector<float> t((size_t)g.n * g.max_rec);
+    cuda_check(cudaMemcpy(t.data(), g.d_rec_times, t.size() * sizeof(float), cudaMemcpyDeviceToHost), "rec");
+    for (int i = 0; i < g.n; i++)
+      g.rec_times_host[i].insert(g.rec_times_host[i].end(), t.begin() + (size_t)i * g.max_rec,
+                                 t.begin() + (size_t)i * g.max_rec + nr[i]);
+    cuda_check(cudaMemset(g.d_n_rec, 0, g.n * sizeof(int)), "n_rec");
+  }
+}
+
+void Engine::check_status() {
+  unsigned st = 0;
+  cuda_check(cudaMemcpy(&st, d_status_, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
+  unsigned fresh = st & ~status_seen_;
+  status_seen_ |= st;
+  if (fresh && verbosity >= 1) {
+    if (fresh & ST_RING_OVERFLOW) printf("Warning: spike ring slot overflow, spikes dropped\n");
+    if (fresh & ST_RK5_TRIALS) printf("Warning: RK5 step hit its iteration cap\n");
+    if (fresh & ST_NUMERIC) printf("Warning: V_m or w out of bounds, neuron state reset\n");
+    if (fresh & ST_REC_TIMES_FULL) printf("Maximum number of recorded spike times exceeded\n");
+  }
+}
+
+void Engine::start_simulation() {
+  if (!calibrated_) calibrate();
+  if (in_sim_) return;
+  upload_params();
+  if (first_sim_) {
+    // initial record row (src/nestgpu.cu:384-389)
+    for (auto &rs : records_) {
+      std::vector<float> v{(float)neural_time_};
+      for (size_t c = 0; c < rs.var.size(); c++) {
+        if (rs.var[c] == "spike") {
+          v.push_back(0.0f);
+        } else {
+          std::vector<float> x = get_values({rs.node[c]}, rs.var[c]);
+          v.push_back(locate(rs.node[c], rs.var[c]) == K_PORT_VAR ? x[rs.port[c]] : x[0]);
+        }
+      }
+      if (rs.fp) {
+        fprintf(rs.fp, "%f", v[0]);
+        for (size_t j = 1; j < v.size(); j++) fprintf(rs.fp, "\t%f", v[j]);
+        fprintf(rs.fp, "\n");
+      }
+      rs.data.push_back(v);
+    }
+    first_sim_ = false;
+  }
+  if (verbosity >= 1) printf("Simulating ...\nNeural activity simulation time: %.3lf ms\n", (double)sim_time);
+  neur_t0_ = neural_time_;
+  it_ = 0;
+  Nt_ = (long long)roundf(sim_time / dt);
+  tidx_base_ = (long long)(int)std::round(neur_t0_ / (double)dt);
+  Clock c;
+  std::memset(&c, 0, sizeof(c));
+  c.it0 = 0;
+  c.tidx_base = tidx_base_;
+  c.t0 = neur_t0_;
+  c.rec_it0 = 0;
+  c.pending = 0;
+  cuda_check(cudaMemcpy(d_clk_, &c, sizeof(Clock), cudaMemcpyHostToDevice), "clock");
+  in_sim_ = true;
+}
+
+void Engine::end_simulation() {
+  if (!in_sim_) return;
+  launch_flush();
+  cuda_check(cudaStreamSynchronize(stream_), "end of simulation");
+  check_status();
+  drain_rec_spike_times();
+  if (it_ > 0) neural_time_ = neur_t0_ + (double)dt * (double)it_;
+  in_sim_ = false;
+}
+
+void Engine::simulation_step() {
+  if (!in_sim_) start_simulation();
+  // one step, then fold its inputs so that state queries between steps see what
+  // the reference shows; the next step then has nothing pending
+  run_steps(1);
+  it_ += 1;
+  launch_flush();
+  cuda_check(cudaStreamSynchronize(stream_), "step");
+  Clock c;
+  cuda_check(cudaMemcpy(&c, d_clk_, sizeof(Clock), cudaMemcpyDeviceToHost), "clock");
+  neural_time_ = neur_t0_ + (double)dt * (double)it_;
+}
+
+void Engine::simulate(float t) {
+  sim_time = t;
+  start_simulation();
+  auto t0 = std::chrono::steady_clock::now();
+  run_steps(Nt_);
+  it_ += Nt_;
+  end_simulation();
+  auto t1 = std::chrono::steady_clock::now();
+  last_sim_seconds_ = std::chrono::duration<double>(t1 - t0).count();
+  total_steps_ += Nt_;
+  if (verbosity >= 1) printf("Simulation time: %g\n", last_sim_seconds_);
+}
+
+EngineStats Engine::stats() {
+  EngineStats s;
+  if (calibrated_) {
+    unsigned long long c[4];
+    cuda_check(cudaStreamSynchronize(stream_), "sync");
+    cuda_check(cudaMemcpy(c, d_counters_, sizeof(c), cudaMemcpyDeviceToHost), "counters");
+    s.n_derivs = c[0];
+    s.n_events = c[1];
+    s.n_spikes = c[2];
+    cuda_check(cudaMemcpy(&s.status, d_status_, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
+  }
+  s.sim_seconds = last_sim_seconds_;
+  s.steps = total_steps_;
+  return s;
+}
+
+}  // namespace ngpu

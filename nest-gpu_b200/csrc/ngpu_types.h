@@ -1,0 +1,166 @@
+// Plain structures shared by the host runtime (ngpu_engine.cpp, ngpu_sim.cpp)
+// and the CUDA kernels (ngpu_kernels.cu): kernel argument blocks passed by value.
+#pragma once
+#include <vector_types.h>
+
+#include <cstdint>
+
+namespace ngpu {
+
+enum Model {
+  M_AEIF_COND_BETA = 0,
+  M_AEIF_COND_ALPHA,
+  M_AEIF_PSC_EXP,
+  M_AEIF_PSC_ALPHA,
+  M_IAF_PSC_EXP,
+  M_SPIKE_GEN,
+  M_POISS_GEN,
+  M_NMODEL
+};
+
+constexpr int MAX_PORT = 20;          // aeif_*_multisynapse port limit (reference MAX_PORT_NUM)
+constexpr int MAX_TPL_PORT = 4;       // port counts with a dedicated kernel instantiation
+
+// Status bits reported by the device (read back after each Simulate chunk).
+enum Status : unsigned {
+  ST_RING_OVERFLOW = 1u << 0,         // more spikes in one step than a ring slot holds
+  ST_RK5_TRIALS = 1u << 1,            // RK5 step gave up after the trial cap
+  ST_NUMERIC = 1u << 2,               // V_m or w left their guard bounds (reset applied)
+  ST_REC_TIMES_FULL = 1u << 3,        // a neuron exceeded its recorded-spike-time capacity
+};
+
+// Simulation clock in device memory.  One CUDA graph covers K steps; step k of
+// a chunk has per-call index it = it0 + k.
+struct Clock {
+  long long it0;         // per-call step index of step 0 of the current chunk
+  long long tidx_base;   // round(t0 / dt): time index of the call's start
+  double t0;             // neural time at the call's start [ms]
+  long long rec_it0;     // per-call index of the first step of the record window
+  int pending;           // 1 if inputs of the previous step still have to be folded
+  int pad;
+};
+
+// Spike output context shared by all spiking models.
+struct SpikeOut {
+  int2 *ring;            // [R][cap] (source node, height bits)
+  int *ring_cnt;         // [R]
+  int R, cap;
+  const unsigned char *has_out;   // per node: 1 if it has recurrent out-edges
+  int *last_tidx;        // per node: time index of the most recent spike
+  float *last_height;    // per node: height of the most recent spike
+  unsigned *status;
+  unsigned long long *n_spikes;
+};
+
+// Per-group spike bookkeeping (optional outputs).
+struct GroupSpikeRec {
+  int *spike_count;      // [n] or null
+  int *n_rec;            // [n] or null
+  float *rec_times;      // [n * max_rec] or null
+  int max_rec;
+};
+
+// Incoming poiss_gen edge, target-major, with its canonical direct-edge id.
+struct PoissonIn {
+  uint32_t edge_id;
+  int gen;               // index into the generator parameter table
+  float weight;
+  float delay;
+  int port;
+  int pad;
+};
+
+// Generator parameters: rate [Hz], origin, start, stop [ms].
+struct GenPar {
+  float rate, origin, start, stop;
+};
+
+// Parameter slot: value if uniform across the group, else a device array.
+constexpr int AEIF_NSCAL = 13;
+enum AeifPar {
+  AP_V_th = 0, AP_Delta_T, AP_inv_Delta_T, AP_g_L, AP_E_L, AP_inv_C_m, AP_a, AP_b,
+  AP_inv_tau_w, AP_I_e, AP_V_peak, AP_V_reset, AP_refr_steps
+};
+// per port: E_rev, inv_t1, inv_t2, port weight
+constexpr int AEIF_NPORTPAR = 4;
+constexpr int AEIF_NPAR = AEIF_NSCAL + AEIF_NPORTPAR * MAX_PORT;
+
+struct AeifArgs {
+  int n;
+  int i0;
+  int nport;
+  int nvar;
+  float *var;            // SoA [nvar][n]: V_m, w, port vars (port-major)
+  float *refr;           // [n]
+  double *x;             // [n]
+  float *h;              // [n]
+  double *acc;           // [nport][n]
+  const int *pin_off;    // [n+1] or null
+  const PoissonIn *pin;
+  const GenPar *gen;
+  float lam_scale;       // dt / 1000 (rate in Hz -> expected count per step)
+  float dt;
+  float hmin;
+  float hmin_acc;        // hmin * 1.00001f: forced-accept threshold
+  uint64_t seed;
+  unsigned long long *nderiv;
+  GroupSpikeRec rec;
+  float pval[AEIF_NPAR];
+  const float *parr[AEIF_NPAR];
+};
+
+enum IafPar {
+  IP_I_e = 0, IP_Theta_rel, IP_V_reset_rel, IP_refr_steps, IP_P20, IP_P11ex, IP_P11in,
+  IP_P21ex, IP_P21in, IP_P22, IP_NPAR
+};
+
+struct IafArgs {
+  int n;
+  int i0;
+  float *var;            // SoA [4][n]: I_syn_ex, I_syn_in, V_m_rel, refractory_step
+  double *acc;           // [2][n]
+  const int *pin_off;
+  const PoissonIn *pin;
+  const GenPar *gen;
+  float lam_scale;
+  uint64_t seed;
+  GroupSpikeRec rec;
+  float pval[IP_NPAR];
+  const float *parr[IP_NPAR];
+};
+
+struct SpikeGenArgs {
+  int n;
+  int i0;
+  const int *off;        // [n+1] into tidx/height
+  const int *tidx;       // spike step indices (per-call step counter)
+  const float *height;
+  int *next;             // [n]
+  GroupSpikeRec rec;
+};
+
+// Recurrent edge: packed accumulator index and weight.
+struct EdgeW {
+  uint32_t acc;
+  float w;
+};
+
+struct DeliverArgs {
+  const int2 *ring;
+  int *ring_cnt;
+  int R, cap;
+  int dmin, dspan;       // delay indices dmin .. dmin+dspan-1
+  const long long *ev_off;   // [n_nodes * dspan + 1]
+  const EdgeW *edge;
+  double *acc;
+  unsigned long long *n_events;
+};
+
+// Record column: float variable pointer, or "spike" activity of a node.
+struct RecCol {
+  const float *ptr;      // null for spike activity
+  int node;
+  int pad;
+};
+
+}  // namespace ngpu

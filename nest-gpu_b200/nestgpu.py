@@ -1,0 +1,1241 @@
+"""Python interface of the B200 spiking engine.
+
+Same module name, functions, argument meaning and errors as NEST GPU's
+pythonlib/nestgpu.py (NEST GPU 1.08), written against the same C ABI: it loads
+libnestgpu_b200.so from this package's lib/ directory, or the library named by
+the NESTGPU_LIB environment variable (so the reference library can be driven by
+the same scripts).  Every failing call raises ValueError with the engine's
+message (the reference turns C-ABI error codes into ValueError the same way).
+
+Extensions with no counterpart in the reference: Reset, GetStats, ConnectArrays,
+SetGraphSteps (they need libnestgpu_b200.so).
+"""
+import ctypes
+import gc
+import os
+
+_here = os.path.dirname(os.path.abspath(__file__))
+_default_lib = os.path.join(_here, "lib", "libnestgpu_b200.so")
+lib_path = os.environ.get("NESTGPU_LIB", _default_lib)
+if not os.path.exists(lib_path):
+    raise ImportError("nestgpu: engine library not found at %s (build it with `make -C %s`)"
+                      % (lib_path, _here))
+_lib = ctypes.CDLL(lib_path)
+is_b200_engine = hasattr(_lib, "NGPU_Reset")
+
+c_float_p = ctypes.POINTER(ctypes.c_float)
+c_int_p = ctypes.POINTER(ctypes.c_int)
+c_char_p = ctypes.POINTER(ctypes.c_char)
+c_void_p = ctypes.c_void_p
+c_int_pp = ctypes.POINTER(ctypes.POINTER(ctypes.c_int))
+c_float_pp = ctypes.POINTER(ctypes.POINTER(ctypes.c_float))
+c_float_ppp = ctypes.POINTER(ctypes.POINTER(ctypes.POINTER(ctypes.c_float)))
+c_char_pp = ctypes.POINTER(ctypes.c_char_p)
+
+conn_rule_name = ("one_to_one", "all_to_all", "fixed_total_number", "fixed_indegree",
+                  "fixed_outdegree")
+
+
+def _bind(name, res, args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = args
+    return f
+
+
+_I, _F, _U8 = ctypes.c_int, ctypes.c_float, ctypes.c_ubyte
+_sigs = {
+    "NESTGPU_GetErrorMessage": (ctypes.c_char_p, []),
+    "NESTGPU_GetErrorCode": (ctypes.c_ubyte, []),
+    "NESTGPU_SetOnException": (None, [_I]),
+    "NESTGPU_SetRandomSeed": (_I, [ctypes.c_ulonglong]),
+    "NESTGPU_SetTimeResolution": (_I, [_F]),
+    "NESTGPU_GetTimeResolution": (_F, []),
+    "NESTGPU_SetMaxSpikeBufferSize": (_I, [_I]),
+    "NESTGPU_GetMaxSpikeBufferSize": (_I, []),
+    "NESTGPU_SetSimTime": (_I, [_F]),
+    "NESTGPU_SetVerbosityLevel": (_I, [_I]),
+    "NESTGPU_Create": (_I, [ctypes.c_char_p, _I, _I]),
+    "NESTGPU_CreatePoissonGenerator": (_I, [_I, _F]),
+    "NESTGPU_CreateRecord": (_I, [ctypes.c_char_p, c_char_pp, c_int_p, c_int_p, _I]),
+    "NESTGPU_GetRecordDataRows": (_I, [_I]),
+    "NESTGPU_GetRecordDataColumns": (_I, [_I]),
+    "NESTGPU_GetRecordData": (c_float_pp, [_I]),
+    "NESTGPU_SetNeuronScalParam": (_I, [_I, _I, ctypes.c_char_p, _F]),
+    "NESTGPU_SetNeuronArrayParam": (_I, [_I, _I, ctypes.c_char_p, c_float_p, _I]),
+    "NESTGPU_SetNeuronPtScalParam": (_I, [c_void_p, _I, ctypes.c_char_p, _F]),
+    "NESTGPU_SetNeuronPtArrayParam": (_I, [c_void_p, _I, ctypes.c_char_p, c_float_p, _I]),
+    "NESTGPU_IsNeuronScalParam": (_I, [_I, ctypes.c_char_p]),
+    "NESTGPU_IsNeuronPortParam": (_I, [_I, ctypes.c_char_p]),
+    "NESTGPU_IsNeuronArrayParam": (_I, [_I, ctypes.c_char_p]),
+    "NESTGPU_SetNeuronIntVar": (_I, [_I, _I, ctypes.c_char_p, _I]),
+    "NESTGPU_SetNeuronScalVar": (_I, [_I, _I, ctypes.c_char_p, _F]),
+    "NESTGPU_SetNeuronArrayVar": (_I, [_I, _I, ctypes.c_char_p, c_float_p, _I]),
+    "NESTGPU_SetNeuronPtIntVar": (_I, [c_void_p, _I, ctypes.c_char_p, _I]),
+    "NESTGPU_SetNeuronPtScalVar": (_I, [c_void_p, _I, ctypes.c_char_p, _F]),
+    "NESTGPU_SetNeuronPtArrayVar": (_I, [c_void_p, _I, ctypes.c_char_p, c_float_p, _I]),
+    "NESTGPU_IsNeuronIntVar": (_I, [_I, ctypes.c_char_p]),
+    "NESTGPU_IsNeuronScalVar": (_I, [_I, ctypes.c_char_p]),
+    "NESTGPU_IsNeuronPortVar": (_I, [_I, ctypes.c_char_p]),
+    "NESTGPU_IsNeuronArrayVar": (_I, [_I, ctypes.c_char_p]),
+    "NESTGPU_GetNeuronParamSize": (_I, [_I, ctypes.c_char_p]),
+    "NESTGPU_GetNeuronVarSize": (_I, [_I, ctypes.c_char_p]),
+    "NESTGPU_GetNeuronParam": (c_float_p, [_I, _I, ctypes.c_char_p]),
+    "NESTGPU_GetNeuronPtParam": (c_float_p, [c_void_p, _I, ctypes.c_char_p]),
+    "NESTGPU_GetArrayParam": (c_float_p, [_I, ctypes.c_char_p]),
+    "NESTGPU_GetNeuronIntVar": (c_int_p, [_I, _I, ctypes.c_char_p]),
+    "NESTGPU_GetNeuronPtIntVar": (c_int_p, [c_void_p, _I, ctypes.c_char_p]),
+    "NESTGPU_GetNeuronVar": (c_float_p, [_I, _I, ctypes.c_char_p]),
+    "NESTGPU_GetNeuronPtVar": (c_float_p, [c_void_p, _I, ctypes.c_char_p]),
+    "NESTGPU_GetArrayVar": (c_float_p, [_I, ctypes.c_char_p]),
+    "NESTGPU_Calibrate": (_I, []),
+    "NESTGPU_Simulate": (_I, []),
+    "NESTGPU_StartSimulation": (_I, []),
+    "NESTGPU_SimulationStep": (_I, []),
+    "NESTGPU_EndSimulation": (_I, []),
+    "NESTGPU_MpiId": (_I, []),
+    "NESTGPU_MpiNp": (_I, []),
+    "NESTGPU_ProcMaster": (_I, []),
+    "NESTGPU_MpiFinalize": (_I, []),
+    "NESTGPU_RandomInt": (ctypes.POINTER(ctypes.c_uint), [ctypes.c_size_t]),
+    "NESTGPU_RandomUniform": (c_float_p, [ctypes.c_size_t]),
+    "NESTGPU_RandomNormal": (c_float_p, [ctypes.c_size_t, _F, _F]),
+    "NESTGPU_RandomNormalClipped": (c_float_p, [ctypes.c_size_t, _F, _F, _F, _F, _F]),
+    "NESTGPU_Connect": (_I, [_I, _I, _U8, _U8, _F, _F]),
+    "NESTGPU_ConnSpecInit": (_I, []),
+    "NESTGPU_SetConnSpecParam": (_I, [ctypes.c_char_p, _I]),
+    "NESTGPU_ConnSpecIsParam": (_I, [ctypes.c_char_p]),
+    "NESTGPU_SynSpecInit": (_I, []),
+    "NESTGPU_SetSynSpecIntParam": (_I, [ctypes.c_char_p, _I]),
+    "NESTGPU_SetSynSpecFloatParam": (_I, [ctypes.c_char_p, _F]),
+    "NESTGPU_SetSynSpecFloatPtParam": (_I, [ctypes.c_char_p, c_void_p]),
+    "NESTGPU_SynSpecIsIntParam": (_I, [ctypes.c_char_p]),
+    "NESTGPU_SynSpecIsFloatParam": (_I, [ctypes.c_char_p]),
+    "NESTGPU_SynSpecIsFloatPtParam": (_I, [ctypes.c_char_p]),
+    "NESTGPU_ConnectSeqSeq": (_I, [_I, _I, _I, _I]),
+    "NESTGPU_ConnectSeqGroup": (_I, [_I, _I, c_void_p, _I]),
+    "NESTGPU_ConnectGroupSeq": (_I, [c_void_p, _I, _I, _I]),
+    "NESTGPU_ConnectGroupGroup": (_I, [c_void_p, _I, c_void_p, _I]),
+    "NESTGPU_GetSeqSeqConnections": (c_int_p, [_I, _I, _I, _I, _I, c_int_p]),
+    "NESTGPU_GetSeqGroupConnections": (c_int_p, [_I, _I, c_void_p, _I, _I, c_int_p]),
+    "NESTGPU_GetGroupSeqConnections": (c_int_p, [c_void_p, _I, _I, _I, _I, c_int_p]),
+    "NESTGPU_GetGroupGroupConnections": (c_int_p, [c_void_p, _I, c_void_p, _I, _I, c_int_p]),
+    "NESTGPU_GetConnectionStatus": (_I, [_I, _I, _I, c_int_p, c_char_p, c_char_p, c_float_p, c_float_p]),
+    "NESTGPU_ActivateSpikeCount": (_I, [_I, _I]),
+    "NESTGPU_ActivateRecSpikeTimes": (_I, [_I, _I, _I]),
+    "NESTGPU_SetRecSpikeTimesStep": (_I, [_I, _I, _I]),
+    "NESTGPU_GetNRecSpikeTimes": (_I, [_I]),
+    "NESTGPU_GetRecSpikeTimes": (_I, [_I, _I, c_int_pp, c_float_ppp]),
+    "NESTGPU_SetNeuronGroupParam": (_I, [_I, _I, ctypes.c_char_p, _F]),
+    "NESTGPU_IsNeuronGroupParam": (_I, [_I, ctypes.c_char_p]),
+    "NESTGPU_GetNeuronGroupParam": (_F, [_I, ctypes.c_char_p]),
+    "NESTGPU_GetNBoolParam": (_I, []),
+    "NESTGPU_GetBoolParamNames": (c_char_pp, []),
+    "NESTGPU_IsBoolParam": (_I, [ctypes.c_char_p]),
+    "NESTGPU_GetBoolParam": (ctypes.c_bool, [ctypes.c_char_p]),
+    "NESTGPU_SetBoolParam": (_I, [ctypes.c_char_p, ctypes.c_bool]),
+    "NESTGPU_GetNFloatParam": (_I, []),
+    "NESTGPU_GetFloatParamNames": (c_char_pp, []),
+    "NESTGPU_IsFloatParam": (_I, [ctypes.c_char_p]),
+    "NESTGPU_GetFloatParam": (_F, [ctypes.c_char_p]),
+    "NESTGPU_SetFloatParam": (_I, [ctypes.c_char_p, _F]),
+    "NESTGPU_GetNIntParam": (_I, []),
+    "NESTGPU_GetIntParamNames": (c_char_pp, []),
+    "NESTGPU_IsIntParam": (_I, [ctypes.c_char_p]),
+    "NESTGPU_GetIntParam": (_I, [ctypes.c_char_p]),
+    "NESTGPU_SetIntParam": (_I, [ctypes.c_char_p, _I]),
+    "NESTGPU_CreateSynGroup": (_I, [ctypes.c_char_p]),
+}
+for _n in ("IntVar", "ScalVar", "PortVar", "ScalParam", "PortParam", "GroupParam", "ArrayParam",
+           "ArrayVar"):
+    _sigs["NESTGPU_Get%sNames" % _n] = (c_char_pp, [_I])
+    _sigs["NESTGPU_GetN%s" % _n] = (_I, [_I])
+_c = {name: _bind(name, r, a) for name, (r, a) in _sigs.items()}
+if is_b200_engine:
+    _c["NGPU_FreeArray"] = _bind("NGPU_FreeArray", None, [c_void_p])
+    _c["NGPU_Reset"] = _bind("NGPU_Reset", _I, [])
+    _c["NGPU_GetStats"] = _bind("NGPU_GetStats", _I, [ctypes.POINTER(ctypes.c_ulonglong)] * 3 +
+                                [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
+                                 ctypes.POINTER(ctypes.c_uint)])
+    _c["NGPU_ConnectArrays"] = _bind("NGPU_ConnectArrays", _I, [ctypes.c_size_t, c_void_p, c_void_p,
+                                                                 c_void_p, c_void_p, c_void_p])
+    _c["NGPU_SetGraphSteps"] = _bind("NGPU_SetGraphSteps", _I, [_I])
+
+
+def _b(s):
+    return s.encode("utf-8") if isinstance(s, str) else s
+
+
+def _check(ret=None):
+    if _c["NESTGPU_GetErrorCode"]() != 0:
+        raise ValueError(GetErrorMessage())
+    return ret
+
+
+def _free(p):
+    if is_b200_engine and p:
+        _c["NGPU_FreeArray"](ctypes.cast(p, c_void_p))
+
+
+def _names(fn, *args):
+    n = _c["NESTGPU_GetN" + fn](*args) if fn else None
+    pp = _c["NESTGPU_Get%sNames" % fn](*args)
+    _check()
+    out = [pp[i].decode("utf-8") for i in range(n)]
+    return out
+
+
+class NodeSeq(object):
+    """Contiguous range of node indices (i0, n); n = -1 with i0 = None means all nodes."""
+
+    def __init__(self, i0, n=1):
+        if i0 is None:
+            i0, n = 0, -1
+        self.i0 = i0
+        self.n = n
+
+    def Subseq(self, first, last):
+        if last < 0 and last >= -self.n:
+            last = last % self.n
+        if first < 0 or last < first:
+            raise ValueError("Sequence subset range error")
+        if last >= self.n:
+            raise ValueError("Sequence subset out of range")
+        return NodeSeq(self.i0 + first, last - first + 1)
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            if i.step is not None:
+                raise ValueError("Subsequence cannot have a step")
+            start = 0 if i.start is None else i.start
+            stop = self.n if i.stop is None else i.stop
+            return self.Subseq(start, stop - 1)
+        if i < -self.n:
+            raise ValueError("Sequence index error")
+        if i >= self.n:
+            raise ValueError("Sequence index out of range")
+        if i < 0:
+            i = i % self.n
+        return self.i0 + i
+
+    def ToList(self):
+        return list(range(self.i0, self.i0 + self.n))
+
+    def __len__(self):
+        return self.n
+
+
+class RemoteNodeSeq(object):
+    def __init__(self, i_host=0, node_seq=NodeSeq(None)):
+        self.i_host = i_host
+        self.node_seq = node_seq
+
+
+class ConnectionId(object):
+    def __init__(self, i_source, i_group, i_conn):
+        self.i_source = i_source
+        self.i_group = i_group
+        self.i_conn = i_conn
+
+
+class SynGroup(object):
+    def __init__(self, i_syn_group):
+        self.i_syn_group = i_syn_group
+
+
+# ---------------------------------------------------------------- errors, kernel
+def GetErrorMessage():
+    return _c["NESTGPU_GetErrorMessage"]().decode("utf-8")
+
+
+def GetErrorCode():
+    return _c["NESTGPU_GetErrorCode"]()
+
+
+def SetOnException(on_exception):
+    _c["NESTGPU_SetOnException"](on_exception)
+
+
+SetOnException(1)   # return errors to Python instead of exiting (reference nestgpu.py:115-119)
+
+
+def SetRandomSeed(seed):
+    return _check(_c["NESTGPU_SetRandomSeed"](seed))
+
+
+def SetTimeResolution(time_res):
+    return _check(_c["NESTGPU_SetTimeResolution"](time_res))
+
+
+def GetTimeResolution():
+    return _check(_c["NESTGPU_GetTimeResolution"]())
+
+
+def SetMaxSpikeBufferSize(max_size):
+    return _check(_c["NESTGPU_SetMaxSpikeBufferSize"](max_size))
+
+
+def GetMaxSpikeBufferSize():
+    return _check(_c["NESTGPU_GetMaxSpikeBufferSize"]())
+
+
+def SetSimTime(sim_time):
+    return _check(_c["NESTGPU_SetSimTime"](sim_time))
+
+
+def SetVerbosityLevel(verbosity_level):
+    return _check(_c["NESTGPU_SetVerbosityLevel"](verbosity_level))
+
+
+# ---------------------------------------------------------------- nodes
+def Create(model_name, n_node=1, n_ports=1, status_dict=None):
+    "Create a neuron group"
+    if isinstance(status_dict, dict):
+        group = Create(model_name, n_node, n_ports)
+        SetStatus(group, status_dict)
+        return group
+    elif status_dict is not None:
+        raise ValueError("Wrong argument in Create")
+    i_node = _c["NESTGPU_Create"](_b(model_name), n_node, n_ports)
+    return _check(NodeSeq(i_node, n_node))
+
+
+def CreatePoissonGenerator(n_node, rate):
+    i_node = _c["NESTGPU_CreatePoissonGenerator"](n_node, rate)
+    return _check(NodeSeq(i_node, n_node))
+
+
+def CreateRecord(file_name, var_name_list, i_node_list, i_port_list):
+    "Create a record of neuron variables"
+    n = len(i_node_list)
+    names = (ctypes.c_char_p * n)(*[_b(v) for v in var_name_list])
+    ret = _c["NESTGPU_CreateRecord"](_b(file_name), names, (ctypes.c_int * n)(*i_node_list),
+                                     (ctypes.c_int * n)(*i_port_list), n)
+    return _check(ret)
+
+
+def GetRecordDataRows(i_record):
+    return _check(_c["NESTGPU_GetRecordDataRows"](i_record))
+
+
+def GetRecordDataColumns(i_record):
+    return _check(_c["NESTGPU_GetRecordDataColumns"](i_record))
+
+
+def GetRecordData(i_record):
+    "Get record data: one list per recorded step, time first"
+    pt = _c["NESTGPU_GetRecordData"](i_record)
+    _check()
+    nr = GetRecordDataRows(i_record)
+    nc = GetRecordDataColumns(i_record)
+    return [[pt[ir][ic] for ic in range(nc)] for ir in range(nr)]
+
+
+def _float_arr(vals):
+    vals = list(vals)
+    return (ctypes.c_float * len(vals))(*vals), len(vals)
+
+
+def _int_arr(nodes):
+    nodes = list(nodes)
+    return ctypes.cast((ctypes.c_int * len(nodes))(*nodes), c_void_p), len(nodes)
+
+
+def SetNeuronScalParam(i_node, n_node, param_name, val):
+    return _check(_c["NESTGPU_SetNeuronScalParam"](i_node, n_node, _b(param_name), val))
+
+
+def SetNeuronArrayParam(i_node, n_node, param_name, param_list):
+    arr, n = _float_arr(param_list)
+    return _check(_c["NESTGPU_SetNeuronArrayParam"](i_node, n_node, _b(param_name), arr, n))
+
+
+def SetNeuronPtScalParam(nodes, param_name, val):
+    pt, n = _int_arr(nodes)
+    return _check(_c["NESTGPU_SetNeuronPtScalParam"](pt, n, _b(param_name), val))
+
+
+def SetNeuronPtArrayParam(nodes, param_name, param_list):
+    pt, n = _int_arr(nodes)
+    arr, na = _float_arr(param_list)
+    return _check(_c["NESTGPU_SetNeuronPtArrayParam"](pt, n, _b(param_name), arr, na))
+
+
+def IsNeuronScalParam(i_node, param_name):
+    return _check(_c["NESTGPU_IsNeuronScalParam"](i_node, _b(param_name)) != 0)
+
+
+def IsNeuronPortParam(i_node, param_name):
+    return _check(_c["NESTGPU_IsNeuronPortParam"](i_node, _b(param_name)) != 0)
+
+
+def IsNeuronArrayParam(i_node, param_name):
+    return _check(_c["NESTGPU_IsNeuronArrayParam"](i_node, _b(param_name)) != 0)
+
+
+def IsNeuronGroupParam(i_node, param_name):
+    return _check(_c["NESTGPU_IsNeuronGroupParam"](i_node, _b(param_name)) != 0)
+
+
+def SetNeuronIntVar(i_node, n_node, var_name, val):
+    return _check(_c["NESTGPU_SetNeuronIntVar"](i_node, n_node, _b(var_name), int(val)))
+
+
+def SetNeuronScalVar(i_node, n_node, var_name, val):
+    return _check(_c["NESTGPU_SetNeuronScalVar"](i_node, n_node, _b(var_name), val))
+
+
+def SetNeuronArrayVar(i_node, n_node, var_name, var_list):
+    arr, n = _float_arr(var_list)
+    return _check(_c["NESTGPU_SetNeuronArrayVar"](i_node, n_node, _b(var_name), arr, n))
+
+
+def SetNeuronPtIntVar(nodes, var_name, val):
+    pt, n = _int_arr(nodes)
+    return _check(_c["NESTGPU_SetNeuronPtIntVar"](pt, n, _b(var_name), int(val)))
+
+
+def SetNeuronPtScalVar(nodes, var_name, val):
+    pt, n = _int_arr(nodes)
+    return _check(_c["NESTGPU_SetNeuronPtScalVar"](pt, n, _b(var_name), val))
+
+
+def SetNeuronPtArrayVar(nodes, var_name, var_list):
+    pt, n = _int_arr(nodes)
+    arr, na = _float_arr(var_list)
+    return _check(_c["NESTGPU_SetNeuronPtArrayVar"](pt, n, _b(var_name), arr, na))
+
+
+def IsNeuronIntVar(i_node, var_name):
+    return _check(_c["NESTGPU_IsNeuronIntVar"](i_node, _b(var_name)) != 0)
+
+
+def IsNeuronScalVar(i_node, var_name):
+    return _check(_c["NESTGPU_IsNeuronScalVar"](i_node, _b(var_name)) != 0)
+
+
+def IsNeuronPortVar(i_node, var_name):
+    return _check(_c["NESTGPU_IsNeuronPortVar"](i_node, _b(var_name)) != 0)
+
+
+def IsNeuronArrayVar(i_node, var_name):
+    return _check(_c["NESTGPU_IsNeuronArrayVar"](i_node, _b(var_name)) != 0)
+
+
+def GetNeuronParamSize(i_node, param_name):
+    return _check(_c["NESTGPU_GetNeuronParamSize"](i_node, _b(param_name)))
+
+
+def GetNeuronVarSize(i_node, var_name):
+    return _check(_c["NESTGPU_GetNeuronVarSize"](i_node, _b(var_name)))
+
+
+def _rows(pt, n_node, size):
+    out = []
+    for i in range(n_node):
+        if size > 1:
+            out.append([pt[i * size + j] for j in range(size)])
+        else:
+            out.append(pt[i])
+    _free(pt)
+    return out
+
+
+def GetNeuronParam(i_node, n_node, param_name):
+    pt = _c["NESTGPU_GetNeuronParam"](i_node, n_node, _b(param_name))
+    _check()
+    return _rows(pt, n_node, GetNeuronParamSize(i_node, param_name))
+
+
+def GetNeuronPtParam(nodes, param_name):
+    pt_n, n = _int_arr(nodes)
+    pt = _c["NESTGPU_GetNeuronPtParam"](pt_n, n, _b(param_name))
+    _check()
+    return _rows(pt, n, GetNeuronParamSize(nodes[0], param_name))
+
+
+def GetArrayParam(i_node, n_node, param_name):
+    out = []
+    for j in range(n_node):
+        pt = _c["NESTGPU_GetArrayParam"](i_node + j, _b(param_name))
+        _check()
+        size = GetNeuronParamSize(i_node + j, param_name)
+        out.append([pt[i] for i in range(size)])
+        _free(pt)
+    return out
+
+
+def GetNeuronListArrayParam(node_list, param_name):
+    out = []
+    for nd in node_list:
+        out += GetArrayParam(nd, 1, param_name)
+    return out
+
+
+def GetNeuronGroupParam(i_node, param_name):
+    return _check(_c["NESTGPU_GetNeuronGroupParam"](i_node, _b(param_name)))
+
+
+def GetNeuronIntVar(i_node, n_node, var_name):
+    pt = _c["NESTGPU_GetNeuronIntVar"](i_node, n_node, _b(var_name))
+    _check()
+    out = [pt[i] for i in range(n_node)]
+    _free(pt)
+    return out
+
+
+def GetNeuronVar(i_node, n_node, var_name):
+    pt = _c["NESTGPU_GetNeuronVar"](i_node, n_node, _b(var_name))
+    _check()
+    return _rows(pt, n_node, GetNeuronVarSize(i_node, var_name))
+
+
+def GetNeuronPtIntVar(nodes, var_name):
+    pt_n, n = _int_arr(nodes)
+    pt = _c["NESTGPU_GetNeuronPtIntVar"](pt_n, n, _b(var_name))
+    _check()
+    out = [pt[i] for i in range(n)]
+    _free(pt)
+    return out
+
+
+def GetNeuronPtVar(nodes, var_name):
+    pt_n, n = _int_arr(nodes)
+    pt = _c["NESTGPU_GetNeuronPtVar"](pt_n, n, _b(var_name))
+    _check()
+    return _rows(pt, n, GetNeuronVarSize(nodes[0], var_name))
+
+
+def GetArrayVar(i_node, n_node, var_name):
+    out = []
+    for j in range(n_node):
+        pt = _c["NESTGPU_GetArrayVar"](i_node + j, _b(var_name))
+        _check()
+        size = GetNeuronVarSize(i_node + j, var_name)
+        out.append([pt[i] for i in range(size)])
+    return out
+
+
+def GetNeuronListArrayVar(node_list, var_name):
+    out = []
+    for nd in node_list:
+        out += GetArrayVar(nd, 1, var_name)
+    return out
+
+
+def _node_list(nodes):
+    if isinstance(nodes, NodeSeq):
+        return nodes.ToList()
+    return list(nodes)
+
+
+def GetNeuronStatus(nodes, var_name):
+    "Get neuron group scalar or array variable or parameter"
+    if not isinstance(nodes, (list, tuple, NodeSeq)):
+        raise ValueError("Unknown node type")
+    if isinstance(nodes, NodeSeq):
+        i0, n = nodes.i0, nodes.n
+        if IsNeuronScalParam(i0, var_name) or IsNeuronPortParam(i0, var_name):
+            return GetNeuronParam(i0, n, var_name)
+        if IsNeuronArrayParam(i0, var_name):
+            return GetArrayParam(i0, n, var_name)
+        if IsNeuronIntVar(i0, var_name):
+            return GetNeuronIntVar(i0, n, var_name)
+        if IsNeuronScalVar(i0, var_name) or IsNeuronPortVar(i0, var_name):
+            return GetNeuronVar(i0, n, var_name)
+        if IsNeuronArrayVar(i0, var_name):
+            return GetArrayVar(i0, n, var_name)
+        if IsNeuronGroupParam(i0, var_name):
+            return GetNeuronStatus(nodes.ToList(), var_name)
+        raise ValueError("Unknown neuron variable or parameter")
+    nd0 = nodes[0]
+    if IsNeuronScalParam(nd0, var_name) or IsNeuronPortParam(nd0, var_name):
+        return GetNeuronPtParam(nodes, var_name)
+    if IsNeuronArrayParam(nd0, var_name):
+        return GetNeuronListArrayParam(nodes, var_name)
+    if IsNeuronIntVar(nd0, var_name):
+        return GetNeuronPtIntVar(nodes, var_name)
+    if IsNeuronScalVar(nd0, var_name) or IsNeuronPortVar(nd0, var_name):
+        return GetNeuronPtVar(nodes, var_name)
+    if IsNeuronArrayVar(nd0, var_name):
+        return GetNeuronListArrayVar(nodes, var_name)
+    if IsNeuronGroupParam(nd0, var_name):
+        return [GetNeuronGroupParam(nd, var_name) for nd in nodes]
+    raise ValueError("Unknown neuron variable or parameter")
+
+
+def GetNIntVar(i_node):
+    return _check(_c["NESTGPU_GetNIntVar"](i_node))
+
+
+def GetNScalVar(i_node):
+    return _check(_c["NESTGPU_GetNScalVar"](i_node))
+
+
+def GetIntVarNames(i_node):
+    return _names("IntVar", i_node)
+
+
+def GetScalVarNames(i_node):
+    return _names("ScalVar", i_node)
+
+
+def GetNPortVar(i_node):
+    return _check(_c["NESTGPU_GetNPortVar"](i_node))
+
+
+def GetPortVarNames(i_node):
+    return _names("PortVar", i_node)
+
+
+def GetNScalParam(i_node):
+    return _check(_c["NESTGPU_GetNScalParam"](i_node))
+
+
+def GetScalParamNames(i_node):
+    return _names("ScalParam", i_node)
+
+
+def GetNPortParam(i_node):
+    return _check(_c["NESTGPU_GetNPortParam"](i_node))
+
+
+def GetPortParamNames(i_node):
+    return _names("PortParam", i_node)
+
+
+def GetNArrayParam(i_node):
+    return _check(_c["NESTGPU_GetNArrayParam"](i_node))
+
+
+def GetArrayParamNames(i_node):
+    return _names("ArrayParam", i_node)
+
+
+def GetNGroupParam(i_node):
+    return _check(_c["NESTGPU_GetNGroupParam"](i_node))
+
+
+def GetGroupParamNames(i_node):
+    return _names("GroupParam", i_node)
+
+
+def GetNArrayVar(i_node):
+    return _check(_c["NESTGPU_GetNArrayVar"](i_node))
+
+
+def GetArrayVarNames(i_node):
+    return _names("ArrayVar", i_node)
+
+
+def SetNeuronGroupParam(nodes, param_name, val):
+    nodes = nodes if isinstance(nodes, NodeSeq) else NodeSeq(nodes[0], len(nodes))
+    return _check(_c["NESTGPU_SetNeuronGroupParam"](nodes.i0, nodes.n, _b(param_name), val))
+
+
+def SetNeuronStatus(nodes, var_name, val):
+    "Set neuron group scalar or array variable or parameter"
+    if not isinstance(nodes, (list, tuple, NodeSeq)):
+        raise ValueError("Unknown node type")
+    if isinstance(val, dict):
+        arr = DictToArray(val, len(nodes))
+        nl = _node_list(nodes)
+        for i in range(len(nl)):
+            SetNeuronStatus([nl[i]], var_name, arr[i])
+        return
+    if isinstance(nodes, NodeSeq):
+        i0, n = nodes.i0, nodes.n
+        if IsNeuronGroupParam(i0, var_name):
+            SetNeuronGroupParam(nodes, var_name, val)
+        elif IsNeuronScalParam(i0, var_name):
+            SetNeuronScalParam(i0, n, var_name, val)
+        elif IsNeuronPortParam(i0, var_name) or IsNeuronArrayParam(i0, var_name):
+            SetNeuronArrayParam(i0, n, var_name, val)
+        elif IsNeuronIntVar(i0, var_name):
+            SetNeuronIntVar(i0, n, var_name, val)
+        elif IsNeuronScalVar(i0, var_name):
+            SetNeuronScalVar(i0, n, var_name, val)
+        elif IsNeuronPortVar(i0, var_name) or IsNeuronArrayVar(i0, var_name):
+            SetNeuronArrayVar(i0, n, var_name, val)
+        else:
+            raise ValueError("Unknown neuron variable or parameter")
+    else:
+        nd0 = nodes[0]
+        if IsNeuronScalParam(nd0, var_name):
+            SetNeuronPtScalParam(nodes, var_name, val)
+        elif IsNeuronPortParam(nd0, var_name) or IsNeuronArrayParam(nd0, var_name):
+            SetNeuronPtArrayParam(nodes, var_name, val)
+        elif IsNeuronIntVar(nd0, var_name):
+            SetNeuronPtIntVar(nodes, var_name, val)
+        elif IsNeuronScalVar(nd0, var_name):
+            SetNeuronPtScalVar(nodes, var_name, val)
+        elif IsNeuronPortVar(nd0, var_name) or IsNeuronArrayVar(nd0, var_name):
+            SetNeuronPtArrayVar(nodes, var_name, val)
+        elif IsNeuronGroupParam(nd0, var_name):
+            SetNeuronGroupParam(nodes, var_name, val)
+        else:
+            raise ValueError("Unknown neuron variable or parameter")
+
+
+# ---------------------------------------------------------------- simulation
+def Calibrate():
+    return _check(_c["NESTGPU_Calibrate"]())
+
+
+def Simulate(sim_time=1000.0):
+    "Simulate neural activity"
+    SetSimTime(sim_time)
+    return _check(_c["NESTGPU_Simulate"]())
+
+
+def StartSimulation():
+    return _check(_c["NESTGPU_StartSimulation"]())
+
+
+def SimulationStep():
+    return _check(_c["NESTGPU_SimulationStep"]())
+
+
+def EndSimulation():
+    return _check(_c["NESTGPU_EndSimulation"]())
+
+
+def ConnectMpiInit():
+    raise ValueError("MPI is not available (single-GPU engine)")
+
+
+def MpiId():
+    return _c["NESTGPU_MpiId"]()
+
+
+def Rank():
+    return MpiId()
+
+
+def MpiNp():
+    return _c["NESTGPU_MpiNp"]()
+
+
+def ProcMaster():
+    return _c["NESTGPU_ProcMaster"]()
+
+
+def MpiFinalize():
+    return _c["NESTGPU_MpiFinalize"]()
+
+
+# ---------------------------------------------------------------- random numbers
+def RandomInt(n):
+    pt = _c["NESTGPU_RandomInt"](n)
+    _check()
+    out = [pt[i] for i in range(n)]
+    _free(pt)
+    return out
+
+
+def RandomUniform(n):
+    pt = _c["NESTGPU_RandomUniform"](n)
+    _check()
+    out = [pt[i] for i in range(n)]
+    _free(pt)
+    return out
+
+
+def RandomNormal(n, mean, stddev):
+    pt = _c["NESTGPU_RandomNormal"](n, mean, stddev)
+    _check()
+    out = (ctypes.c_float * n)(*[pt[i] for i in range(n)])
+    _free(pt)
+    return out
+
+
+def RandomNormalClipped(n, mean, stddev, vmin, vmax, vstep=0):
+    pt = _c["NESTGPU_RandomNormalClipped"](n, mean, stddev, vmin, vmax, vstep)
+    _check()
+    n4 = (n // 4 + 1) * 4
+    out = (ctypes.c_float * n4)(*[pt[i] for i in range(n4)])
+    _free(pt)
+    return out
+
+
+# ---------------------------------------------------------------- connections
+def SingleConnect(i_source_node, i_target_node, i_port, weight, delay):
+    return _check(_c["NESTGPU_Connect"](i_source_node, i_target_node, i_port, 0, weight, delay))
+
+
+def ConnSpecInit():
+    return _check(_c["NESTGPU_ConnSpecInit"]())
+
+
+def SetConnSpecParam(param_name, val):
+    return _check(_c["NESTGPU_SetConnSpecParam"](_b(param_name), val))
+
+
+def ConnSpecIsParam(param_name):
+    return _check(_c["NESTGPU_ConnSpecIsParam"](_b(param_name)) != 0)
+
+
+def SynSpecInit():
+    return _check(_c["NESTGPU_SynSpecInit"]())
+
+
+def SetSynSpecIntParam(param_name, val):
+    return _check(_c["NESTGPU_SetSynSpecIntParam"](_b(param_name), val))
+
+
+def SetSynSpecFloatParam(param_name, val):
+    return _check(_c["NESTGPU_SetSynSpecFloatParam"](_b(param_name), val))
+
+
+def SetSynSpecFloatPtParam(param_name, arr):
+    if isinstance(arr, (list, tuple)):
+        arr = (ctypes.c_float * len(arr))(*arr)
+    return _check(_c["NESTGPU_SetSynSpecFloatPtParam"](_b(param_name), ctypes.cast(arr, c_void_p)))
+
+
+def SynSpecIsIntParam(param_name):
+    return _check(_c["NESTGPU_SynSpecIsIntParam"](_b(param_name)) != 0)
+
+
+def SynSpecIsFloatParam(param_name):
+    return _check(_c["NESTGPU_SynSpecIsFloatParam"](_b(param_name)) != 0)
+
+
+def SynSpecIsFloatPtParam(param_name):
+    return _check(_c["NESTGPU_SynSpecIsFloatPtParam"](_b(param_name)) != 0)
+
+
+def DictToArray(param_dict, array_size):
+    """Array of `array_size` values from {"array": [...]} or a distribution
+    ("normal", "normal_clipped" with mu, sigma, low, high, step)."""
+    dist_name, arr, low, high, mu, sigma, vstep = None, None, -1.0e35, 1.0e35, None, None, 0
+    for k, v in param_dict.items():
+        if k == "array":
+            dist_name, arr = "array", v
+        elif k == "distribution":
+            dist_name = v
+        elif k == "low":
+            low = v
+        elif k == "high":
+            high = v
+        elif k == "mu":
+            mu = v
+        elif k == "sigma":
+            sigma = v
+        elif k == "step":
+            vstep = v
+        else:
+            raise ValueError("Unknown parameter name in dictionary")
+    if dist_name == "array":
+        if isinstance(arr, (list, tuple)):
+            if len(arr) != array_size:
+                raise ValueError("Wrong array size.")
+            arr = (ctypes.c_float * len(arr))(*arr)
+        return arr
+    elif dist_name == "normal":
+        return RandomNormal(array_size, mu, sigma)
+    elif dist_name == "normal_clipped":
+        return RandomNormalClipped(array_size, mu, sigma, low, high, vstep)
+    raise ValueError("Unknown distribution")
+
+
+def RuleArraySize(conn_dict, source, target):
+    rule = conn_dict["rule"]
+    if rule == "one_to_one":
+        return len(source)
+    if rule == "all_to_all":
+        return len(source) * len(target)
+    if rule == "fixed_total_number":
+        return conn_dict["total_num"]
+    if rule == "fixed_indegree":
+        return len(target) * conn_dict["indegree"]
+    if rule == "fixed_outdegree":
+        return len(source) * conn_dict["outdegree"]
+    raise ValueError("Unknown number of connections for this rule")
+
+
+def SetSynParamFromArray(param_name, par_dict, array_size):
+    arr_param_name = param_name + "_array"
+    if not SynSpecIsFloatPtParam(arr_param_name):
+        raise ValueError("Synapse parameter cannot be set by arrays or distributions")
+    arr = DictToArray(par_dict, array_size)
+    SetSynSpecFloatPtParam(arr_param_name, arr)
+    return arr
+
+
+def Connect(source, target, conn_dict, syn_dict):
+    "Connect two node groups"
+    if not isinstance(source, (list, tuple, NodeSeq)):
+        raise ValueError("Unknown source type")
+    if not isinstance(target, (list, tuple, NodeSeq)):
+        raise ValueError("Unknown target type")
+    gc.disable()
+    keep = []   # arrays handed to the engine by pointer stay alive during the call
+    try:
+        ConnSpecInit()
+        SynSpecInit()
+        for param_name in conn_dict:
+            if param_name == "rule":
+                if conn_dict[param_name] not in conn_rule_name:
+                    raise ValueError("Unknown connection rule")
+                SetConnSpecParam(param_name, conn_rule_name.index(conn_dict[param_name]))
+            elif ConnSpecIsParam(param_name):
+                SetConnSpecParam(param_name, conn_dict[param_name])
+            else:
+                raise ValueError("Unknown connection parameter")
+        array_size = RuleArraySize(conn_dict, source, target)
+        for param_name in syn_dict:
+            if SynSpecIsIntParam(param_name):
+                val = syn_dict[param_name]
+                if param_name == "synapse_group" and isinstance(val, SynGroup):
+                    val = val.i_syn_group
+                SetSynSpecIntParam(param_name, val)
+            elif SynSpecIsFloatParam(param_name):
+                fpar = syn_dict[param_name]
+                if isinstance(fpar, dict):
+                    keep.append(SetSynParamFromArray(param_name, fpar, array_size))
+                else:
+                    SetSynSpecFloatParam(param_name, fpar)
+            elif SynSpecIsFloatPtParam(param_name):
+                arr = syn_dict[param_name]
+                if isinstance(arr, (list, tuple)):
+                    arr = (ctypes.c_float * len(arr))(*arr)
+                keep.append(arr)
+                SetSynSpecFloatPtParam(param_name, arr)
+            else:
+                raise ValueError("Unknown synapse parameter")
+        if isinstance(source, NodeSeq) and isinstance(target, NodeSeq):
+            ret = _c["NESTGPU_ConnectSeqSeq"](source.i0, source.n, target.i0, target.n)
+        else:
+            if not isinstance(source, NodeSeq):
+                s_arr = (ctypes.c_int * len(source))(*source)
+                keep.append(s_arr)
+                s_pt = ctypes.cast(s_arr, c_void_p)
+            if not isinstance(target, NodeSeq):
+                t_arr = (ctypes.c_int * len(target))(*target)
+                keep.append(t_arr)
+                t_pt = ctypes.cast(t_arr, c_void_p)
+            if isinstance(source, NodeSeq):
+                ret = _c["NESTGPU_ConnectSeqGroup"](source.i0, source.n, t_pt, len(target))
+            elif isinstance(target, NodeSeq):
+                ret = _c["NESTGPU_ConnectGroupSeq"](s_pt, len(source), target.i0, target.n)
+            else:
+                ret = _c["NESTGPU_ConnectGroupGroup"](s_pt, len(source), t_pt, len(target))
+        return _check(ret)
+    finally:
+        gc.enable()
+
+
+def RemoteConnect(i_source_host, source, i_target_host, target, conn_dict, syn_dict):
+    raise ValueError("MPI is not available (single-GPU engine)")
+
+
+def GetConnections(source=None, target=None, syn_group=-1):
+    "Get connections between two node groups"
+    if source is None:
+        source = NodeSeq(None)
+    if target is None:
+        target = NodeSeq(None)
+    if isinstance(source, int):
+        source = [source]
+    if isinstance(target, int):
+        target = [target]
+    if not isinstance(source, (list, tuple, NodeSeq)):
+        raise ValueError("Unknown source type")
+    if not isinstance(target, (list, tuple, NodeSeq)):
+        raise ValueError("Unknown target type")
+    n_conn = ctypes.c_int(0)
+    if isinstance(source, NodeSeq) and isinstance(target, NodeSeq):
+        arr = _c["NESTGPU_GetSeqSeqConnections"](source.i0, source.n, target.i0, target.n, syn_group,
+                                                  ctypes.byref(n_conn))
+    else:
+        if not isinstance(source, NodeSeq):
+            s_arr = (ctypes.c_int * len(source))(*source)
+            s_pt = ctypes.cast(s_arr, c_void_p)
+        if not isinstance(target, NodeSeq):
+            t_arr = (ctypes.c_int * len(target))(*target)
+            t_pt = ctypes.cast(t_arr, c_void_p)
+        if isinstance(source, NodeSeq):
+            arr = _c["NESTGPU_GetSeqGroupConnections"](source.i0, source.n, t_pt, len(target),
+                                                        syn_group, ctypes.byref(n_conn))
+        elif isinstance(target, NodeSeq):
+            arr = _c["NESTGPU_GetGroupSeqConnections"](s_pt, len(source), target.i0, target.n,
+                                                        syn_group, ctypes.byref(n_conn))
+        else:
+            arr = _c["NESTGPU_GetGroupGroupConnections"](s_pt, len(source), t_pt, len(target),
+                                                          syn_group, ctypes.byref(n_conn))
+    _check()
+    out = [ConnectionId(arr[3 * i], arr[3 * i + 1], arr[3 * i + 2]) for i in range(n_conn.value)]
+    _free(arr)
+    return out
+
+
+def GetConnectionStatus(conn_id):
+    i_target = ctypes.c_int(0)
+    i_port = ctypes.c_char()
+    i_syn = ctypes.c_char()
+    delay = ctypes.c_float(0.0)
+    weight = ctypes.c_float(0.0)
+    _c["NESTGPU_GetConnectionStatus"](conn_id.i_source, conn_id.i_group, conn_id.i_conn,
+                                      ctypes.byref(i_target), ctypes.byref(i_port), ctypes.byref(i_syn),
+                                      ctypes.byref(delay), ctypes.byref(weight))
+    _check()
+    return {"source": conn_id.i_source, "target": i_target.value, "port": ord(i_port.value),
+            "syn": ord(i_syn.value), "delay": delay.value, "weight": weight.value}
+
+
+def SetStatus(gen_object, params, val=None):
+    "Set neuron group parameters or variables using dictionaries"
+    if isinstance(gen_object, RemoteNodeSeq):
+        if gen_object.i_host == MpiId():
+            SetStatus(gen_object.node_seq, params, val)
+        return
+    if isinstance(gen_object, SynGroup):
+        raise ValueError("synapse groups (plasticity) are not supported by this engine")
+    gc.disable()
+    try:
+        nodes = gen_object
+        if val is not None:
+            SetNeuronStatus(nodes, params, val)
+        elif isinstance(params, dict):
+            for param_name in params:
+                SetNeuronStatus(nodes, param_name, params[param_name])
+        elif isinstance(params, (list, tuple)):
+            if len(params) != len(nodes):
+                raise ValueError("List should have the same size as nodes")
+            for param_dict in params:
+                if not isinstance(param_dict, dict):
+                    raise ValueError("Type of list elements should be dict")
+                for param_name in param_dict:
+                    SetNeuronStatus(nodes, param_name, param_dict[param_name])
+        else:
+            raise ValueError("Wrong argument in SetStatus")
+        _check()
+    finally:
+        gc.enable()
+
+
+def GetStatus(gen_object, var_key=None):
+    "Get neuron group or connection status"
+    if isinstance(gen_object, SynGroup):
+        raise ValueError("synapse groups (plasticity) are not supported by this engine")
+    if isinstance(gen_object, NodeSeq):
+        if isinstance(var_key, str):
+            return GetNeuronStatus(gen_object, var_key)
+        gen_object = gen_object.ToList()
+    if isinstance(gen_object, (list, tuple)):
+        if isinstance(var_key, str) and len(gen_object) and isinstance(gen_object[0], int):
+            return GetNeuronStatus(list(gen_object), var_key)
+        return [GetStatus(elem, var_key) for elem in gen_object]
+    if isinstance(var_key, (list, tuple)):
+        return [GetStatus(gen_object, v) for v in var_key]
+    if var_key is None:
+        if isinstance(gen_object, ConnectionId):
+            return GetConnectionStatus(gen_object)
+        if isinstance(gen_object, int):
+            i_node = gen_object
+            names = (GetIntVarNames(i_node) + GetScalVarNames(i_node) + GetScalParamNames(i_node) +
+                     GetPortVarNames(i_node) + GetPortParamNames(i_node) + GetArrayVarNames(i_node) +
+                     GetArrayParamNames(i_node) + GetGroupParamNames(i_node))
+            return {name: GetStatus(i_node, name) for name in names}
+        raise ValueError("Unknown object type in GetStatus")
+    if isinstance(var_key, (str, bytes)):
+        if isinstance(gen_object, ConnectionId):
+            return GetConnectionStatus(gen_object)[var_key]
+        if isinstance(gen_object, int):
+            return GetNeuronStatus([gen_object], var_key)[0]
+        raise ValueError("Unknown object type in GetStatus")
+    raise ValueError("Unknown key type in GetStatus", type(var_key))
+
+
+def CreateSynGroup(model_name, status_dict=None):
+    return _check(_c["NESTGPU_CreateSynGroup"](_b(model_name)))
+
+
+# ---------------------------------------------------------------- spike recording
+def _seq_args(nodes):
+    if isinstance(nodes, NodeSeq):
+        return nodes.i0, nodes.n
+    nodes = list(nodes)
+    if nodes != list(range(nodes[0], nodes[0] + len(nodes))):
+        raise ValueError("Only node sequences are allowed here")
+    return nodes[0], len(nodes)
+
+
+def ActivateSpikeCount(nodes):
+    i0, n = _seq_args(nodes)
+    return _check(_c["NESTGPU_ActivateSpikeCount"](i0, n))
+
+
+def ActivateRecSpikeTimes(nodes, max_n_rec_spike_times):
+    i0, n = _seq_args(nodes)
+    return _check(_c["NESTGPU_ActivateRecSpikeTimes"](i0, n, max_n_rec_spike_times))
+
+
+def SetRecSpikeTimesStep(nodes, rec_spike_times_step):
+    i0, n = _seq_args(nodes)
+    return _check(_c["NESTGPU_SetRecSpikeTimesStep"](i0, n, rec_spike_times_step))
+
+
+def GetNRecSpikeTimes(i_node):
+    return _check(_c["NESTGPU_GetNRecSpikeTimes"](i_node))
+
+
+def GetRecSpikeTimes(nodes):
+    i0, n = _seq_args(nodes)
+    n_pt = ctypes.POINTER(ctypes.c_int)()
+    t_pt = ctypes.POINTER(ctypes.POINTER(ctypes.c_float))()
+    _c["NESTGPU_GetRecSpikeTimes"](i0, n, ctypes.byref(n_pt), ctypes.byref(t_pt))
+    _check()
+    return [[t_pt[i][j] for j in range(n_pt[i])] for i in range(n)]
+
+
+# ---------------------------------------------------------------- kernel parameters
+def GetNBoolParam():
+    return _c["NESTGPU_GetNBoolParam"]()
+
+
+def GetBoolParamNames():
+    pp = _c["NESTGPU_GetBoolParamNames"]()
+    return [pp[i].decode() for i in range(GetNBoolParam())]
+
+
+def IsBoolParam(param_name):
+    return _c["NESTGPU_IsBoolParam"](_b(param_name)) != 0
+
+
+def GetBoolParam(param_name):
+    return _check(_c["NESTGPU_GetBoolParam"](_b(param_name)))
+
+
+def SetBoolParam(param_name, val):
+    return _check(_c["NESTGPU_SetBoolParam"](_b(param_name), val))
+
+
+def GetNFloatParam():
+    return _c["NESTGPU_GetNFloatParam"]()
+
+
+def GetFloatParamNames():
+    pp = _c["NESTGPU_GetFloatParamNames"]()
+    return [pp[i].decode() for i in range(GetNFloatParam())]
+
+
+def IsFloatParam(param_name):
+    return _c["NESTGPU_IsFloatParam"](_b(param_name)) != 0
+
+
+def GetFloatParam(param_name):
+    return _check(_c["NESTGPU_GetFloatParam"](_b(param_name)))
+
+
+def SetFloatParam(param_name, val):
+    return _check(_c["NESTGPU_SetFloatParam"](_b(param_name), val))
+
+
+def GetNIntParam():
+    return _c["NESTGPU_GetNIntParam"]()
+
+
+def GetIntParamNames():
+    pp = _c["NESTGPU_GetIntParamNames"]()
+    return [pp[i].decode() for i in range(GetNIntParam())]
+
+
+def IsIntParam(param_name):
+    return _c["NESTGPU_IsIntParam"](_b(param_name)) != 0
+
+
+def GetIntParam(param_name):
+    return _check(_c["NESTGPU_GetIntParam"](_b(param_name)))
+
+
+def SetIntParam(param_name, val):
+    return _check(_c["NESTGPU_SetIntParam"](_b(param_name), val))
+
+
+def GetKernelStatus(var_key=None):
+    if isinstance(var_key, (list, tuple)):
+        return [GetKernelStatus(v) for v in var_key]
+    if var_key is None:
+        d = {}
+        for n in GetFloatParamNames():
+            d[n] = GetFloatParam(n)
+        for n in GetIntParamNames():
+            d[n] = GetIntParam(n)
+        for n in GetBoolParamNames():
+            d[n] = GetBoolParam(n)
+        return d
+    if IsFloatParam(var_key):
+        return GetFloatParam(var_key)
+    if IsIntParam(var_key):
+        return GetIntParam(var_key)
+    if IsBoolParam(var_key):
+        return GetBoolParam(var_key)
+    raise ValueError("Unknown parameter in GetKernelStatus", var_key)
+
+
+def SetKernelStatus(params, val=None):
+    if isinstance(params, str) and val is not None:
+        params = {params: val}
+    if not isinstance(params, dict):
+        raise ValueError("Wrong argument in SetKernelStatus")
+    for k, v in params.items():
+        if IsFloatParam(k):
+            SetFloatParam(k, v)
+        elif IsIntParam(k):
+            SetIntParam(k, v)
+        elif IsBoolParam(k):
+            SetBoolParam(k, v)
+        else:
+            raise ValueError("Unknown parameter in SetKernelStatus", k)
+
+
+def RemoteCreate(i_host, model_name, n_node=1, n_ports=1, status_dict=None):
+    raise ValueError("MPI is not available (single-GPU engine)")
+
+
+# ---------------------------------------------------------------- engine extensions
+def Reset():
+    """Discard the current network and start an empty one (engine extension)."""
+    if not is_b200_engine:
+        raise ValueError("Reset needs libnestgpu_b200.so")
+    return _check(_c["NGPU_Reset"]())
+
+
+def GetStats():
+    """Engine counters: RK5 derivative evaluations, synaptic events, spikes, wall time of
+    the last Simulate loop [s], steps, device status bits (engine extension)."""
+    if not is_b200_engine:
+        raise ValueError("GetStats needs libnestgpu_b200.so")
+    a, b, c = ctypes.c_ulonglong(), ctypes.c_ulonglong(), ctypes.c_ulonglong()
+    s, st, stat = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_uint()
+    _c["NGPU_GetStats"](ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(s),
+                        ctypes.byref(st), ctypes.byref(stat))
+    _check()
+    return {"n_derivs": a.value, "n_events": b.value, "n_spikes": c.value, "sim_seconds": s.value,
+            "steps": st.value, "status": stat.value}
+
+
+def ConnectArrays(source, target, weight, delay, port=None):
+    """Bulk connect edge lists (numpy arrays or sequences, one entry per edge)."""
+    import numpy as np
+    if not is_b200_engine:
+        raise ValueError("ConnectArrays needs libnestgpu_b200.so")
+    s = np.ascontiguousarray(source, dtype=np.int32)
+    t = np.ascontiguousarray(target, dtype=np.int32)
+    w = np.ascontiguousarray(weight, dtype=np.float32)
+    d = np.ascontiguousarray(delay, dtype=np.float32)
+    p = np.ascontiguousarray(port, dtype=np.uint8) if port is not None else None
+    n = s.size
+    if not (t.size == n and w.size == n and d.size == n and (p is None or p.size == n)):
+        raise ValueError("edge arrays must have the same length")
+    return _check(_c["NGPU_ConnectArrays"](n, s.ctypes.data, t.ctypes.data,
+                                           p.ctypes.data if p is not None else None,
+                                           w.ctypes.data, d.ctypes.data))
+
+
+def SetGraphSteps(n):
+    if not is_b200_engine:
+        raise ValueError("SetGraphSteps needs libnestgpu_b200.so")
+    return _check(_c["NGPU_SetGraphSteps"](n))

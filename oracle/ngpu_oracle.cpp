@@ -605,8 +605,8 @@ struct Net {
               float denom2 = 0.0f;
               float g0;
               if (denom1 != 0.0f) {
-                float t_p = td * tr * std::log(td / tr) / denom1;
-                denom2 = std::exp(-t_p / td) - std::exp(-t_p / tr);
+                float t_p = td * tr * logf(td / tr) / denom1;
+                denom2 = expf(-t_p / td) - expf(-t_p / tr);
               }
               if (denom2 == 0.0f) g0 = (float)(M_E / td);
               else g0 = (float)((1.0 / tr - 1.0 / td) / denom2);

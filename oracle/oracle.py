@@ -476,4 +476,4 @@ def _conn_status(self, conn_ids, var_key=None):
 
 
 Oracle.GetConnections = _get_connections
-Oracle.GetConnectionStatus = _conn_status
+Oracle.GetConnStatusList = _conn_status

@@ -89,7 +89,7 @@ def connect_scenario(api):
     api.Connect(even, odd, {"rule": "all_to_all"}, {"weight_array": e2o_w, "delay_array": e2o_d})
     api.Connect(odd, even, {"rule": "all_to_all"}, {"weight_array": o2e_w, "delay_array": o2e_d})
     out = {}
-    status = getattr(api, "GetConnectionStatus", None)
+    status = getattr(api, "GetConnStatusList", None)
 
     def st(ids, key=None):
         if status is not None:
