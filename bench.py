@@ -1,0 +1,351 @@
+"""Benchmark: 1,000,000 aeif_cond_beta_multisynapse neurons x 1000 synapses on one B200.
+
+Workload (1 GPU): 800k excitatory + 200k inhibitory AdEx neurons with two beta
+receptors (E_rev 0 / -85 mV, reference default parameters), every neuron with
+800 excitatory inputs (0.05 nS, receptor 0) and 200 inhibitory inputs (0.35 nS,
+receptor 1), sources drawn per target, delays uniform on {1.0, 1.1, ..., 2.0} ms
+(1e9 synapses, fp32 weights), one poisson_generator at 8 kHz into every neuron
+(0.1 nS, receptor 0), dt = 0.1 ms, seeded synthetic network.
+
+A bench "step" is 100 ms of biological time (1000 integration steps of dt)
+simulated through the engine's Simulate call.  `value` is synaptic events per
+second (device time, whole job: replicas on every GPU add up); RTF and RK5
+derivative evaluations per neuron-ms are reported next to it.  The network's
+CSR (8 GB) is far larger than L2, so no flush is needed between steps.
+
+`--impl reference` times the CPU implementation of the same path (the oracle
+restatement of the reference algorithm, OpenMP over the host cores) on a
+bounded sample of the workload: 20,000 neurons with the same in-degree, rates
+and delays for 100 ms of biological time per step; events/s and the RTF
+extrapolated per neuron are reported.
+
+Multi-GPU (torchrun): the network does not shard into independent parts, so each
+rank simulates its own replica (different seed); no collective is on the data
+path, only a barrier and a max-reduction of the step time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RANK = int(os.environ.get("RANK", "0"))
+WORLD = int(os.environ.get("WORLD_SIZE", "1"))
+LOCAL_RANK = int(os.environ.get("LOCAL_RANK", "0"))
+
+N_EXC, N_INH = 800_000, 200_000
+K_EXC, K_INH = 800, 200
+W_EXC, W_INH, W_PG = 0.05, 0.35, 0.1
+PG_RATE = 8000.0
+DELAY_MIN, DELAY_MAX = 1.0, 2.0
+STEP_MS = 100.0
+FLOPS_PER_DERIV = 110        # FP32 flops per derivative evaluation incl. stage algebra, 2 ports
+DELIVERY_BYTES_PER_EVENT = 8  # 4 B packed target/port + 4 B weight per synaptic event
+DELIVERY_BYTES_PER_SPIKE = 8  # ring entry (source, height)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    p.add_argument("--scale", type=float, default=1.0, help="fraction of the 1M-neuron network (tests)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+class ClockSampler(object):
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        sm.sort()
+        loaded = [x for x in sm if mx and x > 0.5 * mx] or sm
+        med = loaded[len(loaded) // 2] if loaded else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_engine_network(ngpu, scale, seed):
+    n_exc, n_inh = int(N_EXC * scale), int(N_INH * scale)
+    ngpu.SetVerbosityLevel(0)
+    ngpu.SetKernelStatus("rnd_seed", seed)
+    neuron = ngpu.Create("aeif_cond_beta_multisynapse", n_exc + n_inh, 2)
+    ngpu.SetStatus(neuron, {"E_rev": [0.0, -85.0]})
+    exc, inh = neuron[0:n_exc], neuron[n_exc:n_exc + n_inh]
+    pg = ngpu.Create("poisson_generator")
+    ngpu.SetStatus(pg, "rate", PG_RATE)
+    ngpu.Connect(pg, neuron, {"rule": "all_to_all"}, {"weight": W_PG, "delay": 1.0, "receptor": 0})
+    ngpu.ConnectFixedIndegreeGPU(exc, neuron, K_EXC, W_EXC, DELAY_MIN, DELAY_MAX, receptor=0, seed=seed)
+    ngpu.ConnectFixedIndegreeGPU(inh, neuron, K_INH, W_INH, DELAY_MIN, DELAY_MAX, receptor=1,
+                                 seed=seed + 7919)
+    ngpu.ActivateSpikeCount(neuron)
+    return neuron, pg
+
+
+def engine_arm(args):
+    if WORLD > 1:
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(LOCAL_RANK)
+    sys.path.insert(0, os.path.join(HERE, "nest-gpu_b200"))
+    import numpy as np
+    import nestgpu as ngpu
+    dist = None
+    if WORLD > 1:
+        import torch
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(0)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        dist = tdist
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    seed = 20240 + 101 * RANK
+    t_build0 = time.time()
+    neuron, pg = build_engine_network(ngpu, args.scale, seed)
+    ngpu.Calibrate()
+    build_s = time.time() - t_build0
+    n_neurons = len(neuron)
+
+    for _ in range(args.warmup):
+        ngpu.Simulate(STEP_MS)
+    st0 = ngpu.GetStats()
+    l0 = ngpu.GetLaunchCount()
+    sampler = ClockSampler(LOCAL_RANK)
+    barrier()
+    sampler.start()
+    dev_ms = 0.0
+    wall0 = time.time()
+    for _ in range(args.steps):
+        ngpu.Simulate(STEP_MS)
+        dev_ms += ngpu.GetSimDeviceMs()
+    wall = time.time() - wall0
+    clocks = sampler.stop()
+    barrier()
+    st1 = ngpu.GetStats()
+    launches = ngpu.GetLaunchCount() - l0
+    events = st1["n_events"] - st0["n_events"]
+    derivs = st1["n_derivs"] - st0["n_derivs"]
+    spikes = st1["n_spikes"] - st0["n_spikes"]
+    bio_s = args.steps * STEP_MS / 1000.0
+    t_max = max_over_ranks(dev_ms / 1000.0)
+    events_all = sum_over_ranks(float(events))
+    value = events_all / t_max
+    rtf = (dev_ms / 1000.0) / bio_s
+    evals_per_neuron_ms = derivs / (n_neurons * args.steps * STEP_MS)
+    rate_hz = spikes / (n_neurons * bio_s)
+
+    # per-kernel device times (ordinary steps, each kernel bracketed by CUDA events)
+    prof_steps = 200
+    st_p0 = ngpu.GetStats()
+    upd_ms, rec_ms, del_ms = ngpu.ProfileSteps(prof_steps)
+    st_p1 = ngpu.GetStats()
+    p_derivs = (st_p1["n_derivs"] - st_p0["n_derivs"]) / prof_steps
+    p_events = (st_p1["n_events"] - st_p0["n_events"]) / prof_steps
+    p_spikes = (st_p1["n_spikes"] - st_p0["n_spikes"]) / prof_steps
+    fp32_peak = (148 * 128 * 2 * (clocks["sm_mhz"] or 1965.0) * 1e6) / 1e12
+    rk5_tflops = p_derivs * FLOPS_PER_DERIV / (upd_ms / 1e3) / 1e12
+    deliver_gbs = (p_events * DELIVERY_BYTES_PER_EVENT + p_spikes * DELIVERY_BYTES_PER_SPIKE) / (del_ms / 1e3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+
+    # end to end through the public API: per step a host->device parameter write, the
+    # Simulate call and a device->host read of every neuron's spike count
+    e2e_steps = max(1, args.steps)
+    wall_e0 = time.time()
+    ev_e0 = ngpu.GetStats()["n_events"]
+    for _ in range(e2e_steps):
+        ngpu.SetStatus(pg, "rate", PG_RATE)
+        ngpu.Simulate(STEP_MS)
+        counts = ngpu.GetStatus(neuron, "spike_count")
+    e2e_wall = time.time() - wall_e0
+    e2e_events = ngpu.GetStats()["n_events"] - ev_e0
+    e2e_t = max_over_ranks(e2e_wall)
+    e2e_value = sum_over_ranks(float(e2e_events)) / e2e_t
+    assert len(counts) == n_neurons
+
+    result = {
+        "metric": "synaptic events/s, 1M aeif_cond_beta_multisynapse x 1000 synapses (1e9), dt 0.1 ms",
+        "value": value,
+        "unit": "events/s",
+        "n_gpus": WORLD,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_max * 1000.0 / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32",
+        "data": "synthetic (seeded random network and Poisson drive)",
+        "config": {"workload": "1M AdEx x 1000 syn (config 2)", "neurons": n_neurons,
+                   "synapses": n_neurons * (K_EXC + K_INH), "bio_ms_per_step": STEP_MS,
+                   "dt_ms": 0.1, "parallelism": "replicas%d" % WORLD,
+                   "l2": "inputs larger than L2 (8 GB edge array)", "scale": args.scale},
+        "rtf": rtf,
+        "rk5_evals_per_neuron_ms": evals_per_neuron_ms,
+        "firing_rate_hz": rate_hz,
+        "build_s": build_s,
+        "gpu_launches": launches,
+        "e2e": {"value": e2e_value, "unit": "events/s", "h2d_bytes_per_step": 4,
+                "d2h_bytes_per_step": 4 * n_neurons},
+        "roofline": {"bound": "fp32", "kernel": "aeif_update_kernel (RK5)",
+                     "achieved": rk5_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": rk5_tflops / fp32_peak, "traffic": None,
+                     "peak_source": "nominal FP32 rate 148 SM x 128 lanes x 2 x sampled SM clock",
+                     "ms_per_step": upd_ms},
+        "roofline_delivery": {"bound": "hbm", "kernel": "deliver_kernel", "achieved": deliver_gbs,
+                              "peak": hbm_peak, "unit": "GB/s", "frac": deliver_gbs / hbm_peak,
+                              "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                              "ms_per_step": del_ms},
+        "clocks": clocks,
+    }
+    if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_sample(steps=1, warmup=0)["cpu_baseline"]
+    if RANK == 0:
+        print(json.dumps(result), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_sample(steps, warmup):
+    """CPU restatement (oracle, OpenMP) on a 20k-neuron sample of the workload."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import numpy as np
+    import oracle as orc
+    n = 20_000
+    ne = int(0.8 * n)
+    rng = np.random.RandomState(7)
+    o = orc.Oracle(fp64=False)
+    o.SetKernelStatus("rnd_seed", 7)
+    neuron = o.Create("aeif_cond_beta_multisynapse", n, 2)
+    o.SetStatus(neuron, {"E_rev": [0.0, -85.0]})
+    pg = o.Create("poisson_generator")
+    o.SetStatus(pg, "rate", PG_RATE)
+    o.Connect(pg, neuron, {"rule": "all_to_all"}, {"weight": W_PG, "delay": 1.0, "receptor": 0})
+    tgt = np.repeat(np.arange(n, dtype=np.int32), K_EXC + K_INH)
+    src = np.concatenate([rng.randint(0, ne, size=(n, K_EXC)), rng.randint(ne, n, size=(n, K_INH))],
+                         axis=1).astype(np.int32).ravel()
+    port = np.tile(np.r_[np.zeros(K_EXC), np.ones(K_INH)].astype(np.int32), n)
+    w = np.tile(np.r_[np.full(K_EXC, W_EXC), np.full(K_INH, W_INH)].astype(np.float32), n)
+    d = (rng.randint(10, 21, size=src.size) * 0.1).astype(np.float32)
+    o.ConnectArrays(src, tgt, port, w, d)
+    o.ActivateSpikeCount(neuron)
+    threads = o.Threads()
+    for _ in range(warmup):
+        o.Simulate(STEP_MS)
+    e0 = o.NEvents()
+    t0 = time.time()
+    for _ in range(steps):
+        o.Simulate(STEP_MS)
+    dt = time.time() - t0
+    ev = o.NEvents() - e0
+    bio = steps * STEP_MS / 1000.0
+    ev_s = ev / dt
+    rtf_full = (dt / bio) * (1_000_000 / n)
+    return {"value": ev_s, "rtf_extrapolated_1M": rtf_full, "seconds": dt,
+            "cpu_baseline": {"value": ev_s, "unit": "events/s", "cores": threads, "kind": "port",
+                             "sample": "20,000-neuron sample (same in-degree, weights, delays, Poisson "
+                                       "drive), %g ms bio per step; RTF extrapolated to 1M neurons = %.1f"
+                                       % (STEP_MS, rtf_full)}}
+
+
+def reference_arm(args):
+    if RANK != 0:
+        return
+    r = cpu_sample(args.steps, args.warmup)
+    out = {
+        "impl": "reference",
+        "metric": "synaptic events/s, 1M aeif_cond_beta_multisynapse x 1000 synapses (1e9), dt 0.1 ms",
+        "value": r["value"],
+        "unit": "events/s",
+        "n_gpus": WORLD,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": r["seconds"] * 1000.0 / max(args.steps, 1),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32",
+        "data": "synthetic (seeded random network and Poisson drive)",
+        "config": {"workload": "1M AdEx x 1000 syn (config 2)", "sample_neurons": 20000,
+                   "bio_ms_per_step": STEP_MS, "dt_ms": 0.1},
+        "rtf_extrapolated_1M": r["rtf_extrapolated_1M"],
+        "cpu_baseline": dict(r["cpu_baseline"]),
+        "e2e": {"value": r["value"], "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        engine_arm(args)
+
+
+if __name__ == "__main__":
+    main()

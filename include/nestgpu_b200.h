@@ -228,8 +228,36 @@ int NGPU_GetStats(unsigned long long *n_derivs, unsigned long long *n_events,
 int NGPU_ConnectArrays(size_t n, int *source, int *target, unsigned char *port, float *weight,
                        float *delay);
 
+/* Number of engine kernels launched since the engine was created (a CUDA-graph replay counts
+   each kernel node it runs). */
+long long NGPU_GetLaunchCount();
+
+/* Device time [ms] of the last NESTGPU_Simulate call: CUDA events recorded on the engine's
+   stream around its step loop and final input fold. */
+double NGPU_GetSimDeviceMs();
+
+/* Run n ordinary simulation steps with each kernel bracketed by CUDA events; writes the
+   average device time per step [ms] of the neuron-update kernels, the record gather and the
+   spike delivery into ms_out[0..2]; returns 3. */
+int NGPU_ProfileSteps(int n, double *ms_out);
+
+/* Fixed in-degree block generated on the device at calibration: each of the n_target
+   targets draws `indegree` sources uniformly (with replacement) from the n_source nodes
+   starting at i_source, with delays uniform on the time grid in [delay_min, delay_max] ms.
+   Unlike NESTGPU's fixed_indegree rule (one draw shared by all targets of a call), every
+   target draws its own sources.  The edges live only on the device (GetConnections does not
+   list them). */
+int NGPU_ConnectFixedIndegreeGPU(int i_source, int n_source, int i_target, int n_target, int indegree,
+                                 int port, float weight, float delay_min, float delay_max,
+                                 unsigned long long seed);
+
 /* Steps captured per CUDA graph (default 100). */
 int NGPU_SetGraphSteps(int n);
+
+/* 1: draw connection random numbers with cuRAND's host generator instead of the device
+   generator the reference uses (integer streams are identical, normal streams are not);
+   lets a CPU checker reproduce normal-distributed weights and delays exactly. */
+int NGPU_SetHostRng(int on);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,146 @@
+// Device-side construction of the recurrent CSR (edges sorted by (source, delay)).
+//
+// Edges come from two places: the host connection store (rule-based Connect
+// calls, kept for GetConnections) and generated blocks (fixed in-degree with
+// per-target random sources and uniform delays on the time grid, drawn on the
+// GPU from Philox4x32-10 so that 1e9-edge networks never touch host memory).
+// Counting sort on the device: per-key counters, an exclusive scan into the
+// segment offsets, host edges first in each segment (insertion order), then the
+// generated edges through atomic cursors.  The order inside a segment does not
+// change results: the input accumulator sums in FP64 and is read only after the
+// delivery kernel has finished.
+#include <cub/device/device_scan.cuh>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "ngpu_math.cuh"
+#include "ngpu_types.h"
+
+namespace ngpu {
+
+
+__device__ __forceinline__ void gen_edge(const GenBlockDev &b, long long e, int &src, int &d, int &tgt) {
+  const int t = (int)(e / b.k);
+  const int kk = (int)(e - (long long)t * b.k);
+  U4 c = {(uint32_t)t, (uint32_t)kk, (uint32_t)b.block_id, 0x9E3779B9u};
+  U4 r = philox(c, (uint32_t)b.seed, (uint32_t)(b.seed >> 32));
+  src = b.src0 + (int)(((unsigned long long)r.x * (unsigned)b.nsrc) >> 32);
+  d = b.dlo + (int)(((unsigned long long)r.y * (unsigned)(b.dhi - b.dlo + 1)) >> 32);
+  tgt = t;
+}
+
+__global__ void gen_count_kernel(GenBlockDev b, int dmin, int dspan, unsigned long long *cnt) {
+  const long long total = (long long)b.ntgt * b.k;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    int s, d, t;
+    gen_edge(b, e, s, d, t);
+    atomicAdd(&cnt[(size_t)s * dspan + (d - dmin)], 1ULL);
+  }
+}
+
+__global__ void gen_fill_kernel(GenBlockDev b, int dmin, int dspan, unsigned long long *cursor,
+                                EdgeW *edge) {
+  const long long total = (long long)b.ntgt * b.k;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    int s, d, t;
+    gen_edge(b, e, s, d, t);
+    unsigned long long pos = atomicAdd(&cursor[(size_t)s * dspan + (d - dmin)], 1ULL);
+    EdgeW x;
+    x.acc = (uint32_t)(b.acc_base + (unsigned long long)(b.tgt_i0_rel + t));
+    x.w = b.w;
+    edge[pos] = x;
+  }
+}
+
+__global__ void host_edge_scatter_kernel(size_t n, const long long *key, const int *rank,
+                                         const EdgeW *ew, const unsigned long long *off, EdgeW *edge) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    edge[off[key[i]] + rank[i]] = ew[i];
+}
+
+__global__ void cursor_init_kernel(size_t nkey, const unsigned long long *off, const int *cnt_host,
+                                   unsigned long long *cursor) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nkey; i += (size_t)gridDim.x * blockDim.x)
+    cursor[i] = off[i] + (cnt_host ? (unsigned long long)cnt_host[i] : 0ULL);
+}
+
+__global__ void has_out_kernel(int n_nodes, int dspan, const unsigned long long *off, unsigned char *has_out) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_nodes; s += gridDim.x * blockDim.x)
+    has_out[s] = off[(size_t)(s + 1) * dspan] > off[(size_t)s * dspan] ? 1 : 0;
+}
+
+static void ck(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+// Build the CSR.  cnt_host: per-key counts of host edges (or empty); host edges given as
+// (key, rank in segment, EdgeW).  Returns device offsets (nkey+1, unsigned 64-bit) and edges.
+void build_csr_device(int n_nodes, int dmin, int dspan, const std::vector<int> &cnt_host,
+                      const std::vector<long long> &h_key, const std::vector<int> &h_rank,
+                      const std::vector<EdgeW> &h_ew, const std::vector<GenBlockDev> &blocks,
+                      unsigned long long **d_off_out, EdgeW **d_edge_out, size_t *n_edge_out,
+                      unsigned char *d_has_out, cudaStream_t st) {
+  const size_t nkey = (size_t)n_nodes * dspan;
+  unsigned long long *d_cnt = nullptr, *d_off = nullptr, *d_cursor = nullptr;
+  int *d_cnt_host = nullptr;
+  ck(cudaMalloc(&d_cnt, (nkey + 1) * sizeof(unsigned long long)), "cudaMalloc");
+  ck(cudaMalloc(&d_off, (nkey + 1) * sizeof(unsigned long long)), "cudaMalloc");
+  ck(cudaMemsetAsync(d_cnt, 0, (nkey + 1) * sizeof(unsigned long long), st), "memset");
+  if (!cnt_host.empty()) {
+    ck(cudaMalloc(&d_cnt_host, nkey * sizeof(int)), "cudaMalloc");
+    ck(cudaMemcpyAsync(d_cnt_host, cnt_host.data(), nkey * sizeof(int), cudaMemcpyHostToDevice, st), "copy");
+    std::vector<unsigned long long> c64(cnt_host.begin(), cnt_host.end());
+    ck(cudaMemcpyAsync(d_cnt, c64.data(), nkey * sizeof(unsigned long long), cudaMemcpyHostToDevice, st), "copy");
+    ck(cudaStreamSynchronize(st), "sync");
+  }
+  const int gb = 148 * 8, tb = 256;
+  for (const auto &b : blocks) gen_count_kernel<<<gb, tb, 0, st>>>(b, dmin, dspan, d_cnt);
+  size_t tmp_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_cnt, d_off, nkey + 1, st);
+  void *d_tmp = nullptr;
+  ck(cudaMalloc(&d_tmp, tmp_bytes), "cudaMalloc");
+  cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_cnt, d_off, nkey + 1, st);
+  unsigned long long total = 0;
+  ck(cudaMemcpyAsync(&total, d_off + nkey, sizeof(total), cudaMemcpyDeviceToHost, st), "copy");
+  ck(cudaStreamSynchronize(st), "sync");
+  EdgeW *d_edge = nullptr;
+  ck(cudaMalloc(&d_edge, std::max<unsigned long long>(total, 1) * sizeof(EdgeW)), "cudaMalloc (edges)");
+  if (!h_ew.empty()) {
+    long long *d_key = nullptr;
+    int *d_rank = nullptr;
+    EdgeW *d_hew = nullptr;
+    size_t n = h_ew.size();
+    ck(cudaMalloc(&d_key, n * sizeof(long long)), "cudaMalloc");
+    ck(cudaMalloc(&d_rank, n * sizeof(int)), "cudaMalloc");
+    ck(cudaMalloc(&d_hew, n * sizeof(EdgeW)), "cudaMalloc");
+    ck(cudaMemcpyAsync(d_key, h_key.data(), n * sizeof(long long), cudaMemcpyHostToDevice, st), "copy");
+    ck(cudaMemcpyAsync(d_rank, h_rank.data(), n * sizeof(int), cudaMemcpyHostToDevice, st), "copy");
+    ck(cudaMemcpyAsync(d_hew, h_ew.data(), n * sizeof(EdgeW), cudaMemcpyHostToDevice, st), "copy");
+    host_edge_scatter_kernel<<<gb, tb, 0, st>>>(n, d_key, d_rank, d_hew, d_off, d_edge);
+    ck(cudaStreamSynchronize(st), "scatter");
+    cudaFree(d_key);
+    cudaFree(d_rank);
+    cudaFree(d_hew);
+  }
+  if (!blocks.empty()) {
+    ck(cudaMalloc(&d_cursor, nkey * sizeof(unsigned long long)), "cudaMalloc");
+    cursor_init_kernel<<<gb, tb, 0, st>>>(nkey, d_off, d_cnt_host, d_cursor);
+    for (const auto &b : blocks) gen_fill_kernel<<<gb, tb, 0, st>>>(b, dmin, dspan, d_cursor, d_edge);
+  }
+  has_out_kernel<<<gb, tb, 0, st>>>(n_nodes, dspan, d_off, d_has_out);
+  ck(cudaStreamSynchronize(st), "build");
+  ck(cudaGetLastError(), "build kernels");
+  cudaFree(d_tmp);
+  cudaFree(d_cnt);
+  if (d_cursor) cudaFree(d_cursor);
+  if (d_cnt_host) cudaFree(d_cnt_host);
+  *d_off_out = d_off;
+  *d_edge_out = d_edge;
+  *n_edge_out = (size_t)total;
+}
+
+}  // namespace ngpu

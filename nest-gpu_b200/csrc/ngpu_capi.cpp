@@ -36,6 +36,7 @@ struct SynSpecC {
 };
 ConnSpecC g_conn;
 SynSpecC g_syn;
+double g_last_device_ms = 0.0;
 
 void fail(unsigned char code, const std::string &msg) {
   g_err.flag = true;
@@ -622,6 +623,7 @@ int NGPU_GetStats(unsigned long long *n_derivs, unsigned long long *n_events, un
                   double *sim_seconds, long long *steps, unsigned int *status) {
   return guard([&] {
     EngineStats s = E().stats();
+    g_last_device_ms = s.sim_device_ms;
     if (n_derivs) *n_derivs = s.n_derivs;
     if (n_events) *n_events = s.n_events;
     if (n_spikes) *n_spikes = s.n_spikes;
@@ -635,6 +637,40 @@ int NGPU_GetStats(unsigned long long *n_derivs, unsigned long long *n_events, un
 int NGPU_ConnectArrays(size_t n, int *source, int *target, unsigned char *port, float *weight,
                        float *delay) {
   return guard([&] { E().connect_arrays(n, source, target, port, weight, delay); return 0; }, 0);
+}
+
+int NGPU_SetHostRng(int on) {
+  return guard([&] {
+    E().use_device_rng = (on == 0);
+    E().set_seed(E().seed);   // recreate the generator of the chosen kind, same seed
+    return 0;
+  }, 0);
+}
+
+long long NGPU_GetLaunchCount() {
+  return guard([&] { return E().n_launches(); }, 0LL);
+}
+
+double NGPU_GetSimDeviceMs() {
+  return guard([&] { return E().stats().sim_device_ms; }, 0.0);
+}
+
+int NGPU_ProfileSteps(int n, double *ms_out) {
+  return guard([&] {
+    std::vector<double> v = E().profile_steps(n);
+    for (size_t i = 0; i < v.size(); i++) ms_out[i] = v[i];
+    return (int)v.size();
+  }, 0);
+}
+
+int NGPU_ConnectFixedIndegreeGPU(int i_source, int n_source, int i_target, int n_target, int indegree,
+                                 int port, float weight, float delay_min, float delay_max,
+                                 unsigned long long seed) {
+  return guard([&] {
+    E().connect_fixed_indegree_per_target(i_source, n_source, i_target, n_target, indegree, port, weight,
+                                          delay_min, delay_max, seed);
+    return 0;
+  }, 0);
 }
 
 int NGPU_SetGraphSteps(int n) {

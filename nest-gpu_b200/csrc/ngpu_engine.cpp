@@ -588,6 +588,25 @@ void Engine::connect_rule(int rule, const int *src_arr, int src0, int ns, const 
   }
 }
 
+// Fixed in-degree with per-target random sources (with replacement) and delays uniform on
+// the time grid in [dmin_ms, dmax_ms], generated on the device at calibration.  Unlike the
+// reference's fixed_indegree rule every target draws its own sources.
+void Engine::connect_fixed_indegree_per_target(int src0, int ns, int tgt0, int nt, int k, int port,
+                                               float w, float dmin_ms, float dmax_ms, uint64_t s) {
+  if (calibrated_) throw NgpuError("Connections cannot be created after calibration");
+  if (ns <= 0 || nt <= 0 || k <= 0) throw NgpuError("empty connection block");
+  if (src0 < 0 || src0 + ns > n_nodes()) throw NgpuError("Unrecognized source node");
+  Group &tg = group_of(tgt0);
+  if (tgt0 + nt > tg.i0 + tg.n) throw NgpuError("Targets of a generated block must belong to one node group");
+  if (port < 0 || port >= tg.nport) throw NgpuError("Port index out of range");
+  if (dmin_ms < dt || dmax_ms < dmin_ms) throw NgpuError("Delay must be >= time resolution");
+  for (int i = src0; i < src0 + ns; i++)
+    if (groups_[node_group_[i]].model == M_POISS_GEN) throw NgpuError("poisson_generator cannot be a source of a generated block");
+  if ((long long)nt * k > (1LL << 40)) throw NgpuError("connection block too large");
+  blocks_.push_back({src0, ns, tgt0, nt, k, port, w, dmin_ms, dmax_ms, s});
+  n_generated_ += (size_t)nt * k;
+}
+
 void Engine::connect_arrays(size_t n, const int *src, const int *tgt, const unsigned char *port,
                             const float *w, const float *d) {
   if (calibrated_) throw NgpuError("Connections cannot be created after calibration");

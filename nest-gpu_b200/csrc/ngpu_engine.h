@@ -77,6 +77,7 @@ struct EngineStats {
   unsigned long long n_events = 0;      // synaptic events delivered
   unsigned long long n_spikes = 0;
   double sim_seconds = 0.0;             // wall time inside the step loop of the last Simulate
+  double sim_device_ms = 0.0;           // device time (CUDA events) of the last Simulate
   long long steps = 0;
   unsigned status = 0;
 };
@@ -135,7 +136,7 @@ class Engine {
   void connect_rule(int rule, const int *src_arr, int src0, int ns, const int *tgt_arr, int tgt0,
                     int nt, int degree, int port, int syn_group, float w, float d,
                     const float *warr, const float *darr);
-  size_t n_connections() const { return c_src_.size(); }
+  size_t n_connections() const { return c_src_.size() + n_generated_; }
   // ids (source, group, index) in reference order, filtered
   std::vector<int> get_connections(const int *src_arr, int src0, int ns, const int *tgt_arr,
                                    int tgt0, int nt);
@@ -166,6 +167,11 @@ class Engine {
   bool calibrated() const { return calibrated_; }
   double neural_time() const { return neural_time_; }
   EngineStats stats();
+  // Run n steps with every kernel bracketed by CUDA events on the engine stream;
+  // returns the average device time per step [ms] of: neuron updates (all groups),
+  // record gather, spike delivery.  The steps are ordinary simulation steps.
+  std::vector<double> profile_steps(int n);
+  long long n_launches() const { return n_launch_; }
 
   // device buffers exposed to the engine-level helpers
   cudaStream_t stream() const { return stream_; }
@@ -179,6 +185,14 @@ class Engine {
   std::vector<unsigned char> c_port_;
   std::vector<float> c_w_;
   std::vector<int> c_d_;
+  // generated blocks (connect_fixed_indegree_per_target)
+  struct GenBlock {
+    int src0, nsrc, tgt0, ntgt, k, port;
+    float w, dmin_ms, dmax_ms;
+    uint64_t seed;
+  };
+  std::vector<GenBlock> blocks_;
+  size_t n_generated_ = 0;
   // reference order cache: permutation, group index and index-in-group per edge
   bool order_valid_ = false;
   std::vector<long long> ord_;          // edge ids in reference order
@@ -226,6 +240,13 @@ class Engine {
   std::map<int, cudaGraphExec_t> graphs_;
   std::vector<void *> allocs_;
   double last_sim_seconds_ = 0.0;
+  double last_sim_device_ms_ = 0.0;
+  long long n_launch_ = 0;                 // kernels launched (graph replays count their nodes)
+  std::map<int, long long> graph_nodes_;   // kernels per captured graph
+  bool capturing_ = false;
+  long long capture_count_ = 0;
+  void count_launch(long long n) { if (capturing_) capture_count_ += n; else n_launch_ += n; }
+  cudaEvent_t ev_a_ = nullptr, ev_b_ = nullptr;
   long long total_steps_ = 0;
   unsigned status_seen_ = 0;
 
@@ -264,5 +285,10 @@ void launch_record(const RecCol *cols, int ncol, float *buf, const int *last_tid
 void launch_clock_advance(Clock *clk, int K, cudaStream_t st);
 void launch_clock_clear_pending(Clock *clk, cudaStream_t st);
 int deliver_max_dspan();
+void build_csr_device(int n_nodes, int dmin, int dspan, const std::vector<int> &cnt_host,
+                      const std::vector<long long> &h_key, const std::vector<int> &h_rank,
+                      const std::vector<EdgeW> &h_ew, const std::vector<GenBlockDev> &blocks,
+                      unsigned long long **d_off_out, EdgeW **d_edge_out, size_t *n_edge_out,
+                      unsigned char *d_has_out, cudaStream_t st);
 
 }  // namespace ngpu

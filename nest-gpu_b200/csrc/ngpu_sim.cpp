@@ -165,41 +165,71 @@ void Engine::calibrate() {
     dmin = std::min(dmin, c_d_[e]);
     dmax = std::max(dmax, c_d_[e]);
   }
-  if (n_rec_edges == 0) { dmin = 0; dmax = 0; }
+  std::vector<GenBlockDev> gblocks;
+  for (size_t bi = 0; bi < blocks_.size(); bi++) {
+    const GenBlock &b = blocks_[bi];
+    Group &tg = group_of(b.tgt0);
+    GenBlockDev d;
+    d.src0 = b.src0;
+    d.nsrc = b.nsrc;
+    d.ntgt = b.ntgt;
+    d.k = b.k;
+    d.tgt_i0_rel = b.tgt0 - tg.i0;
+    d.group_n = tg.n;
+    d.acc_base = tg.acc_off + (unsigned long long)b.port * tg.n;
+    d.w = b.w;
+    d.dlo = (int)std::round(b.dmin_ms / dt) - 1;
+    d.dhi = (int)std::round(b.dmax_ms / dt) - 1;
+    d.seed = b.seed;
+    d.block_id = (int)bi;
+    dmin = std::min(dmin, d.dlo);
+    dmax = std::max(dmax, d.dhi);
+    gblocks.push_back(d);
+  }
+  if (n_rec_edges == 0 && gblocks.empty()) { dmin = 0; dmax = 0; }
   dmin_ = dmin;
   dspan_ = dmax - dmin + 1;
   if (dspan_ > deliver_max_dspan())
     throw NgpuError("delay range exceeds " + std::to_string(deliver_max_dspan()) + " time steps");
-  std::vector<unsigned char> has_out(N, 0);
-  {
-    const size_t nkey = (size_t)N * dspan_;
-    std::vector<long long> off(nkey + 1, 0);
-    for (size_t e = 0; e < E; e++) {
-      if (is_pg[c_src_[e]]) continue;
-      off[(size_t)c_src_[e] * dspan_ + (c_d_[e] - dmin) + 1]++;
-      has_out[c_src_[e]] = 1;
-    }
-    for (size_t k = 0; k < nkey; k++) off[k + 1] += off[k];
-    std::vector<EdgeW> ew(n_rec_edges);
-    std::vector<long long> pos(off.begin(), off.end() - 1);
-    for (size_t e = 0; e < E; e++) {
-      if (is_pg[c_src_[e]]) continue;
-      const Group &tg = groups_[node_group_[c_tgt_[e]]];
-      size_t key = (size_t)c_src_[e] * dspan_ + (c_d_[e] - dmin);
-      EdgeW x;
-      x.acc = (uint32_t)(tg.acc_off + (size_t)c_port_[e] * tg.n + (c_tgt_[e] - tg.i0));
-      x.w = c_w_[e];
-      ew[pos[key]++] = x;
-    }
-    d_ev_off_ = dalloc<long long>(nkey + 1);
-    cuda_check(cudaMemcpy(d_ev_off_, off.data(), (nkey + 1) * sizeof(long long), cudaMemcpyHostToDevice), "ev_off");
-    d_edge_ = dalloc<EdgeW>(n_rec_edges);
-    if (n_rec_edges)
-      cuda_check(cudaMemcpy(d_edge_, ew.data(), n_rec_edges * sizeof(EdgeW), cudaMemcpyHostToDevice), "edges");
-    n_edge_dev_ = n_rec_edges;
-  }
   d_has_out_ = dalloc<unsigned char>(N);
-  cuda_check(cudaMemcpy(d_has_out_, has_out.data(), N, cudaMemcpyHostToDevice), "has_out");
+  {
+    // host edges: per-key counts and each edge's rank inside its (source, delay) segment,
+    // in insertion order; the device does the scan, placement and generated blocks
+    const size_t nkey = (size_t)N * dspan_;
+    std::vector<int> cnt;
+    std::vector<long long> hkey;
+    std::vector<int> hrank;
+    std::vector<EdgeW> hew;
+    if (n_rec_edges) {
+      cnt.assign(nkey, 0);
+      hkey.reserve(n_rec_edges);
+      hrank.reserve(n_rec_edges);
+      hew.reserve(n_rec_edges);
+      for (size_t e = 0; e < E; e++) {
+        if (is_pg[c_src_[e]]) continue;
+        const Group &tg = groups_[node_group_[c_tgt_[e]]];
+        long long key = (long long)c_src_[e] * dspan_ + (c_d_[e] - dmin);
+        hkey.push_back(key);
+        hrank.push_back(cnt[key]++);
+        EdgeW x;
+        x.acc = (uint32_t)(tg.acc_off + (size_t)c_port_[e] * tg.n + (c_tgt_[e] - tg.i0));
+        x.w = c_w_[e];
+        hew.push_back(x);
+      }
+    }
+    unsigned long long *d_off = nullptr;
+    EdgeW *d_edge = nullptr;
+    size_t n_edge = 0;
+    build_csr_device(N, dmin_, dspan_, cnt, hkey, hrank, hew, gblocks, &d_off, &d_edge, &n_edge,
+                     d_has_out_, stream_);
+    allocs_.push_back(d_off);
+    allocs_.push_back(d_edge);
+    d_ev_off_ = (long long *)d_off;
+    d_edge_ = d_edge;
+    n_edge_dev_ = n_edge;
+  }
+  std::vector<unsigned char> has_out(N, 0);
+  cuda_check(cudaMemcpy(has_out.data(), d_has_out_, N, cudaMemcpyDeviceToHost), "has_out");
   int n_src_out = 0;
   for (int i = 0; i < N; i++) n_src_out += has_out[i];
 
@@ -582,23 +612,27 @@ DeliverArgs Engine::deliver_args() {
 void Engine::launch_step(int k) {
   SpikeOut so = spike_out();
   for (auto &g : groups_) {
-    if (is_aeif(g.model)) launch_aeif(g.model, false, aeif_args(g), so, d_clk_, k, stream_);
-    else if (g.model == M_IAF_PSC_EXP) launch_iaf(false, iaf_args(g), so, d_clk_, k, dt, stream_);
-    else if (g.model == M_SPIKE_GEN) launch_spike_gen(sg_args(g), so, d_clk_, k, dt, stream_);
+    if (is_aeif(g.model)) { launch_aeif(g.model, false, aeif_args(g), so, d_clk_, k, stream_); count_launch(1); }
+    else if (g.model == M_IAF_PSC_EXP) { launch_iaf(false, iaf_args(g), so, d_clk_, k, dt, stream_); count_launch(1); }
+    else if (g.model == M_SPIKE_GEN) { launch_spike_gen(sg_args(g), so, d_clk_, k, dt, stream_); count_launch(1); }
   }
-  if (rec_ncol_)
+  if (rec_ncol_) {
     launch_record(d_cols_, rec_ncol_, d_recbuf_, d_last_tidx_, d_last_h_, d_has_out_, d_clk_, k, dt,
                   stream_);
+    count_launch(1);
+  }
   launch_deliver(deliver_args(), deliver_blocks_, d_clk_, k, dt, stream_);
+  count_launch(1);
 }
 
 void Engine::launch_flush() {
   SpikeOut so = spike_out();
   for (auto &g : groups_) {
-    if (is_aeif(g.model)) launch_aeif(g.model, true, aeif_args(g), so, d_clk_, 0, stream_);
-    else if (g.model == M_IAF_PSC_EXP) launch_iaf(true, iaf_args(g), so, d_clk_, 0, dt, stream_);
+    if (is_aeif(g.model)) { launch_aeif(g.model, true, aeif_args(g), so, d_clk_, 0, stream_); count_launch(1); }
+    else if (g.model == M_IAF_PSC_EXP) { launch_iaf(true, iaf_args(g), so, d_clk_, 0, dt, stream_); count_launch(1); }
   }
   launch_clock_clear_pending(d_clk_, stream_);
+  count_launch(1);
 }
 
 void Engine::run_steps(long long n) {
@@ -622,8 +656,13 @@ void Engine::run_steps(long long n) {
       if (itg == graphs_.end()) {
         cudaGraph_t graph;
         cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+        capturing_ = true;
+        capture_count_ = 0;
         for (int k = 0; k < steps; k++) launch_step(k);
         launch_clock_advance(d_clk_, steps, stream_);
+        count_launch(1);
+        capturing_ = false;
+        graph_nodes_[steps] = capture_count_;
         cuda_check(cudaStreamEndCapture(stream_, &graph), "capture");
         cudaGraphExec_t exec;
         cuda_check(cudaGraphInstantiate(&exec, graph, 0), "instantiate");
@@ -631,6 +670,7 @@ void Engine::run_steps(long long n) {
         itg = graphs_.emplace(steps, exec).first;
       }
       cuda_check(cudaGraphLaunch(itg->second, stream_), "graph launch");
+      n_launch_ += graph_nodes_[steps];
     };
     for (long long i = 0; i < full; i++) run(K);
     if (rem) run((int)rem);
@@ -742,7 +782,7 @@ void Engine::start_simulation() {
 
 void Engine::end_simulation() {
   if (!in_sim_) return;
-  launch_flush();
+  launch_flush();   // folding twice is harmless: the first fold clears `pending`
   cuda_check(cudaStreamSynchronize(stream_), "end of simulation");
   check_status();
   drain_rec_spike_times();
@@ -766,14 +806,68 @@ void Engine::simulation_step() {
 void Engine::simulate(float t) {
   sim_time = t;
   start_simulation();
+  if (!ev_a_) {
+    cuda_check(cudaEventCreate(&ev_a_), "event");
+    cuda_check(cudaEventCreate(&ev_b_), "event");
+  }
   auto t0 = std::chrono::steady_clock::now();
+  cuda_check(cudaEventRecord(ev_a_, stream_), "event");
   run_steps(Nt_);
   it_ += Nt_;
+  launch_flush();
+  cuda_check(cudaEventRecord(ev_b_, stream_), "event");
   end_simulation();
+  float ms = 0.0f;
+  cuda_check(cudaEventElapsedTime(&ms, ev_a_, ev_b_), "event");
+  last_sim_device_ms_ = ms;
   auto t1 = std::chrono::steady_clock::now();
   last_sim_seconds_ = std::chrono::duration<double>(t1 - t0).count();
   total_steps_ += Nt_;
   if (verbosity >= 1) printf("Simulation time: %g\n", last_sim_seconds_);
+}
+
+std::vector<double> Engine::profile_steps(int n) {
+  if (in_sim_) throw NgpuError("profile_steps cannot run inside a simulation");
+  sim_time = (float)n * dt;
+  start_simulation();
+  if (rec_ncol_ && n > rec_rows_cap_) {
+    d_recbuf_ = dalloc<float>((size_t)n * (rec_ncol_ + 1));
+    rec_rows_cap_ = n;
+    invalidate_graphs();
+  }
+  std::vector<cudaEvent_t> ev(4);
+  for (auto &e : ev) cuda_check(cudaEventCreate(&e), "event");
+  std::vector<double> acc(3, 0.0);
+  SpikeOut so = spike_out();
+  for (int s = 0; s < n; s++) {
+    cuda_check(cudaEventRecord(ev[0], stream_), "event");
+    for (auto &g : groups_) {
+      if (is_aeif(g.model)) launch_aeif(g.model, false, aeif_args(g), so, d_clk_, 0, stream_);
+      else if (g.model == M_IAF_PSC_EXP) launch_iaf(false, iaf_args(g), so, d_clk_, 0, dt, stream_);
+      else if (g.model == M_SPIKE_GEN) launch_spike_gen(sg_args(g), so, d_clk_, 0, dt, stream_);
+    }
+    cuda_check(cudaEventRecord(ev[1], stream_), "event");
+    if (rec_ncol_)
+      launch_record(d_cols_, rec_ncol_, d_recbuf_, d_last_tidx_, d_last_h_, d_has_out_, d_clk_, 0, dt,
+                    stream_);
+    cuda_check(cudaEventRecord(ev[2], stream_), "event");
+    launch_deliver(deliver_args(), deliver_blocks_, d_clk_, 0, dt, stream_);
+    cuda_check(cudaEventRecord(ev[3], stream_), "event");
+    launch_clock_advance(d_clk_, 1, stream_);
+    cuda_check(cudaEventSynchronize(ev[3]), "event");
+    for (int j = 0; j < 3; j++) {
+      float ms = 0.0f;
+      cuda_check(cudaEventElapsedTime(&ms, ev[j], ev[j + 1]), "event");
+      acc[j] += ms;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  if (rec_ncol_) drain_records(n);
+  it_ += n;
+  end_simulation();
+  total_steps_ += n;
+  for (auto &a : acc) a /= std::max(1, n);
+  return acc;
 }
 
 EngineStats Engine::stats() {
@@ -788,6 +882,7 @@ EngineStats Engine::stats() {
     cuda_check(cudaMemcpy(&s.status, d_status_, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
   }
   s.sim_seconds = last_sim_seconds_;
+  s.sim_device_ms = last_sim_device_ms_;
   s.steps = total_steps_;
   return s;
 }

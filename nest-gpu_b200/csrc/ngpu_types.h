@@ -156,6 +156,19 @@ struct DeliverArgs {
   unsigned long long *n_events;
 };
 
+// Generated connection block: fixed in-degree with per-target random sources
+// and uniform delays, drawn on the device (see ngpu_build.cu).
+struct GenBlockDev {
+  int src0, nsrc, ntgt, k;
+  int tgt_i0_rel;          // first target relative to its group
+  int group_n;             // targets' group size
+  unsigned long long acc_base;   // accumulator offset of the targets' group + port row
+  float w;
+  int dlo, dhi;            // delay indices, inclusive
+  uint64_t seed;
+  int block_id;
+};
+
 // Record column: float variable pointer, or "spike" activity of a node.
 struct RecCol {
   const float *ptr;      // null for spike activity

@@ -160,6 +160,12 @@ if is_b200_engine:
     _c["NGPU_ConnectArrays"] = _bind("NGPU_ConnectArrays", _I, [ctypes.c_size_t, c_void_p, c_void_p,
                                                                  c_void_p, c_void_p, c_void_p])
     _c["NGPU_SetGraphSteps"] = _bind("NGPU_SetGraphSteps", _I, [_I])
+    _c["NGPU_SetHostRng"] = _bind("NGPU_SetHostRng", _I, [_I])
+    _c["NGPU_GetSimDeviceMs"] = _bind("NGPU_GetSimDeviceMs", ctypes.c_double, [])
+    _c["NGPU_GetLaunchCount"] = _bind("NGPU_GetLaunchCount", ctypes.c_longlong, [])
+    _c["NGPU_ProfileSteps"] = _bind("NGPU_ProfileSteps", _I, [_I, ctypes.POINTER(ctypes.c_double)])
+    _c["NGPU_ConnectFixedIndegreeGPU"] = _bind("NGPU_ConnectFixedIndegreeGPU", _I,
+                                               [_I, _I, _I, _I, _I, _I, _F, _F, _F, ctypes.c_ulonglong])
 
 
 def _b(s):
@@ -1233,6 +1239,39 @@ def ConnectArrays(source, target, weight, delay, port=None):
     return _check(_c["NGPU_ConnectArrays"](n, s.ctypes.data, t.ctypes.data,
                                            p.ctypes.data if p is not None else None,
                                            w.ctypes.data, d.ctypes.data))
+
+
+def GetSimDeviceMs():
+    """Device time [ms] of the last Simulate call, from CUDA events on the engine stream."""
+    return _check(_c["NGPU_GetSimDeviceMs"]())
+
+
+def GetLaunchCount():
+    """Engine kernels launched so far (graph replays count every kernel node)."""
+    return _check(_c["NGPU_GetLaunchCount"]())
+
+
+def ProfileSteps(n):
+    """Run n simulation steps with per-kernel CUDA events; average ms per step of
+    (neuron updates, record gather, spike delivery)."""
+    out = (ctypes.c_double * 3)()
+    _c["NGPU_ProfileSteps"](n, out)
+    _check()
+    return list(out)
+
+
+def ConnectFixedIndegreeGPU(source, target, indegree, weight, delay_min, delay_max, receptor=0,
+                            seed=1):
+    """Per-target fixed in-degree block generated on the GPU (engine extension)."""
+    return _check(_c["NGPU_ConnectFixedIndegreeGPU"](source.i0, source.n, target.i0, target.n, indegree,
+                                                     receptor, weight, delay_min, delay_max, seed))
+
+
+def SetHostRng(on=True):
+    """Use cuRAND's host generator for connection random numbers (engine extension)."""
+    if not is_b200_engine:
+        raise ValueError("SetHostRng needs libnestgpu_b200.so")
+    return _check(_c["NGPU_SetHostRng"](1 if on else 0))
 
 
 def SetGraphSteps(n):

@@ -35,6 +35,7 @@
 // (CURAND_RNG_PSEUDO_DEFAULT), the library the reference itself calls.
 
 #include <curand.h>
+#include <omp.h>
 
 #include <algorithm>
 #include <cmath>
@@ -265,7 +266,7 @@ struct Net {
   long long it = 0, Nt = 0;
   std::vector<std::vector<Queued>> queue;         // per source, most recent first
   // direct (poiss_gen) edges in canonical order
-  struct Direct { int gen; int tgt; unsigned char port; float w; float delay; };
+  struct Direct { int gen; int tgt; unsigned char port; float w; float delay; int group; };
   std::vector<Direct> direct;
   std::vector<Rec> recs;
   std::vector<std::vector<float>> rec_rows;
@@ -590,7 +591,7 @@ struct Net {
       for (int s = g.i0; s < g.i0 + g.n; s++)
         for (auto &dg : conn[s])
           for (auto &e : dg.tg)
-            direct.push_back({s - g.i0 + (int)0, e.tgt, e.port, e.w, dt * (float)(dg.delay + 1)});
+            direct.push_back({s - g.i0, e.tgt, e.port, e.w, dt * (float)(dg.delay + 1), (int)gi});
     }
     for (auto &g : groups) {
       if (is_aeif(g.model)) {
@@ -849,6 +850,7 @@ struct Net {
   void push_spike(int node, float height, long long tidx) {
     Group &g = group_of(node);
     int i = node - g.i0;
+#pragma omp atomic
     n_spikes_total++;
     if (g.spike_count_on) g.spike_count[i]++;
     if (g.max_rec > 0) {
@@ -869,6 +871,8 @@ struct Net {
     int NV = 2 + s.n_port_var * P;
     R hmin = (R)(g.h_min_rel * dt);
     if (fp64) hmin = (R)((double)g.h_min_rel * (double)dt);
+    long long nd_total = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : nd_total)
     for (int i = 0; i < g.n; i++) {
       Par<R> q;
       auto gp = [&](int j) { return (R)g.par[j][i]; };
@@ -895,7 +899,7 @@ struct Net {
       int guard = 0;
       while (!end) {
         R hmax = (R)(x1 - x);
-        n_derivs += rk5_step<R>(g.model, P, NV, x, y, h, hmin, hmax, q, refr);
+        nd_total += rk5_step<R>(g.model, P, NV, x, y, h, hmin, hmax, q, refr);
         end = (x >= x1 - (double)hmin);
         if (++guard > 1000000) break;
         // ExternalUpdate (src/aeif_cond_beta_multisynapse_kernel.h:190-226)
@@ -919,9 +923,11 @@ struct Net {
       g.x[i] = x;
       g.h[i] = (double)h;
     }
+    n_derivs += nd_total;
   }
 
   template <class R> void update_iaf(Group &g, long long tidx) {
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < g.n; i++) {
       R Iex = (R)g.var[I_I_syn_ex][i], Iin = (R)g.var[I_I_syn_in][i];
       R V = (R)g.var[I_V_m_rel][i], refr = (R)g.var[I_refractory_step][i];
@@ -983,15 +989,20 @@ struct Net {
     // 1. spike buffer update (src/spike_buffer.cu:247-317)
     struct Ev { int src; int grp; float height; };
     std::vector<Ev> events;
+    const int nthr = omp_get_max_threads();
+    std::vector<std::vector<Ev>> tev(nthr);
+#pragma omp parallel for schedule(dynamic, 1024)
     for (size_t s = 0; s < queue.size(); s++) {
       std::vector<Queued> &q = queue[s];
+      if (q.empty()) continue;
+      std::vector<Ev> &ev = tev[omp_get_thread_num()];
       int ng = (int)conn[s].size();
       int Ns = (int)q.size();
       bool drop_oldest = false;
       for (int is = 0; is < Ns; is++) {
         Queued &e = q[is];
         if (e.cursor < ng && e.age == conn[s][e.cursor].delay) {
-          events.push_back({(int)s, e.cursor, e.height});
+          ev.push_back({(int)s, e.cursor, e.height});
           e.cursor++;
         }
         if (is == Ns - 1 && e.cursor >= ng) drop_oldest = true;
@@ -999,6 +1010,7 @@ struct Net {
       }
       if (drop_oldest) q.pop_back();
     }
+    for (auto &v : tev) events.insert(events.end(), v.begin(), v.end());
     // 2. time
     neural_time = neur_t0 + (double)dt * (double)(it + 1);
     long long tidx = (long long)(int)std::round(neur_t0 / (double)dt) + it + 1;
@@ -1022,39 +1034,39 @@ struct Net {
     }
     // 4. records
     write_records((float)neural_time);
-    // 5. collect spikes (src/get_spike.cu:60-108)
-    for (auto &ev : events) {
+    // 5. collect spikes (src/get_spike.cu:60-108); FP64 sums, order-independent for
+    //    weights whose partial sums are exact
+    long long nev = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : nev)
+    for (size_t k = 0; k < events.size(); k++) {
+      const Ev &ev = events[k];
       for (auto &e : conn[ev.src][ev.grp].tg) {
         Group &tg = groups[node_group[e.tgt]];
-        tg.acc[(size_t)e.port * tg.n + (e.tgt - tg.i0)] += (double)(ev.height * e.w);
-        n_events++;
+        double &a = tg.acc[(size_t)e.port * tg.n + (e.tgt - tg.i0)];
+        double v = (double)(ev.height * e.w);
+#pragma omp atomic
+        a += v;
+        nev++;
       }
     }
+    n_events += nev;
     // 6. poiss_gen direct spikes (src/poiss_gen.cu:55-86)
     float time_step = (float)(dt / 1000.0);
-    if (!direct.empty()) {
-      // generators are located by the canonical edge order: source-major over poiss_gen groups
-      size_t ie = 0;
-      for (auto &g : groups) {
-        if (g.model != POISS_GEN) continue;
-        for (int s = g.i0; s < g.i0 + g.n; s++) {
-          int gi = s - g.i0;
-          float rate = (float)g.par[PG_rate][gi], origin = (float)g.par[PG_origin][gi];
-          float start_ = (float)g.par[PG_start][gi], stop_ = (float)g.par[PG_stop][gi];
-          float lam = time_step * rate;
-          for (auto &dg : conn[s])
-            for (auto &e : dg.tg) {
-              const Direct &d = direct[ie];
-              double t_rel = neural_time - (double)origin - (double)d.delay;
-              if (t_rel >= (double)start_ && t_rel <= (double)stop_) {
-                int n = poisson_draw(lam, kernel_seed, (uint64_t)ie, tidx);
-                if (n > 0) {
-                  Group &tg = groups[node_group[e.tgt]];
-                  tg.acc[(size_t)e.port * tg.n + (e.tgt - tg.i0)] += (double)(e.w * (float)n);
-                }
-              }
-              ie++;
-            }
+#pragma omp parallel for schedule(static)
+    for (size_t ie = 0; ie < direct.size(); ie++) {
+      const Direct &d = direct[ie];
+      const Group &g = groups[d.group];
+      float rate = (float)g.par[PG_rate][d.gen], origin = (float)g.par[PG_origin][d.gen];
+      float start_ = (float)g.par[PG_start][d.gen], stop_ = (float)g.par[PG_stop][d.gen];
+      double t_rel = neural_time - (double)origin - (double)d.delay;
+      if (t_rel >= (double)start_ && t_rel <= (double)stop_) {
+        int n = poisson_draw(time_step * rate, kernel_seed, (uint64_t)ie, tidx);
+        if (n > 0) {
+          Group &tg = groups[node_group[d.tgt]];
+          double &a = tg.acc[(size_t)d.port * tg.n + (d.tgt - tg.i0)];
+          double v = (double)(d.w * (float)n);
+#pragma omp atomic
+          a += v;
         }
       }
     }
@@ -1063,6 +1075,7 @@ struct Net {
       if (g.nport == 0) continue;
       ModelShape s = shape_of(g.model);
       for (int p = 0; p < g.nport; p++)
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < g.n; i++) {
           double a = g.acc[(size_t)p * g.n + i];
           if (a == 0.0) continue;
@@ -1203,6 +1216,16 @@ int orc_connect(void *p, int rule, const int *src, int src0, int ns, const int *
 int orc_connect1(void *p, int src, int tgt, int port, float w, float d) {
   OR_TRY((Net *)p)->connect1(src, tgt, port, w, d); return 0; OR_CATCH(-1)
 }
+
+int orc_connect_arrays(void *p, size_t n, const int *src, const int *tgt, const int *port,
+                       const float *w, const float *d) {
+  OR_TRY
+  Net *net = (Net *)p;
+  for (size_t i = 0; i < n; i++) net->connect1(src[i], tgt[i], port[i], w[i], d[i]);
+  return 0;
+  OR_CATCH(-1)
+}
+int orc_threads() { return omp_get_max_threads(); }
 
 long long orc_n_conn(void *p) {
   Net *n = (Net *)p;

@@ -64,6 +64,8 @@ def lib():
                                     c_float, c_float, fp, fp]),
             "orc_connect1": (c_int, [c_void, c_int, c_int, c_int, c_float, c_float]),
             "orc_n_conn": (ctypes.c_longlong, [c_void]),
+            "orc_connect_arrays": (c_int, [c_void, ctypes.c_size_t, ip, ip, ip, fp, fp]),
+            "orc_threads": (c_int, []),
             "orc_get_conns": (c_int, [c_void, ip, ip, ip, ip, ip, fp, fp]),
             "orc_record": (c_int, [c_void, c_int, ctypes.c_char_p, c_int]),
             "orc_record_rows": (c_int, [c_void]),
@@ -358,6 +360,18 @@ class Oracle(object):
             self.h, ir, _iptr(sarr) if src_list else None, 0 if src_list else source.i0, ns,
             _iptr(tarr) if tgt_list else None, 0 if tgt_list else target.i0, nt, degree, port, w, d,
             _fptr(warr) if warr is not None else None, _fptr(darr) if darr is not None else None))
+
+    def ConnectArrays(self, source, target, port, weight, delay):
+        """Bulk single connections (inserted in array order)."""
+        s = np.ascontiguousarray(source, dtype=np.int32)
+        t = np.ascontiguousarray(target, dtype=np.int32)
+        p = np.ascontiguousarray(port, dtype=np.int32)
+        w = np.ascontiguousarray(weight, dtype=np.float32)
+        d = np.ascontiguousarray(delay, dtype=np.float32)
+        self._chk(self.L.orc_connect_arrays(self.h, s.size, _iptr(s), _iptr(t), _iptr(p), _fptr(w), _fptr(d)))
+
+    def Threads(self):
+        return self.L.orc_threads()
 
     def ConnectionArrays(self):
         """All connections in reference order as a dict of numpy arrays."""

@@ -1,0 +1,196 @@
+"""Parity of the CUDA engine (through the C ABI) with the CPU oracle.
+
+The engine and the oracle's FP32 mode perform the same arithmetic in the same
+order (explicit fused multiply-adds, the same own exp/log, the same Philox
+Poisson stream), so traces, spike counts and spike times are compared bit for
+bit.  The single-neuron traces are also held to the reference tests' NEST
+golden tolerances, and the FP32 traces to 1e-5 relative of the FP64 oracle.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import nestgpu as ngpu
+import oracle as orc
+from scenarios import (fixed_train_network, golden_traces, poisson_network, trace_rmse,
+                       trace_scenario)
+
+pytestmark = pytest.mark.gpu
+
+MODELS = ["aeif_cond_beta_multisynapse", "aeif_cond_alpha_multisynapse",
+          "aeif_psc_exp_multisynapse", "aeif_psc_alpha_multisynapse", "iaf_psc_exp"]
+
+
+@pytest.fixture(autouse=True)
+def fresh_engine():
+    ngpu.Reset()
+    ngpu.SetVerbosityLevel(0)
+    yield
+    ngpu.Reset()
+
+
+@pytest.mark.parametrize("model", MODELS)
+def test_single_neuron_trace(model):
+    g = golden_traces()
+    t, v = trace_scenario(ngpu, model)
+    _, v32 = trace_scenario(orc.Oracle(fp64=False), model)
+    _, v64 = trace_scenario(orc.Oracle(fp64=True), model)
+    assert np.array_equal(np.float32(v), np.float32(v32))
+    assert trace_rmse(v, g[model]) < float(g[model + "__tolerance"])
+    assert np.max(np.abs(v - v64) / np.maximum(np.abs(v64), 1.0)) < 1e-5
+    assert len(t) == 8001 and abs(t[-1] - 800.0) < 1e-3
+
+
+@pytest.mark.parametrize("model", ["aeif_cond_beta_multisynapse", "aeif_psc_alpha_multisynapse",
+                                   "iaf_psc_exp"])
+def test_recurrent_network_fixed_trains_bitexact(model):
+    ngpu.SetHostRng(True)
+    c_gpu, d_gpu = fixed_train_network(ngpu, model=model)
+    c_orc, d_orc = fixed_train_network(orc.Oracle(), model=model)
+    assert c_gpu.sum() > 0
+    assert np.array_equal(c_gpu, c_orc)
+    assert np.array_equal(np.float32(d_gpu), np.float32(d_orc))
+    st = ngpu.GetStats()
+    assert st["status"] == 0
+    assert st["n_spikes"] >= c_gpu.sum()
+
+
+@pytest.mark.parametrize("model", ["aeif_cond_beta_multisynapse", "iaf_psc_exp"])
+def test_poisson_driven_network_bitexact(model):
+    c_gpu = poisson_network(ngpu, model=model)
+    c_orc = poisson_network(orc.Oracle(), model=model)
+    assert c_gpu.sum() > 100
+    assert np.array_equal(c_gpu, c_orc)
+
+
+def _continuation(api, chunks):
+    api.SetKernelStatus("rnd_seed", 5)
+    pg = api.Create("poisson_generator")
+    api.SetStatus(pg, "rate", 9000.0)
+    n = api.Create("aeif_cond_beta_multisynapse", 50, 2)
+    api.SetStatus(n, {"E_rev": [0.0, -85.0], "t_ref": 1.0})
+    api.Connect(pg, n, {"rule": "all_to_all"}, {"weight": 0.5, "delay": 0.5})
+    api.Connect(n, n, {"rule": "fixed_total_number", "total_num": 400}, {"weight": 0.3, "delay": 1.1})
+    api.ActivateSpikeCount(n)
+    for c in chunks:
+        api.Simulate(c)
+    return (np.asarray(api.GetStatus(n, "spike_count")).ravel(), np.float32(api.GetStatus(n, "V_m")),
+            np.float32(api.GetStatus(n, "g1")))
+
+
+def test_simulate_in_chunks_equals_one_call():
+    a = _continuation(ngpu, [60.0])
+    ngpu.Reset()
+    ngpu.SetVerbosityLevel(0)
+    b = _continuation(ngpu, [20.0, 25.0, 15.0])
+    o = _continuation(orc.Oracle(), [20.0, 25.0, 15.0])
+    for x, y, z in zip(a, b, o):
+        assert np.array_equal(x, y)
+        assert np.array_equal(y, z)
+
+
+def test_simulation_step_api_matches_simulate():
+    ngpu.SetKernelStatus("rnd_seed", 11)
+    sg = ngpu.Create("spike_generator")
+    ngpu.SetStatus(sg, {"spike_times": [0.3, 0.7, 1.2, 2.0]})
+    n = ngpu.Create("iaf_psc_exp", 3)
+    ngpu.Connect(sg, n, {"rule": "all_to_all"}, {"weight": 400.0, "delay": 0.2})
+    ngpu.SetSimTime(3.0)
+    ngpu.StartSimulation()
+    v = []
+    for _ in range(30):
+        ngpu.SimulationStep()
+        v.append(ngpu.GetStatus(n[0], "I_syn_ex"))
+    ngpu.EndSimulation()
+    o = orc.Oracle()
+    sg2 = o.Create("spike_generator")
+    o.SetStatus(sg2, {"spike_times": [0.3, 0.7, 1.2, 2.0]})
+    n2 = o.Create("iaf_psc_exp", 3)
+    o.Connect(sg2, n2, {"rule": "all_to_all"}, {"weight": 400.0, "delay": 0.2})
+    o.CreateRecord("", ["I_syn_ex"], [n2[0]], [0])
+    o.Simulate(3.0)
+    # after a step the engine has folded that step's input, the record row has not
+    assert np.float32(v[-1]) == np.float32(o.GetStatus(n2[0], "I_syn_ex")[0])
+    assert max(v) > 0.0
+
+
+def test_status_after_simulate_matches_oracle():
+    def run(api):
+        api.SetKernelStatus("rnd_seed", 21)
+        pg = api.Create("poisson_generator")
+        api.SetStatus(pg, "rate", 15000.0)
+        n = api.Create("aeif_cond_beta_multisynapse", 30, 2)
+        api.Connect(pg, n, {"rule": "all_to_all"}, {"weight": 0.4, "delay": 0.3, "receptor": 1})
+        api.Simulate(37.0)
+        return [np.float32(api.GetStatus(n, k)) for k in ("V_m", "w", "g", "g1", "refractory_step")]
+    for a, b in zip(run(ngpu), run(orc.Oracle())):
+        assert np.array_equal(a, b)
+
+
+def test_rec_spike_times_and_spike_record():
+    def run(api):
+        api.SetKernelStatus("rnd_seed", 3)
+        pg = api.Create("poisson_generator")
+        api.SetStatus(pg, "rate", 500.0)
+        n = api.Create("aeif_cond_beta_multisynapse", 30)
+        api.ActivateSpikeCount(n)
+        api.ActivateRecSpikeTimes(n, 500)
+        api.Connect(pg, n, {"rule": "all_to_all"}, {"weight": 4.0, "delay": 0.2})
+        api.Connect(n, n[0:1], {"rule": "all_to_all"}, {"weight": 0.01, "delay": 0.2})
+        rec = api.CreateRecord("", ["spike"] * 3, [n[0], n[1], n[2]], [0, 0, 0])
+        api.Simulate(490.0)
+        api.SetStatus(pg, "rate", 0.0)
+        api.Simulate(10.0)
+        return (np.asarray(api.GetStatus(n, "spike_count")).ravel(), api.GetRecSpikeTimes(n),
+                np.asarray(api.GetRecordData(rec)))
+    cg, tg, rg = run(ngpu)
+    co, to, ro = run(orc.Oracle())
+    assert cg.sum() > 30
+    assert np.array_equal(cg, co)
+    assert [len(x) for x in tg] == list(cg)
+    for a, b in zip(tg, to):
+        assert np.array_equal(np.float32(a), np.float32(b))
+    assert np.array_equal(np.float32(rg), np.float32(ro))
+    # "spike" records a spike only for nodes with recurrent out-connections (node 0 here)
+    assert rg[:, 1].sum() == cg[0] and rg[:, 2].sum() == 0
+
+
+def test_brunel_rate_statistics():
+    """python/test/test_brunel_list.py: mean rate of 1000 aeif neurons within
+    3 sqrt(rate) of 30.78 spikes/s."""
+    order, n_rec = 200, 100
+    ngpu.SetKernelStatus("rnd_seed", 1234)
+    NE, NI = 4 * order, order
+    pg = ngpu.Create("poisson_generator")
+    ngpu.SetStatus(pg, "rate", 20000.0)
+    neuron = ngpu.Create("aeif_cond_beta_multisynapse", NE + NI, 2)
+    exc, inh = neuron[0:NE], neuron[NE:NE + NI]
+    ngpu.SetStatus(neuron, {"E_rev": [0.0, -85.0], "tau_decay": [1.0, 1.0], "tau_rise": [1.0, 1.0]})
+    dly = {"distribution": "normal_clipped", "mu": 0.5, "low": 0.1, "high": 0.5 + 3 * 0.25, "sigma": 0.25}
+    ngpu.Connect(exc, neuron.ToList(), {"rule": "fixed_indegree", "indegree": 800},
+                 {"weight": 0.05, "delay": dly, "receptor": 0})
+    ngpu.Connect(inh.ToList(), exc.ToList(), {"rule": "fixed_indegree", "indegree": 200},
+                 {"weight": 0.35, "delay": dly, "receptor": 1})
+    ngpu.Connect(inh.ToList(), inh, {"rule": "fixed_indegree", "indegree": 200},
+                 {"weight": 0.35, "delay": dly, "receptor": 1})
+    ngpu.Connect(pg.ToList(), neuron.ToList(), {"rule": "all_to_all"},
+                 {"weight": 0.37, "delay": 0.2, "receptor": 0})
+    ngpu.ActivateSpikeCount(neuron)
+    ngpu.Simulate(1000.0)
+    counts = np.asarray(ngpu.GetStatus(neuron, "spike_count")).ravel()
+    expected = 30.78
+    rng = np.random.RandomState(0)
+    sample = counts[rng.choice(NE + NI, n_rec, replace=False)]
+    assert sample.min() >= expected - 3.0 * math.sqrt(expected)
+    assert sample.max() <= expected + 3.0 * math.sqrt(expected)
+    assert abs(sample.mean() - expected) < 3.0 * math.sqrt(expected) / math.sqrt(n_rec)
+    assert len(ngpu.GetConnections(neuron[1], neuron)) == NE + NI
+
+
+def test_device_rng_matches_reference_generator_for_ints():
+    ngpu.SetRandomSeed(1234)
+    a = np.array(ngpu.RandomInt(4096), dtype=np.uint32)
+    o = orc.Oracle()
+    o.SetRandomSeed(1234)
+    assert np.array_equal(a, o.RandomInt(4096))
