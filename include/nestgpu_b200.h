@@ -251,6 +251,14 @@ int NGPU_ConnectFixedIndegreeGPU(int i_source, int n_source, int i_target, int n
                                  int port, float weight, float delay_min, float delay_max,
                                  unsigned long long seed);
 
+/* Thread blocks of the spike-delivery kernel (0 = chosen from the number of nodes with
+   outgoing connections, at most 8 per SM).  Results do not depend on it. */
+int NGPU_SetDeliverBlocks(int n);
+
+/* RK5 steps a neuron may take in the main update kernel per time step before it is handed
+   to the straggler kernel (default 4; 0 = no hand-off).  Results do not depend on it. */
+int NGPU_SetRk5Budget(int n);
+
 /* Steps captured per CUDA graph (default 100). */
 int NGPU_SetGraphSteps(int n);
 

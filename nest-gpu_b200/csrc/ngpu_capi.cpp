@@ -673,6 +673,22 @@ int NGPU_ConnectFixedIndegreeGPU(int i_source, int n_source, int i_target, int n
   }, 0);
 }
 
+int NGPU_SetDeliverBlocks(int n) {
+  return guard([&] {
+    if (n < 0) throw NgpuError("block count must be >= 0");
+    E().deliver_blocks_req = n;
+    return 0;
+  }, 0);
+}
+
+int NGPU_SetRk5Budget(int n) {
+  return guard([&] {
+    if (n < 0) throw NgpuError("RK5 budget must be >= 0");
+    E().rk5_budget = n;
+    return 0;
+  }, 0);
+}
+
 int NGPU_SetGraphSteps(int n) {
   return guard([&] {
     if (n < 1) throw NgpuError("graph steps must be >= 1");

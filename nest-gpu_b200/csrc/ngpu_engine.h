@@ -55,6 +55,8 @@ struct Group {
   int *d_spike_count = nullptr;
   int *d_n_rec = nullptr;
   float *d_rec_times = nullptr;
+  int *d_strag = nullptr;        // aeif: straggler list [n] and counters [2]
+  int *d_strag_cnt = nullptr;
   int *d_pin_off = nullptr;
   PoissonIn *d_pin = nullptr;
   int *d_sg_off = nullptr, *d_sg_tidx = nullptr, *d_sg_next = nullptr;
@@ -99,6 +101,8 @@ class Engine {
   int remote_spike_height = 0;
   float sim_time = 1000.0f;
   int graph_steps = 100;          // steps per captured CUDA graph
+  int rk5_budget = 4;             // RK5 steps per neuron before the straggler kernel takes over
+  int deliver_blocks_req = 0;     // delivery grid size (0: from the number of spiking sources)
   bool use_device_rng = true;     // cuRAND device generator (as the reference) if a GPU exists
 
   void set_seed(unsigned long long s);
@@ -272,8 +276,8 @@ Engine &engine();
 void engine_reset();
 
 // launchers (ngpu_kernels.cu)
-void launch_aeif(int model, bool flush, const AeifArgs &A, const SpikeOut &so, Clock *clk, int k,
-                 cudaStream_t st);
+int launch_aeif(int model, bool flush, const AeifArgs &A, const SpikeOut &so, Clock *clk, int k,
+                cudaStream_t st);
 void launch_iaf(bool flush, const IafArgs &A, const SpikeOut &so, Clock *clk, int k, float dt,
                 cudaStream_t st);
 void launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, Clock *clk, int k, float dt,

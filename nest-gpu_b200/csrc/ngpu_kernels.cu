@@ -13,6 +13,8 @@
 // update, neuron update, record, CollectSpike, poiss_gen, GetSpikes fold.
 #include <cub/block/block_scan.cuh>
 
+#include <algorithm>
+
 #include "ngpu_math.cuh"
 #include "ngpu_types.h"
 
@@ -252,11 +254,63 @@ __device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmi
   return nd;
 }
 
+// RK5 steps of neuron i from x towards tnow (src/rk5.h:161-174), each followed by the
+// model's ExternalUpdate.  Stops after `budget` steps (0: no limit); returns true when
+// the neuron reached the end of the time step.
+template <int MODEL, int P>
+__device__ __forceinline__ bool aeif_integrate(const AeifArgs &A, const SpikeOut &so, int i,
+                                               const AeifQ<MODEL, P> &q, float *y, float &refr,
+                                               double &x, float &h, long long tidx, double tnow,
+                                               int budget, unsigned long long &nd_acc) {
+  const double x1 = tnow;
+  bool end = false;
+  int guard = 0, steps = 0;
+  unsigned long long nd = 0;
+  while (!end) {
+    if (budget > 0 && steps == budget) {
+      nd_acc += nd;
+      return false;
+    }
+    float hmax = (float)(x1 - x);
+    nd += rk5_step<MODEL, P>(x, y, h, A.hmin, A.hmin_acc, hmax, q, refr, so.status);
+    steps++;
+    end = (x >= x1 - (double)A.hmin);
+    if (++guard > ck::max_substeps) {
+      atomicOr(so.status, ST_RK5_TRIALS);
+      break;
+    }
+    // ExternalUpdate (src/aeif_cond_beta_multisynapse_kernel.h:190-226)
+    if (y[0] < -1.0e3f) {
+      y[0] = q.V_reset;
+      y[1] = 0.0f;
+      atomicOr(so.status, ST_NUMERIC);
+      continue;
+    }
+    if (y[1] < -1.0e6f || y[1] > 1.0e6f) {
+      y[0] = q.V_reset;
+      y[1] = 0.0f;
+      atomicOr(so.status, ST_NUMERIC);
+      continue;
+    }
+    if (refr > 0.0f) {
+      y[0] = q.V_reset;
+      if (end) refr = __fsub_rn(refr, 1.0f);
+    } else if (y[0] >= q.V_peak) {
+      push_spike(so, A.rec, A.i0 + i, i, 1.0f, tidx, tnow);
+      y[0] = q.V_reset;
+      y[1] = __fadd_rn(y[1], q.b);
+      refr = q.refr_steps;
+    }
+  }
+  nd_acc += nd;
+  return true;
+}
+
 // One neuron, one step.  FLUSH: only fold the pending inputs.
 template <int MODEL, int P, bool FLUSH>
 __device__ __forceinline__ void aeif_neuron(const AeifArgs &A, const SpikeOut &so, int i,
                                             long long tidx, double tnow, long long tidx_prev,
-                                            double t_prev, bool pending,
+                                            double t_prev, bool pending, int *strag_cnt,
                                             unsigned long long &nd_acc) {
   typedef AeifShape<MODEL> S;
   constexpr int NV = 2 + S::npv * P;
@@ -291,47 +345,17 @@ __device__ __forceinline__ void aeif_neuron(const AeifArgs &A, const SpikeOut &s
   float refr = A.refr[i];
   double x = A.x[i];
   float h = A.h[i];
-  const double x1 = tnow;
-  bool end = false;
-  int guard = 0;
-  unsigned long long nd = 0;
-  while (!end) {
-    float hmax = (float)(x1 - x);
-    nd += rk5_step<MODEL, P>(x, y, h, A.hmin, A.hmin_acc, hmax, q, refr, so.status);
-    end = (x >= x1 - (double)A.hmin);
-    if (++guard > ck::max_substeps) {
-      atomicOr(so.status, ST_RK5_TRIALS);
-      break;
-    }
-    // ExternalUpdate (src/aeif_cond_beta_multisynapse_kernel.h:190-226)
-    if (y[0] < -1.0e3f) {
-      y[0] = q.V_reset;
-      y[1] = 0.0f;
-      atomicOr(so.status, ST_NUMERIC);
-      continue;
-    }
-    if (y[1] < -1.0e6f || y[1] > 1.0e6f) {
-      y[0] = q.V_reset;
-      y[1] = 0.0f;
-      atomicOr(so.status, ST_NUMERIC);
-      continue;
-    }
-    if (refr > 0.0f) {
-      y[0] = q.V_reset;
-      if (end) refr = __fsub_rn(refr, 1.0f);
-    } else if (y[0] >= q.V_peak) {
-      push_spike(so, A.rec, A.i0 + i, i, 1.0f, tidx, tnow);
-      y[0] = q.V_reset;
-      y[1] = __fadd_rn(y[1], q.b);
-      refr = q.refr_steps;
-    }
-  }
-  nd_acc += nd;
+  const bool done = aeif_integrate<MODEL, P>(A, so, i, q, y, refr, x, h, tidx, tnow, A.budget, nd_acc);
 #pragma unroll
   for (int v = 0; v < NV; v++) A.var[(size_t)v * n + i] = y[v];
   A.refr[i] = refr;
   A.x[i] = x;
   A.h[i] = h;
+  if (!done) {
+    // more RK5 steps needed than the budget allows: the straggler kernel finishes it
+    int pos = atomicAdd(strag_cnt, 1);
+    A.strag_list[pos] = i;
+  }
 }
 
 // Step timing of an update/flush launch.  Update: step `it` integrates to tnow and
@@ -367,12 +391,48 @@ __global__ void __launch_bounds__(128) aeif_update_kernel(const AeifArgs A, cons
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long nd = 0;
   if (i < A.n)
-    aeif_neuron<MODEL, P, FLUSH>(A, so, i, t.tidx, t.tnow, t.tidx_prev, t.t_prev, pending, nd);
+    aeif_neuron<MODEL, P, FLUSH>(A, so, i, t.tidx, t.tnow, t.tidx_prev, t.t_prev, pending,
+                                 A.strag_cnt + (t.it & 1), nd);
   if (!FLUSH) {
     // one counter update per warp
     for (int o = 16; o > 0; o >>= 1) nd += __shfl_down_sync(0xffffffffu, nd, o);
     if ((threadIdx.x & 31) == 0 && nd) atomicAdd(A.nderiv, nd);
   }
+}
+
+// Neurons that needed more RK5 steps than the main kernel's budget (typically the
+// few that spike in this step) finish here, packed densely into warps, so that their
+// long step sequences no longer stall 31 idle lanes each.  The list of step `it` is
+// indexed by its parity; the other parity's counter is cleared for the next step.
+template <int MODEL, int P>
+__global__ void __launch_bounds__(128) aeif_straggler_kernel(const AeifArgs A, const SpikeOut so,
+                                                             Clock *clk, int k) {
+  constexpr int NV = 2 + AeifShape<MODEL>::npv * P;
+  const StepT t = step_times<false>(clk, k, A.dt);
+  const int par = (int)(t.it & 1);
+  const int cnt = A.strag_cnt[par];
+  if (blockIdx.x == 0 && threadIdx.x == 0) A.strag_cnt[par ^ 1] = 0;
+  unsigned long long nd = 0;
+  const int n = A.n;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
+    const int i = A.strag_list[j];
+    AeifQ<MODEL, P> q;
+    load_aeif_par<MODEL, P>(A, i, q);
+    float y[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) y[v] = A.var[(size_t)v * n + i];
+    float refr = A.refr[i];
+    double x = A.x[i];
+    float h = A.h[i];
+    aeif_integrate<MODEL, P>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, 0, nd);
+#pragma unroll
+    for (int v = 0; v < NV; v++) A.var[(size_t)v * n + i] = y[v];
+    A.refr[i] = refr;
+    A.x[i] = x;
+    A.h[i] = h;
+  }
+  for (int o = 16; o > 0; o >>= 1) nd += __shfl_down_sync(0xffffffffu, nd, o);
+  if ((threadIdx.x & 31) == 0 && nd) atomicAdd(A.nderiv, nd);
 }
 
 // Generic port count (P > MAX_TPL_PORT): ports handled with runtime loops over
@@ -735,38 +795,55 @@ __global__ void __launch_bounds__(128) aeif_update_kernel_gen(const AeifArgs A, 
 // Host-side launchers
 // ---------------------------------------------------------------------------
 template <int MODEL, bool FLUSH>
-static void launch_aeif_model(const AeifArgs &A, const SpikeOut &so, Clock *clk, int k,
-                              cudaStream_t st) {
+static int launch_aeif_model(const AeifArgs &A, const SpikeOut &so, Clock *clk, int k,
+                             cudaStream_t st) {
   dim3 grid((A.n + 127) / 128), block(128);
+  dim3 sgrid(std::min((A.n + 127) / 128, 148 * 2));
+  const bool strag = !FLUSH && A.budget > 0;
   switch (A.nport) {
-  case 1: aeif_update_kernel<MODEL, 1, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k); break;
-  case 2: aeif_update_kernel<MODEL, 2, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k); break;
-  case 3: aeif_update_kernel<MODEL, 3, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k); break;
-  case 4: aeif_update_kernel<MODEL, 4, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k); break;
-  default: aeif_update_kernel_gen<MODEL, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k); break;
+  case 1:
+    aeif_update_kernel<MODEL, 1, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k);
+    if (strag) aeif_straggler_kernel<MODEL, 1><<<sgrid, block, 0, st>>>(A, so, clk, k);
+    break;
+  case 2:
+    aeif_update_kernel<MODEL, 2, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k);
+    if (strag) aeif_straggler_kernel<MODEL, 2><<<sgrid, block, 0, st>>>(A, so, clk, k);
+    break;
+  case 3:
+    aeif_update_kernel<MODEL, 3, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k);
+    if (strag) aeif_straggler_kernel<MODEL, 3><<<sgrid, block, 0, st>>>(A, so, clk, k);
+    break;
+  case 4:
+    aeif_update_kernel<MODEL, 4, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k);
+    if (strag) aeif_straggler_kernel<MODEL, 4><<<sgrid, block, 0, st>>>(A, so, clk, k);
+    break;
+  default:
+    aeif_update_kernel_gen<MODEL, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k);
+    return 1;
   }
+  return strag ? 2 : 1;
 }
 
-void launch_aeif(int model, bool flush, const AeifArgs &A, const SpikeOut &so, Clock *clk, int k,
-                 cudaStream_t st) {
-  if (A.n <= 0 || A.nport <= 0) {
-    if (A.n <= 0) return;
-  }
+// Returns the number of kernels launched.
+int launch_aeif(int model, bool flush, const AeifArgs &A, const SpikeOut &so, Clock *clk, int k,
+                cudaStream_t st) {
+  if (A.n <= 0) return 0;
   if (flush) {
     switch (model) {
-    case M_AEIF_COND_BETA: launch_aeif_model<M_AEIF_COND_BETA, true>(A, so, clk, k, st); break;
-    case M_AEIF_COND_ALPHA: launch_aeif_model<M_AEIF_COND_ALPHA, true>(A, so, clk, k, st); break;
-    case M_AEIF_PSC_EXP: launch_aeif_model<M_AEIF_PSC_EXP, true>(A, so, clk, k, st); break;
-    case M_AEIF_PSC_ALPHA: launch_aeif_model<M_AEIF_PSC_ALPHA, true>(A, so, clk, k, st); break;
+    case M_AEIF_COND_BETA: return launch_aeif_model<M_AEIF_COND_BETA, true>(A, so, clk, k, st);
+    case M_AEIF_COND_ALPHA: return launch_aeif_model<M_AEIF_COND_ALPHA, true>(A, so, clk, k, st);
+    case M_AEIF_PSC_EXP: return launch_aeif_model<M_AEIF_PSC_EXP, true>(A, so, clk, k, st);
+    case M_AEIF_PSC_ALPHA: return launch_aeif_model<M_AEIF_PSC_ALPHA, true>(A, so, clk, k, st);
     }
   } else {
     switch (model) {
-    case M_AEIF_COND_BETA: launch_aeif_model<M_AEIF_COND_BETA, false>(A, so, clk, k, st); break;
-    case M_AEIF_COND_ALPHA: launch_aeif_model<M_AEIF_COND_ALPHA, false>(A, so, clk, k, st); break;
-    case M_AEIF_PSC_EXP: launch_aeif_model<M_AEIF_PSC_EXP, false>(A, so, clk, k, st); break;
-    case M_AEIF_PSC_ALPHA: launch_aeif_model<M_AEIF_PSC_ALPHA, false>(A, so, clk, k, st); break;
+    case M_AEIF_COND_BETA: return launch_aeif_model<M_AEIF_COND_BETA, false>(A, so, clk, k, st);
+    case M_AEIF_COND_ALPHA: return launch_aeif_model<M_AEIF_COND_ALPHA, false>(A, so, clk, k, st);
+    case M_AEIF_PSC_EXP: return launch_aeif_model<M_AEIF_PSC_EXP, false>(A, so, clk, k, st);
+    case M_AEIF_PSC_ALPHA: return launch_aeif_model<M_AEIF_PSC_ALPHA, false>(A, so, clk, k, st);
     }
   }
+  return 0;
 }
 
 void launch_iaf(bool flush, const IafArgs &A, const SpikeOut &so, Clock *clk, int k, float dt,

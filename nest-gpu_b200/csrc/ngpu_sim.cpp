@@ -297,7 +297,7 @@ void Engine::calibrate() {
   cuda_check(cudaMemset(d_counters_, 0, 4 * sizeof(unsigned long long)), "counters");
   d_clk_ = dalloc<Clock>(1);
   cuda_check(cudaMemset(d_clk_, 0, sizeof(Clock)), "clock");
-  deliver_blocks_ = std::max(1, std::min(148 * 2, (n_src_out + 63) / 64));
+  deliver_blocks_ = std::max(1, std::min(148 * 8, (n_src_out + 63) / 64));
 
   // ---- per-group device state
   for (auto &g : groups_) {
@@ -309,6 +309,9 @@ void Engine::calibrate() {
                               cudaMemcpyHostToDevice), "var");
     }
     if (is_aeif(g.model)) {
+      g.d_strag = dalloc<int>(g.n);
+      g.d_strag_cnt = dalloc<int>(2);
+      cuda_check(cudaMemset(g.d_strag_cnt, 0, 2 * sizeof(int)), "strag");
       g.d_refr = dalloc<float>(g.n);
       cuda_check(cudaMemcpy(g.d_refr, g.par[A_refractory_step].data(), g.n * sizeof(float),
                             cudaMemcpyHostToDevice), "refr");
@@ -551,6 +554,9 @@ AeifArgs Engine::aeif_args(Group &g) {
   A.hmin_acc = A.hmin * 1.00001f;
   A.seed = kernel_seed;
   A.nderiv = d_counters_;
+  A.budget = rk5_budget;
+  A.strag_list = g.d_strag;
+  A.strag_cnt = g.d_strag_cnt;
   A.rec = spike_rec(g);
   for (int j = 0; j < AEIF_NPAR; j++) {
     A.pval[j] = g.der_val[j];
@@ -612,7 +618,7 @@ DeliverArgs Engine::deliver_args() {
 void Engine::launch_step(int k) {
   SpikeOut so = spike_out();
   for (auto &g : groups_) {
-    if (is_aeif(g.model)) { launch_aeif(g.model, false, aeif_args(g), so, d_clk_, k, stream_); count_launch(1); }
+    if (is_aeif(g.model)) count_launch(launch_aeif(g.model, false, aeif_args(g), so, d_clk_, k, stream_));
     else if (g.model == M_IAF_PSC_EXP) { launch_iaf(false, iaf_args(g), so, d_clk_, k, dt, stream_); count_launch(1); }
     else if (g.model == M_SPIKE_GEN) { launch_spike_gen(sg_args(g), so, d_clk_, k, dt, stream_); count_launch(1); }
   }
@@ -621,14 +627,15 @@ void Engine::launch_step(int k) {
                   stream_);
     count_launch(1);
   }
-  launch_deliver(deliver_args(), deliver_blocks_, d_clk_, k, dt, stream_);
+  launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_, d_clk_, k,
+                 dt, stream_);
   count_launch(1);
 }
 
 void Engine::launch_flush() {
   SpikeOut so = spike_out();
   for (auto &g : groups_) {
-    if (is_aeif(g.model)) { launch_aeif(g.model, true, aeif_args(g), so, d_clk_, 0, stream_); count_launch(1); }
+    if (is_aeif(g.model)) count_launch(launch_aeif(g.model, true, aeif_args(g), so, d_clk_, 0, stream_));
     else if (g.model == M_IAF_PSC_EXP) { launch_iaf(true, iaf_args(g), so, d_clk_, 0, dt, stream_); count_launch(1); }
   }
   launch_clock_clear_pending(d_clk_, stream_);
@@ -851,7 +858,8 @@ std::vector<double> Engine::profile_steps(int n) {
       launch_record(d_cols_, rec_ncol_, d_recbuf_, d_last_tidx_, d_last_h_, d_has_out_, d_clk_, 0, dt,
                     stream_);
     cuda_check(cudaEventRecord(ev[2], stream_), "event");
-    launch_deliver(deliver_args(), deliver_blocks_, d_clk_, 0, dt, stream_);
+    launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_, d_clk_, 0,
+                   dt, stream_);
     cuda_check(cudaEventRecord(ev[3], stream_), "event");
     launch_clock_advance(d_clk_, 1, stream_);
     cuda_check(cudaEventSynchronize(ev[3]), "event");

@@ -104,6 +104,9 @@ struct AeifArgs {
   float hmin_acc;        // hmin * 1.00001f: forced-accept threshold
   uint64_t seed;
   unsigned long long *nderiv;
+  int budget;            // RK5 steps per neuron in the main kernel (0: no limit)
+  int *strag_list;       // [n] neurons left for the straggler kernel
+  int *strag_cnt;        // [2] list lengths, indexed by step parity
   GroupSpikeRec rec;
   float pval[AEIF_NPAR];
   const float *parr[AEIF_NPAR];

@@ -161,6 +161,8 @@ if is_b200_engine:
                                                                  c_void_p, c_void_p, c_void_p])
     _c["NGPU_SetGraphSteps"] = _bind("NGPU_SetGraphSteps", _I, [_I])
     _c["NGPU_SetHostRng"] = _bind("NGPU_SetHostRng", _I, [_I])
+    _c["NGPU_SetRk5Budget"] = _bind("NGPU_SetRk5Budget", _I, [_I])
+    _c["NGPU_SetDeliverBlocks"] = _bind("NGPU_SetDeliverBlocks", _I, [_I])
     _c["NGPU_GetSimDeviceMs"] = _bind("NGPU_GetSimDeviceMs", ctypes.c_double, [])
     _c["NGPU_GetLaunchCount"] = _bind("NGPU_GetLaunchCount", ctypes.c_longlong, [])
     _c["NGPU_ProfileSteps"] = _bind("NGPU_ProfileSteps", _I, [_I, ctypes.POINTER(ctypes.c_double)])
@@ -1272,6 +1274,17 @@ def SetHostRng(on=True):
     if not is_b200_engine:
         raise ValueError("SetHostRng needs libnestgpu_b200.so")
     return _check(_c["NGPU_SetHostRng"](1 if on else 0))
+
+
+def SetDeliverBlocks(n):
+    """Thread blocks of the delivery kernel (engine extension; 0 = automatic)."""
+    return _check(_c["NGPU_SetDeliverBlocks"](n))
+
+
+def SetRk5Budget(n):
+    """RK5 steps per neuron in the main update kernel before the straggler kernel takes over
+    (engine extension; 0 disables the hand-off)."""
+    return _check(_c["NGPU_SetRk5Budget"](n))
 
 
 def SetGraphSteps(n):

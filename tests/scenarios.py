@@ -118,10 +118,16 @@ def fixed_train_network(api, n=60, n_in=20, seed=7, t_sim=300.0, model="aeif_con
         api.SetStatus(neuron, {"I_e": 370.0})
         w_exc, w_inh, w_in = 35.0, -60.0, 90.0
         rec_var = "V_m_rel"
-    else:
+    elif model in ("aeif_cond_beta_multisynapse", "aeif_cond_alpha_multisynapse"):
         neuron = api.Create(model, n, 2)
         api.SetStatus(neuron, {"E_rev": [0.0, -85.0], "I_e": 500.0})
         w_exc, w_inh, w_in = 2.0, 4.0, 6.0
+        rec_var = "V_m"
+    else:
+        # current-based aeif: inhibition through a negative weight on receptor 1
+        neuron = api.Create(model, n, 2)
+        api.SetStatus(neuron, {"I_e": 500.0, "tau_syn": [2.0, 5.0]})
+        w_exc, w_inh, w_in = 60.0, -120.0, 200.0
         rec_var = "V_m"
     n_exc = int(0.8 * n)
     exc = neuron[0:n_exc]

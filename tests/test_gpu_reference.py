@@ -1,0 +1,86 @@
+"""The engine against the reference's own CUDA build on the same GPU.
+
+oracle/_ref/libnestgpukernel.so is compiled from the reference sources by
+oracle/Makefile.ref (at build time, where the sources are present) and travels
+with the repository; each scenario runs in a child process through the same
+nestgpu.py interface with NESTGPU_LIB pointing at it.  Skipped when that
+library was not built.
+
+Compared: the connection random stream and every connection of a rule-based
+network (bit-exact), single-neuron traces (1e-5 relative), and spike counts of
+recurrent networks driven by fixed spike trains (exact).
+"""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import nestgpu as ngpu
+from scenarios import fixed_train_network, trace_scenario
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libnestgpukernel.so")
+RUNNER = os.path.join(ROOT, "tests", "ref_runner.py")
+
+needs_ref = pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference library not built")
+
+
+def run_reference(what, timeout=600):
+    env = dict(os.environ, NESTGPU_LIB=REF_LIB)
+    p = subprocess.run([sys.executable, RUNNER, what], env=env, capture_output=True, text=True,
+                       timeout=timeout)
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = [x for x in p.stdout.splitlines() if x.startswith("JSON:")][-1]
+    return json.loads(line[5:])
+
+
+@pytest.fixture(autouse=True)
+def fresh_engine():
+    ngpu.Reset()
+    ngpu.SetVerbosityLevel(0)
+    yield
+    ngpu.Reset()
+
+
+@needs_ref
+def test_random_stream_matches_reference():
+    ref = run_reference("random:2024")
+    ngpu.SetRandomSeed(2024)
+    assert [int(x) for x in ngpu.RandomInt(1000)] == ref["int"]
+    assert np.array_equal(np.float32(ngpu.RandomNormal(1001, 0.5, 2.0)), np.float32(ref["normal"]))
+
+
+@needs_ref
+def test_connectivity_matches_reference():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from ref_runner import conn_arrays, rules_network
+    ref = run_reference("rules")
+    rules_network(4321)
+    got = conn_arrays()
+    for k in ("source", "group", "index", "target", "port"):
+        assert got[k] == ref[k], k
+    assert np.array_equal(np.float32(got["weight"]), np.float32(ref["weight"]))
+    assert np.array_equal(np.float32(got["delay"]), np.float32(ref["delay"]))
+
+
+@needs_ref
+@pytest.mark.parametrize("model", ["aeif_cond_beta_multisynapse", "iaf_psc_exp"])
+def test_trace_close_to_reference(model):
+    ref = run_reference("trace:" + model)
+    _, v = trace_scenario(ngpu, model)
+    vr = np.asarray(ref["v"])
+    assert np.max(np.abs(v - vr) / np.maximum(np.abs(vr), 1.0)) < 1e-5
+
+
+@needs_ref
+@pytest.mark.parametrize("model", ["aeif_cond_beta_multisynapse", "iaf_psc_exp"])
+def test_spike_counts_match_reference(model):
+    ref = run_reference("fixed_train:" + model)
+    counts, _ = fixed_train_network(ngpu, model=model)
+    assert counts.sum() > 0
+    assert counts.tolist() == ref["counts"]
