@@ -259,6 +259,21 @@ int NGPU_SetDeliverBlocks(int n);
    to the straggler kernel (default 4; 0 = no hand-off).  Results do not depend on it. */
 int NGPU_SetRk5Budget(int n);
 
+/* Pack a device-resident edge list into the spike-delivery layout: edges grouped into
+   segments by (source node, delay index).  All pointers are device pointers.
+     src[n]     source node of each edge, 0 <= src < n_nodes
+     dly[n]     delay index relative to the smallest delay, 0 <= dly < dspan
+     target[n]  accumulator index of each edge (receptor row offset + target)
+     weight[n]  weight
+   Writes seg_off[n_nodes*dspan + 1] (start of each segment; seg_off[last] = n) and edge[n]
+   (8-byte records {uint32 target, float weight}; order inside a segment unspecified).
+   Scratch (per-segment counters, scan workspace) comes from cudaMalloc and is released
+   before returning.  stream: a cudaStream_t or NULL.  Returns 0, or -1 with the error set
+   (code 255 for an out-of-range source or delay index). */
+int NGPU_BuildDeliveryCsr(const int *src, const int *dly, const unsigned *target, const float *weight,
+                          size_t n, int n_nodes, int dspan, unsigned long long *seg_off, void *edge,
+                          void *stream);
+
 /* Steps captured per CUDA graph (default 100). */
 int NGPU_SetGraphSteps(int n);
 

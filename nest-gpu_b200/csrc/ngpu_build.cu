@@ -143,4 +143,62 @@ void build_csr_device(int n_nodes, int dmin, int dspan, const std::vector<int> &
   *n_edge_out = (size_t)total;
 }
 
+// ---------------------------------------------------------------------------
+// Standalone packing of a device edge list into the delivery layout.
+// ---------------------------------------------------------------------------
+__global__ void list_count_kernel(size_t n, const int *src, const int *dly, int n_nodes, int dspan,
+                                  unsigned long long *cnt, unsigned *bad) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int s = src[e], d = dly[e];
+    if (s < 0 || s >= n_nodes || d < 0 || d >= dspan) {
+      atomicOr(bad, 1u);
+      continue;
+    }
+    atomicAdd(&cnt[(size_t)s * dspan + d], 1ULL);
+  }
+}
+
+__global__ void list_fill_kernel(size_t n, const int *src, const int *dly, const unsigned *target,
+                                 const float *weight, int n_nodes, int dspan, unsigned long long *cursor,
+                                 EdgeW *edge) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int s = src[e], d = dly[e];
+    if (s < 0 || s >= n_nodes || d < 0 || d >= dspan) continue;
+    const unsigned long long pos = atomicAdd(&cursor[(size_t)s * dspan + d], 1ULL);
+    EdgeW x;
+    x.acc = target[e];
+    x.w = weight[e];
+    edge[pos] = x;
+  }
+}
+
+// Counting sort with scratch from cudaMalloc: counters, cursors, scan workspace.
+void pack_delivery_csr(const int *src, const int *dly, const unsigned *target, const float *weight,
+                       size_t n, int n_nodes, int dspan, unsigned long long *seg_off, EdgeW *edge,
+                       cudaStream_t st) {
+  const size_t nkey = (size_t)n_nodes * dspan;
+  unsigned long long *d_cnt = nullptr;
+  unsigned *d_bad = nullptr;
+  void *d_tmp = nullptr;
+  size_t tmp_bytes = 0;
+  ck(cudaMalloc(&d_cnt, (nkey + 1) * sizeof(unsigned long long) + 256), "cudaMalloc");
+  d_bad = (unsigned *)(d_cnt + nkey + 1);
+  ck(cudaMemsetAsync(d_cnt, 0, (nkey + 1) * sizeof(unsigned long long) + sizeof(unsigned), st), "memset");
+  const int gb = 148 * 8, tb = 256;
+  list_count_kernel<<<gb, tb, 0, st>>>(n, src, dly, n_nodes, dspan, d_cnt, d_bad);
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_cnt, seg_off, nkey + 1, st);
+  ck(cudaMalloc(&d_tmp, tmp_bytes), "cudaMalloc");
+  cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_cnt, seg_off, nkey + 1, st);
+  // the counters become the fill cursors
+  ck(cudaMemcpyAsync(d_cnt, seg_off, nkey * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, st), "copy");
+  list_fill_kernel<<<gb, tb, 0, st>>>(n, src, dly, target, weight, n_nodes, dspan, d_cnt, edge);
+  unsigned bad = 0;
+  ck(cudaMemcpyAsync(&bad, d_bad, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "copy");
+  ck(cudaStreamSynchronize(st), "pack");
+  ck(cudaGetLastError(), "pack kernels");
+  cudaFree(d_tmp);
+  cudaFree(d_cnt);
+  if (bad) throw std::runtime_error("edge list holds a source or delay index out of range");
+}
+
 }  // namespace ngpu

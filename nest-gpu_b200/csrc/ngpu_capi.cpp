@@ -673,6 +673,19 @@ int NGPU_ConnectFixedIndegreeGPU(int i_source, int n_source, int i_target, int n
   }, 0);
 }
 
+int NGPU_BuildDeliveryCsr(const int *src, const int *dly, const unsigned *target, const float *weight,
+                          size_t n, int n_nodes, int dspan, unsigned long long *seg_off, void *edge,
+                          void *stream) {
+  return guard([&] {
+    if (n_nodes <= 0 || dspan <= 0) throw NgpuError("n_nodes and dspan must be positive");
+    if ((n > 0 && (!src || !dly || !target || !weight || !edge)) || !seg_off)
+      throw NgpuError("null device pointer");
+    pack_delivery_csr(src, dly, target, weight, n, n_nodes, dspan, seg_off, (EdgeW *)edge,
+                      (cudaStream_t)stream);
+    return 0;
+  }, -1);
+}
+
 int NGPU_SetDeliverBlocks(int n) {
   return guard([&] {
     if (n < 0) throw NgpuError("block count must be >= 0");

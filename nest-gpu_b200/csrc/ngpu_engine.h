@@ -289,6 +289,9 @@ void launch_record(const RecCol *cols, int ncol, float *buf, const int *last_tid
 void launch_clock_advance(Clock *clk, int K, cudaStream_t st);
 void launch_clock_clear_pending(Clock *clk, cudaStream_t st);
 int deliver_max_dspan();
+void pack_delivery_csr(const int *src, const int *dly, const unsigned *target, const float *weight,
+                       size_t n, int n_nodes, int dspan, unsigned long long *seg_off, EdgeW *edge,
+                       cudaStream_t st);
 void build_csr_device(int n_nodes, int dmin, int dspan, const std::vector<int> &cnt_host,
                       const std::vector<long long> &h_key, const std::vector<int> &h_rank,
                       const std::vector<EdgeW> &h_ew, const std::vector<GenBlockDev> &blocks,

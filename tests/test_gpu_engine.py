@@ -152,8 +152,8 @@ def test_rec_spike_times_and_spike_record():
     for a, b in zip(tg, to):
         assert np.array_equal(np.float32(a), np.float32(b))
     assert np.array_equal(np.float32(rg), np.float32(ro))
-    # "spike" records a spike only for nodes with recurrent out-connections (node 0 here)
-    assert rg[:, 1].sum() == cg[0] and rg[:, 2].sum() == 0
+    # every neuron projects to neuron 0, so "spike" records each of their spikes
+    assert rg[:, 1].sum() == cg[0] and rg[:, 2].sum() == cg[1] and rg[:, 3].sum() == cg[2]
 
 
 def test_brunel_rate_statistics():
