@@ -255,8 +255,15 @@ int NGPU_ConnectFixedIndegreeGPU(int i_source, int n_source, int i_target, int n
    outgoing connections, at most 8 per SM).  Results do not depend on it. */
 int NGPU_SetDeliverBlocks(int n);
 
-/* RK5 steps a neuron may take in the main update kernel per time step before it is handed
-   to the straggler kernel (default 4; 0 = no hand-off).  Results do not depend on it. */
+/* Upper bound of the number of time steps integrated per batch (default 32, before
+   calibration).  A batch never exceeds the minimum connection delay in steps, so spikes
+   emitted inside it cannot reach a target inside it; 1 advances step by step.  Results do
+   not depend on it. */
+int NGPU_SetBatchMax(int n);
+
+/* RK5 steps a neuron may take in the main update kernel per batch beyond one per time step
+   before it is handed to the straggler kernel (default 4; 0 = no hand-off).  Results do not
+   depend on it. */
 int NGPU_SetRk5Budget(int n);
 
 /* Pack a device-resident edge list into the spike-delivery layout: edges grouped into

@@ -694,6 +694,15 @@ int NGPU_SetDeliverBlocks(int n) {
   }, 0);
 }
 
+int NGPU_SetBatchMax(int n) {
+  return guard([&] {
+    if (n < 1) throw NgpuError("batch length must be >= 1");
+    if (E().calibrated()) throw NgpuError("the batch length must be set before calibration");
+    E().batch_max = n;
+    return 0;
+  }, 0);
+}
+
 int NGPU_SetRk5Budget(int n) {
   return guard([&] {
     if (n < 0) throw NgpuError("RK5 budget must be >= 0");

@@ -55,8 +55,10 @@ struct Group {
   int *d_spike_count = nullptr;
   int *d_n_rec = nullptr;
   float *d_rec_times = nullptr;
-  int *d_strag = nullptr;        // aeif: straggler list [n] and counters [2]
-  int *d_strag_cnt = nullptr;
+  int2 *d_strag = nullptr;       // aeif: straggler list [n] (neuron, step of the batch)
+  int strag_slot = -1;           // index of its counter in the engine's counter array
+  int *d_rec_first = nullptr;    // record columns: CSR over neurons
+  int2 *d_rec_col = nullptr;
   int *d_pin_off = nullptr;
   PoissonIn *d_pin = nullptr;
   int *d_sg_off = nullptr, *d_sg_tidx = nullptr, *d_sg_next = nullptr;
@@ -103,6 +105,7 @@ class Engine {
   int graph_steps = 100;          // steps per captured CUDA graph
   int rk5_budget = 4;             // RK5 steps per neuron before the straggler kernel takes over
   int deliver_blocks_req = 0;     // delivery grid size (0: from the number of spiking sources)
+  int batch_max = MAX_BATCH;      // upper bound of the time-batch length (1: step by step)
   bool use_device_rng = true;     // cuRAND device generator (as the reference) if a GPU exists
 
   void set_seed(unsigned long long s);
@@ -236,10 +239,11 @@ class Engine {
   GenPar *d_gen_ = nullptr;
   int n_gen_ = 0;
   unsigned long long *d_counters_ = nullptr;   // [0] derivs, [1] events
-  RecCol *d_cols_ = nullptr;
   float *d_recbuf_ = nullptr;
   int rec_ncol_ = 0, rec_rows_cap_ = 0;
-  std::vector<std::pair<int, int>> rec_cols_;  // (record, column)
+  int batch_ = 1;                // steps per batch
+  int *d_strag_cnt_ = nullptr;   // straggler counters, one per aeif group
+  int n_strag_ = 0;
   int deliver_blocks_ = 148;
   std::map<int, cudaGraphExec_t> graphs_;
   std::vector<void *> allocs_;
@@ -258,8 +262,10 @@ class Engine {
   void free_device();
   void upload_params();
   void build_records();
-  void launch_step(int k);
-  void launch_flush();
+  void launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev);
+  void ensure_record_window(long long rows);
+  GroupRecord group_record(Group &g);
+  GroupInput group_input(Group &g);
   void run_steps(long long n);
   void drain_records(long long rows);
   void drain_rec_spike_times();
@@ -276,19 +282,14 @@ Engine &engine();
 void engine_reset();
 
 // launchers (ngpu_kernels.cu)
-int launch_aeif(int model, bool flush, const AeifArgs &A, const SpikeOut &so, Clock *clk, int k,
+int launch_aeif(int model, const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                 cudaStream_t st);
-void launch_iaf(bool flush, const IafArgs &A, const SpikeOut &so, Clock *clk, int k, float dt,
-                cudaStream_t st);
-void launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, Clock *clk, int k, float dt,
-                      cudaStream_t st);
-void launch_deliver(const DeliverArgs &A, int n_blocks, Clock *clk, int k, float dt, cudaStream_t st);
-void launch_record(const RecCol *cols, int ncol, float *buf, const int *last_tidx,
-                   const float *last_height, const unsigned char *has_out, Clock *clk, int k,
-                   float dt, cudaStream_t st);
-void launch_clock_advance(Clock *clk, int K, cudaStream_t st);
-void launch_clock_clear_pending(Clock *clk, cudaStream_t st);
-int deliver_max_dspan();
+int launch_iaf(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st);
+int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
+                     cudaStream_t st);
+int launch_deliver(const DeliverArgs &A, int n_blocks, const Clock *clk, int k0, int M, cudaStream_t st);
+int launch_clock_advance(Clock *clk, int K, cudaStream_t st);
+int deliver_max_pairs();
 void pack_delivery_csr(const int *src, const int *dly, const unsigned *target, const float *weight,
                        size_t n, int n_nodes, int dspan, unsigned long long *seg_off, EdgeW *edge,
                        cudaStream_t st);

@@ -1,16 +1,18 @@
 // CUDA kernels of the spiking engine (sm_100a).
 //
-// Per time step the host graph runs, in order:
-//   1. one update kernel per node group (aeif RK5 / iaf_psc_exp / spike_generator);
-//      each neuron first folds the inputs that arrived at the end of the previous
-//      step (delivered spikes in the FP64 accumulator plus that step's poiss_gen
-//      draws), then integrates one step and appends its spikes to the ring slot
-//      of this step;
-//   2. the record gather (when records exist);
-//   3. the delivery kernel: the spikes emitted D steps ago walk their CSR segment
-//      of delay D and add height*weight into the accumulator with FP64 atomics.
-// This reproduces the reference order (src/nestgpu.cu:469-635): spike-buffer
-// update, neuron update, record, CollectSpike, poiss_gen, GetSpikes fold.
+// Time is advanced in batches of M steps, M <= the minimum synaptic delay in
+// steps (a spike emitted in step s reaches its targets in step s+1+d, d >= dmin,
+// so no spike emitted inside a batch affects the batch).  Per batch the graph runs:
+//   1. deliver_batch_kernel: the spikes of the last dmax+1 steps walk their CSR
+//      segments and add height*weight into the accumulator slot of the step in
+//      which they arrive (FP64 atomics, one slot per step of the batch);
+//   2. per node group one update kernel that integrates each neuron through all M
+//      steps with its state in registers; at the end of every step it records,
+//      then folds that step's arrivals and poiss_gen draws into the state, exactly
+//      where the reference folds (src/nestgpu.cu:469-635: update, record,
+//      CollectSpike, poiss_gen, GetSpikes); aeif neurons that need more RK5 steps
+//      than a budget (those that spike) are finished by a straggler kernel, packed
+//      densely, so their long step sequences do not stall whole warps.
 #include <cub/block/block_scan.cuh>
 
 #include <algorithm>
@@ -41,11 +43,18 @@ constexpr int max_trials = 100000;
 constexpr int max_substeps = 1000000;
 }  // namespace ck
 
-__device__ __forceinline__ void step_time(const Clock *c, int k, float dt, long long &it,
-                                          long long &tidx, double &tnow) {
-  it = c->it0 + k;
-  tidx = c->tidx_base + it + 1;
-  tnow = c->t0 + (double)dt * (double)(it + 1);
+// Step `m` of the batch starting at graph step k0.
+struct StepT {
+  long long it, tidx;
+  double tnow;
+};
+
+__device__ __forceinline__ StepT step_at(const Clock *c, int k0, int m, float dt) {
+  StepT s;
+  s.it = c->it0 + k0 + m;
+  s.tidx = c->tidx_base + s.it + 1;
+  s.tnow = c->t0 + (double)dt * (double)(s.it + 1);
+  return s;
 }
 
 // PushSpike (src/spike_buffer.cu:162-242) on the ring design.
@@ -72,25 +81,25 @@ __device__ __forceinline__ void push_spike(const SpikeOut &so, const GroupSpikeR
   }
 }
 
-// Input of the previous step for neuron i: accumulator plus poiss_gen draws
-// (src/get_spike.cu:142-166, src/poiss_gen.cu:55-86).  `in` has nport entries.
-__device__ __forceinline__ void gather_inputs(double *in, int nport, int n, int i, double *acc,
-                                              const int *pin_off, const PoissonIn *pin,
-                                              const GenPar *gen, float lam_scale, uint64_t seed,
-                                              long long tidx_prev, double t_prev) {
+// Input arriving in step (tidx, tnow) for neuron i: the accumulator slot m (spikes
+// delivered this step, src/get_spike.cu:60-108) plus this step's poiss_gen draws
+// (src/poiss_gen.cu:55-86); the slot is cleared for its next use.
+__device__ __forceinline__ void step_inputs(double *in, int nport, int n, int i, const GroupInput &G,
+                                            int m, long long tidx, double tnow) {
+  double *acc = G.acc + (size_t)m * G.slot_stride;
   for (int p = 0; p < nport; p++) {
     double a = acc[(size_t)p * n + i];
     in[p] = a;
     if (a != 0.0) acc[(size_t)p * n + i] = 0.0;
   }
-  if (pin_off) {
-    int e0 = pin_off[i], e1 = pin_off[i + 1];
+  if (G.pin_off) {
+    const int e0 = G.pin_off[i], e1 = G.pin_off[i + 1];
     for (int e = e0; e < e1; e++) {
-      PoissonIn pe = pin[e];
-      GenPar g = gen[pe.gen];
-      double t_rel = t_prev - (double)g.origin - (double)pe.delay;
+      const PoissonIn pe = G.pin[e];
+      const GenPar g = G.gen[pe.gen];
+      const double t_rel = tnow - (double)g.origin - (double)pe.delay;
       if (t_rel >= (double)g.start && t_rel <= (double)g.stop) {
-        int k = poisson_draw(__fmul_rn(lam_scale, g.rate), seed, pe.edge_id, tidx_prev);
+        int k = poisson_draw(__fmul_rn(G.lam_scale, g.rate), G.seed, pe.edge_id, tidx);
         if (k > 0) in[pe.port] += (double)__fmul_rn(pe.weight, (float)k);
       }
     }
@@ -106,23 +115,29 @@ template <int MODEL> struct AeifShape {
   static constexpr bool cond = (MODEL == M_AEIF_COND_BETA || MODEL == M_AEIF_COND_ALPHA);
 };
 
-template <int MODEL, int P> struct AeifQ {
+// PMAX: compile-time bound on the port count; FIXED: the group has exactly PMAX ports.
+template <int MODEL, int PMAX, bool FIXED> struct AeifQ {
+  int np;
   float V_th, Delta_T, inv_Delta_T, g_L, E_L, inv_C_m, a, b, inv_tau_w, I_e, V_peak, V_reset,
       refr_steps;
-  float E_rev[P], inv_t1[P], inv_t2[P], pw[P];
+  float E_rev[PMAX], inv_t1[PMAX], inv_t2[PMAX], pw[PMAX];
+  __device__ __forceinline__ int ports() const { return FIXED ? PMAX : np; }
 };
 
-template <int MODEL, int P>
-__device__ __forceinline__ void aeif_derivs(const float *y, float *dy, const AeifQ<MODEL, P> &q,
-                                            float refr) {
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ void aeif_derivs(const float *y, float *dy,
+                                            const AeifQ<MODEL, PMAX, FIXED> &q, float refr) {
   typedef AeifShape<MODEL> S;
+  const int np = q.ports();
   const float V = (refr > 0.0f) ? q.V_reset : ((y[0] < q.V_peak) ? y[0] : q.V_peak);
   const float w = y[1];
   float I = 0.0f;
 #pragma unroll
-  for (int i = 0; i < P; i++) {
-    if (S::cond) I = __fmaf_rn(y[2 + 2 * i], __fsub_rn(q.E_rev[i], V), I);
-    else I = __fadd_rn(I, y[2 + S::npv * i]);
+  for (int i = 0; i < PMAX; i++) {
+    if (i < np) {
+      if (S::cond) I = __fmaf_rn(y[2 + 2 * i], __fsub_rn(q.E_rev[i], V), I);
+      else I = __fadd_rn(I, y[2 + S::npv * i]);
+    }
   }
   float Vs;
   if (!S::cond && q.Delta_T == 0.0f) Vs = 0.0f;
@@ -133,12 +148,14 @@ __device__ __forceinline__ void aeif_derivs(const float *y, float *dy, const Aei
   dy[0] = (refr > 0.0f) ? 0.0f : __fmul_rn(s, q.inv_C_m);
   dy[1] = __fmul_rn(__fmaf_rn(q.a, __fsub_rn(V, q.E_L), -w), q.inv_tau_w);
 #pragma unroll
-  for (int i = 0; i < P; i++) {
-    if (MODEL == M_AEIF_PSC_EXP) {
-      dy[2 + i] = __fmul_rn(-y[2 + i], q.inv_t1[i]);
-    } else {
-      dy[3 + 2 * i] = __fmul_rn(-y[3 + 2 * i], q.inv_t1[i]);
-      dy[2 + 2 * i] = __fmaf_rn(-y[2 + 2 * i], q.inv_t2[i], y[3 + 2 * i]);
+  for (int i = 0; i < PMAX; i++) {
+    if (i < np) {
+      if (MODEL == M_AEIF_PSC_EXP) {
+        dy[2 + i] = __fmul_rn(-y[2 + i], q.inv_t1[i]);
+      } else {
+        dy[3 + 2 * i] = __fmul_rn(-y[3 + 2 * i], q.inv_t1[i]);
+        dy[2 + 2 * i] = __fmaf_rn(-y[2 + 2 * i], q.inv_t2[i], y[3 + 2 * i]);
+      }
     }
   }
 }
@@ -148,8 +165,9 @@ __device__ __forceinline__ float pget(const AeifArgs &A, int j, int i) {
   return p ? __ldg(p + i) : A.pval[j];
 }
 
-template <int MODEL, int P>
-__device__ __forceinline__ void load_aeif_par(const AeifArgs &A, int i, AeifQ<MODEL, P> &q) {
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ void load_aeif_par(const AeifArgs &A, int i, AeifQ<MODEL, PMAX, FIXED> &q) {
+  q.np = A.nport;
   q.V_th = pget(A, AP_V_th, i);
   q.Delta_T = pget(A, AP_Delta_T, i);
   q.inv_Delta_T = pget(A, AP_inv_Delta_T, i);
@@ -163,28 +181,34 @@ __device__ __forceinline__ void load_aeif_par(const AeifArgs &A, int i, AeifQ<MO
   q.V_peak = pget(A, AP_V_peak, i);
   q.V_reset = pget(A, AP_V_reset, i);
   q.refr_steps = pget(A, AP_refr_steps, i);
+  const int np = q.ports();
 #pragma unroll
-  for (int p = 0; p < P; p++) {
-    const int b = AEIF_NSCAL + AEIF_NPORTPAR * p;
-    q.E_rev[p] = pget(A, b + 0, i);
-    q.inv_t1[p] = pget(A, b + 1, i);
-    q.inv_t2[p] = pget(A, b + 2, i);
-    q.pw[p] = pget(A, b + 3, i);
+  for (int p = 0; p < PMAX; p++) {
+    if (p < np) {
+      const int b = AEIF_NSCAL + AEIF_NPORTPAR * p;
+      q.E_rev[p] = pget(A, b + 0, i);
+      q.inv_t1[p] = pget(A, b + 1, i);
+      q.inv_t2[p] = pget(A, b + 2, i);
+      q.pw[p] = pget(A, b + 3, i);
+    }
   }
 }
 
-// One accepted RK5 step; returns the number of derivative evaluations.
-template <int MODEL, int P>
+// One accepted RK5 step (src/rk5.h:69-159); returns the number of derivative evaluations.
+template <int MODEL, int PMAX, bool FIXED>
 __device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmin, float hmin_acc,
-                                        float hmax, const AeifQ<MODEL, P> &q, float refr,
+                                        float hmax, const AeifQ<MODEL, PMAX, FIXED> &q, float refr,
                                         unsigned *status) {
-  constexpr int NV = 2 + AeifShape<MODEL>::npv * P;
-  float k1[NV], k2[NV], k3[NV], k4[NV], k5[NV], k6[NV], yn[NV], iys[NV];
-  aeif_derivs<MODEL, P>(y, k1, q, refr);
+  constexpr int NVM = 2 + AeifShape<MODEL>::npv * PMAX;
+  const int NV = 2 + AeifShape<MODEL>::npv * q.ports();
+  float k1[NVM], k2[NVM], k3[NVM], k4[NVM], k5[NVM], k6[NVM], yn[NVM], iys[NVM];
+  aeif_derivs(y, k1, q, refr);
 #pragma unroll
-  for (int i = 0; i < NV; i++) {
-    float ys = __fadd_rn(__fadd_rn(fabsf(y[i]), fabsf(__fmul_rn(k1[i], h))), ck::scal_min);
-    iys[i] = __fdiv_rn(1.0f, ys);
+  for (int i = 0; i < NVM; i++) {
+    if (i < NV) {
+      float ys = __fadd_rn(__fadd_rn(fabsf(y[i]), fabsf(__fmul_rn(k1[i], h))), ck::scal_min);
+      iys[i] = __fdiv_rn(1.0f, ys);
+    }
   }
   int nd = 1;
   int trials = 0;
@@ -201,37 +225,44 @@ __device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmi
                 b76 = __fmul_rn(h, ck::a76), f1 = __fmul_rn(h, ck::e1), f3 = __fmul_rn(h, ck::e3),
                 f4 = __fmul_rn(h, ck::e4), f5 = __fmul_rn(h, ck::e5), f6 = __fmul_rn(h, ck::e6);
 #pragma unroll
-    for (int i = 0; i < NV; i++) yn[i] = __fmaf_rn(b21, k1[i], y[i]);
-    aeif_derivs<MODEL, P>(yn, k2, q, refr);
+    for (int i = 0; i < NVM; i++)
+      if (i < NV) yn[i] = __fmaf_rn(b21, k1[i], y[i]);
+    aeif_derivs(yn, k2, q, refr);
 #pragma unroll
-    for (int i = 0; i < NV; i++) yn[i] = __fmaf_rn(b32, k2[i], __fmaf_rn(b31, k1[i], y[i]));
-    aeif_derivs<MODEL, P>(yn, k3, q, refr);
+    for (int i = 0; i < NVM; i++)
+      if (i < NV) yn[i] = __fmaf_rn(b32, k2[i], __fmaf_rn(b31, k1[i], y[i]));
+    aeif_derivs(yn, k3, q, refr);
 #pragma unroll
-    for (int i = 0; i < NV; i++)
-      yn[i] = __fmaf_rn(b43, k3[i], __fmaf_rn(b42, k2[i], __fmaf_rn(b41, k1[i], y[i])));
-    aeif_derivs<MODEL, P>(yn, k4, q, refr);
+    for (int i = 0; i < NVM; i++)
+      if (i < NV) yn[i] = __fmaf_rn(b43, k3[i], __fmaf_rn(b42, k2[i], __fmaf_rn(b41, k1[i], y[i])));
+    aeif_derivs(yn, k4, q, refr);
 #pragma unroll
-    for (int i = 0; i < NV; i++)
-      yn[i] = __fmaf_rn(b54, k4[i],
-                        __fmaf_rn(b53, k3[i], __fmaf_rn(b52, k2[i], __fmaf_rn(b51, k1[i], y[i]))));
-    aeif_derivs<MODEL, P>(yn, k5, q, refr);
+    for (int i = 0; i < NVM; i++)
+      if (i < NV)
+        yn[i] = __fmaf_rn(b54, k4[i],
+                          __fmaf_rn(b53, k3[i], __fmaf_rn(b52, k2[i], __fmaf_rn(b51, k1[i], y[i]))));
+    aeif_derivs(yn, k5, q, refr);
 #pragma unroll
-    for (int i = 0; i < NV; i++)
-      yn[i] = __fmaf_rn(
-          b65, k5[i],
-          __fmaf_rn(b64, k4[i], __fmaf_rn(b63, k3[i], __fmaf_rn(b62, k2[i], __fmaf_rn(b61, k1[i], y[i])))));
-    aeif_derivs<MODEL, P>(yn, k6, q, refr);
+    for (int i = 0; i < NVM; i++)
+      if (i < NV)
+        yn[i] = __fmaf_rn(b65, k5[i],
+                          __fmaf_rn(b64, k4[i], __fmaf_rn(b63, k3[i],
+                                                          __fmaf_rn(b62, k2[i], __fmaf_rn(b61, k1[i], y[i])))));
+    aeif_derivs(yn, k6, q, refr);
 #pragma unroll
-    for (int i = 0; i < NV; i++)
-      yn[i] = __fmaf_rn(b76, k6[i],
-                        __fmaf_rn(b74, k4[i], __fmaf_rn(b73, k3[i], __fmaf_rn(b71, k1[i], y[i]))));
+    for (int i = 0; i < NVM; i++)
+      if (i < NV)
+        yn[i] = __fmaf_rn(b76, k6[i],
+                          __fmaf_rn(b74, k4[i], __fmaf_rn(b73, k3[i], __fmaf_rn(b71, k1[i], y[i]))));
     err = 0.0f;
 #pragma unroll
-    for (int i = 0; i < NV; i++) {
-      float v = __fmaf_rn(f6, k6[i],
-                          __fmaf_rn(f5, k5[i], __fmaf_rn(f4, k4[i], __fmaf_rn(f3, k3[i], __fmul_rn(f1, k1[i])))));
-      float av = fabsf(__fmul_rn(v, iys[i]));
-      err = (err > av) ? err : av;
+    for (int i = 0; i < NVM; i++) {
+      if (i < NV) {
+        float v = __fmaf_rn(f6, k6[i], __fmaf_rn(f5, k5[i], __fmaf_rn(f4, k4[i],
+                                                                      __fmaf_rn(f3, k3[i], __fmul_rn(f1, k1[i])))));
+        float av = fabsf(__fmul_rn(v, iys[i]));
+        err = (err > av) ? err : av;
+      }
     }
     err = __fmul_rn(err, ck::inv_eps);
     nd += 5;
@@ -250,36 +281,33 @@ __device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmi
   else h = __fmul_rn(5.0f, h);
   if (!(h == h)) h = hmin;
 #pragma unroll
-  for (int i = 0; i < NV; i++) y[i] = yn[i];
+  for (int i = 0; i < NVM; i++)
+    if (i < NV) y[i] = yn[i];
   return nd;
 }
 
 // RK5 steps of neuron i from x towards tnow (src/rk5.h:161-174), each followed by the
-// model's ExternalUpdate.  Stops after `budget` steps (0: no limit); returns true when
-// the neuron reached the end of the time step.
-template <int MODEL, int P>
+// model's ExternalUpdate (src/aeif_cond_beta_multisynapse_kernel.h:190-226).  Consumes
+// one unit of `budget` per step when budget >= 0 and stops when it runs out; returns
+// true when the neuron reached the end of the time step.
+template <int MODEL, int PMAX, bool FIXED>
 __device__ __forceinline__ bool aeif_integrate(const AeifArgs &A, const SpikeOut &so, int i,
-                                               const AeifQ<MODEL, P> &q, float *y, float &refr,
-                                               double &x, float &h, long long tidx, double tnow,
-                                               int budget, unsigned long long &nd_acc) {
+                                               const AeifQ<MODEL, PMAX, FIXED> &q, float *y,
+                                               float &refr, double &x, float &h, long long tidx,
+                                               double tnow, int &budget, unsigned long long &nd) {
   const double x1 = tnow;
   bool end = false;
-  int guard = 0, steps = 0;
-  unsigned long long nd = 0;
+  int guard = 0;
   while (!end) {
-    if (budget > 0 && steps == budget) {
-      nd_acc += nd;
-      return false;
-    }
+    if (budget == 0) return false;
+    if (budget > 0) budget--;
     float hmax = (float)(x1 - x);
-    nd += rk5_step<MODEL, P>(x, y, h, A.hmin, A.hmin_acc, hmax, q, refr, so.status);
-    steps++;
+    nd += rk5_step(x, y, h, A.hmin, A.hmin_acc, hmax, q, refr, so.status);
     end = (x >= x1 - (double)A.hmin);
     if (++guard > ck::max_substeps) {
       atomicOr(so.status, ST_RK5_TRIALS);
       break;
     }
-    // ExternalUpdate (src/aeif_cond_beta_multisynapse_kernel.h:190-226)
     if (y[0] < -1.0e3f) {
       y[0] = q.V_reset;
       y[1] = 0.0f;
@@ -296,150 +324,146 @@ __device__ __forceinline__ bool aeif_integrate(const AeifArgs &A, const SpikeOut
       y[0] = q.V_reset;
       if (end) refr = __fsub_rn(refr, 1.0f);
     } else if (y[0] >= q.V_peak) {
-      push_spike(so, A.rec, A.i0 + i, i, 1.0f, tidx, tnow);
+      push_spike(so, A.srec, A.i0 + i, i, 1.0f, tidx, tnow);
       y[0] = q.V_reset;
       y[1] = __fadd_rn(y[1], q.b);
       refr = q.refr_steps;
     }
   }
-  nd_acc += nd;
   return true;
 }
 
-// One neuron, one step.  FLUSH: only fold the pending inputs.
-template <int MODEL, int P, bool FLUSH>
-__device__ __forceinline__ void aeif_neuron(const AeifArgs &A, const SpikeOut &so, int i,
-                                            long long tidx, double tnow, long long tidx_prev,
-                                            double t_prev, bool pending, int *strag_cnt,
-                                            unsigned long long &nd_acc) {
+// Records of the step (values after the update, before the fold).
+__device__ __forceinline__ void write_records(const GroupRecord &R, const SpikeOut &so, int node, int i,
+                                              const float *y, int nvar, float refr, long long row,
+                                              long long tidx) {
+  if (!R.first) return;
+  const int c0 = R.first[i], c1 = R.first[i + 1];
+  for (int c = c0; c < c1; c++) {
+    const int2 rc = R.col[c];
+    float v;
+    if (rc.x < 0) v = (so.has_out[node] && so.last_tidx[node] == (int)tidx) ? so.last_height[node] : 0.0f;
+    else if (rc.x == nvar) v = refr;
+    else v = y[rc.x];
+    R.buf[(size_t)row * R.ncol + rc.y] = v;
+  }
+}
+
+// End of step m: records, then the input fold (src/get_spike.cu:142-166) in FP64.
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ void aeif_end_step(const AeifArgs &A, const SpikeOut &so, int i,
+                                              const AeifQ<MODEL, PMAX, FIXED> &q, float *y, float refr,
+                                              int m, const StepT &t, long long rec_it0) {
   typedef AeifShape<MODEL> S;
-  constexpr int NV = 2 + S::npv * P;
-  const int n = A.n;
-  AeifQ<MODEL, P> q;
-  load_aeif_par<MODEL, P>(A, i, q);
-  float y[NV];
+  const int np = q.ports();
+  if (A.rec.first) write_records(A.rec, so, A.i0 + i, i, y, 2 + S::npv * np, refr, t.it - rec_it0, t.tidx);
+  double in[PMAX];
+  step_inputs(in, np, A.n, i, A.in, m, t.tidx, t.tnow);
 #pragma unroll
-  for (int v = 0; v < NV; v++) y[v] = A.var[(size_t)v * n + i];
-  if (pending) {
-    double in[P];
-    gather_inputs(in, P, n, i, A.acc, A.pin_off, A.pin, A.gen, A.lam_scale, A.seed, tidx_prev,
-                  t_prev);
-#pragma unroll
-    for (int p = 0; p < P; p++) {
-      if (in[p] != 0.0) {
-        const int iv = 2 + S::npv * p + S::in_var;
-        y[iv] = (float)__fma_rn(in[p], (double)q.pw[p], (double)y[iv]);
-      }
+  for (int p = 0; p < PMAX; p++) {
+    if (p < np && in[p] != 0.0) {
+      const int iv = 2 + S::npv * p + S::in_var;
+      y[iv] = (float)__fma_rn(in[p], (double)q.pw[p], (double)y[iv]);
     }
   }
-  if (FLUSH) {
-    if (pending) {
+}
+
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ void aeif_load(const AeifArgs &A, int i, float *y, float &refr, double &x,
+                                          float &h, int NV) {
+  constexpr int NVM = 2 + AeifShape<MODEL>::npv * PMAX;
 #pragma unroll
-      for (int p = 0; p < P; p++) {
-        const int iv = 2 + S::npv * p + S::in_var;
-        A.var[(size_t)iv * n + i] = y[iv];
-      }
-    }
-    return;
-  }
-  float refr = A.refr[i];
-  double x = A.x[i];
-  float h = A.h[i];
-  const bool done = aeif_integrate<MODEL, P>(A, so, i, q, y, refr, x, h, tidx, tnow, A.budget, nd_acc);
+  for (int v = 0; v < NVM; v++)
+    if (v < NV) y[v] = A.var[(size_t)v * A.n + i];
+  refr = A.refr[i];
+  x = A.x[i];
+  h = A.h[i];
+}
+
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ void aeif_store(const AeifArgs &A, int i, const float *y, float refr, double x,
+                                           float h, int NV) {
+  constexpr int NVM = 2 + AeifShape<MODEL>::npv * PMAX;
 #pragma unroll
-  for (int v = 0; v < NV; v++) A.var[(size_t)v * n + i] = y[v];
+  for (int v = 0; v < NVM; v++)
+    if (v < NV) A.var[(size_t)v * A.n + i] = y[v];
   A.refr[i] = refr;
   A.x[i] = x;
   A.h[i] = h;
-  if (!done) {
-    // more RK5 steps needed than the budget allows: the straggler kernel finishes it
-    int pos = atomicAdd(strag_cnt, 1);
-    A.strag_list[pos] = i;
-  }
 }
 
-// Step timing of an update/flush launch.  Update: step `it` integrates to tnow and
-// folds the inputs of step it-1.  Flush (after the last step of a call, when it0
-// was already advanced past it): folds the inputs of that last step.
-struct StepT {
-  long long it, tidx, tidx_prev;
-  double tnow, t_prev;
-};
-
-template <bool FLUSH>
-__device__ __forceinline__ StepT step_times(const Clock *c, int k, float dt) {
-  StepT s;
-  step_time(c, k, dt, s.it, s.tidx, s.tnow);
-  if (FLUSH) {
-    s.it -= 1;
-    s.tidx -= 1;
-    s.tnow = c->t0 + (double)dt * (double)(s.it + 1);
-    s.tidx_prev = s.tidx;
-    s.t_prev = s.tnow;
-  } else {
-    s.tidx_prev = s.tidx - 1;
-    s.t_prev = c->t0 + (double)dt * (double)s.it;
-  }
-  return s;
+__device__ __forceinline__ void warp_add(unsigned long long *ctr, unsigned long long v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr, v);
 }
 
-template <int MODEL, int P, bool FLUSH>
-__global__ void __launch_bounds__(128) aeif_update_kernel(const AeifArgs A, const SpikeOut so,
-                                                          Clock *clk, int k) {
-  const StepT t = step_times<FLUSH>(clk, k, A.dt);
-  const bool pending = clk->pending != 0;
+// Main aeif kernel: one thread per neuron, steps m = 0..M-1 of the batch.
+template <int MODEL, int PMAX, bool FIXED>
+__global__ void __launch_bounds__(128) aeif_batch_kernel(const AeifArgs A, const SpikeOut so,
+                                                         const Clock *clk, int k0, int M) {
+  typedef AeifShape<MODEL> S;
+  constexpr int NVM = 2 + S::npv * PMAX;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long nd = 0;
-  if (i < A.n)
-    aeif_neuron<MODEL, P, FLUSH>(A, so, i, t.tidx, t.tnow, t.tidx_prev, t.t_prev, pending,
-                                 A.strag_cnt + (t.it & 1), nd);
-  if (!FLUSH) {
-    // one counter update per warp
-    for (int o = 16; o > 0; o >>= 1) nd += __shfl_down_sync(0xffffffffu, nd, o);
-    if ((threadIdx.x & 31) == 0 && nd) atomicAdd(A.nderiv, nd);
+  if (i < A.n) {
+    AeifQ<MODEL, PMAX, FIXED> q;
+    load_aeif_par(A, i, q);
+    const int NV = 2 + S::npv * q.ports();
+    float y[NVM];
+    float refr, h;
+    double x;
+    aeif_load<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
+    const long long rec_it0 = clk->rec_it0;
+    int budget = A.budget > 0 ? A.budget : -1;
+    int m = 0;
+    bool deferred = false;
+    for (; m < M; m++) {
+      const StepT t = step_at(clk, k0, m, A.dt);
+      if (!aeif_integrate(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, budget, nd)) {
+        deferred = true;
+        break;
+      }
+      aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0);
+    }
+    aeif_store<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
+    if (deferred) {
+      const int pos = atomicAdd(A.strag_cnt, 1);
+      A.strag_list[pos] = make_int2(i, m);
+    }
   }
+  warp_add(A.nderiv, nd);
 }
 
-// Neurons that needed more RK5 steps than the main kernel's budget (typically the
-// few that spike in this step) finish here, packed densely into warps, so that their
-// long step sequences no longer stall 31 idle lanes each.  The list of step `it` is
-// indexed by its parity; the other parity's counter is cleared for the next step.
-template <int MODEL, int P>
+// Neurons the main kernel left unfinished (typically the few that spike in the batch)
+// continue here from the step where they stopped, one per thread.
+template <int MODEL, int PMAX, bool FIXED>
 __global__ void __launch_bounds__(128) aeif_straggler_kernel(const AeifArgs A, const SpikeOut so,
-                                                             Clock *clk, int k) {
-  constexpr int NV = 2 + AeifShape<MODEL>::npv * P;
-  const StepT t = step_times<false>(clk, k, A.dt);
-  const int par = (int)(t.it & 1);
-  const int cnt = A.strag_cnt[par];
-  if (blockIdx.x == 0 && threadIdx.x == 0) A.strag_cnt[par ^ 1] = 0;
+                                                             const Clock *clk, int k0, int M) {
+  typedef AeifShape<MODEL> S;
+  constexpr int NVM = 2 + S::npv * PMAX;
+  const int cnt = *A.strag_cnt;
+  const long long rec_it0 = clk->rec_it0;
   unsigned long long nd = 0;
-  const int n = A.n;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
-    const int i = A.strag_list[j];
-    AeifQ<MODEL, P> q;
-    load_aeif_par<MODEL, P>(A, i, q);
-    float y[NV];
-#pragma unroll
-    for (int v = 0; v < NV; v++) y[v] = A.var[(size_t)v * n + i];
-    float refr = A.refr[i];
-    double x = A.x[i];
-    float h = A.h[i];
-    aeif_integrate<MODEL, P>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, 0, nd);
-#pragma unroll
-    for (int v = 0; v < NV; v++) A.var[(size_t)v * n + i] = y[v];
-    A.refr[i] = refr;
-    A.x[i] = x;
-    A.h[i] = h;
+    const int2 e = A.strag_list[j];
+    const int i = e.x;
+    AeifQ<MODEL, PMAX, FIXED> q;
+    load_aeif_par(A, i, q);
+    const int NV = 2 + S::npv * q.ports();
+    float y[NVM];
+    float refr, h;
+    double x;
+    aeif_load<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
+    int budget = -1;
+    for (int m = e.y; m < M; m++) {
+      const StepT t = step_at(clk, k0, m, A.dt);
+      aeif_integrate(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, budget, nd);
+      aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0);
+    }
+    aeif_store<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
   }
-  for (int o = 16; o > 0; o >>= 1) nd += __shfl_down_sync(0xffffffffu, nd, o);
-  if ((threadIdx.x & 31) == 0 && nd) atomicAdd(A.nderiv, nd);
+  warp_add(A.nderiv, nd);
 }
-
-// Generic port count (P > MAX_TPL_PORT): ports handled with runtime loops over
-// MAX_PORT-sized arrays.  Same arithmetic, slower (local memory).
-template <int MODEL, bool FLUSH>
-__global__ void __launch_bounds__(128) aeif_update_kernel_gen(const AeifArgs A, const SpikeOut so,
-                                                              Clock *clk, int k);
 
 // ---------------------------------------------------------------------------
 // iaf_psc_exp exact propagator (src/iaf_psc_exp.cu:85-110)
@@ -449,42 +473,40 @@ __device__ __forceinline__ float iget(const IafArgs &A, int j, int i) {
   return p ? __ldg(p + i) : A.pval[j];
 }
 
-template <bool FLUSH>
-__global__ void __launch_bounds__(256) iaf_update_kernel(const IafArgs A, const SpikeOut so,
-                                                         Clock *clk, int k, float dt) {
-  const StepT t = step_times<FLUSH>(clk, k, dt);
-  const long long tidx = t.tidx;
-  const double tnow = t.tnow;
+__global__ void __launch_bounds__(256) iaf_batch_kernel(const IafArgs A, const SpikeOut so,
+                                                        const Clock *clk, int k0, int M) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
   const int n = A.n;
   float Iex = A.var[i], Iin = A.var[(size_t)n + i], V = A.var[2 * (size_t)n + i],
         refr = A.var[3 * (size_t)n + i];
-  if (clk->pending) {
+  const float I_e = iget(A, IP_I_e, i), P20 = iget(A, IP_P20, i), P21ex = iget(A, IP_P21ex, i),
+              P21in = iget(A, IP_P21in, i), P22 = iget(A, IP_P22, i), P11ex = iget(A, IP_P11ex, i),
+              P11in = iget(A, IP_P11in, i), theta = iget(A, IP_Theta_rel, i),
+              V_reset = iget(A, IP_V_reset_rel, i), refr_steps = iget(A, IP_refr_steps, i);
+  const long long rec_it0 = clk->rec_it0;
+  for (int m = 0; m < M; m++) {
+    const StepT t = step_at(clk, k0, m, A.dt);
+    if (refr > 0.0f) {
+      refr = __fsub_rn(refr, 1.0f);
+    } else {
+      V = __fmaf_rn(I_e, P20, __fmaf_rn(Iin, P21in, __fmaf_rn(Iex, P21ex, __fmul_rn(V, P22))));
+    }
+    Iex = __fmul_rn(Iex, P11ex);
+    Iin = __fmul_rn(Iin, P11in);
+    if (V >= theta) {
+      push_spike(so, A.srec, A.i0 + i, i, 1.0f, t.tidx, t.tnow);
+      V = V_reset;
+      refr = refr_steps;
+    }
+    if (A.rec.first) {
+      const float yr[4] = {Iex, Iin, V, refr};
+      write_records(A.rec, so, A.i0 + i, i, yr, 4, refr, t.it - rec_it0, t.tidx);
+    }
     double in[2];
-    gather_inputs(in, 2, n, i, A.acc, A.pin_off, A.pin, A.gen, A.lam_scale, A.seed, t.tidx_prev,
-                  t.t_prev);
+    step_inputs(in, 2, n, i, A.in, m, t.tidx, t.tnow);
     if (in[0] != 0.0) Iex = (float)__fma_rn(in[0], 1.0, (double)Iex);
     if (in[1] != 0.0) Iin = (float)__fma_rn(in[1], 1.0, (double)Iin);
-  }
-  if (FLUSH) {
-    A.var[i] = Iex;
-    A.var[(size_t)n + i] = Iin;
-    return;
-  }
-  if (refr > 0.0f) {
-    refr = __fsub_rn(refr, 1.0f);
-  } else {
-    V = __fmaf_rn(iget(A, IP_I_e, i), iget(A, IP_P20, i),
-                  __fmaf_rn(Iin, iget(A, IP_P21in, i),
-                            __fmaf_rn(Iex, iget(A, IP_P21ex, i), __fmul_rn(V, iget(A, IP_P22, i)))));
-  }
-  Iex = __fmul_rn(Iex, iget(A, IP_P11ex, i));
-  Iin = __fmul_rn(Iin, iget(A, IP_P11in, i));
-  if (V >= iget(A, IP_Theta_rel, i)) {
-    push_spike(so, A.rec, A.i0 + i, i, 1.0f, tidx, tnow);
-    V = iget(A, IP_V_reset_rel, i);
-    refr = iget(A, IP_refr_steps, i);
   }
   A.var[i] = Iex;
   A.var[(size_t)n + i] = Iin;
@@ -496,49 +518,55 @@ __global__ void __launch_bounds__(256) iaf_update_kernel(const IafArgs A, const 
 // spike_generator (src/spike_generator.cu:49-67): compares against the per-call
 // step counter, at most one spike per step.
 // ---------------------------------------------------------------------------
-__global__ void spike_gen_kernel(const SpikeGenArgs A, const SpikeOut so, Clock *clk, int k,
-                                 float dt) {
-  long long it, tidx;
-  double tnow;
-  step_time(clk, k, dt, it, tidx, tnow);
+__global__ void spike_gen_batch_kernel(const SpikeGenArgs A, const SpikeOut so, const Clock *clk, int k0,
+                                       int M) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
-  int e = A.off[i] + A.next[i];
-  if (e < A.off[i + 1] && (long long)A.tidx[e] == it) {
-    push_spike(so, A.rec, A.i0 + i, i, A.height[e], tidx, tnow);
-    A.next[i] += 1;
+  const int e0 = A.off[i], e1 = A.off[i + 1];
+  int nx = A.next[i];
+  const long long rec_it0 = clk->rec_it0;
+  for (int m = 0; m < M; m++) {
+    const StepT t = step_at(clk, k0, m, A.dt);
+    const int e = e0 + nx;
+    if (e < e1 && (long long)A.tidx[e] == t.it) {
+      push_spike(so, A.srec, A.i0 + i, i, A.height[e], t.tidx, t.tnow);
+      nx++;
+    }
+    if (A.rec.first) write_records(A.rec, so, A.i0 + i, i, nullptr, 0, 0.0f, t.it - rec_it0, t.tidx);
   }
+  A.next[i] = nx;
 }
 
 // ---------------------------------------------------------------------------
-// Delivery: ring slots of the last dspan steps -> CSR segments -> FP64 atomics.
-// One warp per (source, delay) event, lanes stride over the segment.
+// Delivery of the spikes arriving during a batch.  Work items are (emission step,
+// spike, delay group) with arrival step in the batch; one warp per item streams
+// the item's CSR segment with coalesced 8-byte loads and FP64 atomics into the
+// accumulator slot of the arrival step.
 // ---------------------------------------------------------------------------
 constexpr int DELIVER_THREADS = 256;
-constexpr int MAX_DSPAN = 8192;
+constexpr int MAX_PAIRS = 8192;     // dspan * M
 
-__global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(const DeliverArgs A, Clock *clk,
-                                                                  int k, float dt) {
-  extern __shared__ int s_pref[];   // dspan + 1 prefix sums
+__global__ void __launch_bounds__(DELIVER_THREADS) deliver_batch_kernel(const DeliverArgs A,
+                                                                        const Clock *clk, int k0, int M) {
+  extern __shared__ int s_pref[];   // npairs + 1 prefix sums over (delay group, arrival step)
   typedef cub::BlockScan<int, DELIVER_THREADS> Scan;
   __shared__ typename Scan::TempStorage scan_tmp;
-  long long it, tidx;
-  double tnow;
-  step_time(clk, k, dt, it, tidx, tnow);
-  const int dspan = A.dspan;
-  const int per = (dspan + DELIVER_THREADS - 1) / DELIVER_THREADS;
+  const long long t_first = clk->tidx_base + clk->it0 + k0 + 1;   // time index of step 0
+  const int npairs = A.dspan * M;
+  const int per = (npairs + DELIVER_THREADS - 1) / DELIVER_THREADS;
   int local = 0;
   const int b0 = threadIdx.x * per;
   for (int j = 0; j < per; j++) {
-    int dd = b0 + j;
-    if (dd < dspan) {
-      long long ts = tidx - 1 - (A.dmin + dd);
+    const int pr = b0 + j;
+    if (pr < npairs) {
+      const int dd = pr / M, m = pr - dd * M;
+      const long long te = t_first + m - 1 - (A.dmin + dd);   // emission step
       int c = 0;
-      if (ts >= 0) {
-        c = A.ring_cnt[(int)(ts % A.R)];
+      if (te >= 1) {
+        c = A.ring_cnt[(int)(te % A.R)];
         c = c < A.cap ? c : A.cap;
       }
-      s_pref[dd + 1] = c;
+      s_pref[pr + 1] = c;
       local += c;
     }
   }
@@ -546,341 +574,112 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_kernel(const DeliverA
   Scan(scan_tmp).ExclusiveSum(local, excl);
   __syncthreads();
   for (int j = 0; j < per; j++) {
-    int dd = b0 + j;
-    if (dd < dspan) {
-      excl += s_pref[dd + 1];
-      s_pref[dd + 1] = excl;
+    const int pr = b0 + j;
+    if (pr < npairs) {
+      excl += s_pref[pr + 1];
+      s_pref[pr + 1] = excl;
     }
   }
   if (threadIdx.x == 0) s_pref[0] = 0;
   __syncthreads();
-  const int total = s_pref[dspan];
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    // slot tidx+1 was last read two steps ago (R >= dmax + 3): reset for the next step
-    A.ring_cnt[(int)((tidx + 1) % A.R)] = 0;
-    clk->pending = 1;
+  const int total = s_pref[npairs];
+  if (blockIdx.x == 0) {
+    // ring slots of this batch's steps start empty (their previous steps are older than
+    // any emission step read here because R >= M + dmax + 3); straggler lists start empty
+    for (int m = threadIdx.x; m < M; m += blockDim.x) A.ring_cnt[(int)((t_first + m) % A.R)] = 0;
+    for (int g = threadIdx.x; g < A.n_strag; g += blockDim.x) A.strag_cnt[g] = 0;
   }
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * DELIVER_THREADS + threadIdx.x) >> 5;
   const int nwarp = (gridDim.x * DELIVER_THREADS) >> 5;
   unsigned long long nev = 0;
   for (int item = warp; item < total; item += nwarp) {
-    int lo = 0, hi = dspan;   // find dd with s_pref[dd] <= item < s_pref[dd+1]
+    int lo = 0, hi = npairs;   // pair with s_pref[pr] <= item < s_pref[pr+1]
     while (hi - lo > 1) {
-      int mid = (lo + hi) >> 1;
+      const int mid = (lo + hi) >> 1;
       if (s_pref[mid] <= item) lo = mid; else hi = mid;
     }
-    const int dd = lo;
-    const int j = item - s_pref[dd];
-    const long long ts = tidx - 1 - (A.dmin + dd);
-    const int2 sp = A.ring[(size_t)(ts % A.R) * A.cap + j];
+    const int dd = lo / M, m = lo - dd * M;
+    const int j = item - s_pref[lo];
+    const long long te = t_first + m - 1 - (A.dmin + dd);
+    const int2 sp = A.ring[(size_t)(te % A.R) * A.cap + j];
     const float height = __int_as_float(sp.y);
-    const size_t key = (size_t)sp.x * dspan + dd;
+    const size_t key = (size_t)sp.x * A.dspan + dd;
     const long long e0 = A.ev_off[key], e1 = A.ev_off[key + 1];
+    double *acc = A.acc + (size_t)m * A.slot_stride;
     for (long long e = e0 + lane; e < e1; e += 32) {
       const EdgeW ew = A.edge[e];
-      atomicAdd(&A.acc[ew.acc], (double)__fmul_rn(height, ew.w));
+      atomicAdd(&acc[ew.acc], (double)__fmul_rn(height, ew.w));
     }
     nev += (unsigned long long)(e1 - e0);
   }
   if (lane == 0 && nev) atomicAdd(A.n_events, nev);
 }
 
-// ---------------------------------------------------------------------------
-// Records (src/multimeter.cu:76-110): one row per step into a device buffer.
-// ---------------------------------------------------------------------------
-__global__ void record_kernel(const RecCol *cols, int ncol, float *buf, const int *last_tidx,
-                              const float *last_height, const unsigned char *has_out, Clock *clk,
-                              int k, float dt) {
-  long long it, tidx;
-  double tnow;
-  step_time(clk, k, dt, it, tidx, tnow);
-  const long long row = it - clk->rec_it0;
-  float *r = buf + (size_t)row * (ncol + 1);
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c == 0) r[0] = (float)tnow;
-  if (c < ncol) {
-    RecCol rc = cols[c];
-    float v;
-    if (rc.ptr) v = *rc.ptr;
-    else v = (has_out[rc.node] && last_tidx[rc.node] == (int)tidx) ? last_height[rc.node] : 0.0f;
-    r[c + 1] = v;
-  }
-}
-
 __global__ void clock_advance_kernel(Clock *clk, int K) { clk->it0 += K; }
 
-__global__ void clock_clear_pending_kernel(Clock *clk) { clk->pending = 0; }
-
 // ---------------------------------------------------------------------------
-// Generic-port aeif kernel
+// Host-side launchers.  Each returns the number of kernels it launched.
 // ---------------------------------------------------------------------------
-template <int MODEL>
-__device__ __forceinline__ void aeif_derivs_gen(const float *y, float *dy, const float *sp,
-                                                const float *E_rev, const float *it1,
-                                                const float *it2, int P, float refr) {
-  typedef AeifShape<MODEL> S;
-  const float V = (refr > 0.0f) ? sp[AP_V_reset] : ((y[0] < sp[AP_V_peak]) ? y[0] : sp[AP_V_peak]);
-  const float w = y[1];
-  float I = 0.0f;
-  for (int i = 0; i < P; i++) {
-    if (S::cond) I = __fmaf_rn(y[2 + 2 * i], __fsub_rn(E_rev[i], V), I);
-    else I = __fadd_rn(I, y[2 + S::npv * i]);
-  }
-  float Vs;
-  if (!S::cond && sp[AP_Delta_T] == 0.0f) Vs = 0.0f;
-  else Vs = __fmul_rn(sp[AP_Delta_T], exp_m(__fmul_rn(__fsub_rn(V, sp[AP_V_th]), sp[AP_inv_Delta_T])));
-  float s = __fmaf_rn(-sp[AP_g_L], __fsub_rn(__fsub_rn(V, sp[AP_E_L]), Vs), I);
-  s = __fsub_rn(s, w);
-  s = __fadd_rn(s, sp[AP_I_e]);
-  dy[0] = (refr > 0.0f) ? 0.0f : __fmul_rn(s, sp[AP_inv_C_m]);
-  dy[1] = __fmul_rn(__fmaf_rn(sp[AP_a], __fsub_rn(V, sp[AP_E_L]), -w), sp[AP_inv_tau_w]);
-  for (int i = 0; i < P; i++) {
-    if (MODEL == M_AEIF_PSC_EXP) {
-      dy[2 + i] = __fmul_rn(-y[2 + i], it1[i]);
-    } else {
-      dy[3 + 2 * i] = __fmul_rn(-y[3 + 2 * i], it1[i]);
-      dy[2 + 2 * i] = __fmaf_rn(-y[2 + 2 * i], it2[i], y[3 + 2 * i]);
-    }
-  }
-}
-
-template <int MODEL, bool FLUSH>
-__global__ void __launch_bounds__(128) aeif_update_kernel_gen(const AeifArgs A, const SpikeOut so,
-                                                              Clock *clk, int k) {
-  typedef AeifShape<MODEL> S;
-  constexpr int NVM = 2 + 2 * MAX_PORT;
-  const StepT t = step_times<FLUSH>(clk, k, A.dt);
-  const long long tidx = t.tidx;
-  const double tnow = t.tnow;
-  const bool pending = clk->pending != 0;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long nd = 0;
-  if (i < A.n) {
-    const int n = A.n, P = A.nport, NV = A.nvar;
-    float sp[AEIF_NSCAL], E_rev[MAX_PORT], it1[MAX_PORT], it2[MAX_PORT], pw[MAX_PORT];
-    for (int j = 0; j < AEIF_NSCAL; j++) sp[j] = pget(A, j, i);
-    for (int p = 0; p < P; p++) {
-      const int b = AEIF_NSCAL + AEIF_NPORTPAR * p;
-      E_rev[p] = pget(A, b, i);
-      it1[p] = pget(A, b + 1, i);
-      it2[p] = pget(A, b + 2, i);
-      pw[p] = pget(A, b + 3, i);
-    }
-    float y[NVM];
-    for (int v = 0; v < NV; v++) y[v] = A.var[(size_t)v * n + i];
-    if (pending) {
-      double in[MAX_PORT];
-      gather_inputs(in, P, n, i, A.acc, A.pin_off, A.pin, A.gen, A.lam_scale, A.seed, t.tidx_prev,
-                    t.t_prev);
-      for (int p = 0; p < P; p++) {
-        if (in[p] != 0.0) {
-          const int iv = 2 + S::npv * p + S::in_var;
-          y[iv] = (float)__fma_rn(in[p], (double)pw[p], (double)y[iv]);
-          if (FLUSH) A.var[(size_t)iv * n + i] = y[iv];
-        }
-      }
-    }
-    if (!FLUSH) {
-      float refr = A.refr[i];
-      double x = A.x[i];
-      float h = A.h[i];
-      const double x1 = tnow;
-      bool end = false;
-      int guard = 0;
-      while (!end) {
-        float hmax = (float)(x1 - x);
-        // --- RK5 step with runtime port count
-        float k1[NVM], k2[NVM], k3[NVM], k4[NVM], k5[NVM], k6[NVM], yn[NVM], iys[NVM];
-        aeif_derivs_gen<MODEL>(y, k1, sp, E_rev, it1, it2, P, refr);
-        for (int v = 0; v < NV; v++) {
-          float ys = __fadd_rn(__fadd_rn(fabsf(y[v]), fabsf(__fmul_rn(k1[v], h))), ck::scal_min);
-          iys[v] = __fdiv_rn(1.0f, ys);
-        }
-        int trials = 0;
-        float err;
-        nd += 1;
-        for (;;) {
-          if (h > hmax) h = hmax;
-          if (h < A.hmin) h = A.hmin;
-          const float b21 = __fmul_rn(h, ck::a21), b31 = __fmul_rn(h, ck::a31), b32 = __fmul_rn(h, ck::a32),
-                      b41 = __fmul_rn(h, ck::a41), b42 = __fmul_rn(h, ck::a42), b43 = __fmul_rn(h, ck::a43),
-                      b51 = __fmul_rn(h, ck::a51), b52 = __fmul_rn(h, ck::a52), b53 = __fmul_rn(h, ck::a53),
-                      b54 = __fmul_rn(h, ck::a54), b61 = __fmul_rn(h, ck::a61), b62 = __fmul_rn(h, ck::a62),
-                      b63 = __fmul_rn(h, ck::a63), b64 = __fmul_rn(h, ck::a64), b65 = __fmul_rn(h, ck::a65),
-                      b71 = __fmul_rn(h, ck::a71), b73 = __fmul_rn(h, ck::a73), b74 = __fmul_rn(h, ck::a74),
-                      b76 = __fmul_rn(h, ck::a76), f1 = __fmul_rn(h, ck::e1), f3 = __fmul_rn(h, ck::e3),
-                      f4 = __fmul_rn(h, ck::e4), f5 = __fmul_rn(h, ck::e5), f6 = __fmul_rn(h, ck::e6);
-          for (int v = 0; v < NV; v++) yn[v] = __fmaf_rn(b21, k1[v], y[v]);
-          aeif_derivs_gen<MODEL>(yn, k2, sp, E_rev, it1, it2, P, refr);
-          for (int v = 0; v < NV; v++) yn[v] = __fmaf_rn(b32, k2[v], __fmaf_rn(b31, k1[v], y[v]));
-          aeif_derivs_gen<MODEL>(yn, k3, sp, E_rev, it1, it2, P, refr);
-          for (int v = 0; v < NV; v++)
-            yn[v] = __fmaf_rn(b43, k3[v], __fmaf_rn(b42, k2[v], __fmaf_rn(b41, k1[v], y[v])));
-          aeif_derivs_gen<MODEL>(yn, k4, sp, E_rev, it1, it2, P, refr);
-          for (int v = 0; v < NV; v++)
-            yn[v] = __fmaf_rn(b54, k4[v], __fmaf_rn(b53, k3[v], __fmaf_rn(b52, k2[v], __fmaf_rn(b51, k1[v], y[v]))));
-          aeif_derivs_gen<MODEL>(yn, k5, sp, E_rev, it1, it2, P, refr);
-          for (int v = 0; v < NV; v++)
-            yn[v] = __fmaf_rn(b65, k5[v], __fmaf_rn(b64, k4[v], __fmaf_rn(b63, k3[v],
-                              __fmaf_rn(b62, k2[v], __fmaf_rn(b61, k1[v], y[v])))));
-          aeif_derivs_gen<MODEL>(yn, k6, sp, E_rev, it1, it2, P, refr);
-          for (int v = 0; v < NV; v++)
-            yn[v] = __fmaf_rn(b76, k6[v], __fmaf_rn(b74, k4[v], __fmaf_rn(b73, k3[v], __fmaf_rn(b71, k1[v], y[v]))));
-          err = 0.0f;
-          for (int v = 0; v < NV; v++) {
-            float e = __fmaf_rn(f6, k6[v], __fmaf_rn(f5, k5[v], __fmaf_rn(f4, k4[v],
-                                __fmaf_rn(f3, k3[v], __fmul_rn(f1, k1[v])))));
-            float av = fabsf(__fmul_rn(e, iys[v]));
-            err = (err > av) ? err : av;
-          }
-          err = __fmul_rn(err, ck::inv_eps);
-          nd += 5;
-          trials++;
-          if (err <= 1.0f || h <= A.hmin_acc) break;
-          if (trials >= ck::max_trials) {
-            atomicOr(so.status, ST_RK5_TRIALS);
-            break;
-          }
-          float hnew = __fmul_rn(__fmul_rn(h, ck::coeff), __fdiv_rn(1.0f, __fsqrt_rn(__fsqrt_rn(err))));
-          float h01 = __fmul_rn(0.1f, h);
-          h = (hnew > h01) ? hnew : h01;
-        }
-        x += (double)h;
-        if (err > ck::err_min) h = __fmul_rn(__fmul_rn(h, ck::coeff), exp_m(__fmul_rn(-0.2f, log_m(err))));
-        else h = __fmul_rn(5.0f, h);
-        if (!(h == h)) h = A.hmin;
-        for (int v = 0; v < NV; v++) y[v] = yn[v];
-        // --- end of step
-        end = (x >= x1 - (double)A.hmin);
-        if (++guard > ck::max_substeps) {
-          atomicOr(so.status, ST_RK5_TRIALS);
-          break;
-        }
-        if (y[0] < -1.0e3f) {
-          y[0] = sp[AP_V_reset];
-          y[1] = 0.0f;
-          atomicOr(so.status, ST_NUMERIC);
-          continue;
-        }
-        if (y[1] < -1.0e6f || y[1] > 1.0e6f) {
-          y[0] = sp[AP_V_reset];
-          y[1] = 0.0f;
-          atomicOr(so.status, ST_NUMERIC);
-          continue;
-        }
-        if (refr > 0.0f) {
-          y[0] = sp[AP_V_reset];
-          if (end) refr = __fsub_rn(refr, 1.0f);
-        } else if (y[0] >= sp[AP_V_peak]) {
-          push_spike(so, A.rec, A.i0 + i, i, 1.0f, tidx, tnow);
-          y[0] = sp[AP_V_reset];
-          y[1] = __fadd_rn(y[1], sp[AP_b]);
-          refr = sp[AP_refr_steps];
-        }
-      }
-      for (int v = 0; v < NV; v++) A.var[(size_t)v * n + i] = y[v];
-      A.refr[i] = refr;
-      A.x[i] = x;
-      A.h[i] = h;
-    }
-  }
-  if (!FLUSH) {
-    for (int o = 16; o > 0; o >>= 1) nd += __shfl_down_sync(0xffffffffu, nd, o);
-    if ((threadIdx.x & 31) == 0 && nd) atomicAdd(A.nderiv, nd);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Host-side launchers
-// ---------------------------------------------------------------------------
-template <int MODEL, bool FLUSH>
-static int launch_aeif_model(const AeifArgs &A, const SpikeOut &so, Clock *clk, int k,
-                             cudaStream_t st) {
+template <int MODEL, int PMAX, bool FIXED>
+static int launch_aeif_p(const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
+                         cudaStream_t st) {
   dim3 grid((A.n + 127) / 128), block(128);
-  dim3 sgrid(std::min((A.n + 127) / 128, 148 * 2));
-  const bool strag = !FLUSH && A.budget > 0;
-  switch (A.nport) {
-  case 1:
-    aeif_update_kernel<MODEL, 1, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k);
-    if (strag) aeif_straggler_kernel<MODEL, 1><<<sgrid, block, 0, st>>>(A, so, clk, k);
-    break;
-  case 2:
-    aeif_update_kernel<MODEL, 2, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k);
-    if (strag) aeif_straggler_kernel<MODEL, 2><<<sgrid, block, 0, st>>>(A, so, clk, k);
-    break;
-  case 3:
-    aeif_update_kernel<MODEL, 3, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k);
-    if (strag) aeif_straggler_kernel<MODEL, 3><<<sgrid, block, 0, st>>>(A, so, clk, k);
-    break;
-  case 4:
-    aeif_update_kernel<MODEL, 4, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k);
-    if (strag) aeif_straggler_kernel<MODEL, 4><<<sgrid, block, 0, st>>>(A, so, clk, k);
-    break;
-  default:
-    aeif_update_kernel_gen<MODEL, FLUSH><<<grid, block, 0, st>>>(A, so, clk, k);
-    return 1;
-  }
-  return strag ? 2 : 1;
+  aeif_batch_kernel<MODEL, PMAX, FIXED><<<grid, block, 0, st>>>(A, so, clk, k0, M);
+  if (A.budget <= 0) return 1;
+  dim3 sgrid(std::max(1, std::min((A.n + 127) / 128, 148 * 4)));
+  aeif_straggler_kernel<MODEL, PMAX, FIXED><<<sgrid, block, 0, st>>>(A, so, clk, k0, M);
+  return 2;
 }
 
-// Returns the number of kernels launched.
-int launch_aeif(int model, bool flush, const AeifArgs &A, const SpikeOut &so, Clock *clk, int k,
+template <int MODEL>
+static int launch_aeif_m(const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
+                         cudaStream_t st) {
+  switch (A.nport) {
+  case 1: return launch_aeif_p<MODEL, 1, true>(A, so, clk, k0, M, st);
+  case 2: return launch_aeif_p<MODEL, 2, true>(A, so, clk, k0, M, st);
+  case 3: return launch_aeif_p<MODEL, 3, true>(A, so, clk, k0, M, st);
+  case 4: return launch_aeif_p<MODEL, 4, true>(A, so, clk, k0, M, st);
+  default: return launch_aeif_p<MODEL, MAX_PORT, false>(A, so, clk, k0, M, st);
+  }
+}
+
+int launch_aeif(int model, const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                 cudaStream_t st) {
   if (A.n <= 0) return 0;
-  if (flush) {
-    switch (model) {
-    case M_AEIF_COND_BETA: return launch_aeif_model<M_AEIF_COND_BETA, true>(A, so, clk, k, st);
-    case M_AEIF_COND_ALPHA: return launch_aeif_model<M_AEIF_COND_ALPHA, true>(A, so, clk, k, st);
-    case M_AEIF_PSC_EXP: return launch_aeif_model<M_AEIF_PSC_EXP, true>(A, so, clk, k, st);
-    case M_AEIF_PSC_ALPHA: return launch_aeif_model<M_AEIF_PSC_ALPHA, true>(A, so, clk, k, st);
-    }
-  } else {
-    switch (model) {
-    case M_AEIF_COND_BETA: return launch_aeif_model<M_AEIF_COND_BETA, false>(A, so, clk, k, st);
-    case M_AEIF_COND_ALPHA: return launch_aeif_model<M_AEIF_COND_ALPHA, false>(A, so, clk, k, st);
-    case M_AEIF_PSC_EXP: return launch_aeif_model<M_AEIF_PSC_EXP, false>(A, so, clk, k, st);
-    case M_AEIF_PSC_ALPHA: return launch_aeif_model<M_AEIF_PSC_ALPHA, false>(A, so, clk, k, st);
-    }
+  switch (model) {
+  case M_AEIF_COND_BETA: return launch_aeif_m<M_AEIF_COND_BETA>(A, so, clk, k0, M, st);
+  case M_AEIF_COND_ALPHA: return launch_aeif_m<M_AEIF_COND_ALPHA>(A, so, clk, k0, M, st);
+  case M_AEIF_PSC_EXP: return launch_aeif_m<M_AEIF_PSC_EXP>(A, so, clk, k0, M, st);
+  case M_AEIF_PSC_ALPHA: return launch_aeif_m<M_AEIF_PSC_ALPHA>(A, so, clk, k0, M, st);
   }
   return 0;
 }
 
-void launch_iaf(bool flush, const IafArgs &A, const SpikeOut &so, Clock *clk, int k, float dt,
-                cudaStream_t st) {
-  if (A.n <= 0) return;
-  dim3 grid((A.n + 255) / 256), block(256);
-  if (flush) iaf_update_kernel<true><<<grid, block, 0, st>>>(A, so, clk, k, dt);
-  else iaf_update_kernel<false><<<grid, block, 0, st>>>(A, so, clk, k, dt);
+int launch_iaf(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
+  if (A.n <= 0) return 0;
+  iaf_batch_kernel<<<(A.n + 255) / 256, 256, 0, st>>>(A, so, clk, k0, M);
+  return 1;
 }
 
-void launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, Clock *clk, int k, float dt,
-                      cudaStream_t st) {
-  if (A.n <= 0) return;
-  spike_gen_kernel<<<(A.n + 255) / 256, 256, 0, st>>>(A, so, clk, k, dt);
+int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
+                     cudaStream_t st) {
+  if (A.n <= 0) return 0;
+  spike_gen_batch_kernel<<<(A.n + 255) / 256, 256, 0, st>>>(A, so, clk, k0, M);
+  return 1;
 }
 
-void launch_deliver(const DeliverArgs &A, int n_blocks, Clock *clk, int k, float dt, cudaStream_t st) {
-  size_t smem = (size_t)(A.dspan + 1) * sizeof(int);
-  deliver_kernel<<<n_blocks, DELIVER_THREADS, smem, st>>>(A, clk, k, dt);
+int launch_deliver(const DeliverArgs &A, int n_blocks, const Clock *clk, int k0, int M, cudaStream_t st) {
+  const size_t smem = (size_t)(A.dspan * M + 1) * sizeof(int);
+  deliver_batch_kernel<<<n_blocks, DELIVER_THREADS, smem, st>>>(A, clk, k0, M);
+  return 1;
 }
 
-void launch_record(const RecCol *cols, int ncol, float *buf, const int *last_tidx,
-                   const float *last_height, const unsigned char *has_out, Clock *clk, int k,
-                   float dt, cudaStream_t st) {
-  int nb = (ncol + 127) / 128;
-  if (nb < 1) nb = 1;
-  record_kernel<<<nb, 128, 0, st>>>(cols, ncol, buf, last_tidx, last_height, has_out, clk, k, dt);
-}
-
-void launch_clock_advance(Clock *clk, int K, cudaStream_t st) {
+int launch_clock_advance(Clock *clk, int K, cudaStream_t st) {
   clock_advance_kernel<<<1, 1, 0, st>>>(clk, K);
+  return 1;
 }
 
-void launch_clock_clear_pending(Clock *clk, cudaStream_t st) {
-  clock_clear_pending_kernel<<<1, 1, 0, st>>>(clk);
-}
-
-int deliver_max_dspan() { return MAX_DSPAN; }
+int deliver_max_pairs() { return MAX_PAIRS; }
 
 }  // namespace ngpu

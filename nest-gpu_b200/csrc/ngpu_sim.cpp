@@ -143,8 +143,6 @@ void Engine::calibrate() {
   }
   if (acc_total >= (1ULL << 32)) throw NgpuError("input accumulator exceeds 2^32 entries");
   n_acc_ = acc_total;
-  d_acc_ = dalloc<double>(n_acc_);
-  cuda_check(cudaMemsetAsync(d_acc_, 0, std::max<size_t>(n_acc_, 1) * sizeof(double), stream_), "memset");
 
   // ---- connections: recurrent edges into CSR by (source, delay); poiss_gen edges apart
   build_order();   // reference order: the canonical numbering of poiss_gen edges
@@ -189,8 +187,8 @@ void Engine::calibrate() {
   if (n_rec_edges == 0 && gblocks.empty()) { dmin = 0; dmax = 0; }
   dmin_ = dmin;
   dspan_ = dmax - dmin + 1;
-  if (dspan_ > deliver_max_dspan())
-    throw NgpuError("delay range exceeds " + std::to_string(deliver_max_dspan()) + " time steps");
+  if (dspan_ > deliver_max_pairs())
+    throw NgpuError("delay range exceeds " + std::to_string(deliver_max_pairs()) + " time steps");
   d_has_out_ = dalloc<unsigned char>(N);
   {
     // host edges: per-key counts and each edge's rank inside its (source, delay) segment,
@@ -281,8 +279,16 @@ void Engine::calibrate() {
     }
   }
 
+  // ---- time batching: M steps per batch, M <= min delay in steps (spikes emitted inside
+  //      a batch arrive after it); one accumulator slot per step of a batch
+  batch_ = (n_rec_edges || !gblocks.empty()) ? std::min(dmin_ + 1, MAX_BATCH) : MAX_BATCH;
+  batch_ = std::max(1, std::min(batch_, batch_max));
+  if (dspan_ * batch_ > deliver_max_pairs()) batch_ = std::max(1, deliver_max_pairs() / dspan_);
+  d_acc_ = dalloc<double>(n_acc_ * batch_);
+  cuda_check(cudaMemset(d_acc_, 0, std::max<size_t>(n_acc_ * batch_, 1) * sizeof(double)), "memset");
+
   // ---- spike ring and per-node spike state
-  R_ = (dmin_ + dspan_ - 1) + 3;
+  R_ = (dmin_ + dspan_ - 1) + batch_ + 3;
   cap_ = (int)std::min<long long>((long long)n_src_out * std::max(1.0f, max_spike_num_fact) + 1024, 1LL << 30);
   d_ring_ = dalloc<int2>((size_t)R_ * cap_);
   d_ring_cnt_ = dalloc<int>(R_);
@@ -309,9 +315,8 @@ void Engine::calibrate() {
                               cudaMemcpyHostToDevice), "var");
     }
     if (is_aeif(g.model)) {
-      g.d_strag = dalloc<int>(g.n);
-      g.d_strag_cnt = dalloc<int>(2);
-      cuda_check(cudaMemset(g.d_strag_cnt, 0, 2 * sizeof(int)), "strag");
+      g.d_strag = dalloc<int2>(g.n);
+      g.strag_slot = n_strag_++;
       g.d_refr = dalloc<float>(g.n);
       cuda_check(cudaMemcpy(g.d_refr, g.par[A_refractory_step].data(), g.n * sizeof(float),
                             cudaMemcpyHostToDevice), "refr");
@@ -364,6 +369,8 @@ void Engine::calibrate() {
       cuda_check(cudaMemset(g.d_sg_next, 0, g.n * sizeof(int)), "sg");
     }
   }
+  d_strag_cnt_ = dalloc<int>(std::max(1, n_strag_));
+  cuda_check(cudaMemset(d_strag_cnt_, 0, std::max(1, n_strag_) * sizeof(int)), "strag");
   build_records();
   cuda_check(cudaDeviceSynchronize(), "calibrate");
 }
@@ -471,39 +478,53 @@ void Engine::upload_params() {
   if (any) invalidate_graphs();
 }
 
+// Record columns: per group a CSR over its neurons of {variable code, column}; the
+// update kernels write them into a [rows][ncol] window buffer, the host adds the time.
 void Engine::build_records() {
-  std::vector<RecCol> cols;
-  rec_cols_.clear();
+  rec_ncol_ = 0;
+  std::vector<std::vector<std::vector<int2>>> per(groups_.size());
   for (size_t r = 0; r < records_.size(); r++) {
     RecordSpec &rs = records_[r];
     for (size_t c = 0; c < rs.var.size(); c++) {
-      RecCol rc{nullptr, rs.node[c], 0};
+      const int gi = group_index(rs.node[c]);
+      Group &g = groups_[gi];
+      const int rel = rs.node[c] - g.i0;
+      int code = -1;
       if (rs.var[c] != "spike") {
-        Group &g = group_of(rs.node[c]);
         int idx;
         Kind k = locate(rs.node[c], rs.var[c], &idx);
-        int rel = rs.node[c] - g.i0;
         if (is_aeif(g.model)) {
-          if (k == K_SCAL_VAR) rc.ptr = g.d_var + (size_t)idx * g.n + rel;
-          else if (k == K_PORT_VAR)
-            rc.ptr = g.d_var + (size_t)(2 + n_port_var(g.model) * rs.port[c] + idx) * g.n + rel;
-          else rc.ptr = g.d_refr + rel;
+          const int nvar = 2 + n_port_var(g.model) * g.nport;
+          if (k == K_SCAL_VAR) code = idx;
+          else if (k == K_PORT_VAR) code = 2 + n_port_var(g.model) * rs.port[c] + idx;
+          else code = nvar;   // refractory counter
         } else {
-          rc.ptr = g.d_var + (size_t)idx * g.n + rel;
+          code = idx;
         }
       }
-      cols.push_back(rc);
-      rec_cols_.push_back({(int)r, (int)c});
+      if (per[gi].empty()) per[gi].resize(g.n);
+      per[gi][rel].push_back(make_int2(code, rec_ncol_));
+      rec_ncol_++;
     }
     if (!rs.file.empty()) {
       rs.fp = fopen(rs.file.c_str(), "w");
       if (!rs.fp) throw NgpuError("cannot open record file " + rs.file);
     }
   }
-  rec_ncol_ = (int)cols.size();
-  if (rec_ncol_) {
-    d_cols_ = dalloc<RecCol>(cols.size());
-    cuda_check(cudaMemcpy(d_cols_, cols.data(), cols.size() * sizeof(RecCol), cudaMemcpyHostToDevice), "rec");
+  for (size_t gi = 0; gi < groups_.size(); gi++) {
+    if (per[gi].empty()) continue;
+    Group &g = groups_[gi];
+    std::vector<int> first(g.n + 1, 0);
+    std::vector<int2> cols;
+    for (int i = 0; i < g.n; i++) {
+      first[i] = (int)cols.size();
+      cols.insert(cols.end(), per[gi][i].begin(), per[gi][i].end());
+    }
+    first[g.n] = (int)cols.size();
+    g.d_rec_first = dalloc<int>(g.n + 1);
+    g.d_rec_col = dalloc<int2>(cols.size());
+    cuda_check(cudaMemcpy(g.d_rec_first, first.data(), (g.n + 1) * sizeof(int), cudaMemcpyHostToDevice), "rec");
+    cuda_check(cudaMemcpy(g.d_rec_col, cols.data(), cols.size() * sizeof(int2), cudaMemcpyHostToDevice), "rec");
   }
 }
 
@@ -533,6 +554,28 @@ static GroupSpikeRec spike_rec(Group &g) {
   return r;
 }
 
+GroupRecord Engine::group_record(Group &g) {
+  GroupRecord r;
+  r.first = g.d_rec_first;
+  r.col = g.d_rec_col;
+  r.buf = d_recbuf_;
+  r.ncol = rec_ncol_;
+  if (!d_recbuf_) r.first = nullptr;
+  return r;
+}
+
+GroupInput Engine::group_input(Group &g) {
+  GroupInput in;
+  in.acc = d_acc_ + g.acc_off;
+  in.slot_stride = n_acc_;
+  in.pin_off = g.d_pin_off;
+  in.pin = g.d_pin;
+  in.gen = d_gen_;
+  in.lam_scale = (float)(dt / 1000.0);
+  in.seed = kernel_seed;
+  return in;
+}
+
 AeifArgs Engine::aeif_args(Group &g) {
   AeifArgs A;
   std::memset(&A, 0, sizeof(A));
@@ -544,20 +587,16 @@ AeifArgs Engine::aeif_args(Group &g) {
   A.refr = g.d_refr;
   A.x = g.d_x;
   A.h = g.d_h;
-  A.acc = d_acc_ + g.acc_off;
-  A.pin_off = g.d_pin_off;
-  A.pin = g.d_pin;
-  A.gen = d_gen_;
-  A.lam_scale = (float)(dt / 1000.0);
+  A.in = group_input(g);
+  A.rec = group_record(g);
   A.dt = dt;
   A.hmin = g.h_min_rel * dt;
   A.hmin_acc = A.hmin * 1.00001f;
-  A.seed = kernel_seed;
   A.nderiv = d_counters_;
-  A.budget = rk5_budget;
+  A.budget = rk5_budget > 0 ? batch_ + rk5_budget : 0;
   A.strag_list = g.d_strag;
-  A.strag_cnt = g.d_strag_cnt;
-  A.rec = spike_rec(g);
+  A.strag_cnt = d_strag_cnt_ + g.strag_slot;
+  A.srec = spike_rec(g);
   for (int j = 0; j < AEIF_NPAR; j++) {
     A.pval[j] = g.der_val[j];
     A.parr[j] = g.d_der[j];
@@ -571,13 +610,10 @@ IafArgs Engine::iaf_args(Group &g) {
   A.n = g.n;
   A.i0 = g.i0;
   A.var = g.d_var;
-  A.acc = d_acc_ + g.acc_off;
-  A.pin_off = g.d_pin_off;
-  A.pin = g.d_pin;
-  A.gen = d_gen_;
-  A.lam_scale = (float)(dt / 1000.0);
-  A.seed = kernel_seed;
-  A.rec = spike_rec(g);
+  A.in = group_input(g);
+  A.rec = group_record(g);
+  A.dt = dt;
+  A.srec = spike_rec(g);
   for (int j = 0; j < IP_NPAR; j++) {
     A.pval[j] = g.der_val[j];
     A.parr[j] = g.d_der[j];
@@ -593,7 +629,9 @@ SpikeGenArgs Engine::sg_args(Group &g) {
   A.tidx = g.d_sg_tidx;
   A.height = g.d_sg_h;
   A.next = g.d_sg_next;
-  A.rec = spike_rec(g);
+  A.rec = group_record(g);
+  A.dt = dt;
+  A.srec = spike_rec(g);
   return A;
 }
 
@@ -608,66 +646,62 @@ DeliverArgs Engine::deliver_args() {
   A.ev_off = d_ev_off_;
   A.edge = d_edge_;
   A.acc = d_acc_;
+  A.slot_stride = n_acc_;
+  A.dt = dt;
   A.n_events = d_counters_ + 1;
+  A.strag_cnt = d_strag_cnt_;
+  A.n_strag = n_strag_;
   return A;
 }
 
 // ---------------------------------------------------------------------------
 // Step loop
 // ---------------------------------------------------------------------------
-void Engine::launch_step(int k) {
+// One batch of M steps starting at graph step k0: delivery, then every group.
+void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   SpikeOut so = spike_out();
+  if (ev) cuda_check(cudaEventRecord((*ev)[0], stream_), "event");
+  count_launch(launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_,
+                              d_clk_, k0, M, stream_));
+  if (ev) cuda_check(cudaEventRecord((*ev)[1], stream_), "event");
   for (auto &g : groups_) {
-    if (is_aeif(g.model)) count_launch(launch_aeif(g.model, false, aeif_args(g), so, d_clk_, k, stream_));
-    else if (g.model == M_IAF_PSC_EXP) { launch_iaf(false, iaf_args(g), so, d_clk_, k, dt, stream_); count_launch(1); }
-    else if (g.model == M_SPIKE_GEN) { launch_spike_gen(sg_args(g), so, d_clk_, k, dt, stream_); count_launch(1); }
+    if (is_aeif(g.model)) count_launch(launch_aeif(g.model, aeif_args(g), so, d_clk_, k0, M, stream_));
+    else if (g.model == M_IAF_PSC_EXP) count_launch(launch_iaf(iaf_args(g), so, d_clk_, k0, M, stream_));
+    else if (g.model == M_SPIKE_GEN) count_launch(launch_spike_gen(sg_args(g), so, d_clk_, k0, M, stream_));
   }
-  if (rec_ncol_) {
-    launch_record(d_cols_, rec_ncol_, d_recbuf_, d_last_tidx_, d_last_h_, d_has_out_, d_clk_, k, dt,
-                  stream_);
-    count_launch(1);
-  }
-  launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_, d_clk_, k,
-                 dt, stream_);
-  count_launch(1);
+  if (ev) cuda_check(cudaEventRecord((*ev)[2], stream_), "event");
 }
 
-void Engine::launch_flush() {
-  SpikeOut so = spike_out();
-  for (auto &g : groups_) {
-    if (is_aeif(g.model)) count_launch(launch_aeif(g.model, true, aeif_args(g), so, d_clk_, 0, stream_));
-    else if (g.model == M_IAF_PSC_EXP) { launch_iaf(true, iaf_args(g), so, d_clk_, 0, dt, stream_); count_launch(1); }
-  }
-  launch_clock_clear_pending(d_clk_, stream_);
-  count_launch(1);
+void Engine::ensure_record_window(long long rows) {
+  if (!rec_ncol_ || rows <= rec_rows_cap_) return;
+  d_recbuf_ = dalloc<float>((size_t)rows * rec_ncol_);
+  rec_rows_cap_ = (int)rows;
+  invalidate_graphs();
 }
 
 void Engine::run_steps(long long n) {
-  const int K = std::max(1, graph_steps);
+  const int M = batch_;
+  const int K = std::max(M, (std::max(1, graph_steps) / M) * M);   // steps per graph
   long long window = n;
   const long long REC_WINDOW = 10000;
   if (rec_ncol_) {
     window = std::min<long long>(n, REC_WINDOW);
-    if (window > rec_rows_cap_) {
-      d_recbuf_ = dalloc<float>((size_t)window * (rec_ncol_ + 1));
-      rec_rows_cap_ = (int)window;
-      invalidate_graphs();
-    }
+    ensure_record_window(window);
   }
   long long done = 0;
   while (done < n) {
-    long long w = std::min(window, n - done);
-    long long full = w / K, rem = w % K;
-    auto run = [&](int steps) {
+    const long long w = std::min(window, n - done);
+    long long left = w;
+    while (left > 0) {
+      const int steps = (int)std::min<long long>(K, left);
       auto itg = graphs_.find(steps);
       if (itg == graphs_.end()) {
         cudaGraph_t graph;
         cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
         capturing_ = true;
         capture_count_ = 0;
-        for (int k = 0; k < steps; k++) launch_step(k);
-        launch_clock_advance(d_clk_, steps, stream_);
-        count_launch(1);
+        for (int k0 = 0; k0 < steps; k0 += M) launch_batch(k0, std::min(M, steps - k0), nullptr);
+        count_launch(launch_clock_advance(d_clk_, steps, stream_));
         capturing_ = false;
         graph_nodes_[steps] = capture_count_;
         cuda_check(cudaStreamEndCapture(stream_, &graph), "capture");
@@ -678,31 +712,33 @@ void Engine::run_steps(long long n) {
       }
       cuda_check(cudaGraphLaunch(itg->second, stream_), "graph launch");
       n_launch_ += graph_nodes_[steps];
-    };
-    for (long long i = 0; i < full; i++) run(K);
-    if (rem) run((int)rem);
+      left -= steps;
+    }
     if (rec_ncol_) drain_records(w);
     done += w;
   }
 }
 
 void Engine::drain_records(long long rows) {
-  std::vector<float> buf((size_t)rows * (rec_ncol_ + 1));
+  std::vector<float> buf((size_t)rows * rec_ncol_);
   cuda_check(cudaMemcpyAsync(buf.data(), d_recbuf_, buf.size() * sizeof(float), cudaMemcpyDeviceToHost,
                              stream_), "record copy");
   cuda_check(cudaStreamSynchronize(stream_), "record sync");
-  // next window starts where this one ended
+  // the next window starts where this one ended
   Clock c;
   cuda_check(cudaMemcpy(&c, d_clk_, sizeof(Clock), cudaMemcpyDeviceToHost), "clock");
+  const long long it_first = c.rec_it0;
   c.rec_it0 = c.it0;
   cuda_check(cudaMemcpy(d_clk_, &c, sizeof(Clock), cudaMemcpyHostToDevice), "clock");
   for (long long r = 0; r < rows; r++) {
-    const float *row = &buf[(size_t)r * (rec_ncol_ + 1)];
+    const float *row = &buf[(size_t)r * rec_ncol_];
+    // time of the step, as the reference writes it (float of the neural time)
+    const float t = (float)(neur_t0_ + (double)dt * (double)(it_first + r + 1));
     size_t c0 = 0;
     for (auto &rs : records_) {
       std::vector<float> v;
-      v.push_back(row[0]);
-      for (size_t c2 = 0; c2 < rs.var.size(); c2++) v.push_back(row[1 + c0 + c2]);
+      v.push_back(t);
+      for (size_t c2 = 0; c2 < rs.var.size(); c2++) v.push_back(row[c0 + c2]);
       c0 += rs.var.size();
       if (rs.fp) {
         fprintf(rs.fp, "%f", v[0]);
@@ -782,14 +818,12 @@ void Engine::start_simulation() {
   c.tidx_base = tidx_base_;
   c.t0 = neur_t0_;
   c.rec_it0 = 0;
-  c.pending = 0;
   cuda_check(cudaMemcpy(d_clk_, &c, sizeof(Clock), cudaMemcpyHostToDevice), "clock");
   in_sim_ = true;
 }
 
 void Engine::end_simulation() {
   if (!in_sim_) return;
-  launch_flush();   // folding twice is harmless: the first fold clears `pending`
   cuda_check(cudaStreamSynchronize(stream_), "end of simulation");
   check_status();
   drain_rec_spike_times();
@@ -799,11 +833,10 @@ void Engine::end_simulation() {
 
 void Engine::simulation_step() {
   if (!in_sim_) start_simulation();
-  // one step, then fold its inputs so that state queries between steps see what
-  // the reference shows; the next step then has nothing pending
+  // every step ends with its input fold, so state queries between steps see what the
+  // reference shows
   run_steps(1);
   it_ += 1;
-  launch_flush();
   cuda_check(cudaStreamSynchronize(stream_), "step");
   Clock c;
   cuda_check(cudaMemcpy(&c, d_clk_, sizeof(Clock), cudaMemcpyDeviceToHost), "clock");
@@ -821,7 +854,6 @@ void Engine::simulate(float t) {
   cuda_check(cudaEventRecord(ev_a_, stream_), "event");
   run_steps(Nt_);
   it_ += Nt_;
-  launch_flush();
   cuda_check(cudaEventRecord(ev_b_, stream_), "event");
   end_simulation();
   float ms = 0.0f;
@@ -837,37 +869,23 @@ std::vector<double> Engine::profile_steps(int n) {
   if (in_sim_) throw NgpuError("profile_steps cannot run inside a simulation");
   sim_time = (float)n * dt;
   start_simulation();
-  if (rec_ncol_ && n > rec_rows_cap_) {
-    d_recbuf_ = dalloc<float>((size_t)n * (rec_ncol_ + 1));
-    rec_rows_cap_ = n;
-    invalidate_graphs();
-  }
-  std::vector<cudaEvent_t> ev(4);
+  ensure_record_window(n);
+  std::vector<cudaEvent_t> ev(3);
   for (auto &e : ev) cuda_check(cudaEventCreate(&e), "event");
   std::vector<double> acc(3, 0.0);
-  SpikeOut so = spike_out();
-  for (int s = 0; s < n; s++) {
-    cuda_check(cudaEventRecord(ev[0], stream_), "event");
-    for (auto &g : groups_) {
-      if (is_aeif(g.model)) launch_aeif(g.model, false, aeif_args(g), so, d_clk_, 0, stream_);
-      else if (g.model == M_IAF_PSC_EXP) launch_iaf(false, iaf_args(g), so, d_clk_, 0, dt, stream_);
-      else if (g.model == M_SPIKE_GEN) launch_spike_gen(sg_args(g), so, d_clk_, 0, dt, stream_);
-    }
-    cuda_check(cudaEventRecord(ev[1], stream_), "event");
-    if (rec_ncol_)
-      launch_record(d_cols_, rec_ncol_, d_recbuf_, d_last_tidx_, d_last_h_, d_has_out_, d_clk_, 0, dt,
-                    stream_);
-    cuda_check(cudaEventRecord(ev[2], stream_), "event");
-    launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_, d_clk_, 0,
-                   dt, stream_);
-    cuda_check(cudaEventRecord(ev[3], stream_), "event");
-    launch_clock_advance(d_clk_, 1, stream_);
-    cuda_check(cudaEventSynchronize(ev[3]), "event");
-    for (int j = 0; j < 3; j++) {
-      float ms = 0.0f;
-      cuda_check(cudaEventElapsedTime(&ms, ev[j], ev[j + 1]), "event");
-      acc[j] += ms;
-    }
+  const int M = batch_;
+  int done = 0;
+  while (done < n) {
+    const int mb = std::min(M, n - done);
+    launch_batch(0, mb, &ev);
+    count_launch(launch_clock_advance(d_clk_, mb, stream_));
+    cuda_check(cudaEventSynchronize(ev[2]), "event");
+    float ms_del = 0.0f, ms_upd = 0.0f;
+    cuda_check(cudaEventElapsedTime(&ms_del, ev[0], ev[1]), "event");
+    cuda_check(cudaEventElapsedTime(&ms_upd, ev[1], ev[2]), "event");
+    acc[0] += ms_upd;
+    acc[2] += ms_del;
+    done += mb;
   }
   for (auto &e : ev) cudaEventDestroy(e);
   if (rec_ncol_) drain_records(n);

@@ -1,5 +1,6 @@
 // Plain structures shared by the host runtime (ngpu_engine.cpp, ngpu_sim.cpp)
-// and the CUDA kernels (ngpu_kernels.cu): kernel argument blocks passed by value.
+// and the CUDA kernels (ngpu_kernels.cu, ngpu_build.cu): kernel argument
+// blocks passed by value.
 #pragma once
 #include <vector_types.h>
 
@@ -20,8 +21,9 @@ enum Model {
 
 constexpr int MAX_PORT = 20;          // aeif_*_multisynapse port limit (reference MAX_PORT_NUM)
 constexpr int MAX_TPL_PORT = 4;       // port counts with a dedicated kernel instantiation
+constexpr int MAX_BATCH = 32;         // time steps per batch at most
 
-// Status bits reported by the device (read back after each Simulate chunk).
+// Status bits reported by the device (read back after each Simulate call).
 enum Status : unsigned {
   ST_RING_OVERFLOW = 1u << 0,         // more spikes in one step than a ring slot holds
   ST_RK5_TRIALS = 1u << 1,            // RK5 step gave up after the trial cap
@@ -29,20 +31,19 @@ enum Status : unsigned {
   ST_REC_TIMES_FULL = 1u << 3,        // a neuron exceeded its recorded-spike-time capacity
 };
 
-// Simulation clock in device memory.  One CUDA graph covers K steps; step k of
-// a chunk has per-call index it = it0 + k.
+// Simulation clock in device memory.  A CUDA graph covers a fixed number of steps
+// split into batches; a kernel of the batch starting at graph step k0 handles the
+// per-call steps it = it0 + k0 + m, m < batch length.
 struct Clock {
-  long long it0;         // per-call step index of step 0 of the current chunk
+  long long it0;         // per-call index of the first step of the running graph
   long long tidx_base;   // round(t0 / dt): time index of the call's start
   double t0;             // neural time at the call's start [ms]
   long long rec_it0;     // per-call index of the first step of the record window
-  int pending;           // 1 if inputs of the previous step still have to be folded
-  int pad;
 };
 
 // Spike output context shared by all spiking models.
 struct SpikeOut {
-  int2 *ring;            // [R][cap] (source node, height bits)
+  int2 *ring;            // [R][cap] (source node, height bits), slot = time index % R
   int *ring_cnt;         // [R]
   int R, cap;
   const unsigned char *has_out;   // per node: 1 if it has recurrent out-edges
@@ -60,6 +61,16 @@ struct GroupSpikeRec {
   int max_rec;
 };
 
+// Record columns of a group, written inside its update kernel before the step's
+// input fold (the reference records after the update, src/nestgpu.cu:507).
+struct GroupRecord {
+  const int *first;      // [n+1] CSR over the group's neurons, or null
+  const int2 *col;       // {variable code, column}; code: state index, nvar = refractory
+                         // counter, -1 = spike activity
+  float *buf;            // [rows][ncol] of the current record window
+  int ncol;
+};
+
 // Incoming poiss_gen edge, target-major, with its canonical direct-edge id.
 struct PoissonIn {
   uint32_t edge_id;
@@ -75,7 +86,18 @@ struct GenPar {
   float rate, origin, start, stop;
 };
 
-// Parameter slot: value if uniform across the group, else a device array.
+// Input side of a group: accumulator slots (one per step of a batch) and poiss_gen edges.
+struct GroupInput {
+  double *acc;           // slot 0 row of this group: acc + m*slot_stride + p*n + i
+  size_t slot_stride;    // doubles per slot (all groups)
+  const int *pin_off;    // [n+1] or null
+  const PoissonIn *pin;
+  const GenPar *gen;
+  float lam_scale;       // dt / 1000 (rate in Hz -> expected count per step)
+  uint64_t seed;
+};
+
+// aeif derived parameters: uniform -> value, else a device array.
 constexpr int AEIF_NSCAL = 13;
 enum AeifPar {
   AP_V_th = 0, AP_Delta_T, AP_inv_Delta_T, AP_g_L, AP_E_L, AP_inv_C_m, AP_a, AP_b,
@@ -94,20 +116,16 @@ struct AeifArgs {
   float *refr;           // [n]
   double *x;             // [n]
   float *h;              // [n]
-  double *acc;           // [nport][n]
-  const int *pin_off;    // [n+1] or null
-  const PoissonIn *pin;
-  const GenPar *gen;
-  float lam_scale;       // dt / 1000 (rate in Hz -> expected count per step)
+  GroupInput in;
+  GroupRecord rec;
   float dt;
   float hmin;
   float hmin_acc;        // hmin * 1.00001f: forced-accept threshold
-  uint64_t seed;
   unsigned long long *nderiv;
-  int budget;            // RK5 steps per neuron in the main kernel (0: no limit)
-  int *strag_list;       // [n] neurons left for the straggler kernel
-  int *strag_cnt;        // [2] list lengths, indexed by step parity
-  GroupSpikeRec rec;
+  int budget;            // RK5 steps per neuron and batch in the main kernel (0: no limit)
+  int2 *strag_list;      // [n] (neuron, step of the batch) left for the straggler kernel
+  int *strag_cnt;        // list length
+  GroupSpikeRec srec;
   float pval[AEIF_NPAR];
   const float *parr[AEIF_NPAR];
 };
@@ -121,13 +139,10 @@ struct IafArgs {
   int n;
   int i0;
   float *var;            // SoA [4][n]: I_syn_ex, I_syn_in, V_m_rel, refractory_step
-  double *acc;           // [2][n]
-  const int *pin_off;
-  const PoissonIn *pin;
-  const GenPar *gen;
-  float lam_scale;
-  uint64_t seed;
-  GroupSpikeRec rec;
+  GroupInput in;
+  GroupRecord rec;
+  float dt;
+  GroupSpikeRec srec;
   float pval[IP_NPAR];
   const float *parr[IP_NPAR];
 };
@@ -139,10 +154,12 @@ struct SpikeGenArgs {
   const int *tidx;       // spike step indices (per-call step counter)
   const float *height;
   int *next;             // [n]
-  GroupSpikeRec rec;
+  GroupRecord rec;
+  float dt;
+  GroupSpikeRec srec;
 };
 
-// Recurrent edge: packed accumulator index and weight.
+// Recurrent edge: packed accumulator index (receptor row + target) and weight.
 struct EdgeW {
   uint32_t acc;
   float w;
@@ -155,8 +172,12 @@ struct DeliverArgs {
   int dmin, dspan;       // delay indices dmin .. dmin+dspan-1
   const long long *ev_off;   // [n_nodes * dspan + 1]
   const EdgeW *edge;
-  double *acc;
+  double *acc;           // slot 0
+  size_t slot_stride;
+  float dt;
   unsigned long long *n_events;
+  int *strag_cnt;        // per-group straggler counters, cleared for the batch
+  int n_strag;
 };
 
 // Generated connection block: fixed in-degree with per-target random sources
@@ -170,13 +191,6 @@ struct GenBlockDev {
   int dlo, dhi;            // delay indices, inclusive
   uint64_t seed;
   int block_id;
-};
-
-// Record column: float variable pointer, or "spike" activity of a node.
-struct RecCol {
-  const float *ptr;      // null for spike activity
-  int node;
-  int pad;
 };
 
 }  // namespace ngpu

@@ -163,6 +163,7 @@ if is_b200_engine:
     _c["NGPU_SetHostRng"] = _bind("NGPU_SetHostRng", _I, [_I])
     _c["NGPU_SetRk5Budget"] = _bind("NGPU_SetRk5Budget", _I, [_I])
     _c["NGPU_SetDeliverBlocks"] = _bind("NGPU_SetDeliverBlocks", _I, [_I])
+    _c["NGPU_SetBatchMax"] = _bind("NGPU_SetBatchMax", _I, [_I])
     _c["NGPU_GetSimDeviceMs"] = _bind("NGPU_GetSimDeviceMs", ctypes.c_double, [])
     _c["NGPU_GetLaunchCount"] = _bind("NGPU_GetLaunchCount", ctypes.c_longlong, [])
     _c["NGPU_ProfileSteps"] = _bind("NGPU_ProfileSteps", _I, [_I, ctypes.POINTER(ctypes.c_double)])
@@ -1279,6 +1280,11 @@ def SetHostRng(on=True):
 def SetDeliverBlocks(n):
     """Thread blocks of the delivery kernel (engine extension; 0 = automatic)."""
     return _check(_c["NGPU_SetDeliverBlocks"](n))
+
+
+def SetBatchMax(n):
+    """Upper bound of time steps integrated per batch (engine extension; before calibration)."""
+    return _check(_c["NGPU_SetBatchMax"](n))
 
 
 def SetRk5Budget(n):

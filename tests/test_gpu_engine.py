@@ -194,3 +194,27 @@ def test_device_rng_matches_reference_generator_for_ints():
     o = orc.Oracle()
     o.SetRandomSeed(1234)
     assert np.array_equal(a, o.RandomInt(4096))
+
+
+@pytest.mark.parametrize("batch_max,budget", [(1, 0), (1, 2), (32, 0), (32, 1), (3, 4)])
+def test_time_batching_and_straggler_handoff_keep_results(batch_max, budget):
+    """Integrating several steps per kernel (up to the minimum delay) and handing long RK5
+    sequences to the straggler kernel are scheduling choices: spike counts and recorded
+    traces equal the oracle's for every setting."""
+    ngpu.SetHostRng(True)
+    ngpu.SetBatchMax(batch_max)
+    ngpu.SetRk5Budget(budget)
+    c_gpu, d_gpu = fixed_train_network(ngpu, model="aeif_cond_beta_multisynapse", t_sim=150.0)
+    c_orc, d_orc = fixed_train_network(orc.Oracle(), model="aeif_cond_beta_multisynapse", t_sim=150.0)
+    assert np.array_equal(c_gpu, c_orc)
+    assert np.array_equal(np.float32(d_gpu), np.float32(d_orc))
+
+
+def test_profile_and_launch_counters():
+    ngpu.SetHostRng(True)
+    fixed_train_network(ngpu, t_sim=20.0, record=False)
+    l0 = ngpu.GetLaunchCount()
+    upd, rec, dlv = ngpu.ProfileSteps(50)
+    assert upd > 0.0 and dlv > 0.0 and rec == 0.0
+    assert ngpu.GetLaunchCount() > l0
+    assert ngpu.GetStats()["steps"] == 250
