@@ -281,6 +281,19 @@ int NGPU_BuildDeliveryCsr(const int *src, const int *dly, const unsigned *target
                           size_t n, int n_nodes, int dspan, unsigned long long *seg_off, void *edge,
                           void *stream);
 
+/* NGPU_BuildDeliveryCsr for callers that cannot allocate device memory.  No counterpart in
+   the reference.  A process whose device heap belongs to another allocator (a PyTorch
+   program) or that divides each GPU into fixed pools at start-up may not call cudaMalloc;
+   this variant takes its scratch from a static device array of about 4.3 MiB that every GPU
+   loading the library holds until exit.  Same arguments and results as
+   NGPU_BuildDeliveryCsr; n_nodes * dspan must not exceed 524288 segments (larger problems
+   are rejected with error code 2).  All calls share the array: calls that overlap on the
+   GPU race.  The first call on a device looks up the array's device address, with that
+   device current; make it before any stream capture. */
+int NGPU_BuildDeliveryCsrNoAlloc(const int *src, const int *dly, const unsigned *target,
+                                 const float *weight, size_t n, int n_nodes, int dspan,
+                                 unsigned long long *seg_off, void *edge, void *stream);
+
 /* Steps captured per CUDA graph (default 100). */
 int NGPU_SetGraphSteps(int n);
 

@@ -686,6 +686,21 @@ int NGPU_BuildDeliveryCsr(const int *src, const int *dly, const unsigned *target
   }, -1);
 }
 
+// Same contract as NGPU_BuildDeliveryCsr, scratch from a static device array
+// (nest-gpu_b200/csrc/ngpu_noalloc.cu): no device memory is allocated.
+int NGPU_BuildDeliveryCsrNoAlloc(const int *src, const int *dly, const unsigned *target, const float *weight,
+                                 size_t n, int n_nodes, int dspan, unsigned long long *seg_off, void *edge,
+                                 void *stream) {
+  return guard([&] {
+    if (n_nodes <= 0 || dspan <= 0) throw NgpuError("n_nodes and dspan must be positive");
+    if ((n > 0 && (!src || !dly || !target || !weight || !edge)) || !seg_off)
+      throw NgpuError("null device pointer");
+    pack_delivery_csr_noalloc(src, dly, target, weight, n, n_nodes, dspan, seg_off, (EdgeW *)edge,
+                              (cudaStream_t)stream);
+    return 0;
+  }, -1);
+}
+
 int NGPU_SetDeliverBlocks(int n) {
   return guard([&] {
     if (n < 0) throw NgpuError("block count must be >= 0");

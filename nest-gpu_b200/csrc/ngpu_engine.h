@@ -290,6 +290,9 @@ int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk
 int launch_deliver(const DeliverArgs &A, int n_blocks, const Clock *clk, int k0, int M, cudaStream_t st);
 int launch_clock_advance(Clock *clk, int K, cudaStream_t st);
 int deliver_max_pairs();
+void pack_delivery_csr_noalloc(const int *src, const int *dly, const unsigned *target, const float *weight,
+                               size_t n, int n_nodes, int dspan, unsigned long long *seg_off, EdgeW *edge,
+                               cudaStream_t st);
 void pack_delivery_csr(const int *src, const int *dly, const unsigned *target, const float *weight,
                        size_t n, int n_nodes, int dspan, unsigned long long *seg_off, EdgeW *edge,
                        cudaStream_t st);
