@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
     p.add_argument("--scale", type=float, default=1.0, help="fraction of the 1M-neuron network (tests)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the learned-step and ensemble measurements")
     return p.parse_args()
 
 
@@ -121,6 +123,37 @@ def build_engine_network(ngpu, scale, seed):
                                  seed=seed + 7919)
     ngpu.ActivateSpikeCount(neuron)
     return neuron, pg
+
+
+def ensemble_run(ngpu, bio_ms=1000.0):
+    """256 independent networks (nest-gpu_b200/ensemble.py) advanced together; the launch
+    mappings are autotuned first."""
+    import numpy as np
+    from ensemble import build_ensemble, ensemble_spec, ensemble_synapses, per_network_rates
+    ngpu.Reset()
+    ngpu.SetVerbosityLevel(0)
+    spec = ensemble_spec()
+    t0 = time.time()
+    groups, layout = build_ensemble(ngpu, spec)
+    ngpu.Calibrate()
+    build_s = time.time() - t0
+    t1 = time.time()
+    chosen = ngpu.Autotune(200)
+    tune_s = time.time() - t1
+    ngpu.Simulate(100.0)
+    counts0 = {m: np.asarray(ngpu.GetStatus(g, "spike_count")).ravel() for m, g in groups.items()}
+    st0, l0 = ngpu.GetStats(), ngpu.GetLaunchCount()
+    ngpu.Simulate(bio_ms)
+    dev_s = ngpu.GetSimDeviceMs() / 1000.0
+    st1, l1 = ngpu.GetStats(), ngpu.GetLaunchCount()
+    rates, _ = per_network_rates(ngpu, groups, layout, counts0, bio_ms)
+    n_neurons = int(sum(x["n"] for x in spec))
+    return {"networks": len(spec), "neurons": n_neurons, "synapses": ensemble_synapses(spec),
+            "bio_ms": bio_ms, "rtf": dev_s / (bio_ms / 1000.0),
+            "events_per_s": (st1["n_events"] - st0["n_events"]) / dev_s,
+            "launches_per_step": (l1 - l0) / (bio_ms / 0.1),
+            "rate_hz_min_median_max": [float(rates.min()), float(np.median(rates)), float(rates.max())],
+            "mapping": chosen, "build_s": build_s, "autotune_s": tune_s}
 
 
 def engine_arm(args):
@@ -261,6 +294,10 @@ def engine_arm(args):
                               "ms_per_step": del_ms},
         "clocks": clocks,
     }
+    if WORLD == 1 and not args.no_extras:
+        from workloads import learned_vs_plain
+        result["rk5_learned"] = [learned_vs_plain(ngpu, w) for w in (0.1, 1.0)]
+        result["ensemble"] = ensemble_run(ngpu)
     if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_sample(steps=1, warmup=0)["cpu_baseline"]
     if RANK == 0:

@@ -297,10 +297,63 @@ int NGPU_BuildDeliveryCsrNoAlloc(const int *src, const int *dly, const unsigned 
 /* Steps captured per CUDA graph (default 100). */
 int NGPU_SetGraphSteps(int n);
 
+/* Threads per block of the aeif update kernel (64, 128 or 256; default 128). */
+int NGPU_SetUpdateThreads(int n);
+/* 1: use the register-capped variant of the aeif update kernel (three 256-thread blocks per
+   SM, more warps in flight, a few register spills); 0: the unconstrained one (default). */
+int NGPU_SetUpdateOccupancy(int on);
+/* Lanes per spike-delivery work item (8, 16 or 32; default 32): one item is the out-edge
+   segment of one (source, delay) pair; short segments leave fewer lanes idle with small
+   groups. */
+int NGPU_SetDeliverGroup(int g);
+/* Autotuner of the launch mappings (no counterpart in the reference): on the calibrated
+   network, times `steps` simulation steps per candidate of the update block size, the
+   update kernel variant, the delivery lane group, the delivery grid and the RK5 step budget (coordinate descent, two
+   passes) and keeps the fastest.  The trials are ordinary simulation steps, so the network
+   advances by them.  Returns the number of trials (-1 on error) and the chosen values. */
+int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliver_blocks,
+                  int *rk5_budget);
+
 /* 1: draw connection random numbers with cuRAND's host generator instead of the device
    generator the reference uses (integer streams are identical, normal streams are not);
    lets a CPU checker reproduce normal-distributed weights and delays exactly. */
 int NGPU_SetHostRng(int on);
+
+/* ---- Learned RK5 step-size proposal.  No counterpart in the reference: the reference's
+   only step-size rule is the controller of src/rk5.h:134-150, which stays in place here.
+   Features of a step (after its first derivative evaluation): V_m, w, the first state
+   variable of ports 0..3, dV_m/dt, the sum of that variable's derivatives over all
+   ports, log of the controller's h, log of the remaining interval.  Network 10-32-32-1
+   (ReLU), BF16 weights, FP32 accumulation; proposal = safety * exp(out * label_sigma +
+   label_mu), raised to at least floor * (the controller's h) when floor > 0.  Flat
+   parameter vector (NGPU_StepModelNParams() = 1465 floats): mu[10], inv_sigma[10],
+   W1[32][10], b1[32], W2[32][32], b2[32], W3[32], b3, label_mu, label_sigma, safety,
+   floor.  All return 0 (count functions: the count) or -1 on error. */
+int NGPU_StepModelNParams(void);
+/* Log one tuple of 12 floats (10 features, accepted h, error of the accepted trial) per
+   accepted RK5 step of every aeif neuron in the following Simulate calls; at most
+   `capacity` tuples are kept. */
+int NGPU_Rk5LogStart(long long capacity);
+int NGPU_Rk5LogStop(void);
+long long NGPU_Rk5LogCount(long long *offered);
+int NGPU_Rk5LogGet(float *out, long long first, long long n);
+/* Train the network on the logged tuples (steps whose controller h would not reach the end
+   of the time step) with the engine's GPU kernels: feature / target normalisation,
+   minibatch Adam on the mean squared error of the target log(h * err^-0.2); the result
+   becomes the engine's model. */
+int NGPU_StepModelTrain(long long iters, int batch, float lr, float safety, float floor,
+                        unsigned long long seed, long long *n_used, float *final_loss);
+int NGPU_StepModelSet(const float *params);
+int NGPU_StepModelGet(float *params);
+/* 1: the network proposes the first trial h of every RK5 step whose controller h would not
+   reach the end of the time step; the error test, the rejection shrink and the controller
+   update are unchanged, and invalid proposals fall back to the controller's h. */
+int NGPU_StepModelEnable(int on);
+/* Network output for n feature rows, and the mean squared error with its gradient over the
+   trainable block W1..b3 (1441 floats), computed by the GPU kernels on host buffers. */
+int NGPU_MlpForward(const float *params, const float *feat, int n, float *out);
+int NGPU_MlpGrad(const float *params, const float *feat, const float *target, int n, float *grad,
+                 float *loss);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,579 @@
+// Device code of the aeif_*_multisynapse update shared by the plain kernels
+// (ngpu_kernels.cu) and the learned-step-size variants (ngpu_learn.cu): the
+// Cash-Karp RK5 step, the sub-step loop with the model's ExternalUpdate, the
+// end-of-step record and input fold, and the batch / straggler kernels.
+//
+// LM (learn mode) selects what a step does besides the reference algorithm:
+//   LM_PLAIN   the reference step-size controller alone;
+//   LM_LOG     additionally appends one tuple (step features, accepted h, error)
+//              per accepted step to a device log;
+//   LM_PROPOSE a small MLP proposes the first trial h of a step whenever the plain
+//              controller's h would not reach the end of the time step; the error
+//              test, the rejection shrink and the controller update are unchanged.
+#pragma once
+#include "ngpu_math.cuh"
+#include "ngpu_stepmodel.h"
+#include "ngpu_types.h"
+
+namespace ngpu {
+
+// Cash-Karp tableau and controller constants (src/rk5.cu:35-72), FP32.
+namespace ck {
+constexpr float a21 = (float)0.2, a31 = (float)(3.0 / 40.0), a32 = (float)(9.0 / 40.0);
+constexpr float a41 = (float)0.3, a42 = (float)-0.9, a43 = (float)1.2;
+constexpr float a51 = (float)(-11.0 / 54.0), a52 = (float)2.5, a53 = (float)(-70.0 / 27.0),
+                a54 = (float)(35.0 / 27.0);
+constexpr float a61 = (float)(1631.0 / 55296.0), a62 = (float)(175.0 / 512.0),
+                a63 = (float)(575.0 / 13824.0), a64 = (float)(44275.0 / 110592.0),
+                a65 = (float)(253.0 / 4096.0);
+constexpr float a71 = (float)(37.0 / 378.0), a73 = (float)(250.0 / 621.0),
+                a74 = (float)(125.0 / 594.0), a76 = (float)(512.0 / 1771.0);
+constexpr float e1 = (float)(37.0 / 378.0 - 2825.0 / 27648.0),
+                e3 = (float)(250.0 / 621.0 - 18575.0 / 48384.0),
+                e4 = (float)(125.0 / 594.0 - 13525.0 / 55296.0), e5 = (float)(-277.00 / 14336.0),
+                e6 = (float)(512.0 / 1771.0 - 0.25);
+constexpr float coeff = (float)0.9, err_min = (float)1.889568e-4, scal_min = (float)1.0e-1;
+constexpr float inv_eps = 1.0e6f;
+constexpr int max_trials = 100000;
+constexpr int max_substeps = 1000000;
+}  // namespace ck
+
+// Step `m` of the batch starting at graph step k0.
+struct StepT {
+  long long it, tidx;
+  double tnow;
+};
+
+__device__ __forceinline__ StepT step_at(const Clock *c, int k0, int m, float dt) {
+  StepT s;
+  s.it = c->it0 + k0 + m;
+  s.tidx = c->tidx_base + s.it + 1;
+  s.tnow = c->t0 + (double)dt * (double)(s.it + 1);
+  return s;
+}
+
+// PushSpike (src/spike_buffer.cu:162-242) on the ring design.
+__device__ __forceinline__ void push_spike(const SpikeOut &so, const GroupSpikeRec &rec, int node,
+                                           int rel, float height, long long tidx, double tnow) {
+  so.last_tidx[node] = (int)tidx;
+  so.last_height[node] = height;
+  atomicAdd(so.n_spikes, 1ULL);
+  if (rec.spike_count) rec.spike_count[rel] += 1;
+  if (rec.n_rec) {
+    int nr = rec.n_rec[rel];
+    if (nr < rec.max_rec - 1) {
+      rec.rec_times[(size_t)rel * rec.max_rec + nr] = (float)tnow;
+      rec.n_rec[rel] = nr + 1;
+    } else {
+      atomicOr(so.status, ST_REC_TIMES_FULL);
+    }
+  }
+  if (so.has_out[node]) {
+    int slot = (int)(tidx % so.R);
+    int pos = atomicAdd(&so.ring_cnt[slot], 1);
+    if (pos < so.cap) so.ring[(size_t)slot * so.cap + pos] = make_int2(node, __float_as_int(height));
+    else atomicOr(so.status, ST_RING_OVERFLOW);
+  }
+}
+
+// Input arriving in step (tidx, tnow) for neuron i: the accumulator slot m (spikes
+// delivered this step, src/get_spike.cu:60-108) plus this step's poiss_gen draws
+// (src/poiss_gen.cu:55-86); the slot is cleared for its next use.
+__device__ __forceinline__ void step_inputs(double *in, int nport, int n, int i, const GroupInput &G,
+                                            int m, long long tidx, double tnow) {
+  double *acc = G.acc + (size_t)m * G.slot_stride;
+  for (int p = 0; p < nport; p++) {
+    double a = acc[(size_t)p * n + i];
+    in[p] = a;
+    if (a != 0.0) acc[(size_t)p * n + i] = 0.0;
+  }
+  if (G.pin_off) {
+    const int e0 = G.pin_off[i], e1 = G.pin_off[i + 1];
+    for (int e = e0; e < e1; e++) {
+      const PoissonIn pe = G.pin[e];
+      const GenPar g = G.gen[pe.gen];
+      const double t_rel = tnow - (double)g.origin - (double)pe.delay;
+      if (t_rel >= (double)g.start && t_rel <= (double)g.stop) {
+        int k = poisson_draw(__fmul_rn(G.lam_scale, g.rate), G.seed, pe.edge_id, tidx);
+        if (k > 0) in[pe.port] += (double)__fmul_rn(pe.weight, (float)k);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// aeif_*_multisynapse: adaptive Cash-Karp RK5 (src/rk5.h:69-207)
+// ---------------------------------------------------------------------------
+template <int MODEL> struct AeifShape {
+  static constexpr int npv = (MODEL == M_AEIF_PSC_EXP) ? 1 : 2;   // port vars per port
+  static constexpr int in_var = (MODEL == M_AEIF_PSC_EXP) ? 0 : 1; // port var receiving input
+  static constexpr bool cond = (MODEL == M_AEIF_COND_BETA || MODEL == M_AEIF_COND_ALPHA);
+};
+
+// PMAX: compile-time bound on the port count; FIXED: the group has exactly PMAX ports.
+template <int MODEL, int PMAX, bool FIXED> struct AeifQ {
+  int np;
+  float V_th, Delta_T, inv_Delta_T, g_L, E_L, inv_C_m, a, b, inv_tau_w, I_e, V_peak, V_reset,
+      refr_steps;
+  float E_rev[PMAX], inv_t1[PMAX], inv_t2[PMAX], pw[PMAX];
+  __device__ __forceinline__ int ports() const { return FIXED ? PMAX : np; }
+};
+
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ void aeif_derivs(const float *y, float *dy,
+                                            const AeifQ<MODEL, PMAX, FIXED> &q, float refr) {
+  typedef AeifShape<MODEL> S;
+  const int np = q.ports();
+  const float V = (refr > 0.0f) ? q.V_reset : ((y[0] < q.V_peak) ? y[0] : q.V_peak);
+  const float w = y[1];
+  float I = 0.0f;
+#pragma unroll
+  for (int i = 0; i < PMAX; i++) {
+    if (i < np) {
+      if (S::cond) I = __fmaf_rn(y[2 + 2 * i], __fsub_rn(q.E_rev[i], V), I);
+      else I = __fadd_rn(I, y[2 + S::npv * i]);
+    }
+  }
+  float Vs;
+  if (!S::cond && q.Delta_T == 0.0f) Vs = 0.0f;
+  else Vs = __fmul_rn(q.Delta_T, exp_m(__fmul_rn(__fsub_rn(V, q.V_th), q.inv_Delta_T)));
+  float s = __fmaf_rn(-q.g_L, __fsub_rn(__fsub_rn(V, q.E_L), Vs), I);
+  s = __fsub_rn(s, w);
+  s = __fadd_rn(s, q.I_e);
+  dy[0] = (refr > 0.0f) ? 0.0f : __fmul_rn(s, q.inv_C_m);
+  dy[1] = __fmul_rn(__fmaf_rn(q.a, __fsub_rn(V, q.E_L), -w), q.inv_tau_w);
+#pragma unroll
+  for (int i = 0; i < PMAX; i++) {
+    if (i < np) {
+      if (MODEL == M_AEIF_PSC_EXP) {
+        dy[2 + i] = __fmul_rn(-y[2 + i], q.inv_t1[i]);
+      } else {
+        dy[3 + 2 * i] = __fmul_rn(-y[3 + 2 * i], q.inv_t1[i]);
+        dy[2 + 2 * i] = __fmaf_rn(-y[2 + 2 * i], q.inv_t2[i], y[3 + 2 * i]);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ float pget(const AeifArgs &A, int j, int i) {
+  const float *p = A.parr[j];
+  return p ? __ldg(p + i) : A.pval[j];
+}
+
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ void load_aeif_par(const AeifArgs &A, int i, AeifQ<MODEL, PMAX, FIXED> &q) {
+  q.np = A.nport;
+  q.V_th = pget(A, AP_V_th, i);
+  q.Delta_T = pget(A, AP_Delta_T, i);
+  q.inv_Delta_T = pget(A, AP_inv_Delta_T, i);
+  q.g_L = pget(A, AP_g_L, i);
+  q.E_L = pget(A, AP_E_L, i);
+  q.inv_C_m = pget(A, AP_inv_C_m, i);
+  q.a = pget(A, AP_a, i);
+  q.b = pget(A, AP_b, i);
+  q.inv_tau_w = pget(A, AP_inv_tau_w, i);
+  q.I_e = pget(A, AP_I_e, i);
+  q.V_peak = pget(A, AP_V_peak, i);
+  q.V_reset = pget(A, AP_V_reset, i);
+  q.refr_steps = pget(A, AP_refr_steps, i);
+  const int np = q.ports();
+#pragma unroll
+  for (int p = 0; p < PMAX; p++) {
+    if (p < np) {
+      const int b = AEIF_NSCAL + AEIF_NPORTPAR * p;
+      q.E_rev[p] = pget(A, b + 0, i);
+      q.inv_t1[p] = pget(A, b + 1, i);
+      q.inv_t2[p] = pget(A, b + 2, i);
+      q.pw[p] = pget(A, b + 3, i);
+    }
+  }
+}
+
+// sign(x) log(1 + |x|): derivatives span many decades (dV/dt near the spike peak).
+__device__ __forceinline__ float slog(float x) {
+  const float l = log_m(__fadd_rn(1.0f, fabsf(x)));
+  return (x < 0.0f) ? -l : l;
+}
+
+// Features of a step for the learned proposal (definition in ngpu_stepmodel.h).
+template <int MODEL, int PMAX>
+__device__ __forceinline__ void step_features(const float *y, const float *k1, int np, float h_in,
+                                              float hmax, float *f) {
+  typedef AeifShape<MODEL> S;
+  f[0] = y[0];
+  f[1] = y[1];
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    float v = 0.0f;
+    if (p < PMAX && p < np) v = y[2 + S::npv * (p < PMAX ? p : 0)];
+    f[2 + p] = v;
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int p = 0; p < PMAX; p++)
+    if (p < np) s = __fadd_rn(s, k1[2 + S::npv * p]);
+  f[6] = slog(k1[0]);
+  f[7] = slog(s);
+  f[8] = log_m(h_in);
+  f[9] = log_m(hmax);
+}
+
+// MLP output for features f; M is the flat parameter vector (in shared memory).
+__device__ __forceinline__ float mlp_out(const float *M, const float *f) {
+  float xn[SM_NF];
+#pragma unroll
+  for (int k = 0; k < SM_NF; k++) {
+    const float v = __fmul_rn(__fsub_rn(f[k], M[SM_MU + k]), M[SM_ISIG + k]);
+    xn[k] = fminf(fmaxf(v, -SM_XCLAMP), SM_XCLAMP);
+  }
+  float a1[SM_NH];
+#pragma unroll
+  for (int j = 0; j < SM_NH; j++) {
+    float z = M[SM_B1 + j];
+#pragma unroll
+    for (int k = 0; k < SM_NF; k++) z = __fmaf_rn(M[SM_W1 + j * SM_NF + k], xn[k], z);
+    a1[j] = (z > 0.0f) ? z : 0.0f;
+  }
+  float out = M[SM_B3];
+#pragma unroll 4
+  for (int j = 0; j < SM_NH; j++) {
+    float z = M[SM_B2 + j];
+#pragma unroll
+    for (int k = 0; k < SM_NH; k++) z = __fmaf_rn(M[SM_W2 + j * SM_NH + k], a1[k], z);
+    z = (z > 0.0f) ? z : 0.0f;
+    out = __fmaf_rn(M[SM_W3 + j], z, out);
+  }
+  return out;
+}
+
+// Proposed step size: safety * exp(out * label_sigma + label_mu).
+__device__ __forceinline__ float mlp_propose(const float *M, const float *f) {
+  const float o = mlp_out(M, f);
+  return __fmul_rn(M[SM_SAFETY], exp_m(__fmaf_rn(o, M[SM_LSIG], M[SM_LMU])));
+}
+
+// One accepted RK5 step (src/rk5.h:69-159); returns the number of derivative evaluations.
+// The error scale y_scal uses the h entering the step (the plain controller's), as in
+// the reference, whatever the learned proposal chooses as the first trial.
+template <int MODEL, int PMAX, bool FIXED, int LM>
+__device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmin, float hmin_acc,
+                                        float hmax, const AeifQ<MODEL, PMAX, FIXED> &q, float refr,
+                                        unsigned *status, const float *smodel, const LearnCtx &L) {
+  constexpr int NVM = 2 + AeifShape<MODEL>::npv * PMAX;
+  const int NV = 2 + AeifShape<MODEL>::npv * q.ports();
+  float k1[NVM], k2[NVM], k3[NVM], k4[NVM], k5[NVM], k6[NVM], yn[NVM], iys[NVM];
+  aeif_derivs(y, k1, q, refr);
+#pragma unroll
+  for (int i = 0; i < NVM; i++) {
+    if (i < NV) {
+      float ys = __fadd_rn(__fadd_rn(fabsf(y[i]), fabsf(__fmul_rn(k1[i], h))), ck::scal_min);
+      iys[i] = __fdiv_rn(1.0f, ys);
+    }
+  }
+  float f[LM == LM_PLAIN ? 1 : SM_NF];
+  if (LM == LM_LOG || (LM == LM_PROPOSE && h < hmax)) step_features<MODEL, PMAX>(y, k1, q.ports(), h, hmax, f);
+  if (LM == LM_PROPOSE && h < hmax) {
+    // the plain h would not reach the end of the time step: let the network propose
+    const float hp = mlp_propose(smodel, f);
+    if (hp > 0.0f && hp <= 3.0e38f) {        // otherwise keep the plain proposal
+      const float lo = __fmul_rn(smodel[SM_FLOOR], h);
+      h = (hp > lo) ? hp : lo;
+    }
+  }
+  int nd = 1;
+  int trials = 0;
+  float err;
+  for (;;) {
+    if (h > hmax) h = hmax;
+    if (h < hmin) h = hmin;
+    const float b21 = __fmul_rn(h, ck::a21), b31 = __fmul_rn(h, ck::a31), b32 = __fmul_rn(h, ck::a32),
+                b41 = __fmul_rn(h, ck::a41), b42 = __fmul_rn(h, ck::a42), b43 = __fmul_rn(h, ck::a43),
+                b51 = __fmul_rn(h, ck::a51), b52 = __fmul_rn(h, ck::a52), b53 = __fmul_rn(h, ck::a53),
+                b54 = __fmul_rn(h, ck::a54), b61 = __fmul_rn(h, ck::a61), b62 = __fmul_rn(h, ck::a62),
+                b63 = __fmul_rn(h, ck::a63), b64 = __fmul_rn(h, ck::a64), b65 = __fmul_rn(h, ck::a65),
+                b71 = __fmul_rn(h, ck::a71), b73 = __fmul_rn(h, ck::a73), b74 = __fmul_rn(h, ck::a74),
+                b76 = __fmul_rn(h, ck::a76), f1 = __fmul_rn(h, ck::e1), f3 = __fmul_rn(h, ck::e3),
+                f4 = __fmul_rn(h, ck::e4), f5 = __fmul_rn(h, ck::e5), f6 = __fmul_rn(h, ck::e6);
+#pragma unroll
+    for (int i = 0; i < NVM; i++)
+      if (i < NV) yn[i] = __fmaf_rn(b21, k1[i], y[i]);
+    aeif_derivs(yn, k2, q, refr);
+#pragma unroll
+    for (int i = 0; i < NVM; i++)
+      if (i < NV) yn[i] = __fmaf_rn(b32, k2[i], __fmaf_rn(b31, k1[i], y[i]));
+    aeif_derivs(yn, k3, q, refr);
+#pragma unroll
+    for (int i = 0; i < NVM; i++)
+      if (i < NV) yn[i] = __fmaf_rn(b43, k3[i], __fmaf_rn(b42, k2[i], __fmaf_rn(b41, k1[i], y[i])));
+    aeif_derivs(yn, k4, q, refr);
+#pragma unroll
+    for (int i = 0; i < NVM; i++)
+      if (i < NV)
+        yn[i] = __fmaf_rn(b54, k4[i],
+                          __fmaf_rn(b53, k3[i], __fmaf_rn(b52, k2[i], __fmaf_rn(b51, k1[i], y[i]))));
+    aeif_derivs(yn, k5, q, refr);
+#pragma unroll
+    for (int i = 0; i < NVM; i++)
+      if (i < NV)
+        yn[i] = __fmaf_rn(b65, k5[i],
+                          __fmaf_rn(b64, k4[i], __fmaf_rn(b63, k3[i],
+                                                          __fmaf_rn(b62, k2[i], __fmaf_rn(b61, k1[i], y[i])))));
+    aeif_derivs(yn, k6, q, refr);
+#pragma unroll
+    for (int i = 0; i < NVM; i++)
+      if (i < NV)
+        yn[i] = __fmaf_rn(b76, k6[i],
+                          __fmaf_rn(b74, k4[i], __fmaf_rn(b73, k3[i], __fmaf_rn(b71, k1[i], y[i]))));
+    err = 0.0f;
+#pragma unroll
+    for (int i = 0; i < NVM; i++) {
+      if (i < NV) {
+        float v = __fmaf_rn(f6, k6[i], __fmaf_rn(f5, k5[i], __fmaf_rn(f4, k4[i],
+                                                                      __fmaf_rn(f3, k3[i], __fmul_rn(f1, k1[i])))));
+        float av = fabsf(__fmul_rn(v, iys[i]));
+        err = (err > av) ? err : av;
+      }
+    }
+    err = __fmul_rn(err, ck::inv_eps);
+    nd += 5;
+    trials++;
+    if (err <= 1.0f || h <= hmin_acc) break;
+    if (trials >= ck::max_trials) {
+      atomicOr(status, ST_RK5_TRIALS);
+      break;
+    }
+    float hnew = __fmul_rn(__fmul_rn(h, ck::coeff), __fdiv_rn(1.0f, __fsqrt_rn(__fsqrt_rn(err))));
+    float h01 = __fmul_rn(0.1f, h);
+    h = (hnew > h01) ? hnew : h01;
+  }
+  if (LM == LM_LOG) {
+    const unsigned long long pos = atomicAdd(L.log_cursor, 1ULL);
+    if (pos < L.log_cap) {
+      float *t = L.log + pos * LOG_W;
+#pragma unroll
+      for (int k = 0; k < SM_NF; k++) t[k] = f[k];
+      t[SM_NF] = h;
+      t[SM_NF + 1] = err;
+    }
+  }
+  x += (double)h;
+  if (err > ck::err_min) h = __fmul_rn(__fmul_rn(h, ck::coeff), exp_m(__fmul_rn(-0.2f, log_m(err))));
+  else h = __fmul_rn(5.0f, h);
+  if (!(h == h)) h = hmin;
+#pragma unroll
+  for (int i = 0; i < NVM; i++)
+    if (i < NV) y[i] = yn[i];
+  return nd;
+}
+
+// RK5 steps of neuron i from x towards tnow (src/rk5.h:161-174), each followed by the
+// model's ExternalUpdate (src/aeif_cond_beta_multisynapse_kernel.h:190-226).  Consumes
+// one unit of `budget` per step when budget >= 0 and stops when it runs out; returns
+// true when the neuron reached the end of the time step.
+template <int MODEL, int PMAX, bool FIXED, int LM>
+__device__ __forceinline__ bool aeif_integrate(const AeifArgs &A, const SpikeOut &so, int i,
+                                               const AeifQ<MODEL, PMAX, FIXED> &q, float *y,
+                                               float &refr, double &x, float &h, long long tidx,
+                                               double tnow, int &budget, unsigned long long &nd,
+                                               const float *smodel) {
+  const double x1 = tnow;
+  bool end = false;
+  int guard = 0;
+  while (!end) {
+    if (budget == 0) return false;
+    if (budget > 0) budget--;
+    float hmax = (float)(x1 - x);
+    nd += rk5_step<MODEL, PMAX, FIXED, LM>(x, y, h, A.hmin, A.hmin_acc, hmax, q, refr, so.status, smodel,
+                                           A.learn);
+    end = (x >= x1 - (double)A.hmin);
+    if (++guard > ck::max_substeps) {
+      atomicOr(so.status, ST_RK5_TRIALS);
+      break;
+    }
+    if (y[0] < -1.0e3f) {
+      y[0] = q.V_reset;
+      y[1] = 0.0f;
+      atomicOr(so.status, ST_NUMERIC);
+      continue;
+    }
+    if (y[1] < -1.0e6f || y[1] > 1.0e6f) {
+      y[0] = q.V_reset;
+      y[1] = 0.0f;
+      atomicOr(so.status, ST_NUMERIC);
+      continue;
+    }
+    if (refr > 0.0f) {
+      y[0] = q.V_reset;
+      if (end) refr = __fsub_rn(refr, 1.0f);
+    } else if (y[0] >= q.V_peak) {
+      push_spike(so, A.srec, A.i0 + i, i, 1.0f, tidx, tnow);
+      y[0] = q.V_reset;
+      y[1] = __fadd_rn(y[1], q.b);
+      refr = q.refr_steps;
+    }
+  }
+  return true;
+}
+
+// Records of the step (values after the update, before the fold).
+__device__ __forceinline__ void write_records(const GroupRecord &R, const SpikeOut &so, int node, int i,
+                                              const float *y, int nvar, float refr, long long row,
+                                              long long tidx) {
+  if (!R.first) return;
+  const int c0 = R.first[i], c1 = R.first[i + 1];
+  for (int c = c0; c < c1; c++) {
+    const int2 rc = R.col[c];
+    float v;
+    if (rc.x < 0) v = (so.has_out[node] && so.last_tidx[node] == (int)tidx) ? so.last_height[node] : 0.0f;
+    else if (rc.x == nvar) v = refr;
+    else v = y[rc.x];
+    R.buf[(size_t)row * R.ncol + rc.y] = v;
+  }
+}
+
+// End of step m: records, then the input fold (src/get_spike.cu:142-166) in FP64.
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ void aeif_end_step(const AeifArgs &A, const SpikeOut &so, int i,
+                                              const AeifQ<MODEL, PMAX, FIXED> &q, float *y, float refr,
+                                              int m, const StepT &t, long long rec_it0) {
+  typedef AeifShape<MODEL> S;
+  const int np = q.ports();
+  if (A.rec.first) write_records(A.rec, so, A.i0 + i, i, y, 2 + S::npv * np, refr, t.it - rec_it0, t.tidx);
+  double in[PMAX];
+  step_inputs(in, np, A.n, i, A.in, m, t.tidx, t.tnow);
+#pragma unroll
+  for (int p = 0; p < PMAX; p++) {
+    if (p < np && in[p] != 0.0) {
+      const int iv = 2 + S::npv * p + S::in_var;
+      y[iv] = (float)__fma_rn(in[p], (double)q.pw[p], (double)y[iv]);
+    }
+  }
+}
+
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ void aeif_load(const AeifArgs &A, int i, float *y, float &refr, double &x,
+                                          float &h, int NV) {
+  constexpr int NVM = 2 + AeifShape<MODEL>::npv * PMAX;
+#pragma unroll
+  for (int v = 0; v < NVM; v++)
+    if (v < NV) y[v] = A.var[(size_t)v * A.n + i];
+  refr = A.refr[i];
+  x = A.x[i];
+  h = A.h[i];
+}
+
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ void aeif_store(const AeifArgs &A, int i, const float *y, float refr, double x,
+                                           float h, int NV) {
+  constexpr int NVM = 2 + AeifShape<MODEL>::npv * PMAX;
+#pragma unroll
+  for (int v = 0; v < NVM; v++)
+    if (v < NV) A.var[(size_t)v * A.n + i] = y[v];
+  A.refr[i] = refr;
+  A.x[i] = x;
+  A.h[i] = h;
+}
+
+__device__ __forceinline__ void warp_add(unsigned long long *ctr, unsigned long long v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr, v);
+}
+
+// Main aeif kernel: one thread per neuron, steps m = 0..M-1 of the batch.
+// OCC = 1 caps the registers so that three 256-thread blocks fit on an SM (more warps
+// in flight to hide the dependent FP32 latency, at the price of a few spills).
+template <int MODEL, int PMAX, bool FIXED, int LM, int OCC = 0>
+__global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const AeifArgs A, const SpikeOut so,
+                                                         const Clock *clk, int k0, int M) {
+  typedef AeifShape<MODEL> S;
+  constexpr int NVM = 2 + S::npv * PMAX;
+  __shared__ float smodel[LM == LM_PROPOSE ? SM_NPAR : 1];
+  if (LM == LM_PROPOSE) {
+    for (int j = threadIdx.x; j < SM_NPAR; j += blockDim.x) smodel[j] = A.learn.model[j];
+    __syncthreads();
+  }
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long nd = 0;
+  if (i < A.n) {
+    AeifQ<MODEL, PMAX, FIXED> q;
+    load_aeif_par(A, i, q);
+    const int NV = 2 + S::npv * q.ports();
+    float y[NVM];
+    float refr, h;
+    double x;
+    aeif_load<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
+    const long long rec_it0 = clk->rec_it0;
+    int budget = A.budget > 0 ? A.budget : -1;
+    int m = 0;
+    bool deferred = false;
+    for (; m < M; m++) {
+      const StepT t = step_at(clk, k0, m, A.dt);
+      if (!aeif_integrate<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, budget, nd,
+                                                  smodel)) {
+        deferred = true;
+        break;
+      }
+      aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0);
+    }
+    aeif_store<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
+    if (deferred) {
+      const int pos = atomicAdd(A.strag_cnt, 1);
+      A.strag_list[pos] = make_int2(i, m);
+    }
+  }
+  warp_add(A.nderiv, nd);
+}
+
+// Neurons the main kernel left unfinished (typically the few that spike in the batch)
+// continue here from the step where they stopped, one per thread.
+template <int MODEL, int PMAX, bool FIXED, int LM>
+__global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, const SpikeOut so,
+                                                             const Clock *clk, int k0, int M) {
+  typedef AeifShape<MODEL> S;
+  constexpr int NVM = 2 + S::npv * PMAX;
+  __shared__ float smodel[LM == LM_PROPOSE ? SM_NPAR : 1];
+  if (LM == LM_PROPOSE) {
+    for (int j = threadIdx.x; j < SM_NPAR; j += blockDim.x) smodel[j] = A.learn.model[j];
+    __syncthreads();
+  }
+  const int cnt = *A.strag_cnt;
+  const long long rec_it0 = clk->rec_it0;
+  unsigned long long nd = 0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
+    const int2 e = A.strag_list[j];
+    const int i = e.x;
+    AeifQ<MODEL, PMAX, FIXED> q;
+    load_aeif_par(A, i, q);
+    const int NV = 2 + S::npv * q.ports();
+    float y[NVM];
+    float refr, h;
+    double x;
+    aeif_load<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
+    int budget = -1;
+    for (int m = e.y; m < M; m++) {
+      const StepT t = step_at(clk, k0, m, A.dt);
+      aeif_integrate<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, budget, nd, smodel);
+      aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0);
+    }
+    aeif_store<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
+  }
+  warp_add(A.nderiv, nd);
+}
+
+// Batch kernel, then the straggler kernel when a step budget is set; returns the
+// number of kernels launched.
+template <int MODEL, int PMAX, bool FIXED, int LM>
+int launch_aeif_p(const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
+  const int tb = (A.threads == 64 || A.threads == 256) ? A.threads : 128;
+  dim3 grid((A.n + tb - 1) / tb), block(tb);
+  if (LM == LM_PLAIN && A.occupancy)
+    aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1><<<grid, block, 0, st>>>(A, so, clk, k0, M);
+  else
+    aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0><<<grid, block, 0, st>>>(A, so, clk, k0, M);
+  if (A.budget <= 0) return 1;
+  dim3 sgrid(A.n < 128 * 148 * 4 ? (A.n + 127) / 128 : 148 * 4), sblock(128);
+  aeif_straggler_kernel<MODEL, PMAX, FIXED, LM><<<sgrid, sblock, 0, st>>>(A, so, clk, k0, M);
+  return 2;
+}
+
+}  // namespace ngpu

@@ -726,12 +726,124 @@ int NGPU_SetRk5Budget(int n) {
   }, 0);
 }
 
+int NGPU_SetUpdateThreads(int n) {
+  return guard([&] {
+    if (n != 64 && n != 128 && n != 256) throw NgpuError("update block size must be 64, 128 or 256");
+    E().update_threads = n;
+    return 0;
+  }, -1);
+}
+
+int NGPU_SetDeliverGroup(int g) {
+  return guard([&] {
+    if (g != 8 && g != 16 && g != 32) throw NgpuError("delivery lane group must be 8, 16 or 32");
+    E().deliver_group = g;
+    return 0;
+  }, -1);
+}
+
+int NGPU_SetUpdateOccupancy(int on) {
+  return guard([&] {
+    E().update_occupancy = on ? 1 : 0;
+    return 0;
+  }, -1);
+}
+
+int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliver_blocks, int *rk5_budget) {
+  return guard([&] {
+    const int n = E().autotune(steps, nullptr);
+    if (update_threads) *update_threads = E().update_threads;
+    if (deliver_group) *deliver_group = E().deliver_group;
+    if (deliver_blocks) *deliver_blocks = E().deliver_blocks_req;
+    if (rk5_budget) *rk5_budget = E().rk5_budget;
+    return n;
+  }, -1);
+}
+
 int NGPU_SetGraphSteps(int n) {
   return guard([&] {
     if (n < 1) throw NgpuError("graph steps must be >= 1");
     E().graph_steps = n;
     return 0;
   }, 0);
+}
+
+// ---- learned RK5 step-size proposal
+int NGPU_StepModelNParams() { return SM_NPAR; }
+
+int NGPU_Rk5LogStart(long long capacity) {
+  return guard([&] { E().rk5_log_start(capacity); return 0; }, -1);
+}
+
+int NGPU_Rk5LogStop() {
+  return guard([&] { E().rk5_log_stop(); return 0; }, -1);
+}
+
+long long NGPU_Rk5LogCount(long long *offered) {
+  return guard([&] { return E().rk5_log_count(offered); }, (long long)-1);
+}
+
+int NGPU_Rk5LogGet(float *out, long long first, long long n) {
+  return guard([&] {
+    if (!out && n > 0) throw NgpuError("null output buffer");
+    E().rk5_log_get(out, first, n);
+    return 0;
+  }, -1);
+}
+
+int NGPU_StepModelTrain(long long iters, int batch, float lr, float safety, float floor,
+                        unsigned long long seed, long long *n_used, float *final_loss) {
+  return guard([&] {
+    if (iters < 1 || batch < 1 || !(lr > 0.0f) || !(safety > 0.0f) || !(floor >= 0.0f))
+      throw NgpuError("invalid training settings");
+    TrainConfig c;
+    c.iters = iters;
+    c.batch = batch;
+    c.lr = lr;
+    c.safety = safety;
+    c.floor = floor;
+    c.seed = seed;
+    TrainResult r = E().step_model_train(c);
+    if (n_used) *n_used = r.n_used;
+    if (final_loss) *final_loss = r.final_loss;
+    return 0;
+  }, -1);
+}
+
+int NGPU_StepModelSet(const float *params) {
+  return guard([&] {
+    if (!params) throw NgpuError("null parameter vector");
+    E().step_model_set(params);
+    return 0;
+  }, -1);
+}
+
+int NGPU_StepModelGet(float *params) {
+  return guard([&] {
+    if (!params) throw NgpuError("null parameter vector");
+    E().step_model_get(params);
+    return 0;
+  }, -1);
+}
+
+int NGPU_StepModelEnable(int on) {
+  return guard([&] { E().step_model_enable(on != 0); return 0; }, -1);
+}
+
+int NGPU_MlpForward(const float *params, const float *feat, int n, float *out) {
+  return guard([&] {
+    if (n < 0 || !params || (n > 0 && (!feat || !out))) throw NgpuError("invalid arguments");
+    mlp_forward_host(params, feat, n, out);
+    return 0;
+  }, -1);
+}
+
+int NGPU_MlpGrad(const float *params, const float *feat, const float *target, int n, float *grad, float *loss) {
+  return guard([&] {
+    if (n < 1 || !params || !feat || !target || !grad) throw NgpuError("invalid arguments");
+    mlp_grad_host(params, feat, target, n, grad, loss);
+    return 0;
+  }, -1);
 }
 
 }  // extern "C"

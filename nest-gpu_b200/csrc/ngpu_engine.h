@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 
+#include "ngpu_stepmodel.h"
 #include "ngpu_types.h"
 
 namespace ngpu {
@@ -21,6 +22,23 @@ namespace ngpu {
 struct NgpuError : public std::runtime_error {
   explicit NgpuError(const std::string &m) : std::runtime_error(m) {}
 };
+
+// Training of the learned step-size proposal.
+struct TrainConfig {
+  long long iters = 3000;        // Adam iterations
+  int batch = 4096;              // samples per iteration (multiple of 128)
+  float lr = 2.0e-3f;
+  float safety = 0.9f;           // proposal = safety * predicted step size
+  float floor = 0.0f;            // proposal >= floor * controller h (0: no floor)
+  uint64_t seed = 1;
+};
+struct TrainResult {
+  long long n_used = 0;          // logged tuples the network is trained on
+  float final_loss = 0.0f;       // mean squared error (normalised target), last iterations
+};
+TrainResult train_step_model(const float *d_tuples, long long n_tuples, const TrainConfig &cfg, float *params);
+void mlp_forward_host(const float *params, const float *feat, int n, float *out);
+void mlp_grad_host(const float *params, const float *feat, const float *target, int n, float *grad, float *loss);
 
 // Kinds of named quantities of a node group.
 enum Kind { K_NONE = -1, K_SCAL_VAR = 0, K_PORT_VAR, K_SCAL_PARAM, K_PORT_PARAM, K_GROUP_PARAM,
@@ -106,6 +124,9 @@ class Engine {
   int rk5_budget = 4;             // RK5 steps per neuron before the straggler kernel takes over
   int deliver_blocks_req = 0;     // delivery grid size (0: from the number of spiking sources)
   int batch_max = MAX_BATCH;      // upper bound of the time-batch length (1: step by step)
+  int update_threads = 128;       // threads per block of the aeif update kernel (64, 128, 256)
+  int deliver_group = 32;         // lanes per delivery work item (8, 16, 32)
+  int update_occupancy = 0;       // 1: register-capped aeif update kernel
   bool use_device_rng = true;     // cuRAND device generator (as the reference) if a GPU exists
 
   void set_seed(unsigned long long s);
@@ -179,6 +200,27 @@ class Engine {
   // record gather, spike delivery.  The steps are ordinary simulation steps.
   std::vector<double> profile_steps(int n);
   long long n_launches() const { return n_launch_; }
+
+  // Tune update_threads, deliver_group, deliver_blocks_req and rk5_budget on the
+  // calibrated network by timing `steps` simulation steps per candidate (coordinate
+  // descent, two passes).  The trials are ordinary simulation steps: the network
+  // advances by them.  Returns the number of trials; the chosen values stay set.
+  int autotune(int steps, std::vector<std::pair<std::string, double>> *log);
+
+  // ---- learned RK5 step-size proposal (kernels and training in ngpu_learn.cu)
+  // Log one tuple per accepted RK5 step of every aeif neuron (at most cap tuples).
+  void rk5_log_start(long long cap);
+  void rk5_log_stop();
+  long long rk5_log_count(long long *offered);
+  void rk5_log_get(float *out, long long first, long long n);
+  // Train the proposal network on the logged tuples with the GPU kernels; the
+  // result becomes the engine's model.
+  TrainResult step_model_train(const TrainConfig &cfg);
+  void step_model_set(const float *p);
+  void step_model_get(float *p) const;
+  bool has_step_model() const { return has_model_; }
+  void step_model_enable(bool on);
+  int learn_mode() const { return learn_mode_; }
 
   // device buffers exposed to the engine-level helpers
   cudaStream_t stream() const { return stream_; }
@@ -257,6 +299,15 @@ class Engine {
   cudaEvent_t ev_a_ = nullptr, ev_b_ = nullptr;
   long long total_steps_ = 0;
   unsigned status_seen_ = 0;
+  // learned step size
+  int learn_mode_ = 0;
+  float *d_log_ = nullptr;
+  unsigned long long *d_log_cursor_ = nullptr;
+  long long log_cap_ = 0;
+  float *d_model_ = nullptr;
+  std::vector<float> model_;
+  bool has_model_ = false;
+  void set_learn_mode(int mode);
 
   template <class T> T *dalloc(size_t n);
   void free_device();
@@ -287,7 +338,8 @@ int launch_aeif(int model, const AeifArgs &A, const SpikeOut &so, const Clock *c
 int launch_iaf(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st);
 int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                      cudaStream_t st);
-int launch_deliver(const DeliverArgs &A, int n_blocks, const Clock *clk, int k0, int M, cudaStream_t st);
+int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *clk, int k0, int M,
+                   cudaStream_t st);
 int launch_clock_advance(Clock *clk, int K, cudaStream_t st);
 int deliver_max_pairs();
 void pack_delivery_csr_noalloc(const int *src, const int *dly, const unsigned *target, const float *weight,

@@ -56,6 +56,13 @@ void Engine::free_device() {
   graphs_.clear();
   for (void *p : allocs_) cudaFree(p);
   allocs_.clear();
+  if (d_log_) cudaFree(d_log_);
+  if (d_log_cursor_) cudaFree(d_log_cursor_);
+  if (d_model_) cudaFree(d_model_);
+  d_log_ = nullptr;
+  d_log_cursor_ = nullptr;
+  d_model_ = nullptr;
+  log_cap_ = 0;
   if (stream_) cudaStreamDestroy(stream_);
   stream_ = nullptr;
 }
@@ -597,6 +604,13 @@ AeifArgs Engine::aeif_args(Group &g) {
   A.strag_list = g.d_strag;
   A.strag_cnt = d_strag_cnt_ + g.strag_slot;
   A.srec = spike_rec(g);
+  A.threads = update_threads;
+  A.occupancy = update_occupancy;
+  A.learn.mode = learn_mode_;
+  A.learn.log = d_log_;
+  A.learn.log_cursor = d_log_cursor_;
+  A.learn.log_cap = (unsigned long long)log_cap_;
+  A.learn.model = d_model_;
   for (int j = 0; j < AEIF_NPAR; j++) {
     A.pval[j] = g.der_val[j];
     A.parr[j] = g.d_der[j];
@@ -662,7 +676,7 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   SpikeOut so = spike_out();
   if (ev) cuda_check(cudaEventRecord((*ev)[0], stream_), "event");
   count_launch(launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_,
-                              d_clk_, k0, M, stream_));
+                              deliver_group, d_clk_, k0, M, stream_));
   if (ev) cuda_check(cudaEventRecord((*ev)[1], stream_), "event");
   for (auto &g : groups_) {
     if (is_aeif(g.model)) count_launch(launch_aeif(g.model, aeif_args(g), so, d_clk_, k0, M, stream_));
@@ -911,6 +925,146 @@ EngineStats Engine::stats() {
   s.sim_device_ms = last_sim_device_ms_;
   s.steps = total_steps_;
   return s;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner of the launch mappings
+// ---------------------------------------------------------------------------
+int Engine::autotune(int steps, std::vector<std::pair<std::string, double>> *log) {
+  if (steps < 1) throw NgpuError("autotune needs at least one step per trial");
+  if (in_sim_) throw NgpuError("autotune cannot run inside a simulation");
+  if (!calibrated_) calibrate();
+  const int verb = verbosity;
+  verbosity = 0;
+  const int base = std::max(148, deliver_blocks_);
+  struct Knob {
+    const char *name;
+    int *var;
+    std::vector<int> cand;
+  };
+  std::vector<Knob> knobs = {
+      {"update_threads", &update_threads, {64, 128, 256}},
+      {"update_occupancy", &update_occupancy, {0, 1}},
+      {"deliver_group", &deliver_group, {8, 16, 32}},
+      {"deliver_blocks", &deliver_blocks_req, {148, 296, 592, 1184, 2368, base}},
+      {"rk5_budget", &rk5_budget, {0, 1, 2, 4, 8}},
+  };
+  if (deliver_blocks_req <= 0) deliver_blocks_req = base;
+  const float t = (float)steps * dt;
+  auto trial = [&]() {
+    invalidate_graphs();
+    simulate(t);   // captures the graphs
+    simulate(t);
+    return last_sim_device_ms_;
+  };
+  int n_trials = 0;
+  try {
+    for (int pass = 0; pass < 2; pass++) {
+      for (auto &k : knobs) {
+        int best = *k.var;
+        double best_ms = trial();
+        n_trials++;
+        if (log) log->push_back({std::string(k.name) + "=" + std::to_string(best), best_ms});
+        for (int c : k.cand) {
+          if (c == best) continue;
+          *k.var = c;
+          const double ms = trial();
+          n_trials++;
+          if (log) log->push_back({std::string(k.name) + "=" + std::to_string(c), ms});
+          if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+          }
+        }
+        *k.var = best;
+      }
+    }
+  } catch (...) {
+    verbosity = verb;
+    throw;
+  }
+  verbosity = verb;
+  invalidate_graphs();
+  return n_trials;
+}
+
+// ---------------------------------------------------------------------------
+// Learned RK5 step-size proposal: logging, training, model
+// ---------------------------------------------------------------------------
+void Engine::set_learn_mode(int mode) {
+  if (stream_) cuda_check(cudaStreamSynchronize(stream_), "sync");
+  if (mode != learn_mode_) invalidate_graphs();
+  learn_mode_ = mode;
+}
+
+void Engine::rk5_log_start(long long cap) {
+  if (cap <= 0) throw NgpuError("RK5 log capacity must be positive");
+  if (stream_) cuda_check(cudaStreamSynchronize(stream_), "sync");
+  if (cap != log_cap_) {
+    if (d_log_) cudaFree(d_log_);
+    d_log_ = nullptr;
+    log_cap_ = 0;
+    cuda_check(cudaMalloc(&d_log_, (size_t)cap * LOG_W * sizeof(float)), "RK5 log buffer");
+    log_cap_ = cap;
+  }
+  if (!d_log_cursor_) cuda_check(cudaMalloc(&d_log_cursor_, sizeof(unsigned long long)), "RK5 log cursor");
+  cuda_check(cudaMemset(d_log_cursor_, 0, sizeof(unsigned long long)), "RK5 log cursor");
+  invalidate_graphs();   // the log buffer is baked into captured kernel arguments
+  set_learn_mode(LM_LOG);
+}
+
+void Engine::rk5_log_stop() {
+  if (learn_mode_ == LM_LOG) set_learn_mode(LM_PLAIN);
+}
+
+long long Engine::rk5_log_count(long long *offered) {
+  unsigned long long c = 0;
+  if (d_log_cursor_) {
+    if (stream_) cuda_check(cudaStreamSynchronize(stream_), "sync");
+    cuda_check(cudaMemcpy(&c, d_log_cursor_, sizeof(c), cudaMemcpyDeviceToHost), "RK5 log cursor");
+  }
+  if (offered) *offered = (long long)c;
+  return std::min<long long>((long long)c, log_cap_);
+}
+
+void Engine::rk5_log_get(float *out, long long first, long long n) {
+  const long long have = rk5_log_count(nullptr);
+  if (first < 0 || n < 0 || first + n > have) throw NgpuError("RK5 log range out of bounds");
+  if (n == 0) return;
+  cuda_check(cudaMemcpy(out, d_log_ + (size_t)first * LOG_W, (size_t)n * LOG_W * sizeof(float),
+                        cudaMemcpyDeviceToHost), "RK5 log download");
+}
+
+TrainResult Engine::step_model_train(const TrainConfig &cfg) {
+  const long long n = rk5_log_count(nullptr);
+  if (n <= 0) throw NgpuError("no RK5 steps logged: call the RK5 log before training");
+  std::vector<float> p(SM_NPAR);
+  TrainResult r = train_step_model(d_log_, n, cfg, p.data());
+  step_model_set(p.data());
+  return r;
+}
+
+void Engine::step_model_set(const float *p) {
+  for (int j = 0; j < SM_NPAR; j++)
+    if (!(std::fabs(p[j]) < 3.0e38f)) throw NgpuError("step model parameter " + std::to_string(j) + " is not finite");
+  if (!(p[SM_SAFETY] > 0.0f)) throw NgpuError("step model safety factor must be positive");
+  if (!(p[SM_FLOOR] >= 0.0f)) throw NgpuError("step model floor must be >= 0");
+  model_.assign(p, p + SM_NPAR);
+  if (stream_) cuda_check(cudaStreamSynchronize(stream_), "sync");
+  if (!d_model_) cuda_check(cudaMalloc(&d_model_, SM_NPAR * sizeof(float)), "step model");
+  cuda_check(cudaMemcpy(d_model_, model_.data(), SM_NPAR * sizeof(float), cudaMemcpyHostToDevice), "step model");
+  has_model_ = true;
+  invalidate_graphs();
+}
+
+void Engine::step_model_get(float *p) const {
+  if (!has_model_) throw NgpuError("no step model has been trained or set");
+  std::copy(model_.begin(), model_.end(), p);
+}
+
+void Engine::step_model_enable(bool on) {
+  if (on && !has_model_) throw NgpuError("no step model has been trained or set");
+  set_learn_mode(on ? LM_PROPOSE : LM_PLAIN);
 }
 
 }  // namespace ngpu

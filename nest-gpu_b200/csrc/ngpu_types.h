@@ -107,6 +107,15 @@ enum AeifPar {
 constexpr int AEIF_NPORTPAR = 4;
 constexpr int AEIF_NPAR = AEIF_NSCAL + AEIF_NPORTPAR * MAX_PORT;
 
+// Learned step-size context of an aeif group (layouts in ngpu_stepmodel.h).
+struct LearnCtx {
+  int mode;                       // LearnMode
+  float *log;                     // [log_cap][LOG_W] tuples (LM_LOG)
+  unsigned long long *log_cursor; // tuples offered so far (may exceed log_cap)
+  unsigned long long log_cap;
+  const float *model;             // SM_NPAR floats (LM_PROPOSE)
+};
+
 struct AeifArgs {
   int n;
   int i0;
@@ -123,9 +132,12 @@ struct AeifArgs {
   float hmin_acc;        // hmin * 1.00001f: forced-accept threshold
   unsigned long long *nderiv;
   int budget;            // RK5 steps per neuron and batch in the main kernel (0: no limit)
+  int threads;           // threads per block of the main kernel (64, 128 or 256)
+  int occupancy;         // 1: register-capped variant of the main kernel (more resident warps)
   int2 *strag_list;      // [n] (neuron, step of the batch) left for the straggler kernel
   int *strag_cnt;        // list length
   GroupSpikeRec srec;
+  LearnCtx learn;
   float pval[AEIF_NPAR];
   const float *parr[AEIF_NPAR];
 };

@@ -164,9 +164,27 @@ if is_b200_engine:
     _c["NGPU_SetRk5Budget"] = _bind("NGPU_SetRk5Budget", _I, [_I])
     _c["NGPU_SetDeliverBlocks"] = _bind("NGPU_SetDeliverBlocks", _I, [_I])
     _c["NGPU_SetBatchMax"] = _bind("NGPU_SetBatchMax", _I, [_I])
+    _c["NGPU_SetUpdateThreads"] = _bind("NGPU_SetUpdateThreads", _I, [_I])
+    _c["NGPU_SetDeliverGroup"] = _bind("NGPU_SetDeliverGroup", _I, [_I])
+    _c["NGPU_SetUpdateOccupancy"] = _bind("NGPU_SetUpdateOccupancy", _I, [_I])
+    _c["NGPU_Autotune"] = _bind("NGPU_Autotune", _I, [_I] + [ctypes.POINTER(_I)] * 4)
     _c["NGPU_GetSimDeviceMs"] = _bind("NGPU_GetSimDeviceMs", ctypes.c_double, [])
     _c["NGPU_GetLaunchCount"] = _bind("NGPU_GetLaunchCount", ctypes.c_longlong, [])
     _c["NGPU_ProfileSteps"] = _bind("NGPU_ProfileSteps", _I, [_I, ctypes.POINTER(ctypes.c_double)])
+    _LL = ctypes.c_longlong
+    _c["NGPU_StepModelNParams"] = _bind("NGPU_StepModelNParams", _I, [])
+    _c["NGPU_Rk5LogStart"] = _bind("NGPU_Rk5LogStart", _I, [_LL])
+    _c["NGPU_Rk5LogStop"] = _bind("NGPU_Rk5LogStop", _I, [])
+    _c["NGPU_Rk5LogCount"] = _bind("NGPU_Rk5LogCount", _LL, [ctypes.POINTER(_LL)])
+    _c["NGPU_Rk5LogGet"] = _bind("NGPU_Rk5LogGet", _I, [c_void_p, _LL, _LL])
+    _c["NGPU_StepModelTrain"] = _bind("NGPU_StepModelTrain", _I, [_LL, _I, ctypes.c_float, ctypes.c_float,
+                                                                  ctypes.c_float, ctypes.c_ulonglong, ctypes.POINTER(_LL),
+                                                                  ctypes.POINTER(ctypes.c_float)])
+    _c["NGPU_StepModelSet"] = _bind("NGPU_StepModelSet", _I, [c_void_p])
+    _c["NGPU_StepModelGet"] = _bind("NGPU_StepModelGet", _I, [c_void_p])
+    _c["NGPU_StepModelEnable"] = _bind("NGPU_StepModelEnable", _I, [_I])
+    _c["NGPU_MlpForward"] = _bind("NGPU_MlpForward", _I, [c_void_p, c_void_p, _I, c_void_p])
+    _c["NGPU_MlpGrad"] = _bind("NGPU_MlpGrad", _I, [c_void_p, c_void_p, c_void_p, _I, c_void_p, c_void_p])
     _c["NGPU_ConnectFixedIndegreeGPU"] = _bind("NGPU_ConnectFixedIndegreeGPU", _I,
                                                [_I, _I, _I, _I, _I, _I, _F, _F, _F, ctypes.c_ulonglong])
 
@@ -1293,7 +1311,140 @@ def SetRk5Budget(n):
     return _check(_c["NGPU_SetRk5Budget"](n))
 
 
+def SetUpdateThreads(n):
+    """Threads per block of the aeif update kernel: 64, 128 or 256 (engine extension)."""
+    _need_b200("SetUpdateThreads")
+    return _check(_c["NGPU_SetUpdateThreads"](n))
+
+
+def SetUpdateOccupancy(on=True):
+    """Register-capped variant of the aeif update kernel (engine extension)."""
+    _need_b200("SetUpdateOccupancy")
+    return _check(_c["NGPU_SetUpdateOccupancy"](1 if on else 0))
+
+
+def SetDeliverGroup(g):
+    """Lanes per spike-delivery work item: 8, 16 or 32 (engine extension)."""
+    _need_b200("SetDeliverGroup")
+    return _check(_c["NGPU_SetDeliverGroup"](g))
+
+
+def Autotune(steps=200):
+    """Pick the update block size, delivery lane group, delivery grid and RK5 step budget
+    by timing `steps` simulation steps per candidate on the calibrated network (the network
+    advances by those steps).  Returns the chosen settings and the number of trials."""
+    _need_b200("Autotune")
+    a, b, c, d = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    n = _c["NGPU_Autotune"](steps, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d))
+    _check()
+    return {"update_threads": a.value, "deliver_group": b.value, "deliver_blocks": c.value,
+            "rk5_budget": d.value, "trials": n}
+
+
 def SetGraphSteps(n):
     if not is_b200_engine:
         raise ValueError("SetGraphSteps needs libnestgpu_b200.so")
     return _check(_c["NGPU_SetGraphSteps"](n))
+
+
+# ---- learned RK5 step-size proposal (engine extension, no reference counterpart)
+def _need_b200(name):
+    if not is_b200_engine:
+        raise ValueError(name + " needs libnestgpu_b200.so")
+
+
+def Rk5LogStart(capacity):
+    """Log one tuple (10 step features, accepted h, error) per accepted RK5 step of every
+    aeif neuron during the following Simulate calls, at most `capacity` tuples."""
+    _need_b200("Rk5LogStart")
+    return _check(_c["NGPU_Rk5LogStart"](int(capacity)))
+
+
+def Rk5LogStop():
+    _need_b200("Rk5LogStop")
+    return _check(_c["NGPU_Rk5LogStop"]())
+
+
+def Rk5LogCount():
+    """(tuples stored, tuples offered) of the RK5 log."""
+    _need_b200("Rk5LogCount")
+    off = ctypes.c_longlong(0)
+    n = _c["NGPU_Rk5LogCount"](ctypes.byref(off))
+    _check()
+    return n, off.value
+
+
+def Rk5LogGet(first=0, n=None):
+    """Logged tuples [n, 12] as a float32 array."""
+    import numpy as np
+    _need_b200("Rk5LogGet")
+    if n is None:
+        n = Rk5LogCount()[0] - first
+    out = np.zeros((n, 12), dtype=np.float32)
+    _c["NGPU_Rk5LogGet"](out.ctypes.data, first, n)
+    _check()
+    return out
+
+
+def StepModelTrain(iters=3000, batch=4096, lr=2.0e-3, safety=0.9, floor=0.0, seed=1):
+    """Train the step-size network on the logged tuples with the GPU kernels and make it
+    the engine's model; returns (tuples used, final mean squared error).  In the RK5 loop
+    the proposal is safety * (predicted step size), raised to at least floor * (the
+    controller's h) when floor > 0."""
+    _need_b200("StepModelTrain")
+    nu, loss = ctypes.c_longlong(0), ctypes.c_float(0)
+    _c["NGPU_StepModelTrain"](int(iters), int(batch), float(lr), float(safety), float(floor), int(seed),
+                              ctypes.byref(nu), ctypes.byref(loss))
+    _check()
+    return nu.value, loss.value
+
+
+def StepModelGet():
+    import numpy as np
+    _need_b200("StepModelGet")
+    p = np.zeros(_c["NGPU_StepModelNParams"](), dtype=np.float32)
+    _c["NGPU_StepModelGet"](p.ctypes.data)
+    _check()
+    return p
+
+
+def StepModelSet(params):
+    import numpy as np
+    _need_b200("StepModelSet")
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    if p.size != _c["NGPU_StepModelNParams"]():
+        raise ValueError("step model parameter vector has the wrong size")
+    return _check(_c["NGPU_StepModelSet"](p.ctypes.data))
+
+
+def StepModelEnable(on=True):
+    """Let the network propose the first trial h of RK5 steps (the error test, the
+    rejection shrink and the plain controller stay as they are)."""
+    _need_b200("StepModelEnable")
+    return _check(_c["NGPU_StepModelEnable"](1 if on else 0))
+
+
+def MlpForward(params, feat):
+    """Network output for features [n, 10] computed by the GPU inference code."""
+    import numpy as np
+    _need_b200("MlpForward")
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    f = np.ascontiguousarray(feat, dtype=np.float32).reshape(-1, 10)
+    out = np.zeros(f.shape[0], dtype=np.float32)
+    _c["NGPU_MlpForward"](p.ctypes.data, f.ctypes.data, f.shape[0], out.ctypes.data)
+    _check()
+    return out
+
+
+def MlpGrad(params, feat, target):
+    """(loss, gradient of the trainable block) computed by the GPU training kernels."""
+    import numpy as np
+    _need_b200("MlpGrad")
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    f = np.ascontiguousarray(feat, dtype=np.float32).reshape(-1, 10)
+    t = np.ascontiguousarray(target, dtype=np.float32)
+    g = np.zeros(1441, dtype=np.float32)
+    loss = ctypes.c_float(0)
+    _c["NGPU_MlpGrad"](p.ctypes.data, f.ctypes.data, t.ctypes.data, f.shape[0], g.ctypes.data, ctypes.byref(loss))
+    _check()
+    return loss.value, g

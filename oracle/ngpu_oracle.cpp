@@ -242,6 +242,108 @@ struct Group {
   std::vector<std::vector<float>> rec_times;
 };
 
+// ---------------------------------------------------------------------------
+// Learned RK5 step-size proposal (no counterpart in the reference).  A CPU
+// statement of the engine's network: features of a step, the 10-32-32-1 MLP with
+// BF16-valued weights and FP32 accumulation (float fused multiply-adds in the
+// kernel's order, so the result is bit-identical), and its exact FP64 gradient.
+// Flat parameter vector: mu[10] inv_sigma[10] W1[32][10] b1[32] W2[32][32] b2[32]
+// W3[32] b3 label_mu label_sigma safety floor (1465 floats); trainable block W1..b3.
+// In the RK5 loop the proposal is raised to at least floor * (the controller's h).
+// ---------------------------------------------------------------------------
+namespace sm {
+constexpr int NF = 10, NH = 32;
+constexpr float XCLAMP = 8.0f;   // normalised inputs are clamped to [-8, 8]
+constexpr int MU = 0, ISIG = MU + NF, W1 = ISIG + NF, B1 = W1 + NH * NF, W2 = B1 + NH, B2 = W2 + NH * NH,
+              W3 = B2 + NH, B3 = W3 + NH, LMU = B3 + 1, LSIG = LMU + 1, SAFETY = LSIG + 1, FLOOR = SAFETY + 1,
+              NPAR = FLOOR + 1;
+constexpr int NTRAIN = B3 + 1 - W1;
+constexpr int LOG_W = NF + 2;
+}  // namespace sm
+
+static float slog_f(float x) {   // sign(x) log(1 + |x|)
+  const float l = log_m(1.0f + std::fabs(x));
+  return (x < 0.0f) ? -l : l;
+}
+
+static float mlp_out_f(const float *M, const float *f) {
+  using namespace sm;
+  float xn[NF];
+  for (int k = 0; k < NF; k++) {
+    const float v = (f[k] - M[MU + k]) * M[ISIG + k];
+    xn[k] = std::fmin(std::fmax(v, -XCLAMP), XCLAMP);
+  }
+  float a1[NH];
+  for (int j = 0; j < NH; j++) {
+    float z = M[B1 + j];
+    for (int k = 0; k < NF; k++) z = std::fma(M[W1 + j * NF + k], xn[k], z);
+    a1[j] = (z > 0.0f) ? z : 0.0f;
+  }
+  float out = M[B3];
+  for (int j = 0; j < NH; j++) {
+    float z = M[B2 + j];
+    for (int k = 0; k < NH; k++) z = std::fma(M[W2 + j * NH + k], a1[k], z);
+    z = (z > 0.0f) ? z : 0.0f;
+    out = std::fma(M[W3 + j], z, out);
+  }
+  return out;
+}
+
+static float mlp_propose_f(const float *M, const float *f) {
+  using namespace sm;
+  return M[SAFETY] * exp_m(std::fma(mlp_out_f(M, f), M[LSIG], M[LMU]));
+}
+
+// Mean squared error over n samples of the normalised target (target - label_mu) /
+// label_sigma, and its gradient with respect to the trainable block, in FP64.
+static double mlp_grad_d(const float *M, const float *feat, const float *target, int n, double *grad) {
+  using namespace sm;
+  for (int o = 0; o < NTRAIN; o++) grad[o] = 0.0;
+  double loss = 0.0;
+  for (int s = 0; s < n; s++) {
+    double xn[NF], z1[NH], a1[NH], z2[NH], a2[NH];
+    for (int k = 0; k < NF; k++) {
+      // the clamp is applied in FP32, as in the engine
+      const float v = (feat[s * NF + k] - M[MU + k]) * M[ISIG + k];
+      xn[k] = (double)std::fmin(std::fmax(v, -XCLAMP), XCLAMP);
+    }
+    for (int j = 0; j < NH; j++) {
+      double z = M[B1 + j];
+      for (int k = 0; k < NF; k++) z += (double)M[W1 + j * NF + k] * xn[k];
+      z1[j] = z;
+      a1[j] = z > 0 ? z : 0;
+    }
+    double out = M[B3];
+    for (int j = 0; j < NH; j++) {
+      double z = M[B2 + j];
+      for (int k = 0; k < NH; k++) z += (double)M[W2 + j * NH + k] * a1[k];
+      z2[j] = z;
+      a2[j] = z > 0 ? z : 0;
+      out += (double)M[W3 + j] * a2[j];
+    }
+    const double tn = ((double)target[s] - M[LMU]) / (double)M[LSIG];
+    const double r = out - tn;
+    loss += r * r;
+    const double d = 2.0 * r / n;
+    double d2[NH], d1[NH];
+    for (int j = 0; j < NH; j++) d2[j] = z2[j] > 0 ? d * M[W3 + j] : 0.0;
+    for (int k = 0; k < NH; k++) {
+      double g = 0;
+      for (int j = 0; j < NH; j++) g += (double)M[W2 + j * NH + k] * d2[j];
+      d1[k] = z1[k] > 0 ? g : 0.0;
+    }
+    for (int j = 0; j < NH; j++) {
+      for (int k = 0; k < NF; k++) grad[W1 - W1 + j * NF + k] += d1[j] * xn[k];
+      grad[B1 - W1 + j] += d1[j];
+      for (int k = 0; k < NH; k++) grad[W2 - W1 + j * NH + k] += d2[j] * a1[k];
+      grad[B2 - W1 + j] += d2[j];
+      grad[W3 - W1 + j] += d * a2[j];
+    }
+    grad[B3 - W1] += d;
+  }
+  return loss / n;
+}
+
 struct Queued { int age; int cursor; float height; };
 
 struct Edge { int tgt; unsigned char port; float w; };
@@ -271,6 +373,12 @@ struct Net {
   std::vector<Rec> recs;
   std::vector<std::vector<float>> rec_rows;
   long long n_derivs = 0;
+  long long n_rk5_steps = 0, n_rk5_trials = 0;
+  // learned step size: 0 plain, 1 log tuples, 2 network proposal (FP32 mode only)
+  int learn_mode = 0;
+  std::vector<float> model;
+  std::vector<float> steplog;
+  long long log_cap = 0, log_offered = 0;
   long long n_spikes_total = 0;
   long long n_events = 0;    // synaptic events delivered (edges traversed)
   std::string err;
@@ -777,6 +885,28 @@ struct Net {
     R err;
     const R hmin_acc = hmin * (R)(fp64 ? 1.00001 : (double)1.00001f);
     int trials = 0;
+    // learned step size: features after k1; the network proposes the first trial h
+    // when the plain h would not reach the end of the time step
+    float feat[sm::NF];
+    if (!fp64 && (learn_mode == 1 || (learn_mode == 2 && h < hmax))) {
+      const int npv = (m == AEIF_PSC_EXP) ? 1 : 2;
+      feat[0] = (float)y[0];
+      feat[1] = (float)y[1];
+      for (int p = 0; p < 4; p++) feat[2 + p] = (p < P) ? (float)y[2 + npv * p] : 0.0f;
+      float sdg = 0.0f;
+      for (int p = 0; p < P; p++) sdg = sdg + (float)k1[2 + npv * p];
+      feat[6] = slog_f((float)k1[0]);
+      feat[7] = slog_f(sdg);
+      feat[8] = log_m((float)h);
+      feat[9] = log_m((float)hmax);
+      if (learn_mode == 2) {
+        const float hp = mlp_propose_f(model.data(), feat);
+        if (hp > 0.0f && hp <= 3.0e38f) {
+          const float lo = model[sm::FLOOR] * (float)h;
+          h = (R)((hp > lo) ? hp : lo);
+        }
+      }
+    }
     for (;;) {
       if (h > hmax) h = hmax;
       if (h < hmin) h = hmin;
@@ -839,6 +969,21 @@ struct Net {
       if (fp64) h01 = (R)(0.1 * (double)h);
       h = (hnew > h01) ? hnew : h01;
     }
+    if (!fp64 && learn_mode == 1) {
+#pragma omp critical(steplog)
+      {
+        if (log_offered < log_cap) {
+          for (int k = 0; k < sm::NF; k++) steplog.push_back(feat[k]);
+          steplog.push_back((float)h);
+          steplog.push_back((float)err);
+        }
+        log_offered++;
+      }
+    }
+#pragma omp atomic
+    n_rk5_steps++;
+#pragma omp atomic
+    n_rk5_trials += trials;
     x += (double)h;
     if (err > K.err_min) h = h * K.coeff * pow_inc<R>(err, fp64);
     else h = (R)5 * h;
@@ -1225,6 +1370,53 @@ int orc_connect_arrays(void *p, size_t n, const int *src, const int *tgt, const 
   return 0;
   OR_CATCH(-1)
 }
+// ---- learned step size
+int orc_step_model_nparams() { return orc::sm::NPAR; }
+int orc_log_start(void *p, long long cap) {
+  OR_TRY
+  Net &n = *(Net *)p;
+  if (n.fp64) throw std::runtime_error("the learned step size needs the FP32 mode");
+  n.learn_mode = 1;
+  n.log_cap = cap;
+  n.log_offered = 0;
+  n.steplog.clear();
+  return 0;
+  OR_CATCH(-1)
+}
+int orc_log_stop(void *p) {
+  Net &n = *(Net *)p;
+  if (n.learn_mode == 1) n.learn_mode = 0;
+  return 0;
+}
+long long orc_log_count(void *p, long long *offered) {
+  Net &n = *(Net *)p;
+  if (offered) *offered = n.log_offered;
+  return (long long)(n.steplog.size() / orc::sm::LOG_W);
+}
+int orc_log_get(void *p, float *out) {
+  Net &n = *(Net *)p;
+  std::copy(n.steplog.begin(), n.steplog.end(), out);
+  return 0;
+}
+int orc_step_model_set(void *p, const float *params, int enable) {
+  OR_TRY
+  Net &n = *(Net *)p;
+  if (n.fp64) throw std::runtime_error("the learned step size needs the FP32 mode");
+  n.model.assign(params, params + orc::sm::NPAR);
+  n.learn_mode = enable ? 2 : 0;
+  return 0;
+  OR_CATCH(-1)
+}
+void orc_mlp_out(const float *params, const float *feat, int n, float *out) {
+  for (int s = 0; s < n; s++) out[s] = orc::mlp_out_f(params, feat + (size_t)s * orc::sm::NF);
+}
+void orc_mlp_propose(const float *params, const float *feat, int n, float *out) {
+  for (int s = 0; s < n; s++) out[s] = orc::mlp_propose_f(params, feat + (size_t)s * orc::sm::NF);
+}
+double orc_mlp_grad(const float *params, const float *feat, const float *target, int n, double *grad) {
+  return orc::mlp_grad_d(params, feat, target, n, grad);
+}
+
 int orc_threads() { return omp_get_max_threads(); }
 
 long long orc_n_conn(void *p) {
@@ -1312,6 +1504,8 @@ int orc_rec_spike_times(void *p, int node, float *out) {
 int orc_calibrate(void *p) { OR_TRY((Net *)p)->calibrate(); return 0; OR_CATCH(-1) }
 int orc_simulate(void *p, float T) { OR_TRY((Net *)p)->simulate(T); return 0; OR_CATCH(-1) }
 long long orc_n_derivs(void *p) { return ((Net *)p)->n_derivs; }
+long long orc_n_rk5_steps(void *p) { return ((Net *)p)->n_rk5_steps; }
+long long orc_n_rk5_trials(void *p) { return ((Net *)p)->n_rk5_trials; }
 long long orc_n_spikes(void *p) { return ((Net *)p)->n_spikes_total; }
 long long orc_n_events(void *p) { return ((Net *)p)->n_events; }
 double orc_neural_time(void *p) { return ((Net *)p)->neural_time; }

@@ -78,6 +78,8 @@ def lib():
             "orc_calibrate": (c_int, [c_void]),
             "orc_simulate": (c_int, [c_void, c_float]),
             "orc_n_derivs": (ctypes.c_longlong, [c_void]),
+            "orc_n_rk5_steps": (ctypes.c_longlong, [c_void]),
+            "orc_n_rk5_trials": (ctypes.c_longlong, [c_void]),
             "orc_n_spikes": (ctypes.c_longlong, [c_void]),
             "orc_n_events": (ctypes.c_longlong, [c_void]),
             "orc_neural_time": (ctypes.c_double, [c_void]),
@@ -85,6 +87,15 @@ def lib():
             "orc_log_m": (c_float, [c_float]),
             "orc_poisson_draw": (c_int, [c_float, c_ull, c_ull, ctypes.c_longlong]),
             "orc_philox": (None, [ctypes.c_uint] * 6 + [ctypes.POINTER(ctypes.c_uint)]),
+            "orc_step_model_nparams": (c_int, []),
+            "orc_log_start": (c_int, [c_void, ctypes.c_longlong]),
+            "orc_log_stop": (c_int, [c_void]),
+            "orc_log_count": (ctypes.c_longlong, [c_void, ctypes.POINTER(ctypes.c_longlong)]),
+            "orc_log_get": (c_int, [c_void, fp]),
+            "orc_step_model_set": (c_int, [c_void, fp, c_int]),
+            "orc_mlp_out": (None, [fp, fp, c_int, fp]),
+            "orc_mlp_propose": (None, [fp, fp, c_int, fp]),
+            "orc_mlp_grad": (ctypes.c_double, [fp, fp, fp, c_int, ctypes.POINTER(ctypes.c_double)]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -423,11 +434,77 @@ class Oracle(object):
     def NDerivs(self):
         return self.L.orc_n_derivs(self.h)
 
+    def NRk5Steps(self):
+        return self.L.orc_n_rk5_steps(self.h)
+
+    def NRk5Trials(self):
+        return self.L.orc_n_rk5_trials(self.h)
+
     def NSpikes(self):
         return self.L.orc_n_spikes(self.h)
 
     def NEvents(self):
         return self.L.orc_n_events(self.h)
+
+    # ---- learned RK5 step size (FP32 mode)
+    def Rk5LogStart(self, capacity):
+        self._chk(self.L.orc_log_start(self.h, int(capacity)))
+
+    def Rk5LogStop(self):
+        self._chk(self.L.orc_log_stop(self.h))
+
+    def Rk5LogCount(self):
+        off = ctypes.c_longlong(0)
+        n = self.L.orc_log_count(self.h, ctypes.byref(off))
+        return n, off.value
+
+    def Rk5LogGet(self):
+        """Logged tuples [n, 12]: 10 step features, accepted h, error of the accepted trial."""
+        n, _ = self.Rk5LogCount()
+        out = np.zeros((n, LOG_W), dtype=np.float32)
+        if n:
+            self.L.orc_log_get(self.h, _fptr(out))
+        return out
+
+    def StepModelSet(self, params, enable=True):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.size == STEP_MODEL_NPAR
+        self._chk(self.L.orc_step_model_set(self.h, _fptr(p), 1 if enable else 0))
+
+
+# learned step-size network: sizes of the flat parameter vector and of a log tuple
+STEP_MODEL_NPAR = 1465
+STEP_MODEL_NTRAIN = 1441
+STEP_MODEL_TRAIN0 = 20
+LOG_W = 12
+
+
+def mlp_out(params, feat):
+    """Network output for features [n, 10] (FP32, the engine kernel's arithmetic)."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    f = np.ascontiguousarray(feat, dtype=np.float32).reshape(-1, 10)
+    out = np.zeros(f.shape[0], dtype=np.float32)
+    lib().orc_mlp_out(_fptr(p), _fptr(f), f.shape[0], _fptr(out))
+    return out
+
+
+def mlp_propose(params, feat):
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    f = np.ascontiguousarray(feat, dtype=np.float32).reshape(-1, 10)
+    out = np.zeros(f.shape[0], dtype=np.float32)
+    lib().orc_mlp_propose(_fptr(p), _fptr(f), f.shape[0], _fptr(out))
+    return out
+
+
+def mlp_grad(params, feat, target):
+    """FP64 mean squared error and its gradient w.r.t. the trainable block W1..b3."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    f = np.ascontiguousarray(feat, dtype=np.float32).reshape(-1, 10)
+    t = np.ascontiguousarray(target, dtype=np.float32)
+    g = np.zeros(STEP_MODEL_NTRAIN, dtype=np.float64)
+    loss = lib().orc_mlp_grad(_fptr(p), _fptr(f), _fptr(t), f.shape[0],
+                              g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return loss, g
 
 
 def exp_m(x):

@@ -113,6 +113,24 @@ def main():
         counts = np.asarray(ngpu.GetStatus(neuron, "spike_count")).ravel()
         out = {"build_s": build, "sim_s": sim, "bio_ms": bio_ms, "rtf": sim / (bio_ms / 1000.0),
                "n_neurons": int(counts.size), "spikes": int(counts.sum())}
+    elif what.startswith("microcircuit:"):
+        # the iaf_psc_exp microcircuit: build, a 100 ms first call, then `bio_ms` timed
+        from workloads import microcircuit
+        _, scale, bio_ms = what.split(":")
+        scale, bio_ms = float(scale), float(bio_ms)
+        t0 = time.time()
+        pops = microcircuit(ngpu, scale=scale)
+        ngpu.Calibrate()
+        build = time.time() - t0
+        ngpu.Simulate(100.0)
+        c0 = [np.asarray(ngpu.GetStatus(p, "spike_count")).ravel() for p in pops]
+        t1 = time.time()
+        ngpu.Simulate(bio_ms)
+        sim = time.time() - t1
+        c1 = [np.asarray(ngpu.GetStatus(p, "spike_count")).ravel() for p in pops]
+        rates = [float((b - a).sum()) / len(b) / (bio_ms / 1000.0) for a, b in zip(c0, c1)]
+        out = {"build_s": build, "sim_s": sim, "bio_ms": bio_ms, "rtf": sim / (bio_ms / 1000.0),
+               "n_neurons": int(sum(len(p) for p in pops)), "pop_rates_hz": rates}
     print("JSON:" + json.dumps(out))
 
 

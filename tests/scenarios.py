@@ -177,3 +177,7 @@ def poisson_network(api, n=200, rate=12000.0, t_sim=200.0, seed=3, model="aeif_c
     api.ActivateSpikeCount(neuron)
     api.Simulate(t_sim)
     return np.asarray(api.GetStatus(neuron, "spike_count")).ravel().astype(np.int64)
+
+
+
+from workloads import c4_network  # noqa: E402,F401  (shared with bench.py)

@@ -218,3 +218,18 @@ def test_profile_and_launch_counters():
     assert upd > 0.0 and dlv > 0.0 and rec == 0.0
     assert ngpu.GetLaunchCount() > l0
     assert ngpu.GetStats()["steps"] == 250
+
+
+@pytest.mark.parametrize("threads,group,occ", [(64, 8, 0), (256, 16, 1), (128, 32, 1)])
+def test_launch_mappings_keep_results(threads, group, occ):
+    """The update block size and kernel variant and the delivery lane group change only
+    the launch mapping."""
+    ngpu.SetHostRng(True)
+    ngpu.SetUpdateThreads(threads)
+    ngpu.SetDeliverGroup(group)
+    ngpu.SetUpdateOccupancy(occ)
+    c_gpu, d_gpu = fixed_train_network(ngpu, model="aeif_cond_beta_multisynapse")
+    c_orc, d_orc = fixed_train_network(orc.Oracle(), model="aeif_cond_beta_multisynapse")
+    assert c_gpu.sum() > 0
+    assert np.array_equal(c_gpu, c_orc)
+    assert np.array_equal(np.float32(d_gpu), np.float32(d_orc))
