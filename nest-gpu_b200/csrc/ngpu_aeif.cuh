@@ -566,10 +566,14 @@ template <int MODEL, int PMAX, bool FIXED, int LM>
 int launch_aeif_p(const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
   const int tb = (A.threads == 64 || A.threads == 256) ? A.threads : 128;
   dim3 grid((A.n + tb - 1) / tb), block(tb);
-  if (LM == LM_PLAIN && A.occupancy)
-    aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1><<<grid, block, 0, st>>>(A, so, clk, k0, M);
-  else
-    aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0><<<grid, block, 0, st>>>(A, so, clk, k0, M);
+  bool occ = false;
+  if constexpr (LM == LM_PLAIN) {
+    if (A.occupancy) {
+      aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1><<<grid, block, 0, st>>>(A, so, clk, k0, M);
+      occ = true;
+    }
+  }
+  if (!occ) aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0><<<grid, block, 0, st>>>(A, so, clk, k0, M);
   if (A.budget <= 0) return 1;
   dim3 sgrid(A.n < 128 * 148 * 4 ? (A.n + 127) / 128 : 148 * 4), sblock(128);
   aeif_straggler_kernel<MODEL, PMAX, FIXED, LM><<<sgrid, sblock, 0, st>>>(A, so, clk, k0, M);

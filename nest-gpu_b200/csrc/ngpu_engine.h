@@ -308,6 +308,11 @@ class Engine {
   std::vector<float> model_;
   bool has_model_ = false;
   void set_learn_mode(int mode);
+  // all iaf_psc_exp groups in one launch when there are several
+  IafArgs *d_iaf_tab_ = nullptr;
+  int *d_iaf_blk0_ = nullptr;
+  int n_iaf_multi_ = 0, iaf_multi_blocks_ = 0;
+  void prepare_multi();
 
   template <class T> T *dalloc(size_t n);
   void free_device();
@@ -336,6 +341,8 @@ void engine_reset();
 int launch_aeif(int model, const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                 cudaStream_t st);
 int launch_iaf(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st);
+int launch_iaf_multi(const IafArgs *tab, const int *blk0, int ngroups, int nblocks, const SpikeOut &so,
+                     const Clock *clk, int k0, int M, cudaStream_t st);
 int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                      cudaStream_t st);
 int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *clk, int k0, int M,

@@ -31,10 +31,8 @@ __device__ __forceinline__ float iget(const IafArgs &A, int j, int i) {
   return p ? __ldg(p + i) : A.pval[j];
 }
 
-__global__ void __launch_bounds__(256) iaf_batch_kernel(const IafArgs A, const SpikeOut so,
-                                                        const Clock *clk, int k0, int M) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
+__device__ __forceinline__ void iaf_neuron(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0,
+                                           int M, int i) {
   const int n = A.n;
   float Iex = A.var[i], Iin = A.var[(size_t)n + i], V = A.var[2 * (size_t)n + i],
         refr = A.var[3 * (size_t)n + i];
@@ -70,6 +68,27 @@ __global__ void __launch_bounds__(256) iaf_batch_kernel(const IafArgs A, const S
   A.var[(size_t)n + i] = Iin;
   A.var[2 * (size_t)n + i] = V;
   A.var[3 * (size_t)n + i] = refr;
+}
+
+__global__ void __launch_bounds__(256) iaf_batch_kernel(const IafArgs A, const SpikeOut so,
+                                                        const Clock *clk, int k0, int M) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < A.n) iaf_neuron(A, so, clk, k0, M, i);
+}
+
+// All iaf_psc_exp groups in one launch (a network of several populations would
+// otherwise pay one launch per population and step): block b serves group g with
+// blk0[g] <= b < blk0[g+1]; the groups' argument blocks are in device memory.
+__global__ void __launch_bounds__(256) iaf_multi_kernel(const IafArgs *tab, const int *blk0, int ngroups,
+                                                        const SpikeOut so, const Clock *clk, int k0, int M) {
+  int lo = 0, hi = ngroups;   // largest g with blk0[g] <= blockIdx.x
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (blk0[mid] <= (int)blockIdx.x) lo = mid; else hi = mid;
+  }
+  const IafArgs &A = tab[lo];
+  const int i = ((int)blockIdx.x - blk0[lo]) * blockDim.x + threadIdx.x;
+  if (i < A.n) iaf_neuron(A, so, clk, k0, M, i);
 }
 
 // ---------------------------------------------------------------------------
@@ -219,6 +238,13 @@ int launch_aeif(int model, const AeifArgs &A, const SpikeOut &so, const Clock *c
 int launch_iaf(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
   if (A.n <= 0) return 0;
   iaf_batch_kernel<<<(A.n + 255) / 256, 256, 0, st>>>(A, so, clk, k0, M);
+  return 1;
+}
+
+int launch_iaf_multi(const IafArgs *tab, const int *blk0, int ngroups, int nblocks, const SpikeOut &so,
+                     const Clock *clk, int k0, int M, cudaStream_t st) {
+  if (nblocks <= 0) return 0;
+  iaf_multi_kernel<<<nblocks, 256, 0, st>>>(tab, blk0, ngroups, so, clk, k0, M);
   return 1;
 }
 

@@ -678,12 +678,40 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   count_launch(launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_,
                               deliver_group, d_clk_, k0, M, stream_));
   if (ev) cuda_check(cudaEventRecord((*ev)[1], stream_), "event");
+  if (n_iaf_multi_ >= 2)
+    count_launch(launch_iaf_multi(d_iaf_tab_, d_iaf_blk0_, n_iaf_multi_, iaf_multi_blocks_, so, d_clk_, k0, M,
+                                  stream_));
   for (auto &g : groups_) {
     if (is_aeif(g.model)) count_launch(launch_aeif(g.model, aeif_args(g), so, d_clk_, k0, M, stream_));
-    else if (g.model == M_IAF_PSC_EXP) count_launch(launch_iaf(iaf_args(g), so, d_clk_, k0, M, stream_));
+    else if (g.model == M_IAF_PSC_EXP && n_iaf_multi_ < 2)
+      count_launch(launch_iaf(iaf_args(g), so, d_clk_, k0, M, stream_));
     else if (g.model == M_SPIKE_GEN) count_launch(launch_spike_gen(sg_args(g), so, d_clk_, k0, M, stream_));
   }
   if (ev) cuda_check(cudaEventRecord((*ev)[2], stream_), "event");
+}
+
+// Argument table of the iaf groups for the single multi-group launch; rebuilt before
+// each graph capture (the arguments hold record-buffer pointers that can change).
+void Engine::prepare_multi() {
+  std::vector<IafArgs> tab;
+  std::vector<int> blk0;
+  int nb = 0;
+  for (auto &g : groups_) {
+    if (g.model != M_IAF_PSC_EXP || g.n <= 0) continue;
+    tab.push_back(iaf_args(g));
+    blk0.push_back(nb);
+    nb += (g.n + 255) / 256;
+  }
+  n_iaf_multi_ = (int)tab.size();
+  iaf_multi_blocks_ = nb;
+  if (n_iaf_multi_ < 2) return;
+  if (!d_iaf_tab_) {
+    d_iaf_tab_ = dalloc<IafArgs>(tab.size());
+    d_iaf_blk0_ = dalloc<int>(blk0.size());
+  }
+  cuda_check(cudaStreamSynchronize(stream_), "sync");
+  cuda_check(cudaMemcpy(d_iaf_tab_, tab.data(), tab.size() * sizeof(IafArgs), cudaMemcpyHostToDevice), "iaf table");
+  cuda_check(cudaMemcpy(d_iaf_blk0_, blk0.data(), blk0.size() * sizeof(int), cudaMemcpyHostToDevice), "iaf table");
 }
 
 void Engine::ensure_record_window(long long rows) {
@@ -710,6 +738,7 @@ void Engine::run_steps(long long n) {
       const int steps = (int)std::min<long long>(K, left);
       auto itg = graphs_.find(steps);
       if (itg == graphs_.end()) {
+        prepare_multi();
         cudaGraph_t graph;
         cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
         capturing_ = true;
@@ -884,6 +913,7 @@ std::vector<double> Engine::profile_steps(int n) {
   sim_time = (float)n * dt;
   start_simulation();
   ensure_record_window(n);
+  prepare_multi();
   std::vector<cudaEvent_t> ev(3);
   for (auto &e : ev) cuda_check(cudaEventCreate(&e), "event");
   std::vector<double> acc(3, 0.0);

@@ -6,17 +6,20 @@ import numpy as np
 def c4_network(api, seed=42, n=1000, drive_w=0.1, n_port=4):
     """The small balanced network (800 exc / 200 inh aeif_cond_beta_multisynapse,
     fixed in-degree 80 exc w=0.05 nS / 20 inh w=0.35 nS, delay 1.5 ms, 4 kHz Poisson
-    drive on receptor 0) with four receptors per neuron: E_rev 0, 0, -85, -85 mV,
-    tau_rise drawn from [0.2, 1] ms and tau_decay from [2, 20] ms (seeded, one value per
-    receptor); each projection is split evenly over its two receptors.  drive_w is the
+    drive on receptor 0) with four receptors per neuron: E_rev 0, 0, -85, -85 mV and, per
+    neuron and receptor, tau_rise uniform in [0.2, 1] ms and tau_decay uniform in [2, 20] ms
+    (seeded); each projection is split evenly over its two receptors.  drive_w is the
     Poisson weight (0.1 nS as in the plain network; larger values make it fire)."""
     api.SetKernelStatus("rnd_seed", seed)
     rng = np.random.RandomState(seed)
-    tau_rise = [float(x) for x in np.round(rng.uniform(0.2, 1.0, n_port), 3)]
-    tau_decay = [float(x) for x in np.round(rng.uniform(2.0, 20.0, n_port), 3)]
+    tau_rise = np.round(rng.uniform(0.2, 1.0, (n, n_port)), 3)
+    tau_decay = np.round(rng.uniform(2.0, 20.0, (n, n_port)), 3)
     neuron = api.Create("aeif_cond_beta_multisynapse", n, n_port)
     e_rev = [0.0] * (n_port // 2) + [-85.0] * (n_port - n_port // 2)
-    api.SetStatus(neuron, {"E_rev": e_rev, "tau_rise": tau_rise, "tau_decay": tau_decay})
+    api.SetStatus(neuron, {"E_rev": e_rev})
+    for i in range(n):
+        api.SetStatus(neuron[i:i + 1], {"tau_rise": [float(x) for x in tau_rise[i]],
+                                        "tau_decay": [float(x) for x in tau_decay[i]]})
     ne = int(0.8 * n)
     exc, inh = neuron[0:ne], neuron[ne:n]
     pg = api.Create("poisson_generator")

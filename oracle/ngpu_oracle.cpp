@@ -374,7 +374,9 @@ struct Net {
   std::vector<std::vector<float>> rec_rows;
   long long n_derivs = 0;
   long long n_rk5_steps = 0, n_rk5_trials = 0;
-  // learned step size: 0 plain, 1 log tuples, 2 network proposal (FP32 mode only)
+  // learned step size: 0 plain, 1 log tuples, 2 network proposal, 3 best possible proposal
+  // (every step starts from the largest step that passes the unchanged error test, found
+  // by bisection; an analysis bound, FP32 mode only)
   int learn_mode = 0;
   std::vector<float> model;
   std::vector<float> steplog;
@@ -871,6 +873,49 @@ struct Net {
     return (R)exp_m(-0.2f * log_m((float)err));
   }
 
+  // Error estimate (divided by the tolerance) of one FP32 trial step of size hh from y,
+  // with the step's k1 and error scale: the trial arithmetic of rk5_step.
+  template <class R>
+  R trial_error(Model m, int P, int NV, const R *y, const R *k1, const R *iys, R hh, const Par<R> &q, R refr) {
+    static const C5<R> K;
+    R a[64] = {}, b2[64] = {}, b3[64] = {}, b4[64] = {}, b5[64] = {}, b6[64] = {};
+    for (int i = 0; i < NV; i++) a[i] = fmaR(hh * K.a21, k1[i], y[i]);
+    derivs<R>(m, P, a, b2, q, refr);
+    for (int i = 0; i < NV; i++) a[i] = fmaR(hh * K.a32, b2[i], fmaR(hh * K.a31, k1[i], y[i]));
+    derivs<R>(m, P, a, b3, q, refr);
+    for (int i = 0; i < NV; i++) a[i] = fmaR(hh * K.a43, b3[i], fmaR(hh * K.a42, b2[i], fmaR(hh * K.a41, k1[i], y[i])));
+    derivs<R>(m, P, a, b4, q, refr);
+    for (int i = 0; i < NV; i++)
+      a[i] = fmaR(hh * K.a54, b4[i], fmaR(hh * K.a53, b3[i], fmaR(hh * K.a52, b2[i], fmaR(hh * K.a51, k1[i], y[i]))));
+    derivs<R>(m, P, a, b5, q, refr);
+    for (int i = 0; i < NV; i++)
+      a[i] = fmaR(hh * K.a65, b5[i],
+                  fmaR(hh * K.a64, b4[i], fmaR(hh * K.a63, b3[i], fmaR(hh * K.a62, b2[i], fmaR(hh * K.a61, k1[i], y[i])))));
+    derivs<R>(m, P, a, b6, q, refr);
+    R e = 0;
+    for (int i = 0; i < NV; i++) {
+      R v = fmaR(hh * K.e6, b6[i], fmaR(hh * K.e5, b5[i], fmaR(hh * K.e4, b4[i], fmaR(hh * K.e3, b3[i], hh * K.e1 * k1[i]))));
+      R av = std::fabs(v * iys[i]);
+      e = (e > av) ? e : av;
+    }
+    return e * (R)1.0e6f;
+  }
+
+  // Largest step in [hmin, hmax] whose trial passes the error test (bisection in log h,
+  // 30 halvings): what a perfect proposal would choose.  Analysis only.
+  template <class R>
+  R largest_passing_step(Model m, int P, int NV, const R *y, const R *k1, const R *iys, R hmin, R hmax,
+                         const Par<R> &q, R refr) {
+    if (trial_error<R>(m, P, NV, y, k1, iys, hmax, q, refr) <= (R)1) return hmax;
+    R lo = hmin, hi = hmax;
+    for (int it = 0; it < 30; it++) {
+      const R mid = (R)std::sqrt((double)lo * (double)hi);
+      if (trial_error<R>(m, P, NV, y, k1, iys, mid, q, refr) <= (R)1) lo = mid;
+      else hi = mid;
+    }
+    return lo;
+  }
+
   // One accepted RK5 step (src/rk5.h:69-159).  Returns derivative calls.
   template <class R>
   int rk5_step(Model m, int P, int NV, double &x, R *y, R &h, R hmin, R hmax, const Par<R> &q, R refr) {
@@ -888,6 +933,7 @@ struct Net {
     // learned step size: features after k1; the network proposes the first trial h
     // when the plain h would not reach the end of the time step
     float feat[sm::NF];
+    if (!fp64 && learn_mode == 3) h = largest_passing_step<R>(m, P, NV, y, k1, iys, hmin, hmax, q, refr);
     if (!fp64 && (learn_mode == 1 || (learn_mode == 2 && h < hmax))) {
       const int npv = (m == AEIF_PSC_EXP) ? 1 : 2;
       feat[0] = (float)y[0];
@@ -1380,6 +1426,14 @@ int orc_log_start(void *p, long long cap) {
   n.log_cap = cap;
   n.log_offered = 0;
   n.steplog.clear();
+  return 0;
+  OR_CATCH(-1)
+}
+int orc_set_bound_mode(void *p, int on) {
+  OR_TRY
+  Net &n = *(Net *)p;
+  if (n.fp64) throw std::runtime_error("the step-size bound needs the FP32 mode");
+  n.learn_mode = on ? 3 : 0;
   return 0;
   OR_CATCH(-1)
 }

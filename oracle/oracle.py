@@ -90,6 +90,7 @@ def lib():
             "orc_step_model_nparams": (c_int, []),
             "orc_log_start": (c_int, [c_void, ctypes.c_longlong]),
             "orc_log_stop": (c_int, [c_void]),
+            "orc_set_bound_mode": (c_int, [c_void, c_int]),
             "orc_log_count": (ctypes.c_longlong, [c_void, ctypes.POINTER(ctypes.c_longlong)]),
             "orc_log_get": (c_int, [c_void, fp]),
             "orc_step_model_set": (c_int, [c_void, fp, c_int]),
@@ -465,6 +466,11 @@ class Oracle(object):
         if n:
             self.L.orc_log_get(self.h, _fptr(out))
         return out
+
+    def StepBoundMode(self, on=True):
+        """Analysis mode: every RK5 step starts from the largest step that passes the error
+        test (bisection).  Its evaluation count is the floor any step proposal can reach."""
+        self._chk(self.L.orc_set_bound_mode(self.h, 1 if on else 0))
 
     def StepModelSet(self, params, enable=True):
         p = np.ascontiguousarray(params, dtype=np.float32)

@@ -113,6 +113,27 @@ def main():
         counts = np.asarray(ngpu.GetStatus(neuron, "spike_count")).ravel()
         out = {"build_s": build, "sim_s": sim, "bio_ms": bio_ms, "rtf": sim / (bio_ms / 1000.0),
                "n_neurons": int(counts.size), "spikes": int(counts.sum())}
+    elif what.startswith("stats:"):
+        # the benchmark network at `scale`: rate and ISI CV of 2000 recorded neurons
+        _, scale, bio_ms = what.split(":")
+        scale, bio_ms = float(scale), float(bio_ms)
+        neuron = big_network(scale, 20240)
+        n_rec = min(2000, len(neuron))
+        ngpu.ActivateRecSpikeTimes(neuron[0:n_rec], 4000)
+        ngpu.Simulate(200.0)   # transient
+        c0 = np.asarray(ngpu.GetStatus(neuron, "spike_count")).ravel()
+        ngpu.GetRecSpikeTimes(neuron[0:n_rec])   # the transient's times
+        ngpu.Simulate(bio_ms)
+        c1 = np.asarray(ngpu.GetStatus(neuron, "spike_count")).ravel()
+        cvs = []
+        for t in ngpu.GetRecSpikeTimes(neuron[0:n_rec]):
+            t = np.asarray(t, dtype=np.float64)
+            t = t[t > 200.0]
+            if t.size >= 4:
+                isi = np.diff(t)
+                cvs.append(isi.std() / isi.mean())
+        out = {"rate_hz": float((c1 - c0).sum()) / len(neuron) / (bio_ms / 1000.0),
+               "isi_cv": float(np.mean(cvs)), "n_cv": len(cvs)}
     elif what.startswith("microcircuit:"):
         # the iaf_psc_exp microcircuit: build, a 100 ms first call, then `bio_ms` timed
         from workloads import microcircuit
@@ -131,6 +152,9 @@ def main():
         rates = [float((b - a).sum()) / len(b) / (bio_ms / 1000.0) for a, b in zip(c0, c1)]
         out = {"build_s": build, "sim_s": sim, "bio_ms": bio_ms, "rtf": sim / (bio_ms / 1000.0),
                "n_neurons": int(sum(len(p) for p in pops)), "pop_rates_hz": rates}
+        if getattr(ngpu, "is_b200_engine", False):
+            out["device_ms_per_step"] = ngpu.GetSimDeviceMs() / (bio_ms / 0.1)
+            out["profile_ms_per_step"] = ngpu.ProfileSteps(1000)
     print("JSON:" + json.dumps(out))
 
 

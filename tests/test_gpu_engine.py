@@ -233,3 +233,20 @@ def test_launch_mappings_keep_results(threads, group, occ):
     assert c_gpu.sum() > 0
     assert np.array_equal(c_gpu, c_orc)
     assert np.array_equal(np.float32(d_gpu), np.float32(d_orc))
+
+
+def test_microcircuit_slice_bitexact():
+    """The layered microcircuit at 3% size (eight iaf_psc_exp populations served by one
+    multi-group launch, fixed_total_number projections with normal_clipped weights and
+    delays, Poisson background): spike counts neuron by neuron equal the oracle's."""
+    from workloads import microcircuit
+    ngpu.SetHostRng(True)
+    pops_g = microcircuit(ngpu, scale=0.03)
+    o = orc.Oracle()
+    pops_o = microcircuit(o, scale=0.03)
+    ngpu.Simulate(150.0)
+    o.Simulate(150.0)
+    c_g = np.concatenate([np.asarray(ngpu.GetStatus(p, "spike_count")).ravel() for p in pops_g])
+    c_o = np.concatenate([np.asarray(o.GetStatus(p, "spike_count")).ravel() for p in pops_o])
+    assert c_g.sum() > 1000
+    assert np.array_equal(c_g, c_o)

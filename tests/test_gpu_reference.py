@@ -39,6 +39,17 @@ def run_reference(what, timeout=600):
     return json.loads(line[5:])
 
 
+def run_own(what, timeout=600):
+    """The same scenario through this engine's library, in a child process."""
+    env = dict(os.environ)
+    env.pop("NESTGPU_LIB", None)
+    p = subprocess.run([sys.executable, RUNNER, what], env=env, capture_output=True, text=True,
+                       timeout=timeout)
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = [x for x in p.stdout.splitlines() if x.startswith("JSON:")][-1]
+    return json.loads(line[5:])
+
+
 @pytest.fixture(autouse=True)
 def fresh_engine():
     ngpu.Reset()
@@ -84,3 +95,28 @@ def test_spike_counts_match_reference(model):
     counts, _ = fixed_train_network(ngpu, model=model)
     assert counts.sum() > 0
     assert counts.tolist() == ref["counts"]
+
+
+@needs_ref
+def test_network_rate_and_isi_cv_match_reference():
+    """Chaotic regime: the benchmark network at 1/10 size (100k AdEx neurons, ~20 Hz),
+    1 s after a 200 ms transient.  Poisson streams differ by design (Philox vs cuRAND), so
+    the comparison is statistical: mean rate and mean ISI CV of 2000 neurons within 2%."""
+    ref = run_reference("stats:0.1:1000", timeout=900)
+    own = run_own("stats:0.1:1000")
+    assert own["rate_hz"] > 5.0 and own["n_cv"] > 500
+    assert abs(own["rate_hz"] - ref["rate_hz"]) <= 0.02 * ref["rate_hz"]
+    assert abs(own["isi_cv"] - ref["isi_cv"]) <= 0.02 * ref["isi_cv"]
+
+
+@needs_ref
+def test_microcircuit_rates_match_reference():
+    """The iaf_psc_exp microcircuit at 1/10 size: mean rate over all populations within 2%
+    of the reference build's, each population within 10% (a few hundred neurons each)."""
+    ref = run_reference("microcircuit:0.1:1000", timeout=900)
+    own = run_own("microcircuit:0.1:1000")
+    r_ref, r_own = np.array(ref["pop_rates_hz"]), np.array(own["pop_rates_hz"])
+    n = np.round(np.array([20683, 5834, 21915, 5479, 4850, 1065, 14395, 2948]) * 0.1)
+    mean_ref, mean_own = (r_ref * n).sum() / n.sum(), (r_own * n).sum() / n.sum()
+    assert abs(mean_own - mean_ref) <= 0.02 * mean_ref
+    assert np.all(np.abs(r_own - r_ref) <= 0.10 * np.maximum(r_ref, 1.0))

@@ -155,3 +155,23 @@ def test_proposal_keeps_error_control():
         assert abs(int(c.sum()) - int(c64.sum())) <= max(2, 0.02 * c64.sum())
         assert np.max(np.abs(v[:100] - v64[:100])) < 1e-3
     assert res["const"][2] != res["plain"][2]
+
+
+def test_bound_mode_is_a_floor():
+    """The bound mode starts every step from the largest step that passes the error test;
+    no proposal, learned or constant, needs fewer derivative evaluations, and the dynamics
+    stay those of the same network."""
+    res = {}
+    for mode in ("plain", "bound", "const"):
+        o = orc.Oracle()
+        n = small_c4(o, seed=11, drive_w=1.5)
+        if mode == "bound":
+            o.StepBoundMode(True)
+        elif mode == "const":
+            o.StepModelSet(constant_model(0.02), enable=True)
+        o.Simulate(50.0)
+        res[mode] = (o.NDerivs(), int(np.array(o.GetStatus(n, "spike_count")).sum()),
+                     o.NRk5Trials() - o.NRk5Steps())
+    assert res["bound"][0] < res["plain"][0] and res["bound"][0] < res["const"][0]
+    assert res["bound"][2] == 0          # the bound never needs a rejected trial
+    assert abs(res["bound"][1] - res["plain"][1]) <= 0.02 * res["plain"][1]
