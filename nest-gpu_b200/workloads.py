@@ -166,19 +166,20 @@ def learned_vs_plain(ngpu, drive_w, log_ms=2000.0, eval_ms=1000.0):
     ngpu.Rk5LogStop()
     n_log, _ = ngpu.Rk5LogCount()
     out = {"drive_nS": drive_w, "logged_steps": n_log}
-    plain, rate_p = evals(43, None, eval_ms)
-    out.update(plain_evals_per_neuron_ms=plain, plain_rate_hz=rate_p)
     t0 = time.time()
     try:
         used, loss = ngpu.StepModelTrain(iters=3000, batch=4096, lr=2e-3, safety=0.9, floor=0.0, seed=3)
+        model = ngpu.StepModelGet()
     except ValueError as e:
         # no step of the plain integrator was limited by accuracy: the network would never
         # be consulted, and the learned method is the plain one
-        out.update(trained_on=0, learned_evals_per_neuron_ms=plain, learned_rate_hz=rate_p, ratio=1.0,
-                   note="not trained: " + str(e))
-        return out
+        used, model, note = 0, None, "not trained: " + str(e)
     train_s = time.time() - t0
-    model = ngpu.StepModelGet()
+    plain, rate_p = evals(43, None, eval_ms)
+    out.update(plain_evals_per_neuron_ms=plain, plain_rate_hz=rate_p)
+    if model is None:
+        out.update(trained_on=0, learned_evals_per_neuron_ms=plain, learned_rate_hz=rate_p, ratio=1.0, note=note)
+        return out
     best = None
     for sf in (0.5, 0.6, 0.7, 0.8, 0.9):
         m = model.copy()

@@ -119,14 +119,14 @@ def main():
         scale, bio_ms = float(scale), float(bio_ms)
         neuron = big_network(scale, 20240)
         n_rec = min(2000, len(neuron))
-        ngpu.ActivateRecSpikeTimes(neuron[0:n_rec], 4000)
+        # the reference records spike times only for whole groups
+        ngpu.ActivateRecSpikeTimes(neuron, int(200 * (bio_ms + 200.0) / 1000.0) + 20)
         ngpu.Simulate(200.0)   # transient
         c0 = np.asarray(ngpu.GetStatus(neuron, "spike_count")).ravel()
-        ngpu.GetRecSpikeTimes(neuron[0:n_rec])   # the transient's times
         ngpu.Simulate(bio_ms)
         c1 = np.asarray(ngpu.GetStatus(neuron, "spike_count")).ravel()
         cvs = []
-        for t in ngpu.GetRecSpikeTimes(neuron[0:n_rec]):
+        for t in ngpu.GetRecSpikeTimes(neuron)[:n_rec]:
             t = np.asarray(t, dtype=np.float64)
             t = t[t > 200.0]
             if t.size >= 4:

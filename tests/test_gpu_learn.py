@@ -101,14 +101,10 @@ def test_learned_proposal_bit_exact(which):
 @pytest.mark.parametrize("drive_w", [0.1, 1.0])
 def test_trained_proposal_on_held_out_seed(drive_w):
     """Log 2 s of the plain integrator, train on the GPU, pick the safety factor on the
-    training seed, evaluate on a held-out seed.  In the quiet network no step is limited by
-    accuracy (one RK5 step per time step), so the network is never consulted; in the firing
-    network it must not cost evaluations and must keep the firing rate."""
+    training seed, evaluate on a held-out seed: the proposal must not cost evaluations and
+    must keep the firing rate, in the quiet network (0.1 nS drive) and the firing one."""
     r = learned_vs_plain(ngpu, drive_w)
     print("\nC4 drive %.2f nS: %s" % (drive_w, r))
     assert abs(r["learned_rate_hz"] - r["plain_rate_hz"]) <= 0.02 * max(r["plain_rate_hz"], 1.0)
-    if r["trained_on"] == 0:
-        assert r["plain_evals_per_neuron_ms"] <= 60.0 * 1.005
-        assert r["logged_steps"] > 0
-    else:
-        assert r["learned_evals_per_neuron_ms"] <= r["plain_evals_per_neuron_ms"]
+    assert r["logged_steps"] > 0 and r["trained_on"] > 0
+    assert r["learned_evals_per_neuron_ms"] <= r["plain_evals_per_neuron_ms"]
