@@ -46,6 +46,11 @@ STEP_MS = 100.0
 FLOPS_PER_DERIV = 110        # FP32 flops per derivative evaluation incl. stage algebra, 2 ports
 DELIVERY_BYTES_PER_EVENT = 8  # 4 B packed target/port + 4 B weight per synaptic event
 DELIVERY_BYTES_PER_SPIKE = 8  # ring entry (source, height)
+# DRAM traffic per unit from the ncu captures of the 1/10-size network (summaries in
+# profiles/deliver_batch_kernel_1M_network_at_0.1_scale.md and
+# profiles/aeif_batch_kernel_1M_network_at_0.1_scale.md), scaled to a launch by its units
+DELIVERY_TRAFFIC_PER_EVENT = 29.1e6 / 1.91e6   # bytes per synaptic event
+RK5_TRAFFIC_PER_NEURON_STEP = 22.84e6 / 1.0e6  # bytes per neuron-step
 
 
 def parse():
@@ -57,6 +62,7 @@ def parse():
     p.add_argument("--scale", type=float, default=1.0, help="fraction of the 1M-neuron network (tests)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="keep the default launch mappings")
+    p.add_argument("--batch-max", type=int, default=0, help="upper bound of the time-batch length")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the learned-step and ensemble measurements")
     return p.parse_args()
@@ -194,6 +200,8 @@ def engine_arm(args):
 
     seed = 20240 + 101 * RANK
     t_build0 = time.time()
+    if args.batch_max > 0:
+        ngpu.SetBatchMax(args.batch_max)
     neuron, pg = build_engine_network(ngpu, args.scale, seed)
     ngpu.Calibrate()
     build_s = time.time() - t_build0
@@ -239,6 +247,7 @@ def engine_arm(args):
     p_derivs = (st_p1["n_derivs"] - st_p0["n_derivs"]) / prof_steps
     p_events = (st_p1["n_events"] - st_p0["n_events"]) / prof_steps
     p_spikes = (st_p1["n_spikes"] - st_p0["n_spikes"]) / prof_steps
+    M = ngpu.GetBatchLength()   # steps per launch of the update and delivery kernels
     fp32_peak = (148 * 128 * 2 * (clocks["sm_mhz"] or 1965.0) * 1e6) / 1e12
     rk5_tflops = p_derivs * FLOPS_PER_DERIV / (upd_ms / 1e3) / 1e12
     deliver_gbs = (p_events * DELIVERY_BYTES_PER_EVENT + p_spikes * DELIVERY_BYTES_PER_SPIKE) / (del_ms / 1e3) / 1e9
@@ -292,12 +301,16 @@ def engine_arm(args):
                 "d2h_bytes_per_step": 4 * n_neurons},
         "roofline": {"bound": "fp32", "kernel": "aeif_batch_kernel + aeif_straggler_kernel (RK5)",
                      "achieved": rk5_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
-                     "frac": rk5_tflops / fp32_peak, "traffic": None,
+                     "frac": rk5_tflops / fp32_peak,
+                     "traffic": RK5_TRAFFIC_PER_NEURON_STEP * n_neurons * M,
+                     "flops_per_launch": p_derivs * FLOPS_PER_DERIV * M, "steps_per_launch": M,
                      "peak_source": "nominal FP32 rate 148 SM x 128 lanes x 2 x sampled SM clock",
                      "ms_per_step": upd_ms},
         "roofline_delivery": {"bound": "hbm", "kernel": "deliver_batch_kernel", "achieved": deliver_gbs,
                               "peak": hbm_peak, "unit": "GB/s", "frac": deliver_gbs / hbm_peak,
-                              "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                              "traffic": DELIVERY_TRAFFIC_PER_EVENT * p_events * M,
+                              "bytes_per_launch": (p_events * DELIVERY_BYTES_PER_EVENT +
+                                                   p_spikes * DELIVERY_BYTES_PER_SPIKE) * M, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                               "ms_per_step": del_ms},
         "clocks": clocks,
     }

@@ -296,6 +296,9 @@ int NGPU_BuildDeliveryCsrNoAlloc(const int *src, const int *dly, const unsigned 
 
 /* Steps captured per CUDA graph (default 100). */
 int NGPU_SetGraphSteps(int n);
+/* Steps per time batch of the calibrated network: the kernels advance this many steps per
+   launch (the minimum delay in steps + 1, at most 32 and at most the batch_max setting). */
+int NGPU_GetBatchLength(void);
 
 /* Threads per block of the aeif update kernel (64, 128 or 256; default 128). */
 int NGPU_SetUpdateThreads(int n);

@@ -76,27 +76,64 @@ __device__ __forceinline__ void push_spike(const SpikeOut &so, const GroupSpikeR
   }
 }
 
-// Input arriving in step (tidx, tnow) for neuron i: the accumulator slot m (spikes
-// delivered this step, src/get_spike.cu:60-108) plus this step's poiss_gen draws
-// (src/poiss_gen.cu:55-86); the slot is cleared for its next use.
-__device__ __forceinline__ void step_inputs(double *in, int nport, int n, int i, const GroupInput &G,
-                                            int m, long long tidx, double tnow) {
-  double *acc = G.acc + (size_t)m * G.slot_stride;
-  for (int p = 0; p < nport; p++) {
-    double a = acc[(size_t)p * n + i];
-    in[p] = a;
-    if (a != 0.0) acc[(size_t)p * n + i] = 0.0;
-  }
+// The poiss_gen edges of a neuron do not change during a batch: with exactly one edge
+// (the common case) it and its generator are loaded once per batch.
+struct PoissonCache {
+  int e0, e1;
+  PoissonIn pe;
+  GenPar g;
+};
+
+__device__ __forceinline__ void poisson_cache_load(const GroupInput &G, int i, PoissonCache &c) {
+  c.e0 = c.e1 = 0;
   if (G.pin_off) {
-    const int e0 = G.pin_off[i], e1 = G.pin_off[i + 1];
-    for (int e = e0; e < e1; e++) {
+    c.e0 = G.pin_off[i];
+    c.e1 = G.pin_off[i + 1];
+    if (c.e1 - c.e0 == 1) {
+      c.pe = G.pin[c.e0];
+      c.g = G.gen[c.pe.gen];
+    }
+  }
+}
+
+__device__ __forceinline__ void poisson_add(double *in, const GroupInput &G, const PoissonIn &pe, const GenPar &g,
+                                            long long tidx, double tnow) {
+  const double t_rel = tnow - (double)g.origin - (double)pe.delay;
+  if (t_rel >= (double)g.start && t_rel <= (double)g.stop) {
+    int k = poisson_draw(__fmul_rn(G.lam_scale, g.rate), G.seed, pe.edge_id, tidx);
+    if (k > 0) in[pe.port] += (double)__fmul_rn(pe.weight, (float)k);
+  }
+}
+
+// Spike input of step m, read at the start of the step so that the load latency hides
+// behind the step's integration (the delivery of the batch finished before the kernel).
+template <int PMAX>
+__device__ __forceinline__ void acc_prefetch(double *a, int np, int n, int i, const GroupInput &G, int m) {
+  const double *acc = G.acc + (size_t)m * G.slot_stride;
+#pragma unroll
+  for (int p = 0; p < PMAX; p++) a[p] = (p < np) ? acc[(size_t)p * n + i] : 0.0;
+}
+
+// Input arriving in step (tidx, tnow) for neuron i: the accumulator slot m (spikes
+// delivered this step, src/get_spike.cu:60-108), prefetched, plus this step's poiss_gen
+// draws (src/poiss_gen.cu:55-86); the nonzero accumulator entries are cleared for their
+// next use.
+template <int PMAX>
+__device__ __forceinline__ void step_inputs_pf(double *in, const double *a, int np, int n, int i,
+                                               const GroupInput &G, const PoissonCache &c, int m, long long tidx,
+                                               double tnow) {
+  double *acc = G.acc + (size_t)m * G.slot_stride;
+#pragma unroll
+  for (int p = 0; p < PMAX; p++) {
+    in[p] = a[p];
+    if (p < np && a[p] != 0.0) acc[(size_t)p * n + i] = 0.0;
+  }
+  if (c.e1 - c.e0 == 1) {
+    poisson_add(in, G, c.pe, c.g, tidx, tnow);
+  } else {
+    for (int e = c.e0; e < c.e1; e++) {
       const PoissonIn pe = G.pin[e];
-      const GenPar g = G.gen[pe.gen];
-      const double t_rel = tnow - (double)g.origin - (double)pe.delay;
-      if (t_rel >= (double)g.start && t_rel <= (double)g.stop) {
-        int k = poisson_draw(__fmul_rn(G.lam_scale, g.rate), G.seed, pe.edge_id, tidx);
-        if (k > 0) in[pe.port] += (double)__fmul_rn(pe.weight, (float)k);
-      }
+      poisson_add(in, G, pe, G.gen[pe.gen], tidx, tnow);
     }
   }
 }
@@ -435,12 +472,13 @@ __device__ __forceinline__ void write_records(const GroupRecord &R, const SpikeO
 template <int MODEL, int PMAX, bool FIXED>
 __device__ __forceinline__ void aeif_end_step(const AeifArgs &A, const SpikeOut &so, int i,
                                               const AeifQ<MODEL, PMAX, FIXED> &q, float *y, float refr,
-                                              int m, const StepT &t, long long rec_it0) {
+                                              int m, const StepT &t, long long rec_it0, const double *apf,
+                                              const PoissonCache &pc) {
   typedef AeifShape<MODEL> S;
   const int np = q.ports();
   if (A.rec.first) write_records(A.rec, so, A.i0 + i, i, y, 2 + S::npv * np, refr, t.it - rec_it0, t.tidx);
   double in[PMAX];
-  step_inputs(in, np, A.n, i, A.in, m, t.tidx, t.tnow);
+  step_inputs_pf<PMAX>(in, apf, np, A.n, i, A.in, pc, m, t.tidx, t.tnow);
 #pragma unroll
   for (int p = 0; p < PMAX; p++) {
     if (p < np && in[p] != 0.0) {
@@ -504,16 +542,20 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
     aeif_load<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
     const long long rec_it0 = clk->rec_it0;
     int budget = A.budget > 0 ? A.budget : -1;
+    PoissonCache pc;
+    poisson_cache_load(A.in, i, pc);
     int m = 0;
     bool deferred = false;
     for (; m < M; m++) {
       const StepT t = step_at(clk, k0, m, A.dt);
+      double apf[PMAX];
+      acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
       if (!aeif_integrate<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, budget, nd,
                                                   smodel)) {
         deferred = true;
         break;
       }
-      aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0);
+      aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
     }
     aeif_store<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
     if (deferred) {
@@ -550,10 +592,14 @@ __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, c
     double x;
     aeif_load<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
     int budget = -1;
+    PoissonCache pc;
+    poisson_cache_load(A.in, i, pc);
     for (int m = e.y; m < M; m++) {
       const StepT t = step_at(clk, k0, m, A.dt);
+      double apf[PMAX];
+      acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
       aeif_integrate<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, budget, nd, smodel);
-      aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0);
+      aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
     }
     aeif_store<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
   }

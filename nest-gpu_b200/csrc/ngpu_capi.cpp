@@ -760,6 +760,13 @@ int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliv
   }, -1);
 }
 
+int NGPU_GetBatchLength() {
+  return guard([&] {
+    if (!E().calibrated()) throw NgpuError("the batch length is known after calibration");
+    return E().batch_length();
+  }, -1);
+}
+
 int NGPU_SetGraphSteps(int n) {
   return guard([&] {
     if (n < 1) throw NgpuError("graph steps must be >= 1");

@@ -221,6 +221,7 @@ class Engine {
   bool has_step_model() const { return has_model_; }
   void step_model_enable(bool on);
   int learn_mode() const { return learn_mode_; }
+  int batch_length() const { return batch_; }
 
   // device buffers exposed to the engine-level helpers
   cudaStream_t stream() const { return stream_; }

@@ -41,8 +41,12 @@ __device__ __forceinline__ void iaf_neuron(const IafArgs &A, const SpikeOut &so,
               P11in = iget(A, IP_P11in, i), theta = iget(A, IP_Theta_rel, i),
               V_reset = iget(A, IP_V_reset_rel, i), refr_steps = iget(A, IP_refr_steps, i);
   const long long rec_it0 = clk->rec_it0;
+  PoissonCache pc;
+  poisson_cache_load(A.in, i, pc);
   for (int m = 0; m < M; m++) {
     const StepT t = step_at(clk, k0, m, A.dt);
+    double apf[2];
+    acc_prefetch<2>(apf, 2, n, i, A.in, m);
     if (refr > 0.0f) {
       refr = __fsub_rn(refr, 1.0f);
     } else {
@@ -60,7 +64,7 @@ __device__ __forceinline__ void iaf_neuron(const IafArgs &A, const SpikeOut &so,
       write_records(A.rec, so, A.i0 + i, i, yr, 4, refr, t.it - rec_it0, t.tidx);
     }
     double in[2];
-    step_inputs(in, 2, n, i, A.in, m, t.tidx, t.tnow);
+    step_inputs_pf<2>(in, apf, 2, n, i, A.in, pc, m, t.tidx, t.tnow);
     if (in[0] != 0.0) Iex = (float)__fma_rn(in[0], 1.0, (double)Iex);
     if (in[1] != 0.0) Iin = (float)__fma_rn(in[1], 1.0, (double)Iin);
   }
@@ -119,7 +123,9 @@ __global__ void spike_gen_batch_kernel(const SpikeGenArgs A, const SpikeOut so, 
 // spike, delay group) with arrival step in the batch; a group of G lanes (G = 8, 16
 // or 32: short segments waste fewer lanes with small G) per item streams the item's
 // CSR segment with coalesced 8-byte loads and FP64 atomics into the accumulator
-// slot of the arrival step.
+// slot of the arrival step.  Items are numbered arrival-step-major, so the items in
+// flight at any moment reduce into one or two slots and those stay in L2 even when
+// all slots of a batch together do not.
 // ---------------------------------------------------------------------------
 constexpr int DELIVER_THREADS = 256;
 constexpr int MAX_PAIRS = 8192;     // dspan * M
@@ -138,7 +144,7 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_batch_kernel(const De
   for (int j = 0; j < per; j++) {
     const int pr = b0 + j;
     if (pr < npairs) {
-      const int dd = pr / M, m = pr - dd * M;
+      const int m = pr / A.dspan, dd = pr - m * A.dspan;
       const long long te = t_first + m - 1 - (A.dmin + dd);   // emission step
       int c = 0;
       if (te >= 1) {
@@ -178,7 +184,7 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_batch_kernel(const De
       const int mid = (lo + hi) >> 1;
       if (s_pref[mid] <= item) lo = mid; else hi = mid;
     }
-    const int dd = lo / M, m = lo - dd * M;
+    const int m = lo / A.dspan, dd = lo - m * A.dspan;
     const int j = item - s_pref[lo];
     const long long te = t_first + m - 1 - (A.dmin + dd);
     const int2 sp = A.ring[(size_t)(te % A.R) * A.cap + j];

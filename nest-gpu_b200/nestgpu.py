@@ -167,6 +167,7 @@ if is_b200_engine:
     _c["NGPU_SetUpdateThreads"] = _bind("NGPU_SetUpdateThreads", _I, [_I])
     _c["NGPU_SetDeliverGroup"] = _bind("NGPU_SetDeliverGroup", _I, [_I])
     _c["NGPU_SetUpdateOccupancy"] = _bind("NGPU_SetUpdateOccupancy", _I, [_I])
+    _c["NGPU_GetBatchLength"] = _bind("NGPU_GetBatchLength", _I, [])
     _c["NGPU_Autotune"] = _bind("NGPU_Autotune", _I, [_I] + [ctypes.POINTER(_I)] * 4)
     _c["NGPU_GetSimDeviceMs"] = _bind("NGPU_GetSimDeviceMs", ctypes.c_double, [])
     _c["NGPU_GetLaunchCount"] = _bind("NGPU_GetLaunchCount", ctypes.c_longlong, [])
@@ -1315,6 +1316,14 @@ def SetUpdateThreads(n):
     """Threads per block of the aeif update kernel: 64, 128 or 256 (engine extension)."""
     _need_b200("SetUpdateThreads")
     return _check(_c["NGPU_SetUpdateThreads"](n))
+
+
+def GetBatchLength():
+    """Steps per time batch (kernel launch) of the calibrated network (engine extension)."""
+    _need_b200("GetBatchLength")
+    n = _c["NGPU_GetBatchLength"]()
+    _check()
+    return n
 
 
 def SetUpdateOccupancy(on=True):
