@@ -192,36 +192,40 @@ __device__ __forceinline__ void aeif_derivs(const float *y, float *dy,
   }
 }
 
+// UNI: every parameter of the group is uniform, so each one is read from the kernel
+// arguments (constant bank) where it is used and needs no register of its own.
+template <bool UNI = false>
 __device__ __forceinline__ float pget(const AeifArgs &A, int j, int i) {
+  if (UNI) return A.pval[j];
   const float *p = A.parr[j];
   return p ? __ldg(p + i) : A.pval[j];
 }
 
-template <int MODEL, int PMAX, bool FIXED>
+template <int MODEL, int PMAX, bool FIXED, bool UNI = false>
 __device__ __forceinline__ void load_aeif_par(const AeifArgs &A, int i, AeifQ<MODEL, PMAX, FIXED> &q) {
   q.np = A.nport;
-  q.V_th = pget(A, AP_V_th, i);
-  q.Delta_T = pget(A, AP_Delta_T, i);
-  q.inv_Delta_T = pget(A, AP_inv_Delta_T, i);
-  q.g_L = pget(A, AP_g_L, i);
-  q.E_L = pget(A, AP_E_L, i);
-  q.inv_C_m = pget(A, AP_inv_C_m, i);
-  q.a = pget(A, AP_a, i);
-  q.b = pget(A, AP_b, i);
-  q.inv_tau_w = pget(A, AP_inv_tau_w, i);
-  q.I_e = pget(A, AP_I_e, i);
-  q.V_peak = pget(A, AP_V_peak, i);
-  q.V_reset = pget(A, AP_V_reset, i);
-  q.refr_steps = pget(A, AP_refr_steps, i);
+  q.V_th = pget<UNI>(A, AP_V_th, i);
+  q.Delta_T = pget<UNI>(A, AP_Delta_T, i);
+  q.inv_Delta_T = pget<UNI>(A, AP_inv_Delta_T, i);
+  q.g_L = pget<UNI>(A, AP_g_L, i);
+  q.E_L = pget<UNI>(A, AP_E_L, i);
+  q.inv_C_m = pget<UNI>(A, AP_inv_C_m, i);
+  q.a = pget<UNI>(A, AP_a, i);
+  q.b = pget<UNI>(A, AP_b, i);
+  q.inv_tau_w = pget<UNI>(A, AP_inv_tau_w, i);
+  q.I_e = pget<UNI>(A, AP_I_e, i);
+  q.V_peak = pget<UNI>(A, AP_V_peak, i);
+  q.V_reset = pget<UNI>(A, AP_V_reset, i);
+  q.refr_steps = pget<UNI>(A, AP_refr_steps, i);
   const int np = q.ports();
 #pragma unroll
   for (int p = 0; p < PMAX; p++) {
     if (p < np) {
       const int b = AEIF_NSCAL + AEIF_NPORTPAR * p;
-      q.E_rev[p] = pget(A, b + 0, i);
-      q.inv_t1[p] = pget(A, b + 1, i);
-      q.inv_t2[p] = pget(A, b + 2, i);
-      q.pw[p] = pget(A, b + 3, i);
+      q.E_rev[p] = pget<UNI>(A, b + 0, i);
+      q.inv_t1[p] = pget<UNI>(A, b + 1, i);
+      q.inv_t2[p] = pget<UNI>(A, b + 2, i);
+      q.pw[p] = pget<UNI>(A, b + 3, i);
     }
   }
 }
@@ -520,7 +524,7 @@ __device__ __forceinline__ void warp_add(unsigned long long *ctr, unsigned long 
 // Main aeif kernel: one thread per neuron, steps m = 0..M-1 of the batch.
 // OCC = 1 caps the registers so that three 256-thread blocks fit on an SM (more warps
 // in flight to hide the dependent FP32 latency, at the price of a few spills).
-template <int MODEL, int PMAX, bool FIXED, int LM, int OCC = 0>
+template <int MODEL, int PMAX, bool FIXED, int LM, int OCC = 0, bool UNI = false>
 __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const AeifArgs A, const SpikeOut so,
                                                          const Clock *clk, int k0, int M) {
   typedef AeifShape<MODEL> S;
@@ -534,7 +538,7 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
   unsigned long long nd = 0;
   if (i < A.n) {
     AeifQ<MODEL, PMAX, FIXED> q;
-    load_aeif_par(A, i, q);
+    load_aeif_par<MODEL, PMAX, FIXED, UNI>(A, i, q);
     const int NV = 2 + S::npv * q.ports();
     float y[NVM];
     float refr, h;
@@ -568,7 +572,7 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
 
 // Neurons the main kernel left unfinished (typically the few that spike in the batch)
 // continue here from the step where they stopped, one per thread.
-template <int MODEL, int PMAX, bool FIXED, int LM>
+template <int MODEL, int PMAX, bool FIXED, int LM, bool UNI = false>
 __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, const SpikeOut so,
                                                              const Clock *clk, int k0, int M) {
   typedef AeifShape<MODEL> S;
@@ -585,7 +589,7 @@ __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, c
     const int2 e = A.strag_list[j];
     const int i = e.x;
     AeifQ<MODEL, PMAX, FIXED> q;
-    load_aeif_par(A, i, q);
+    load_aeif_par<MODEL, PMAX, FIXED, UNI>(A, i, q);
     const int NV = 2 + S::npv * q.ports();
     float y[NVM];
     float refr, h;
@@ -612,17 +616,30 @@ template <int MODEL, int PMAX, bool FIXED, int LM>
 int launch_aeif_p(const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
   const int tb = (A.threads == 64 || A.threads == 256) ? A.threads : 128;
   dim3 grid((A.n + tb - 1) / tb), block(tb);
-  bool occ = false;
-  if constexpr (LM == LM_PLAIN) {
-    if (A.occupancy) {
+  bool done = false;
+  if constexpr (LM == LM_PLAIN && FIXED) {
+    if (A.occupancy && A.uniform) {
+      aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1, true><<<grid, block, 0, st>>>(A, so, clk, k0, M);
+      done = true;
+    } else if (A.occupancy) {
       aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1><<<grid, block, 0, st>>>(A, so, clk, k0, M);
-      occ = true;
+      done = true;
+    } else if (A.uniform) {
+      aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0, true><<<grid, block, 0, st>>>(A, so, clk, k0, M);
+      done = true;
     }
   }
-  if (!occ) aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0><<<grid, block, 0, st>>>(A, so, clk, k0, M);
+  if (!done) aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0><<<grid, block, 0, st>>>(A, so, clk, k0, M);
   if (A.budget <= 0) return 1;
   dim3 sgrid(A.n < 128 * 148 * 4 ? (A.n + 127) / 128 : 148 * 4), sblock(128);
-  aeif_straggler_kernel<MODEL, PMAX, FIXED, LM><<<sgrid, sblock, 0, st>>>(A, so, clk, k0, M);
+  done = false;
+  if constexpr (LM == LM_PLAIN && FIXED) {
+    if (A.uniform) {
+      aeif_straggler_kernel<MODEL, PMAX, FIXED, LM, true><<<sgrid, sblock, 0, st>>>(A, so, clk, k0, M);
+      done = true;
+    }
+  }
+  if (!done) aeif_straggler_kernel<MODEL, PMAX, FIXED, LM><<<sgrid, sblock, 0, st>>>(A, so, clk, k0, M);
   return 2;
 }
 

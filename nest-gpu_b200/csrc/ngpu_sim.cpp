@@ -606,6 +606,9 @@ AeifArgs Engine::aeif_args(Group &g) {
   A.srec = spike_rec(g);
   A.threads = update_threads;
   A.occupancy = update_occupancy;
+  A.uniform = 1;
+  for (int j = 0; j < AEIF_NSCAL + AEIF_NPORTPAR * g.nport && j < AEIF_NPAR; j++)
+    if (g.d_der[j]) A.uniform = 0;
   A.learn.mode = learn_mode_;
   A.learn.log = d_log_;
   A.learn.log_cursor = d_log_cursor_;

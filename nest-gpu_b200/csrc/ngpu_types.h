@@ -134,6 +134,7 @@ struct AeifArgs {
   int budget;            // RK5 steps per neuron and batch in the main kernel (0: no limit)
   int threads;           // threads per block of the main kernel (64, 128 or 256)
   int occupancy;         // 1: register-capped variant of the main kernel (more resident warps)
+  int uniform;           // 1: every parameter is uniform over the group (no parameter arrays)
   int2 *strag_list;      // [n] (neuron, step of the batch) left for the straggler kernel
   int *strag_cnt;        // list length
   GroupSpikeRec srec;

@@ -250,3 +250,21 @@ def test_microcircuit_slice_bitexact():
     c_o = np.concatenate([np.asarray(o.GetStatus(p, "spike_count")).ravel() for p in pops_o])
     assert c_g.sum() > 1000
     assert np.array_equal(c_g, c_o)
+
+
+@pytest.mark.parametrize("occ", [0, 1])
+def test_per_neuron_parameters_bitexact(occ):
+    """Receptor time constants drawn per neuron (parameter arrays instead of uniform kernel
+    arguments): spike counts and derivative evaluations equal the oracle's."""
+    from workloads import c4_network
+    ngpu.SetUpdateOccupancy(occ)
+    n_g = c4_network(ngpu, 5, n=300, drive_w=1.5)
+    o = orc.Oracle()
+    n_o = c4_network(o, 5, n=300, drive_w=1.5)
+    ngpu.Simulate(40.0)
+    o.Simulate(40.0)
+    c_g = np.asarray(ngpu.GetStatus(n_g, "spike_count")).ravel()
+    c_o = np.asarray(o.GetStatus(n_o, "spike_count")).ravel()
+    assert c_g.sum() > 100
+    assert np.array_equal(c_g, c_o)
+    assert ngpu.GetStats()["n_derivs"] == o.NDerivs()
