@@ -77,22 +77,50 @@ __device__ __forceinline__ void push_spike(const SpikeOut &so, const GroupSpikeR
 }
 
 // The poiss_gen edges of a neuron do not change during a batch: with exactly one edge
-// (the common case) it and its generator are loaded once per batch.
+// (the common case) it, its generator, the mean count lam and exp(-lam) are loaded once
+// per batch, and the edge's current Philox block (four steps) is kept across steps.
 struct PoissonCache {
   int e0, e1;
   PoissonIn pe;
   GenPar g;
+  float lam, emlam;
+  long long blk;
+  U4 r;
 };
 
 __device__ __forceinline__ void poisson_cache_load(const GroupInput &G, int i, PoissonCache &c) {
   c.e0 = c.e1 = 0;
+  c.blk = -1;
   if (G.pin_off) {
     c.e0 = G.pin_off[i];
     c.e1 = G.pin_off[i + 1];
     if (c.e1 - c.e0 == 1) {
       c.pe = G.pin[c.e0];
       c.g = G.gen[c.pe.gen];
+      c.lam = __fmul_rn(G.lam_scale, c.g.rate);
+      c.emlam = exp_m(-c.lam);
     }
+  }
+}
+
+// The cached edge's draw: the same value as poisson_draw, without recomputing exp(-lam)
+// and with one Philox call per four steps.
+__device__ __forceinline__ void poisson_add_cached(double *in, const GroupInput &G, PoissonCache &c, long long tidx,
+                                                   double tnow) {
+  const double t_rel = tnow - (double)c.g.origin - (double)c.pe.delay;
+  if (t_rel >= (double)c.g.start && t_rel <= (double)c.g.stop) {
+    int k;
+    if (c.lam > 0.0f && c.lam <= 10.0f) {
+      const long long b = tidx >> 2;
+      if (b != c.blk) {
+        c.r = poisson_block(G.seed, c.pe.edge_id, tidx, 0);
+        c.blk = b;
+      }
+      k = poisson_small(c.lam, c.emlam, u01(word_of(c.r, (int)(tidx & 3))));
+    } else {
+      k = poisson_draw(c.lam, G.seed, c.pe.edge_id, tidx);
+    }
+    if (k > 0) in[c.pe.port] += (double)__fmul_rn(c.pe.weight, (float)k);
   }
 }
 
@@ -120,7 +148,7 @@ __device__ __forceinline__ void acc_prefetch(double *a, int np, int n, int i, co
 // next use.
 template <int PMAX>
 __device__ __forceinline__ void step_inputs_pf(double *in, const double *a, int np, int n, int i,
-                                               const GroupInput &G, const PoissonCache &c, int m, long long tidx,
+                                               const GroupInput &G, PoissonCache &c, int m, long long tidx,
                                                double tnow) {
   double *acc = G.acc + (size_t)m * G.slot_stride;
 #pragma unroll
@@ -129,7 +157,7 @@ __device__ __forceinline__ void step_inputs_pf(double *in, const double *a, int 
     if (p < np && a[p] != 0.0) acc[(size_t)p * n + i] = 0.0;
   }
   if (c.e1 - c.e0 == 1) {
-    poisson_add(in, G, c.pe, c.g, tidx, tnow);
+    poisson_add_cached(in, G, c, tidx, tnow);
   } else {
     for (int e = c.e0; e < c.e1; e++) {
       const PoissonIn pe = G.pin[e];
@@ -407,53 +435,46 @@ __device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmi
   return nd;
 }
 
-// RK5 steps of neuron i from x towards tnow (src/rk5.h:161-174), each followed by the
-// model's ExternalUpdate (src/aeif_cond_beta_multisynapse_kernel.h:190-226).  Consumes
-// one unit of `budget` per step when budget >= 0 and stops when it runs out; returns
-// true when the neuron reached the end of the time step.
+// One RK5 sub-step of neuron i from x towards the end of the time step tnow
+// (src/rk5.h:161-174), followed by the model's ExternalUpdate
+// (src/aeif_cond_beta_multisynapse_kernel.h:190-226); returns true when the time step is
+// complete.  `guard` counts the sub-steps of the current time step.
 template <int MODEL, int PMAX, bool FIXED, int LM>
-__device__ __forceinline__ bool aeif_integrate(const AeifArgs &A, const SpikeOut &so, int i,
-                                               const AeifQ<MODEL, PMAX, FIXED> &q, float *y,
-                                               float &refr, double &x, float &h, long long tidx,
-                                               double tnow, int &budget, unsigned long long &nd,
-                                               const float *smodel) {
+__device__ __forceinline__ bool aeif_substep(const AeifArgs &A, const SpikeOut &so, int i,
+                                             const AeifQ<MODEL, PMAX, FIXED> &q, float *y, float &refr,
+                                             double &x, float &h, long long tidx, double tnow,
+                                             unsigned long long &nd, const float *smodel, int &guard) {
   const double x1 = tnow;
-  bool end = false;
-  int guard = 0;
-  while (!end) {
-    if (budget == 0) return false;
-    if (budget > 0) budget--;
-    float hmax = (float)(x1 - x);
-    nd += rk5_step<MODEL, PMAX, FIXED, LM>(x, y, h, A.hmin, A.hmin_acc, hmax, q, refr, so.status, smodel,
-                                           A.learn);
-    end = (x >= x1 - (double)A.hmin);
-    if (++guard > ck::max_substeps) {
-      atomicOr(so.status, ST_RK5_TRIALS);
-      break;
-    }
-    if (y[0] < -1.0e3f) {
-      y[0] = q.V_reset;
-      y[1] = 0.0f;
-      atomicOr(so.status, ST_NUMERIC);
-      continue;
-    }
-    if (y[1] < -1.0e6f || y[1] > 1.0e6f) {
-      y[0] = q.V_reset;
-      y[1] = 0.0f;
-      atomicOr(so.status, ST_NUMERIC);
-      continue;
-    }
-    if (refr > 0.0f) {
-      y[0] = q.V_reset;
-      if (end) refr = __fsub_rn(refr, 1.0f);
-    } else if (y[0] >= q.V_peak) {
-      push_spike(so, A.srec, A.i0 + i, i, 1.0f, tidx, tnow);
-      y[0] = q.V_reset;
-      y[1] = __fadd_rn(y[1], q.b);
-      refr = q.refr_steps;
-    }
+  const float hmax = (float)(x1 - x);
+  nd += rk5_step<MODEL, PMAX, FIXED, LM>(x, y, h, A.hmin, A.hmin_acc, hmax, q, refr, so.status, smodel,
+                                         A.learn);
+  const bool end = (x >= x1 - (double)A.hmin);
+  if (++guard > ck::max_substeps) {
+    atomicOr(so.status, ST_RK5_TRIALS);
+    return true;
   }
-  return true;
+  if (y[0] < -1.0e3f) {
+    y[0] = q.V_reset;
+    y[1] = 0.0f;
+    atomicOr(so.status, ST_NUMERIC);
+    return end;
+  }
+  if (y[1] < -1.0e6f || y[1] > 1.0e6f) {
+    y[0] = q.V_reset;
+    y[1] = 0.0f;
+    atomicOr(so.status, ST_NUMERIC);
+    return end;
+  }
+  if (refr > 0.0f) {
+    y[0] = q.V_reset;
+    if (end) refr = __fsub_rn(refr, 1.0f);
+  } else if (y[0] >= q.V_peak) {
+    push_spike(so, A.srec, A.i0 + i, i, 1.0f, tidx, tnow);
+    y[0] = q.V_reset;
+    y[1] = __fadd_rn(y[1], q.b);
+    refr = q.refr_steps;
+  }
+  return end;
 }
 
 // Records of the step (values after the update, before the fold).
@@ -477,7 +498,7 @@ template <int MODEL, int PMAX, bool FIXED>
 __device__ __forceinline__ void aeif_end_step(const AeifArgs &A, const SpikeOut &so, int i,
                                               const AeifQ<MODEL, PMAX, FIXED> &q, float *y, float refr,
                                               int m, const StepT &t, long long rec_it0, const double *apf,
-                                              const PoissonCache &pc) {
+                                              PoissonCache &pc) {
   typedef AeifShape<MODEL> S;
   const int np = q.ports();
   if (A.rec.first) write_records(A.rec, so, A.i0 + i, i, y, 2 + S::npv * np, refr, t.it - rec_it0, t.tidx);
@@ -548,18 +569,27 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
     int budget = A.budget > 0 ? A.budget : -1;
     PoissonCache pc;
     poisson_cache_load(A.in, i, pc);
-    int m = 0;
+    // One RK5 sub-step per iteration: a lane that needs extra sub-steps in one time step
+    // does not hold the others of its warp in that step; they go on with their next step.
+    int m = 0, guard = 0;
     bool deferred = false;
-    for (; m < M; m++) {
-      const StepT t = step_at(clk, k0, m, A.dt);
-      double apf[PMAX];
-      acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
-      if (!aeif_integrate<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, budget, nd,
-                                                  smodel)) {
+    StepT t = step_at(clk, k0, 0, A.dt);
+    double apf[PMAX];
+    acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, 0);
+    while (m < M) {
+      if (budget == 0) {
         deferred = true;
         break;
       }
-      aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
+      if (budget > 0) budget--;
+      if (aeif_substep<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, nd, smodel, guard)) {
+        aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
+        guard = 0;
+        if (++m < M) {
+          t = step_at(clk, k0, m, A.dt);
+          acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
+        }
+      }
     }
     aeif_store<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
     if (deferred) {
@@ -595,15 +625,21 @@ __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, c
     float refr, h;
     double x;
     aeif_load<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
-    int budget = -1;
     PoissonCache pc;
     poisson_cache_load(A.in, i, pc);
-    for (int m = e.y; m < M; m++) {
-      const StepT t = step_at(clk, k0, m, A.dt);
-      double apf[PMAX];
-      acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
-      aeif_integrate<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, budget, nd, smodel);
-      aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
+    int m = e.y, guard = 0;
+    StepT t = step_at(clk, k0, m, A.dt);
+    double apf[PMAX];
+    acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
+    while (m < M) {
+      if (aeif_substep<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, nd, smodel, guard)) {
+        aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
+        guard = 0;
+        if (++m < M) {
+          t = step_at(clk, k0, m, A.dt);
+          acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
+        }
+      }
     }
     aeif_store<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
   }

@@ -13,7 +13,8 @@
 //            "Parallel random numbers: as easy as 1, 2, 3", SC'11).
 //   poisson: sequential-search inversion for lambda <= 10; larger lambda is split
 //            into ceil(lambda/10) independent draws (a sum of independent Poisson
-//            variables is Poisson).
+//            variables is Poisson); one Philox block gives the uniforms of four
+//            consecutive time steps of an edge.
 #pragma once
 #include <cstdint>
 
@@ -87,43 +88,57 @@ __device__ __forceinline__ float u01(uint32_t r) {
   return __fmul_rn(__fadd_rn((float)(r >> 8), 0.5f), 5.96046448e-08f);
 }
 
-__device__ __forceinline__ int poisson_small(float lam, float u) {
-  float p = exp_m(-lam);
+// 1/k rounded to float, k = 0..64 (entry 0 unused): the inversion's recurrence
+// multiplies by it instead of dividing.
+#define NGPU_INV8(k) (float)(1.0 / (k)), (float)(1.0 / ((k) + 1)), (float)(1.0 / ((k) + 2)), \
+    (float)(1.0 / ((k) + 3)), (float)(1.0 / ((k) + 4)), (float)(1.0 / ((k) + 5)), (float)(1.0 / ((k) + 6)), \
+    (float)(1.0 / ((k) + 7))
+static __constant__ float c_inv_k[65] = {0.0f, NGPU_INV8(1), NGPU_INV8(9), NGPU_INV8(17), NGPU_INV8(25),
+                                         NGPU_INV8(33), NGPU_INV8(41), NGPU_INV8(49), NGPU_INV8(57)};
+#undef NGPU_INV8
+
+// Inversion by sequential search: the smallest k with u <= F(k), p(k) = p(k-1) lam / k
+// starting from p(0) = emlam = exp(-lam).
+__device__ __forceinline__ int poisson_small(float lam, float emlam, float u) {
+  float p = emlam;
   float F = p;
   int k = 0;
   while (u > F && p > 9.31322575e-10f && k < 1000) {
     k++;
-    p = __fdiv_rn(__fmul_rn(p, lam), (float)k);
+    const float ik = (k <= 64) ? c_inv_k[k] : __fdiv_rn(1.0f, (float)k);
+    p = __fmul_rn(__fmul_rn(p, lam), ik);
     F = __fadd_rn(F, p);
   }
   return k;
 }
 
-// n ~ Poisson(lam) of direct edge `edge` at time index `tidx`.
+__device__ __forceinline__ uint32_t word_of(const U4 &r, int w) {
+  return w == 0 ? r.x : w == 1 ? r.y : w == 2 ? r.z : r.w;
+}
+
+// Philox block of direct edge `edge` for the four time indices 4*(tidx/4) .. +3 and
+// chunk field j (0 for lam <= 10; 1.. for the chunks of a larger lam).
+__device__ __forceinline__ U4 poisson_block(uint64_t seed, uint64_t edge, long long tidx, uint32_t j) {
+  U4 c;
+  c.x = (uint32_t)edge;
+  c.y = (uint32_t)(edge >> 32);
+  c.z = (uint32_t)((unsigned long long)tidx >> 2);
+  c.w = ((uint32_t)((unsigned long long)tidx >> 34) & 0xffffu) | (j << 16);
+  return philox(c, (uint32_t)seed ^ 0x6A09E667u, (uint32_t)(seed >> 32) ^ 0xBB67AE85u);
+}
+
+// n ~ Poisson(lam) of direct edge `edge` at time index `tidx`: word tidx % 4 of the edge's
+// block for tidx / 4 (one Philox call serves four consecutive steps).
 __device__ __forceinline__ int poisson_draw(float lam, uint64_t seed, uint64_t edge, long long tidx) {
   if (!(lam > 0.0f)) return 0;
-  int m = 1;
-  float lc = lam;
-  if (lam > 10.0f) {
-    m = (int)ceilf(__fdiv_rn(lam, 10.0f));
-    lc = __fdiv_rn(lam, (float)m);
-  }
-  uint32_t k0 = (uint32_t)seed ^ 0x6A09E667u;
-  uint32_t k1 = (uint32_t)(seed >> 32) ^ 0xBB67AE85u;
+  const int w = (int)(tidx & 3);
+  if (lam <= 10.0f) return poisson_small(lam, exp_m(-lam), u01(word_of(poisson_block(seed, edge, tidx, 0), w)));
+  const int m = (int)ceilf(__fdiv_rn(lam, 10.0f));
+  const float lc = __fdiv_rn(lam, (float)m);
+  const float emlc = exp_m(-lc);
   int n = 0;
-  U4 r = {0, 0, 0, 0};
-  for (int j = 0; j < m; j++) {
-    if ((j & 3) == 0) {
-      U4 c;
-      c.x = (uint32_t)edge;
-      c.y = (uint32_t)(edge >> 32);
-      c.z = (uint32_t)tidx;
-      c.w = ((uint32_t)((unsigned long long)tidx >> 32) & 0xffffu) | ((uint32_t)(j >> 2) << 16);
-      r = philox(c, k0, k1);
-    }
-    uint32_t v = (j & 3) == 0 ? r.x : (j & 3) == 1 ? r.y : (j & 3) == 2 ? r.z : r.w;
-    n += poisson_small(lc, u01(v));
-  }
+  for (int j = 0; j < m; j++)
+    n += poisson_small(lc, emlc, u01(word_of(poisson_block(seed, edge, tidx, (uint32_t)(j + 1)), w)));
   return n;
 }
 

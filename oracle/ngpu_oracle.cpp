@@ -127,43 +127,46 @@ static U4 philox(U4 c, uint32_t k0, uint32_t k1) {
 }
 static inline float u01(uint32_t r) { return ((float)(r >> 8) + 0.5f) * 5.96046448e-08f; }
 
-static int poisson_small(float lam, float u) {
-  float p = exp_m(-lam);
+// 1/k rounded to float (k = 1..64): the inversion multiplies by it.
+static float inv_k(int k) { return (k <= 64) ? (float)(1.0 / k) : 1.0f / (float)k; }
+
+// Sequential-search inversion from p(0) = emlam = exp(-lam).
+static int poisson_small(float lam, float emlam, float u) {
+  float p = emlam;
   float F = p;
   int k = 0;
   while (u > F && p > 9.31322575e-10f && k < 1000) {
     k++;
-    p = p * lam / (float)k;
+    p = (p * lam) * inv_k(k);
     F = F + p;
   }
   return k;
 }
 
-// n ~ Poisson(lam) for direct edge `edge` at time index `tidx`.
+static uint32_t word_of(const U4 &r, int w) { return w == 0 ? r.x : w == 1 ? r.y : w == 2 ? r.z : r.w; }
+
+// Philox block of edge `edge` for the time indices 4*(tidx/4) .. +3, chunk field j.
+static U4 poisson_block(uint64_t seed, uint64_t edge, int64_t tidx, uint32_t j) {
+  U4 c;
+  c.x = (uint32_t)edge;
+  c.y = (uint32_t)(edge >> 32);
+  c.z = (uint32_t)((uint64_t)tidx >> 2);
+  c.w = ((uint32_t)((uint64_t)tidx >> 34) & 0xffffu) | (j << 16);
+  return philox(c, (uint32_t)seed ^ 0x6A09E667u, (uint32_t)(seed >> 32) ^ 0xBB67AE85u);
+}
+
+// n ~ Poisson(lam) for direct edge `edge` at time index `tidx`: word tidx % 4 of the
+// edge's block for tidx / 4; lam > 10 is split into ceil(lam / 10) chunks (fields 1..).
 static int poisson_draw(float lam, uint64_t seed, uint64_t edge, int64_t tidx) {
   if (!(lam > 0.0f)) return 0;
-  int m = 1;
-  float lc = lam;
-  if (lam > 10.0f) {
-    m = (int)std::ceil(lam / 10.0f);
-    lc = lam / (float)m;
-  }
-  uint32_t k0 = (uint32_t)seed ^ 0x6A09E667u;
-  uint32_t k1 = (uint32_t)(seed >> 32) ^ 0xBB67AE85u;
+  const int w = (int)(tidx & 3);
+  if (lam <= 10.0f) return poisson_small(lam, exp_m(-lam), u01(word_of(poisson_block(seed, edge, tidx, 0), w)));
+  const int m = (int)std::ceil(lam / 10.0f);
+  const float lc = lam / (float)m;
+  const float emlc = exp_m(-lc);
   int n = 0;
-  U4 r = {0, 0, 0, 0};
-  for (int j = 0; j < m; j++) {
-    if ((j & 3) == 0) {
-      U4 c;
-      c.x = (uint32_t)edge;
-      c.y = (uint32_t)(edge >> 32);
-      c.z = (uint32_t)tidx;
-      c.w = ((uint32_t)((uint64_t)tidx >> 32) & 0xffffu) | ((uint32_t)(j >> 2) << 16);
-      r = philox(c, k0, k1);
-    }
-    uint32_t v = (j & 3) == 0 ? r.x : (j & 3) == 1 ? r.y : (j & 3) == 2 ? r.z : r.w;
-    n += poisson_small(lc, u01(v));
-  }
+  for (int j = 0; j < m; j++)
+    n += poisson_small(lc, emlc, u01(word_of(poisson_block(seed, edge, tidx, (uint32_t)(j + 1)), w)));
   return n;
 }
 
