@@ -46,11 +46,11 @@ STEP_MS = 100.0
 FLOPS_PER_DERIV = 110        # FP32 flops per derivative evaluation incl. stage algebra, 2 ports
 DELIVERY_BYTES_PER_EVENT = 8  # 4 B packed target/port + 4 B weight per synaptic event
 DELIVERY_BYTES_PER_SPIKE = 8  # ring entry (source, height)
-# DRAM traffic per unit from the ncu captures of the 1/10-size network (summaries in
-# profiles/deliver_batch_kernel_1M_network_at_0.1_scale.md and
-# profiles/aeif_batch_kernel_1M_network_at_0.1_scale.md), scaled to a launch by its units
-DELIVERY_TRAFFIC_PER_EVENT = 29.1e6 / 1.91e6   # bytes per synaptic event
-RK5_TRAFFIC_PER_NEURON_STEP = 22.84e6 / 1.0e6  # bytes per neuron-step
+# DRAM traffic per unit from the ncu captures of the 3/10-size network (summaries in
+# profiles/deliver_batch_kernel_1M_network_at_0.3_scale.md and
+# profiles/aeif_batch_kernel_1M_network_at_0.3_scale.md), scaled to a launch by its units
+DELIVERY_TRAFFIC_PER_EVENT = 95.6e6 / 5.82e6   # bytes per synaptic event
+RK5_TRAFFIC_PER_NEURON_STEP = 76.1e6 / 3.0e6   # bytes per neuron-step
 
 
 def parse():
