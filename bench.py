@@ -163,6 +163,30 @@ def ensemble_run(ngpu, bio_ms=1000.0):
             "mapping": chosen, "build_s": build_s, "autotune_s": tune_s}
 
 
+def rank_reducers(dist, device):
+    """Barrier and max / sum of one scalar over the ranks (identities without a process
+    group); the only cross-rank traffic of the replicas."""
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def reduce(x, op):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max_over_ranks(x):
+        return reduce(x, dist.ReduceOp.MAX) if dist is not None else x
+
+    def sum_over_ranks(x):
+        return reduce(x, dist.ReduceOp.SUM) if dist is not None else x
+
+    return barrier, max_over_ranks, sum_over_ranks
+
+
 def engine_arm(args):
     if WORLD > 1:
         os.environ["CUDA_VISIBLE_DEVICES"] = str(LOCAL_RANK)
@@ -178,25 +202,7 @@ def engine_arm(args):
         tdist.init_process_group("nccl", timeout=timedelta(seconds=600))
         dist = tdist
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    barrier, max_over_ranks, sum_over_ranks = rank_reducers(dist, "cuda")
 
     seed = 20240 + 101 * RANK
     t_build0 = time.time()
