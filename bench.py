@@ -213,7 +213,7 @@ def engine_arm(args):
     build_s = time.time() - t_build0
     # launch mappings picked on this network (the trial steps are part of the transient)
     t_tune0 = time.time()
-    mapping = ngpu.Autotune(200) if not args.no_autotune else None
+    mapping = ngpu.Autotune(400) if not args.no_autotune else None
     tune_s = time.time() - t_tune0
     n_neurons = len(neuron)
 
