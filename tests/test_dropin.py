@@ -1,0 +1,31 @@
+"""Drop-in check: the reference's own pythonlib/nestgpu.py, unchanged, loads
+libnestgpu_b200.so through NESTGPU_LIB and a user script gives the same network through it as
+through this repository's front-end.  Needs the reference tree (skipped where it is absent)."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "nest-gpu_b200", "lib", "libnestgpu_b200.so")
+REF_PY = os.path.join(os.environ.get("NESTGPU_REF", "/root/reference"), "pythonlib")
+SCRIPT = os.path.join(ROOT, "tests", "dropin_script.py")
+
+
+def run(binding_dir):
+    env = dict(os.environ, NESTGPU_LIB=LIB)
+    p = subprocess.run([sys.executable, SCRIPT, binding_dir], env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert p.returncode == 0, p.stderr[-3000:]
+    return json.loads([x for x in p.stdout.splitlines() if x.startswith("JSON:")][-1][5:])
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_PY, "nestgpu.py")), reason="reference tree absent")
+def test_reference_binding_drives_engine():
+    ref = run(REF_PY)
+    own = run(os.path.join(ROOT, "nest-gpu_b200"))
+    assert ref == own
+    assert ref["n_conn_nm"] == 15 * 4 and ref["n_conn_mn"] == 40
+    assert ref["E_rev"][0] == [0.0, -85.0]
