@@ -459,12 +459,18 @@ def GetNeuronVarSize(i_node, var_name):
 
 
 def _rows(pt, n_node, size):
-    out = []
-    for i in range(n_node):
-        if size > 1:
-            out.append([pt[i * size + j] for j in range(size)])
-        else:
-            out.append(pt[i])
+    """Python rows (lists for size > 1) from an engine-allocated float array, which is freed."""
+    import numpy as np
+    n = n_node * max(size, 1)
+    a = np.ctypeslib.as_array(pt, shape=(n,)).astype(np.float64) if n > 0 else np.zeros(0)
+    _free(pt)
+    return a.reshape(n_node, size).tolist() if size > 1 else a.tolist()
+
+
+def _ints(pt, n):
+    """Python list from an engine-allocated int array, which is freed."""
+    import numpy as np
+    out = np.ctypeslib.as_array(pt, shape=(n,)).tolist() if n > 0 else []
     _free(pt)
     return out
 
@@ -507,9 +513,7 @@ def GetNeuronGroupParam(i_node, param_name):
 def GetNeuronIntVar(i_node, n_node, var_name):
     pt = _c["NESTGPU_GetNeuronIntVar"](i_node, n_node, _b(var_name))
     _check()
-    out = [pt[i] for i in range(n_node)]
-    _free(pt)
-    return out
+    return _ints(pt, n_node)
 
 
 def GetNeuronVar(i_node, n_node, var_name):
@@ -522,9 +526,7 @@ def GetNeuronPtIntVar(nodes, var_name):
     pt_n, n = _int_arr(nodes)
     pt = _c["NESTGPU_GetNeuronPtIntVar"](pt_n, n, _b(var_name))
     _check()
-    out = [pt[i] for i in range(n)]
-    _free(pt)
-    return out
+    return _ints(pt, n)
 
 
 def GetNeuronPtVar(nodes, var_name):
