@@ -309,6 +309,11 @@ int NGPU_SetUpdateOccupancy(int on);
    segment of one (source, delay) pair; short segments leave fewer lanes idle with small
    groups. */
 int NGPU_SetDeliverGroup(int g);
+/* 1: a network whose neurons are all iaf_psc_exp runs its steps in one cooperative launch per
+   CUDA-graph's worth of steps (delivery and update separated by grid barriers with bounded
+   waits); 0 (default): per-batch launches in CUDA graphs.  Results are the same either way; the
+   autotuner tries both. */
+int NGPU_SetPersistent(int on);
 /* Autotuner of the launch mappings (no counterpart in the reference): on the calibrated
    network, times `steps` simulation steps per candidate of the update block size, the
    update kernel variant, the delivery lane group, the delivery grid and the RK5 step budget (coordinate descent, two

@@ -749,6 +749,13 @@ int NGPU_SetUpdateOccupancy(int on) {
   }, -1);
 }
 
+int NGPU_SetPersistent(int on) {
+  return guard([&] {
+    E().persistent = on ? 1 : 0;
+    return 0;
+  }, -1);
+}
+
 int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliver_blocks, int *rk5_budget) {
   return guard([&] {
     const int n = E().autotune(steps, nullptr);

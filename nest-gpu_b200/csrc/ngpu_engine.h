@@ -127,6 +127,7 @@ class Engine {
   int update_threads = 128;       // threads per block of the aeif update kernel (64, 128, 256)
   int deliver_group = 32;         // lanes per delivery work item (8, 16, 32)
   int update_occupancy = 0;       // 1: register-capped aeif update kernel
+  int persistent = 0;             // iaf-only networks: persistent cooperative step loop
   bool use_device_rng = true;     // cuRAND device generator (as the reference) if a GPU exists
 
   void set_seed(unsigned long long s);
@@ -312,8 +313,12 @@ class Engine {
   // all iaf_psc_exp groups in one launch when there are several
   IafArgs *d_iaf_tab_ = nullptr;
   int *d_iaf_blk0_ = nullptr;
+  int *d_iaf_first_ = nullptr;   // neuron prefix over the iaf groups
+  GridBarrier *d_bar_ = nullptr;
   int n_iaf_multi_ = 0, iaf_multi_blocks_ = 0;
   void prepare_multi();
+  bool persistent_eligible() const;
+  void run_persistent(int steps);
 
   template <class T> T *dalloc(size_t n);
   void free_device();
@@ -349,6 +354,9 @@ int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk
 int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *clk, int k0, int M,
                    cudaStream_t st);
 int launch_clock_advance(Clock *clk, int K, cudaStream_t st);
+int launch_persistent_iaf(const DeliverArgs &D, int group, const IafArgs *tab, const int *first, int ngroups,
+                          const SpikeOut &so, const Clock *clk, int steps, int M, GridBarrier *bar, int max_blocks,
+                          cudaStream_t st);
 int deliver_max_pairs();
 void pack_delivery_csr_noalloc(const int *src, const int *dly, const unsigned *target, const float *weight,
                                size_t n, int n_nodes, int dspan, unsigned long long *seg_off, EdgeW *edge,

@@ -130,12 +130,14 @@ __global__ void spike_gen_batch_kernel(const SpikeGenArgs A, const SpikeOut so, 
 constexpr int DELIVER_THREADS = 256;
 constexpr int MAX_PAIRS = 8192;     // dspan * M
 
+typedef cub::BlockScan<int, DELIVER_THREADS> DeliverScan;
+
+// The delivery of one batch by block `block` of `nblocks`; s_pref holds dspan*M+1 ints.
 template <int G>
-__global__ void __launch_bounds__(DELIVER_THREADS) deliver_batch_kernel(const DeliverArgs A,
-                                                                        const Clock *clk, int k0, int M) {
-  extern __shared__ int s_pref[];   // npairs + 1 prefix sums over (delay group, arrival step)
-  typedef cub::BlockScan<int, DELIVER_THREADS> Scan;
-  __shared__ typename Scan::TempStorage scan_tmp;
+__device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock *clk, int k0, int M, int *s_pref,
+                                              typename DeliverScan::TempStorage &scan_tmp, int block,
+                                              int nblocks) {
+  typedef DeliverScan Scan;
   const long long t_first = clk->tidx_base + clk->it0 + k0 + 1;   // time index of step 0
   const int npairs = A.dspan * M;
   const int per = (npairs + DELIVER_THREADS - 1) / DELIVER_THREADS;
@@ -168,15 +170,15 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_batch_kernel(const De
   if (threadIdx.x == 0) s_pref[0] = 0;
   __syncthreads();
   const int total = s_pref[npairs];
-  if (blockIdx.x == 0) {
+  if (block == 0) {
     // ring slots of this batch's steps start empty (their previous steps are older than
     // any emission step read here because R >= M + dmax + 3); straggler lists start empty
     for (int m = threadIdx.x; m < M; m += blockDim.x) A.ring_cnt[(int)((t_first + m) % A.R)] = 0;
     for (int g = threadIdx.x; g < A.n_strag; g += blockDim.x) A.strag_cnt[g] = 0;
   }
   const int sub = threadIdx.x & (G - 1);
-  const int grp = (blockIdx.x * DELIVER_THREADS + threadIdx.x) / G;
-  const int ngrp = (gridDim.x * DELIVER_THREADS) / G;
+  const int grp = (block * DELIVER_THREADS + threadIdx.x) / G;
+  const int ngrp = (nblocks * DELIVER_THREADS) / G;
   unsigned long long nev = 0;
   for (int item = grp; item < total; item += ngrp) {
     int lo = 0, hi = npairs;   // pair with s_pref[pr] <= item < s_pref[pr+1]
@@ -206,9 +208,111 @@ __global__ void __launch_bounds__(DELIVER_THREADS) deliver_batch_kernel(const De
   if ((threadIdx.x & 31) == 0 && nev) atomicAdd(&s_nev, nev);
   __syncthreads();
   if (threadIdx.x == 0 && s_nev) atomicAdd(A.n_events, s_nev);
+  __syncthreads();
+}
+
+template <int G>
+__global__ void __launch_bounds__(DELIVER_THREADS) deliver_batch_kernel(const DeliverArgs A,
+                                                                        const Clock *clk, int k0, int M) {
+  extern __shared__ int s_pref[];   // npairs + 1 prefix sums over (delay group, arrival step)
+  __shared__ typename DeliverScan::TempStorage scan_tmp;
+  deliver_batch<G>(A, clk, k0, M, s_pref, scan_tmp, blockIdx.x, gridDim.x);
 }
 
 __global__ void clock_advance_kernel(Clock *clk, int K) { clk->it0 += K; }
+
+// ---------------------------------------------------------------------------
+// Persistent step loop for networks whose neurons are all iaf_psc_exp.  One
+// cooperative launch (all blocks co-resident) advances K steps in batches of M:
+// delivery, grid barrier, update of every population, grid barrier.  With a minimum
+// delay of one step (M = 1) this replaces two launches per step.
+// ---------------------------------------------------------------------------
+// Counting barrier over the blocks of the launch.  Waits are bounded: after 2^24 polls
+// a block records a timeout in the status word, and every later barrier of the launch
+// returns false at once, so the kernel ends instead of waiting for ever.
+__device__ __forceinline__ bool grid_barrier(GridBarrier *bar, unsigned nblocks, unsigned *status) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = (((volatile unsigned *)status)[0] & ST_BARRIER_TIMEOUT) ? 0 : 1;
+    if (ok) {
+      const unsigned g = ((volatile unsigned *)&bar->gen)[0];
+      __threadfence();
+      if (atomicAdd(&bar->count, 1u) + 1u == nblocks) {
+        atomicExch(&bar->count, 0u);
+        __threadfence();
+        atomicAdd(&bar->gen, 1u);
+      } else {
+        long long polls = 0;
+        while (((volatile unsigned *)&bar->gen)[0] == g) {
+          if (++polls > (1LL << 24)) {
+            atomicOr(status, ST_BARRIER_TIMEOUT);
+            ok = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <int G>
+__global__ void __launch_bounds__(DELIVER_THREADS) persistent_iaf_kernel(
+    const DeliverArgs D, const IafArgs *tab, const int *first, int ngroups, const SpikeOut so, const Clock *clk,
+    int K, int M, GridBarrier *bar) {
+  extern __shared__ int s_pref[];
+  __shared__ typename DeliverScan::TempStorage scan_tmp;
+  const int total_n = first[ngroups];
+  const unsigned nb = gridDim.x;
+  for (int k0 = 0; k0 < K; k0 += M) {
+    const int mb = (K - k0 < M) ? K - k0 : M;
+    deliver_batch<G>(D, clk, k0, mb, s_pref, scan_tmp, blockIdx.x, gridDim.x);
+    if (!grid_barrier(bar, nb, so.status)) return;
+    for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < total_n; gi += gridDim.x * blockDim.x) {
+      int lo = 0, hi = ngroups;   // group with first[g] <= gi < first[g+1]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (first[mid] <= gi) lo = mid; else hi = mid;
+      }
+      iaf_neuron(tab[lo], so, clk, k0, mb, gi - first[lo]);
+    }
+    if (!grid_barrier(bar, nb, so.status)) return;
+  }
+}
+
+// Cooperative launch of the persistent loop over `steps` steps; the grid is the number of
+// blocks that fit on the GPU at once (at most `max_blocks`).
+int launch_persistent_iaf(const DeliverArgs &D, int group, const IafArgs *tab, const int *first, int ngroups,
+                          const SpikeOut &so, const Clock *clk, int steps, int M, GridBarrier *bar, int max_blocks,
+                          cudaStream_t st) {
+  const size_t smem = (size_t)(D.dspan * M + 1) * sizeof(int);
+  void *fn = group == 8 ? (void *)persistent_iaf_kernel<8>
+                        : group == 16 ? (void *)persistent_iaf_kernel<16> : (void *)persistent_iaf_kernel<32>;
+  int dev = 0, n_sm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, DELIVER_THREADS, smem);
+  int nblocks = n_sm * per_sm;
+  if (max_blocks > 0 && nblocks > max_blocks) nblocks = max_blocks;
+  if (nblocks < 1) return -1;
+  DeliverArgs d = D;
+  const IafArgs *t = tab;
+  const int *f = first;
+  int ng = ngroups;
+  SpikeOut s = so;
+  const Clock *c = clk;
+  int k = steps, m = M;
+  GridBarrier *b = bar;
+  void *args[] = {&d, &t, &f, &ng, &s, &c, &k, &m, &b};
+  if (cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(DELIVER_THREADS), args, smem, st) != cudaSuccess)
+    return -1;
+  return 1;
+}
 
 // ---------------------------------------------------------------------------
 // Host-side launchers.  Each returns the number of kernels it launched.

@@ -697,24 +697,53 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
 // each graph capture (the arguments hold record-buffer pointers that can change).
 void Engine::prepare_multi() {
   std::vector<IafArgs> tab;
-  std::vector<int> blk0;
+  std::vector<int> blk0, first{0};
   int nb = 0;
   for (auto &g : groups_) {
     if (g.model != M_IAF_PSC_EXP || g.n <= 0) continue;
     tab.push_back(iaf_args(g));
     blk0.push_back(nb);
     nb += (g.n + 255) / 256;
+    first.push_back(first.back() + g.n);
   }
   n_iaf_multi_ = (int)tab.size();
   iaf_multi_blocks_ = nb;
-  if (n_iaf_multi_ < 2) return;
+  if (n_iaf_multi_ < 1) return;
   if (!d_iaf_tab_) {
     d_iaf_tab_ = dalloc<IafArgs>(tab.size());
     d_iaf_blk0_ = dalloc<int>(blk0.size());
+    d_iaf_first_ = dalloc<int>(first.size());
+    d_bar_ = dalloc<GridBarrier>(1);
   }
   cuda_check(cudaStreamSynchronize(stream_), "sync");
   cuda_check(cudaMemcpy(d_iaf_tab_, tab.data(), tab.size() * sizeof(IafArgs), cudaMemcpyHostToDevice), "iaf table");
   cuda_check(cudaMemcpy(d_iaf_blk0_, blk0.data(), blk0.size() * sizeof(int), cudaMemcpyHostToDevice), "iaf table");
+  cuda_check(cudaMemcpy(d_iaf_first_, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice),
+             "iaf table");
+}
+
+// The persistent step loop serves networks whose only neurons are iaf_psc_exp groups
+// (Poisson generators have no kernel of their own).
+bool Engine::persistent_eligible() const {
+  bool any = false;
+  for (auto &g : groups_) {
+    if (g.n <= 0 || g.model == M_POISS_GEN) continue;
+    if (g.model != M_IAF_PSC_EXP) return false;
+    any = true;
+  }
+  return any;
+}
+
+// `steps` steps in one cooperative launch of the persistent loop, then the clock advance.
+void Engine::run_persistent(int steps) {
+  cuda_check(cudaMemsetAsync(d_bar_, 0, sizeof(GridBarrier), stream_), "barrier reset");
+  const int r = launch_persistent_iaf(deliver_args(), deliver_group, d_iaf_tab_, d_iaf_first_, n_iaf_multi_,
+                                      spike_out(), d_clk_, steps, batch_, d_bar_,
+                                      deliver_blocks_req > 0 ? deliver_blocks_req : 0, stream_);
+  if (r < 0) throw NgpuError(std::string("cooperative launch of the persistent step loop failed: ") +
+                             cudaGetErrorString(cudaGetLastError()));
+  launch_clock_advance(d_clk_, steps, stream_);
+  n_launch_ += 2;
 }
 
 void Engine::ensure_record_window(long long rows) {
@@ -733,12 +762,19 @@ void Engine::run_steps(long long n) {
     window = std::min<long long>(n, REC_WINDOW);
     ensure_record_window(window);
   }
+  const bool pers = persistent && persistent_eligible();
+  if (pers) prepare_multi();
   long long done = 0;
   while (done < n) {
     const long long w = std::min(window, n - done);
     long long left = w;
     while (left > 0) {
       const int steps = (int)std::min<long long>(K, left);
+      if (pers) {
+        run_persistent(steps);
+        left -= steps;
+        continue;
+      }
       auto itg = graphs_.find(steps);
       if (itg == graphs_.end()) {
         prepare_multi();
@@ -825,6 +861,15 @@ void Engine::check_status() {
     if (fresh & ST_RK5_TRIALS) printf("Warning: RK5 step hit its iteration cap\n");
     if (fresh & ST_NUMERIC) printf("Warning: V_m or w out of bounds, neuron state reset\n");
     if (fresh & ST_REC_TIMES_FULL) printf("Maximum number of recorded spike times exceeded\n");
+  }
+  if (st & ST_BARRIER_TIMEOUT) {
+    // the loop stopped early: the state is not that of the requested time
+    const unsigned keep = st & ~ST_BARRIER_TIMEOUT;
+    cuda_check(cudaMemcpy(d_status_, &keep, sizeof(unsigned), cudaMemcpyHostToDevice), "status");
+    status_seen_ &= ~ST_BARRIER_TIMEOUT;
+    persistent = 0;
+    throw NgpuError("a grid barrier of the persistent step loop timed out; the simulation state is invalid "
+                    "(the engine falls back to per-batch launches)");
   }
 }
 
@@ -982,6 +1027,7 @@ int Engine::autotune(int steps, std::vector<std::pair<std::string, double>> *log
       {"deliver_blocks", &deliver_blocks_req, {148, 296, 592, 1184, 2368, base}},
       {"rk5_budget", &rk5_budget, {0, 1, 2, 4, 8}},
   };
+  if (persistent_eligible()) knobs.insert(knobs.begin(), Knob{"persistent", &persistent, {0, 1}});
   if (deliver_blocks_req <= 0) deliver_blocks_req = base;
   const float t = (float)steps * dt;
   auto trial = [&]() {

@@ -29,6 +29,13 @@ enum Status : unsigned {
   ST_RK5_TRIALS = 1u << 1,            // RK5 step gave up after the trial cap
   ST_NUMERIC = 1u << 2,               // V_m or w left their guard bounds (reset applied)
   ST_REC_TIMES_FULL = 1u << 3,        // a neuron exceeded its recorded-spike-time capacity
+  ST_BARRIER_TIMEOUT = 1u << 4,       // a grid barrier of the persistent step loop gave up waiting
+};
+
+// Barrier state of the persistent step loop (device memory, zero-initialised).
+struct GridBarrier {
+  unsigned count;        // blocks arrived at the current barrier
+  unsigned gen;          // barriers completed
 };
 
 // Simulation clock in device memory.  A CUDA graph covers a fixed number of steps

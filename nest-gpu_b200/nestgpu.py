@@ -168,6 +168,7 @@ if is_b200_engine:
     _c["NGPU_SetDeliverGroup"] = _bind("NGPU_SetDeliverGroup", _I, [_I])
     _c["NGPU_SetUpdateOccupancy"] = _bind("NGPU_SetUpdateOccupancy", _I, [_I])
     _c["NGPU_GetBatchLength"] = _bind("NGPU_GetBatchLength", _I, [])
+    _c["NGPU_SetPersistent"] = _bind("NGPU_SetPersistent", _I, [_I])
     _c["NGPU_Autotune"] = _bind("NGPU_Autotune", _I, [_I] + [ctypes.POINTER(_I)] * 4)
     _c["NGPU_GetSimDeviceMs"] = _bind("NGPU_GetSimDeviceMs", ctypes.c_double, [])
     _c["NGPU_GetLaunchCount"] = _bind("NGPU_GetLaunchCount", ctypes.c_longlong, [])
@@ -1318,6 +1319,14 @@ def SetUpdateThreads(n):
     """Threads per block of the aeif update kernel: 64, 128 or 256 (engine extension)."""
     _need_b200("SetUpdateThreads")
     return _check(_c["NGPU_SetUpdateThreads"](n))
+
+
+def SetPersistent(on=True):
+    """iaf_psc_exp-only networks: run the steps in one cooperative launch per graph's worth
+    of steps, or in per-batch launches captured in CUDA graphs (the default; engine
+    extension)."""
+    _need_b200("SetPersistent")
+    return _check(_c["NGPU_SetPersistent"](1 if on else 0))
 
 
 def GetBatchLength():

@@ -143,6 +143,8 @@ def main():
         pops = microcircuit(ngpu, scale=scale)
         ngpu.Calibrate()
         build = time.time() - t0
+        if getattr(ngpu, "is_b200_engine", False) and os.environ.get("NGPU_AUTOTUNE"):
+            out["mapping"] = ngpu.Autotune(500)
         ngpu.Simulate(100.0)
         c0 = [np.asarray(ngpu.GetStatus(p, "spike_count")).ravel() for p in pops]
         t1 = time.time()
@@ -150,8 +152,8 @@ def main():
         sim = time.time() - t1
         c1 = [np.asarray(ngpu.GetStatus(p, "spike_count")).ravel() for p in pops]
         rates = [float((b - a).sum()) / len(b) / (bio_ms / 1000.0) for a, b in zip(c0, c1)]
-        out = {"build_s": build, "sim_s": sim, "bio_ms": bio_ms, "rtf": sim / (bio_ms / 1000.0),
-               "n_neurons": int(sum(len(p) for p in pops)), "pop_rates_hz": rates}
+        out.update({"build_s": build, "sim_s": sim, "bio_ms": bio_ms, "rtf": sim / (bio_ms / 1000.0),
+                    "n_neurons": int(sum(len(p) for p in pops)), "pop_rates_hz": rates})
         if getattr(ngpu, "is_b200_engine", False):
             out["device_ms_per_step"] = ngpu.GetSimDeviceMs() / (bio_ms / 0.1)
             out["profile_ms_per_step"] = ngpu.ProfileSteps(1000)

@@ -268,3 +268,26 @@ def test_per_neuron_parameters_bitexact(occ):
     assert c_g.sum() > 100
     assert np.array_equal(c_g, c_o)
     assert ngpu.GetStats()["n_derivs"] == o.NDerivs()
+
+
+def test_persistent_step_loop_equals_per_batch_launches():
+    """Eight iaf_psc_exp populations (minimum delay one step): the persistent cooperative
+    step loop and per-batch launches give the same spikes and recorded traces."""
+    from workloads import microcircuit
+    res = []
+    for pers in (True, False):
+        ngpu.Reset()
+        ngpu.SetVerbosityLevel(0)
+        ngpu.SetPersistent(pers)
+        pops = microcircuit(ngpu, scale=0.03)
+        rec = ngpu.CreateRecord("", ["V_m_rel", "I_syn_ex", "spike"], [pops[0][0], pops[2][3], pops[4][1]],
+                                [0, 0, 0])
+        ngpu.Simulate(60.0)
+        ngpu.Simulate(45.0)
+        counts = np.concatenate([np.asarray(ngpu.GetStatus(p, "spike_count")).ravel() for p in pops])
+        res.append((counts, np.asarray(ngpu.GetRecordData(rec), dtype=np.float32), ngpu.GetStats()))
+    (c1, r1, s1), (c2, r2, s2) = res
+    assert c1.sum() > 500
+    assert np.array_equal(c1, c2)
+    assert np.array_equal(r1, r2)
+    assert s1["n_events"] == s2["n_events"] and s1["status"] == 0
