@@ -756,37 +756,37 @@ def MpiFinalize():
 
 
 # ---------------------------------------------------------------- random numbers
+def _copy_out(pt, ctype, n):
+    """ctypes array holding a copy of an engine-allocated array of n elements (freed)."""
+    out = (ctype * n)()
+    if n > 0:
+        ctypes.memmove(out, pt, n * ctypes.sizeof(ctype))
+    _free(pt)
+    return out
+
+
 def RandomInt(n):
     pt = _c["NESTGPU_RandomInt"](n)
     _check()
-    out = [pt[i] for i in range(n)]
-    _free(pt)
-    return out
+    return list(_copy_out(pt, ctypes.c_uint, n))
 
 
 def RandomUniform(n):
     pt = _c["NESTGPU_RandomUniform"](n)
     _check()
-    out = [pt[i] for i in range(n)]
-    _free(pt)
-    return out
+    return list(_copy_out(pt, ctypes.c_float, n))
 
 
 def RandomNormal(n, mean, stddev):
     pt = _c["NESTGPU_RandomNormal"](n, mean, stddev)
     _check()
-    out = (ctypes.c_float * n)(*[pt[i] for i in range(n)])
-    _free(pt)
-    return out
+    return _copy_out(pt, ctypes.c_float, n)
 
 
 def RandomNormalClipped(n, mean, stddev, vmin, vmax, vstep=0):
     pt = _c["NESTGPU_RandomNormalClipped"](n, mean, stddev, vmin, vmax, vstep)
     _check()
-    n4 = (n // 4 + 1) * 4
-    out = (ctypes.c_float * n4)(*[pt[i] for i in range(n4)])
-    _free(pt)
-    return out
+    return _copy_out(pt, ctypes.c_float, (n // 4 + 1) * 4)
 
 
 # ---------------------------------------------------------------- connections
