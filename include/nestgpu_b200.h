@@ -314,6 +314,11 @@ int NGPU_SetDeliverGroup(int g);
    waits); 0 (default): per-batch launches in CUDA graphs.  Results are the same either way; the
    autotuner tries both. */
 int NGPU_SetPersistent(int on);
+/* Test hook for the failure path of the persistent loop: with extra > 0 its grid barriers wait
+   for more blocks than the launch has, so each wait runs out after its bounded number of polls
+   (a second or two); the kernel records the timeout and returns, and the Simulate call fails
+   with error code 2 while the GPU context stays usable.  0 (default) disables it. */
+int NGPU_TestBarrierTimeout(int extra);
 /* Autotuner of the launch mappings (no counterpart in the reference): on the calibrated
    network, times `steps` simulation steps per candidate of the update block size, the
    update kernel variant, the delivery lane group, the delivery grid and the RK5 step budget (coordinate descent, two

@@ -749,6 +749,15 @@ int NGPU_SetUpdateOccupancy(int on) {
   }, -1);
 }
 
+// Test hook: the persistent loop's grid barriers wait for `extra` blocks more than the launch
+// has, so their bounded waits run out (the kernel records a timeout and returns).
+int NGPU_TestBarrierTimeout(int extra) {
+  return guard([&] {
+    E().barrier_extra = extra > 0 ? extra : 0;
+    return 0;
+  }, -1);
+}
+
 int NGPU_SetPersistent(int on) {
   return guard([&] {
     E().persistent = on ? 1 : 0;

@@ -128,6 +128,7 @@ class Engine {
   int deliver_group = 32;         // lanes per delivery work item (8, 16, 32)
   int update_occupancy = 0;       // 1: register-capped aeif update kernel
   int persistent = 0;             // iaf-only networks: persistent cooperative step loop
+  int barrier_extra = 0;          // test hook: blocks the persistent loop's barriers wait for in excess
   bool use_device_rng = true;     // cuRAND device generator (as the reference) if a GPU exists
 
   void set_seed(unsigned long long s);
@@ -356,7 +357,7 @@ int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *c
 int launch_clock_advance(Clock *clk, int K, cudaStream_t st);
 int launch_persistent_iaf(const DeliverArgs &D, int group, const IafArgs *tab, const int *first, int ngroups,
                           const SpikeOut &so, const Clock *clk, int steps, int M, GridBarrier *bar, int max_blocks,
-                          cudaStream_t st);
+                          int barrier_extra, cudaStream_t st);
 int deliver_max_pairs();
 void pack_delivery_csr_noalloc(const int *src, const int *dly, const unsigned *target, const float *weight,
                                size_t n, int n_nodes, int dspan, unsigned long long *seg_off, EdgeW *edge,

@@ -264,11 +264,11 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier *bar, unsigned nblocks,
 template <int G>
 __global__ void __launch_bounds__(DELIVER_THREADS) persistent_iaf_kernel(
     const DeliverArgs D, const IafArgs *tab, const int *first, int ngroups, const SpikeOut so, const Clock *clk,
-    int K, int M, GridBarrier *bar) {
+    int K, int M, GridBarrier *bar, int extra) {
   extern __shared__ int s_pref[];
   __shared__ typename DeliverScan::TempStorage scan_tmp;
   const int total_n = first[ngroups];
-  const unsigned nb = gridDim.x;
+  const unsigned nb = gridDim.x + (unsigned)extra;   // extra > 0 only in the timeout test
   for (int k0 = 0; k0 < K; k0 += M) {
     const int mb = (K - k0 < M) ? K - k0 : M;
     deliver_batch<G>(D, clk, k0, mb, s_pref, scan_tmp, blockIdx.x, gridDim.x);
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(DELIVER_THREADS) persistent_iaf_kernel(
 // blocks that fit on the GPU at once (at most `max_blocks`).
 int launch_persistent_iaf(const DeliverArgs &D, int group, const IafArgs *tab, const int *first, int ngroups,
                           const SpikeOut &so, const Clock *clk, int steps, int M, GridBarrier *bar, int max_blocks,
-                          cudaStream_t st) {
+                          int barrier_extra, cudaStream_t st) {
   const size_t smem = (size_t)(D.dspan * M + 1) * sizeof(int);
   void *fn = group == 8 ? (void *)persistent_iaf_kernel<8>
                         : group == 16 ? (void *)persistent_iaf_kernel<16> : (void *)persistent_iaf_kernel<32>;
@@ -308,7 +308,8 @@ int launch_persistent_iaf(const DeliverArgs &D, int group, const IafArgs *tab, c
   const Clock *c = clk;
   int k = steps, m = M;
   GridBarrier *b = bar;
-  void *args[] = {&d, &t, &f, &ng, &s, &c, &k, &m, &b};
+  int x = barrier_extra;
+  void *args[] = {&d, &t, &f, &ng, &s, &c, &k, &m, &b, &x};
   if (cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(DELIVER_THREADS), args, smem, st) != cudaSuccess)
     return -1;
   return 1;

@@ -739,7 +739,7 @@ void Engine::run_persistent(int steps) {
   cuda_check(cudaMemsetAsync(d_bar_, 0, sizeof(GridBarrier), stream_), "barrier reset");
   const int r = launch_persistent_iaf(deliver_args(), deliver_group, d_iaf_tab_, d_iaf_first_, n_iaf_multi_,
                                       spike_out(), d_clk_, steps, batch_, d_bar_,
-                                      deliver_blocks_req > 0 ? deliver_blocks_req : 0, stream_);
+                                      deliver_blocks_req > 0 ? deliver_blocks_req : 0, barrier_extra, stream_);
   if (r < 0) throw NgpuError(std::string("cooperative launch of the persistent step loop failed: ") +
                              cudaGetErrorString(cudaGetLastError()));
   launch_clock_advance(d_clk_, steps, stream_);
@@ -916,10 +916,10 @@ void Engine::start_simulation() {
 void Engine::end_simulation() {
   if (!in_sim_) return;
   cuda_check(cudaStreamSynchronize(stream_), "end of simulation");
-  check_status();
   drain_rec_spike_times();
   if (it_ > 0) neural_time_ = neur_t0_ + (double)dt * (double)it_;
   in_sim_ = false;
+  check_status();
 }
 
 void Engine::simulation_step() {

@@ -169,6 +169,7 @@ if is_b200_engine:
     _c["NGPU_SetUpdateOccupancy"] = _bind("NGPU_SetUpdateOccupancy", _I, [_I])
     _c["NGPU_GetBatchLength"] = _bind("NGPU_GetBatchLength", _I, [])
     _c["NGPU_SetPersistent"] = _bind("NGPU_SetPersistent", _I, [_I])
+    _c["NGPU_TestBarrierTimeout"] = _bind("NGPU_TestBarrierTimeout", _I, [_I])
     _c["NGPU_Autotune"] = _bind("NGPU_Autotune", _I, [_I] + [ctypes.POINTER(_I)] * 4)
     _c["NGPU_GetSimDeviceMs"] = _bind("NGPU_GetSimDeviceMs", ctypes.c_double, [])
     _c["NGPU_GetLaunchCount"] = _bind("NGPU_GetLaunchCount", ctypes.c_longlong, [])

@@ -291,3 +291,27 @@ def test_persistent_step_loop_equals_per_batch_launches():
     assert np.array_equal(c1, c2)
     assert np.array_equal(r1, r2)
     assert s1["n_events"] == s2["n_events"] and s1["status"] == 0
+
+
+def test_persistent_barrier_timeout_is_reported():
+    """Failure path of the persistent step loop: barriers told to wait for one block more
+    than the launch has run out of polls; Simulate fails with an error instead of hanging,
+    and the engine (and its GPU context) keeps working afterwards."""
+    from workloads import microcircuit
+    ngpu.SetPersistent(True)
+    ngpu._c["NGPU_TestBarrierTimeout"](1)
+    microcircuit(ngpu, scale=0.01)
+    with pytest.raises(ValueError, match="timed out"):
+        ngpu.Simulate(1.0)
+    ngpu._c["NGPU_TestBarrierTimeout"](0)
+    ngpu.Reset()
+    ngpu.SetVerbosityLevel(0)
+    ngpu.SetHostRng(True)
+    pops_g = microcircuit(ngpu, scale=0.02)
+    o = orc.Oracle()
+    pops_o = microcircuit(o, scale=0.02)
+    ngpu.Simulate(50.0)
+    o.Simulate(50.0)
+    c_g = np.concatenate([np.asarray(ngpu.GetStatus(p, "spike_count")).ravel() for p in pops_g])
+    c_o = np.concatenate([np.asarray(o.GetStatus(p, "spike_count")).ravel() for p in pops_o])
+    assert np.array_equal(c_g, c_o)
