@@ -267,6 +267,8 @@ class Engine {
 
   // device
   cudaStream_t stream_ = nullptr;
+  cudaStream_t stream2_ = nullptr;      // second stream for non-aeif groups (fork / join per batch)
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   Clock *d_clk_ = nullptr;
   double *d_acc_ = nullptr;
   size_t n_acc_ = 0;

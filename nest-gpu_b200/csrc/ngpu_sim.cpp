@@ -65,6 +65,11 @@ void Engine::free_device() {
   log_cap_ = 0;
   if (stream_) cudaStreamDestroy(stream_);
   stream_ = nullptr;
+  if (stream2_) cudaStreamDestroy(stream2_);
+  stream2_ = nullptr;
+  if (ev_fork_) cudaEventDestroy(ev_fork_);
+  if (ev_join_) cudaEventDestroy(ev_join_);
+  ev_fork_ = ev_join_ = nullptr;
 }
 
 void Engine::invalidate_graphs() {
@@ -98,6 +103,9 @@ void Engine::calibrate() {
   calibrated_ = true;
   neural_time_ = 0.0;
   cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+  cuda_check(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking), "stream");
+  cuda_check(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming), "event");
+  cuda_check(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming), "event");
   const int N = n_nodes();
 
   // ---- model-level calibration on the host parameter tables
@@ -681,14 +689,35 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   count_launch(launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_,
                               deliver_group, d_clk_, k0, M, stream_));
   if (ev) cuda_check(cudaEventRecord((*ev)[1], stream_), "event");
-  if (n_iaf_multi_ >= 2)
-    count_launch(launch_iaf_multi(d_iaf_tab_, d_iaf_blk0_, n_iaf_multi_, iaf_multi_blocks_, so, d_clk_, k0, M,
-                                  stream_));
+  // With aeif groups and other spiking groups in the network, the others run on a second
+  // stream next to the aeif kernels: they then fill the SMs that the aeif straggler tail
+  // leaves idle.  The groups touch disjoint state (their own accumulator rows, node
+  // entries and record columns; the spike ring only through atomics).
+  bool has_aeif = false, has_other = false;
   for (auto &g : groups_) {
+    if (g.n <= 0) continue;
+    if (is_aeif(g.model)) has_aeif = true;
+    else if (g.model == M_IAF_PSC_EXP || g.model == M_SPIKE_GEN) has_other = true;
+  }
+  const bool fork = has_aeif && has_other;
+  cudaStream_t s2 = stream_;
+  if (fork) {
+    cuda_check(cudaEventRecord(ev_fork_, stream_), "fork");
+    cuda_check(cudaStreamWaitEvent(stream2_, ev_fork_, 0), "fork");
+    s2 = stream2_;
+  }
+  if (n_iaf_multi_ >= 2)
+    count_launch(launch_iaf_multi(d_iaf_tab_, d_iaf_blk0_, n_iaf_multi_, iaf_multi_blocks_, so, d_clk_, k0, M, s2));
+  for (auto &g : groups_) {
+    if (g.model == M_IAF_PSC_EXP && n_iaf_multi_ < 2)
+      count_launch(launch_iaf(iaf_args(g), so, d_clk_, k0, M, s2));
+    else if (g.model == M_SPIKE_GEN) count_launch(launch_spike_gen(sg_args(g), so, d_clk_, k0, M, s2));
+  }
+  for (auto &g : groups_)
     if (is_aeif(g.model)) count_launch(launch_aeif(g.model, aeif_args(g), so, d_clk_, k0, M, stream_));
-    else if (g.model == M_IAF_PSC_EXP && n_iaf_multi_ < 2)
-      count_launch(launch_iaf(iaf_args(g), so, d_clk_, k0, M, stream_));
-    else if (g.model == M_SPIKE_GEN) count_launch(launch_spike_gen(sg_args(g), so, d_clk_, k0, M, stream_));
+  if (fork) {
+    cuda_check(cudaEventRecord(ev_join_, stream2_), "join");
+    cuda_check(cudaStreamWaitEvent(stream_, ev_join_, 0), "join");
   }
   if (ev) cuda_check(cudaEventRecord((*ev)[2], stream_), "event");
 }
