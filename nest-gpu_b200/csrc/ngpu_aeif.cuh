@@ -44,11 +44,13 @@ struct StepT {
   double tnow;
 };
 
-__device__ __forceinline__ StepT step_at(const Clock *c, int k0, int m, float dt) {
+// The clock is read once per kernel (it changes only between graphs) and passed by value,
+// so the per-step time needs no memory access.
+__device__ __forceinline__ StepT step_at(const Clock &c, int k0, int m, float dt) {
   StepT s;
-  s.it = c->it0 + k0 + m;
-  s.tidx = c->tidx_base + s.it + 1;
-  s.tnow = c->t0 + (double)dt * (double)(s.it + 1);
+  s.it = c.it0 + k0 + m;
+  s.tidx = c.tidx_base + s.it + 1;
+  s.tnow = c.t0 + (double)dt * (double)(s.it + 1);
   return s;
 }
 
@@ -103,8 +105,18 @@ __device__ __forceinline__ void poisson_cache_load(const GroupInput &G, int i, P
   }
 }
 
+// in[port] += v with the port known only at run time, written as a compare per port so
+// that `in` stays in registers (an indexed store would place it in local memory).
+template <int PMAX>
+__device__ __forceinline__ void add_to_port(double *in, int port, double v) {
+#pragma unroll
+  for (int p = 0; p < PMAX; p++)
+    if (p == port) in[p] += v;
+}
+
 // The cached edge's draw: the same value as poisson_draw, without recomputing exp(-lam)
 // and with one Philox call per four steps.
+template <int PMAX>
 __device__ __forceinline__ void poisson_add_cached(double *in, const GroupInput &G, PoissonCache &c, long long tidx,
                                                    double tnow) {
   const double t_rel = tnow - (double)c.g.origin - (double)c.pe.delay;
@@ -120,16 +132,17 @@ __device__ __forceinline__ void poisson_add_cached(double *in, const GroupInput 
     } else {
       k = poisson_draw(c.lam, G.seed, c.pe.edge_id, tidx);
     }
-    if (k > 0) in[c.pe.port] += (double)__fmul_rn(c.pe.weight, (float)k);
+    if (k > 0) add_to_port<PMAX>(in, c.pe.port, (double)__fmul_rn(c.pe.weight, (float)k));
   }
 }
 
+template <int PMAX>
 __device__ __forceinline__ void poisson_add(double *in, const GroupInput &G, const PoissonIn &pe, const GenPar &g,
                                             long long tidx, double tnow) {
   const double t_rel = tnow - (double)g.origin - (double)pe.delay;
   if (t_rel >= (double)g.start && t_rel <= (double)g.stop) {
     int k = poisson_draw(__fmul_rn(G.lam_scale, g.rate), G.seed, pe.edge_id, tidx);
-    if (k > 0) in[pe.port] += (double)__fmul_rn(pe.weight, (float)k);
+    if (k > 0) add_to_port<PMAX>(in, pe.port, (double)__fmul_rn(pe.weight, (float)k));
   }
 }
 
@@ -157,11 +170,11 @@ __device__ __forceinline__ void step_inputs_pf(double *in, const double *a, int 
     if (p < np && a[p] != 0.0) acc[(size_t)p * n + i] = 0.0;
   }
   if (c.e1 - c.e0 == 1) {
-    poisson_add_cached(in, G, c, tidx, tnow);
+    poisson_add_cached<PMAX>(in, G, c, tidx, tnow);
   } else {
     for (int e = c.e0; e < c.e1; e++) {
       const PoissonIn pe = G.pin[e];
-      poisson_add(in, G, pe, G.gen[pe.gen], tidx, tnow);
+      poisson_add<PMAX>(in, G, pe, G.gen[pe.gen], tidx, tnow);
     }
   }
 }
@@ -478,6 +491,9 @@ __device__ __forceinline__ bool aeif_substep(const AeifArgs &A, const SpikeOut &
 }
 
 // Records of the step (values after the update, before the fold).
+// NVM: compile-time bound on nvar; the state is selected by comparisons so that it stays
+// in registers.
+template <int NVM>
 __device__ __forceinline__ void write_records(const GroupRecord &R, const SpikeOut &so, int node, int i,
                                               const float *y, int nvar, float refr, long long row,
                                               long long tidx) {
@@ -485,10 +501,14 @@ __device__ __forceinline__ void write_records(const GroupRecord &R, const SpikeO
   const int c0 = R.first[i], c1 = R.first[i + 1];
   for (int c = c0; c < c1; c++) {
     const int2 rc = R.col[c];
-    float v;
+    float v = 0.0f;
     if (rc.x < 0) v = (so.has_out[node] && so.last_tidx[node] == (int)tidx) ? so.last_height[node] : 0.0f;
     else if (rc.x == nvar) v = refr;
-    else v = y[rc.x];
+    else {
+#pragma unroll
+      for (int k = 0; k < NVM; k++)
+        if (k == rc.x) v = y[k];
+    }
     R.buf[(size_t)row * R.ncol + rc.y] = v;
   }
 }
@@ -501,7 +521,8 @@ __device__ __forceinline__ void aeif_end_step(const AeifArgs &A, const SpikeOut 
                                               PoissonCache &pc) {
   typedef AeifShape<MODEL> S;
   const int np = q.ports();
-  if (A.rec.first) write_records(A.rec, so, A.i0 + i, i, y, 2 + S::npv * np, refr, t.it - rec_it0, t.tidx);
+  if (A.rec.first)
+    write_records<2 + S::npv * PMAX>(A.rec, so, A.i0 + i, i, y, 2 + S::npv * np, refr, t.it - rec_it0, t.tidx);
   double in[PMAX];
   step_inputs_pf<PMAX>(in, apf, np, A.n, i, A.in, pc, m, t.tidx, t.tnow);
 #pragma unroll
@@ -565,7 +586,8 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
     float refr, h;
     double x;
     aeif_load<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
-    const long long rec_it0 = clk->rec_it0;
+    const Clock cl = *clk;
+    const long long rec_it0 = cl.rec_it0;
     int budget = A.budget > 0 ? A.budget : -1;
     PoissonCache pc;
     poisson_cache_load(A.in, i, pc);
@@ -573,7 +595,7 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
     // does not hold the others of its warp in that step; they go on with their next step.
     int m = 0, guard = 0;
     bool deferred = false;
-    StepT t = step_at(clk, k0, 0, A.dt);
+    StepT t = step_at(cl, k0, 0, A.dt);
     double apf[PMAX];
     acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, 0);
     while (m < M) {
@@ -586,7 +608,7 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
         aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
         guard = 0;
         if (++m < M) {
-          t = step_at(clk, k0, m, A.dt);
+          t = step_at(cl, k0, m, A.dt);
           acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
         }
       }
@@ -613,7 +635,8 @@ __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, c
     __syncthreads();
   }
   const int cnt = *A.strag_cnt;
-  const long long rec_it0 = clk->rec_it0;
+  const Clock cl = *clk;
+  const long long rec_it0 = cl.rec_it0;
   unsigned long long nd = 0;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
     const int2 e = A.strag_list[j];
@@ -628,7 +651,7 @@ __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, c
     PoissonCache pc;
     poisson_cache_load(A.in, i, pc);
     int m = e.y, guard = 0;
-    StepT t = step_at(clk, k0, m, A.dt);
+    StepT t = step_at(cl, k0, m, A.dt);
     double apf[PMAX];
     acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
     while (m < M) {
@@ -636,7 +659,7 @@ __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, c
         aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
         guard = 0;
         if (++m < M) {
-          t = step_at(clk, k0, m, A.dt);
+          t = step_at(cl, k0, m, A.dt);
           acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
         }
       }

@@ -40,11 +40,12 @@ __device__ __forceinline__ void iaf_neuron(const IafArgs &A, const SpikeOut &so,
               P21in = iget(A, IP_P21in, i), P22 = iget(A, IP_P22, i), P11ex = iget(A, IP_P11ex, i),
               P11in = iget(A, IP_P11in, i), theta = iget(A, IP_Theta_rel, i),
               V_reset = iget(A, IP_V_reset_rel, i), refr_steps = iget(A, IP_refr_steps, i);
-  const long long rec_it0 = clk->rec_it0;
+  const Clock cl = *clk;
+  const long long rec_it0 = cl.rec_it0;
   PoissonCache pc;
   poisson_cache_load(A.in, i, pc);
   for (int m = 0; m < M; m++) {
-    const StepT t = step_at(clk, k0, m, A.dt);
+    const StepT t = step_at(cl, k0, m, A.dt);
     double apf[2];
     acc_prefetch<2>(apf, 2, n, i, A.in, m);
     if (refr > 0.0f) {
@@ -61,7 +62,7 @@ __device__ __forceinline__ void iaf_neuron(const IafArgs &A, const SpikeOut &so,
     }
     if (A.rec.first) {
       const float yr[4] = {Iex, Iin, V, refr};
-      write_records(A.rec, so, A.i0 + i, i, yr, 4, refr, t.it - rec_it0, t.tidx);
+      write_records<4>(A.rec, so, A.i0 + i, i, yr, 4, refr, t.it - rec_it0, t.tidx);
     }
     double in[2];
     step_inputs_pf<2>(in, apf, 2, n, i, A.in, pc, m, t.tidx, t.tnow);
@@ -105,15 +106,16 @@ __global__ void spike_gen_batch_kernel(const SpikeGenArgs A, const SpikeOut so, 
   if (i >= A.n) return;
   const int e0 = A.off[i], e1 = A.off[i + 1];
   int nx = A.next[i];
-  const long long rec_it0 = clk->rec_it0;
+  const Clock cl = *clk;
+  const long long rec_it0 = cl.rec_it0;
   for (int m = 0; m < M; m++) {
-    const StepT t = step_at(clk, k0, m, A.dt);
+    const StepT t = step_at(cl, k0, m, A.dt);
     const int e = e0 + nx;
     if (e < e1 && (long long)A.tidx[e] == t.it) {
       push_spike(so, A.srec, A.i0 + i, i, A.height[e], t.tidx, t.tnow);
       nx++;
     }
-    if (A.rec.first) write_records(A.rec, so, A.i0 + i, i, nullptr, 0, 0.0f, t.it - rec_it0, t.tidx);
+    if (A.rec.first) write_records<0>(A.rec, so, A.i0 + i, i, nullptr, 0, 0.0f, t.it - rec_it0, t.tidx);
   }
   A.next[i] = nx;
 }
