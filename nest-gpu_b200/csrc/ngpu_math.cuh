@@ -20,12 +20,16 @@
 
 namespace ngpu {
 
+// Both functions compute the main path for every input and select the special results
+// at the end (no branches).  rint(x log2 e) comes from the magic-number addition
+// 1.5 * 2^23, which rounds to the nearest integer, ties to even, like rintf for
+// |x log2 e| < 2^22; the scale 2^n is applied as 2^(n>>1) * 2^(n - (n>>1)), the first
+// factor keeping the intermediate normal, so the result is the rounding of p * 2^n.
 __device__ __forceinline__ float exp_m(float x) {
-  if (!(x == x)) return x;
-  if (x > 88.72283935546875f) return __int_as_float(0x7f800000);
-  if (x < -103.972084045410156f) return 0.0f;
-  float n = rintf(__fmul_rn(x, 1.44269502162933349609f));
-  float r = __fmaf_rn(n, -0.693145751953125f, x);
+  const float xc = fminf(fmaxf(x, -103.972084045410156f), 88.72283935546875f);   // NaN -> a bound
+  const float t = __fadd_rn(__fmul_rn(xc, 1.44269502162933349609f), 12582912.0f);
+  const float n = __fsub_rn(t, 12582912.0f);
+  float r = __fmaf_rn(n, -0.693145751953125f, xc);
   r = __fmaf_rn(n, -1.428606765330187045e-06f, r);
   float p = 1.98412701e-04f;
   p = __fmaf_rn(p, r, 1.38888892e-03f);
@@ -35,34 +39,39 @@ __device__ __forceinline__ float exp_m(float x) {
   p = __fmaf_rn(p, r, 0.5f);
   p = __fmaf_rn(p, r, 1.0f);
   p = __fmaf_rn(p, r, 1.0f);
-  int ni = (int)n;
-  int n1 = ni / 2;
-  int n2 = ni - n1;
+  const int ni = __float_as_int(t) - 0x4B400000;
+  const int n1 = ni >> 1;
+  const int n2 = ni - n1;
   p = __fmul_rn(p, __int_as_float((n1 + 127) << 23));
   p = __fmul_rn(p, __int_as_float((n2 + 127) << 23));
-  return p;
+  p = (x > 88.72283935546875f) ? __int_as_float(0x7f800000) : p;
+  p = (x < -103.972084045410156f) ? 0.0f : p;
+  return (x == x) ? p : x;
 }
 
 __device__ __forceinline__ float log_m(float x) {
-  if (!(x > 0.0f)) return (x == 0.0f) ? __int_as_float(0xff800000) : __int_as_float(0x7fc00000);
-  if (x == __int_as_float(0x7f800000)) return x;
-  int e = 0;
-  if (x < 1.17549435e-38f) { x = __fmul_rn(x, 16777216.0f); e = -24; }
-  unsigned b = __float_as_uint(x);
-  e += (int)((b >> 23) & 0xff) - 127;
+  const bool sub = x < 1.17549435e-38f;
+  const float xs = sub ? __fmul_rn(x, 16777216.0f) : x;
+  const unsigned b = __float_as_uint(xs);
+  int e = (int)((b >> 23) & 0xff) - (sub ? 151 : 127);
   float m = __uint_as_float((b & 0x7fffffu) | 0x3f800000u);
-  if (m > 1.41421354f) { m = __fmul_rn(m, 0.5f); e += 1; }
-  float s = __fdiv_rn(__fsub_rn(m, 1.0f), __fadd_rn(m, 1.0f));
-  float s2 = __fmul_rn(s, s);
+  const bool hi = m > 1.41421354f;
+  m = hi ? __fmul_rn(m, 0.5f) : m;
+  e += hi ? 1 : 0;
+  const float s = __fdiv_rn(__fsub_rn(m, 1.0f), __fadd_rn(m, 1.0f));
+  const float s2 = __fmul_rn(s, s);
   float q = 9.09090936e-02f;
   q = __fmaf_rn(q, s2, 1.11111112e-01f);
   q = __fmaf_rn(q, s2, 1.42857149e-01f);
   q = __fmaf_rn(q, s2, 2.00000003e-01f);
   q = __fmaf_rn(q, s2, 3.33333343e-01f);
   q = __fmaf_rn(q, s2, 1.0f);
-  float lm = __fmul_rn(__fmul_rn(2.0f, s), q);
-  float fe = (float)e;
-  return __fmaf_rn(fe, 0.693145751953125f, __fmaf_rn(fe, 1.428606765330187045e-06f, lm));
+  const float lm = __fmul_rn(__fmul_rn(2.0f, s), q);
+  const float fe = (float)e;
+  float res = __fmaf_rn(fe, 0.693145751953125f, __fmaf_rn(fe, 1.428606765330187045e-06f, lm));
+  res = (x == __int_as_float(0x7f800000)) ? x : res;
+  res = (x == 0.0f) ? __int_as_float(0xff800000) : res;
+  return (x > 0.0f || x == 0.0f) ? res : __int_as_float(0x7fc00000);
 }
 
 struct U4 { uint32_t x, y, z, w; };
