@@ -320,12 +320,18 @@ int NGPU_SetPersistent(int on);
    with error code 2 while the GPU context stays usable.  0 (default) disables it. */
 int NGPU_TestBarrierTimeout(int extra);
 /* Autotuner of the launch mappings (no counterpart in the reference): on the calibrated
-   network, times `steps` simulation steps per candidate of the update block size, the
-   update kernel variant, the delivery lane group, the delivery grid and the RK5 step budget (coordinate descent, two
-   passes) and keeps the fastest.  The trials are ordinary simulation steps, so the network
-   advances by them.  Returns the number of trials (-1 on error) and the chosen values. */
+   network, after 4 x `steps` warm-up steps, times `steps` simulation steps per candidate of the
+   update block size, the update kernel variant, the delivery lane group, the delivery grid and
+   the RK5 step budget, each candidate twice (forward and reverse order), in a coordinate
+   descent of two passes, and keeps the fastest.  The trials are ordinary simulation steps, so
+   the network advances by them.  Returns the number of trials (-1 on error) and the chosen
+   values. */
 int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliver_blocks,
                   int *rk5_budget);
+/* The current launch mapping: writes min(n, 6) of {update block size, register-capped update
+   variant, delivery lane group, delivery grid (0: automatic), RK5 step budget, persistent loop}
+   and returns 6 (-1 on error).  No counterpart in the reference. */
+int NGPU_GetLaunchMapping(int *vals, int n);
 
 /* 1: draw connection random numbers with cuRAND's host generator instead of the device
    generator the reference uses (integer streams are identical, normal streams are not);

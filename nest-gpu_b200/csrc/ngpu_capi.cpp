@@ -705,6 +705,7 @@ int NGPU_SetDeliverBlocks(int n) {
   return guard([&] {
     if (n < 0) throw NgpuError("block count must be >= 0");
     E().deliver_blocks_req = n;
+    E().invalidate_graphs();
     return 0;
   }, 0);
 }
@@ -722,6 +723,7 @@ int NGPU_SetRk5Budget(int n) {
   return guard([&] {
     if (n < 0) throw NgpuError("RK5 budget must be >= 0");
     E().rk5_budget = n;
+    E().invalidate_graphs();
     return 0;
   }, 0);
 }
@@ -730,6 +732,7 @@ int NGPU_SetUpdateThreads(int n) {
   return guard([&] {
     if (n != 64 && n != 128 && n != 256) throw NgpuError("update block size must be 64, 128 or 256");
     E().update_threads = n;
+    E().invalidate_graphs();
     return 0;
   }, -1);
 }
@@ -738,6 +741,7 @@ int NGPU_SetDeliverGroup(int g) {
   return guard([&] {
     if (g != 8 && g != 16 && g != 32) throw NgpuError("delivery lane group must be 8, 16 or 32");
     E().deliver_group = g;
+    E().invalidate_graphs();
     return 0;
   }, -1);
 }
@@ -745,6 +749,7 @@ int NGPU_SetDeliverGroup(int g) {
 int NGPU_SetUpdateOccupancy(int on) {
   return guard([&] {
     E().update_occupancy = on ? 1 : 0;
+    E().invalidate_graphs();
     return 0;
   }, -1);
 }
@@ -761,6 +766,7 @@ int NGPU_TestBarrierTimeout(int extra) {
 int NGPU_SetPersistent(int on) {
   return guard([&] {
     E().persistent = on ? 1 : 0;
+    E().invalidate_graphs();
     return 0;
   }, -1);
 }
@@ -776,6 +782,15 @@ int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliv
   }, -1);
 }
 
+int NGPU_GetLaunchMapping(int *vals, int n) {
+  return guard([&] {
+    const int v[6] = {E().update_threads, E().update_occupancy, E().deliver_group, E().deliver_blocks_req,
+                      E().rk5_budget, E().persistent};
+    for (int i = 0; i < n && i < 6; i++) vals[i] = v[i];
+    return 6;
+  }, -1);
+}
+
 int NGPU_GetBatchLength() {
   return guard([&] {
     if (!E().calibrated()) throw NgpuError("the batch length is known after calibration");
@@ -787,6 +802,7 @@ int NGPU_SetGraphSteps(int n) {
   return guard([&] {
     if (n < 1) throw NgpuError("graph steps must be >= 1");
     E().graph_steps = n;
+    E().invalidate_graphs();
     return 0;
   }, 0);
 }

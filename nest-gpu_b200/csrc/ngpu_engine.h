@@ -203,10 +203,11 @@ class Engine {
   std::vector<double> profile_steps(int n);
   long long n_launches() const { return n_launch_; }
 
-  // Tune update_threads, deliver_group, deliver_blocks_req and rk5_budget on the
-  // calibrated network by timing `steps` simulation steps per candidate (coordinate
-  // descent, two passes).  The trials are ordinary simulation steps: the network
-  // advances by them.  Returns the number of trials; the chosen values stay set.
+  // Tune update_threads, update_occupancy, deliver_group, deliver_blocks_req and rk5_budget
+  // (and the persistent loop where eligible) on the calibrated network: after 4 x `steps`
+  // warm-up steps, each candidate is timed twice over `steps` simulation steps (coordinate
+  // descent, two passes).  The trials are ordinary simulation steps: the network advances
+  // by them.  Returns the number of trials; the chosen values stay set.
   int autotune(int steps, std::vector<std::pair<std::string, double>> *log);
 
   // ---- learned RK5 step-size proposal (kernels and training in ngpu_learn.cu)
@@ -224,6 +225,8 @@ class Engine {
   void step_model_enable(bool on);
   int learn_mode() const { return learn_mode_; }
   int batch_length() const { return batch_; }
+  // captured graphs hold the launch mappings: drop them when a mapping knob changes
+  void invalidate_graphs();
 
   // device buffers exposed to the engine-level helpers
   cudaStream_t stream() const { return stream_; }
@@ -334,7 +337,6 @@ class Engine {
   void run_steps(long long n);
   void drain_records(long long rows);
   void drain_rec_spike_times();
-  void invalidate_graphs();
   SpikeOut spike_out() const;
   AeifArgs aeif_args(Group &g);
   IafArgs iaf_args(Group &g);

@@ -1044,19 +1044,31 @@ int Engine::autotune(int steps, std::vector<std::pair<std::string, double>> *log
   const int verb = verbosity;
   verbosity = 0;
   const int base = std::max(148, deliver_blocks_);
+  // A knob sets one or more variables together: the delivery lane group and grid interact
+  // (a coordinate descent over them one at a time settles in local optima), so their
+  // combinations are one knob.
   struct Knob {
     const char *name;
-    int *var;
-    std::vector<int> cand;
+    std::vector<int *> vars;
+    std::vector<std::vector<int>> cand;
   };
+  auto single = [](const char *name, int *var, std::vector<int> vals) {
+    Knob k{name, {var}, {}};
+    for (int v : vals) k.cand.push_back({v});
+    return k;
+  };
+  Knob deliver{"deliver_group,deliver_blocks", {&deliver_group, &deliver_blocks_req}, {}};
+  std::vector<int> blocks{148, 296, 592, 1184, 2368};
+  if (std::find(blocks.begin(), blocks.end(), base) == blocks.end()) blocks.push_back(base);
+  for (int g : {8, 16, 32})
+    for (int b : blocks) deliver.cand.push_back({g, b});
   std::vector<Knob> knobs = {
-      {"update_threads", &update_threads, {64, 128, 256}},
-      {"update_occupancy", &update_occupancy, {0, 1}},
-      {"deliver_group", &deliver_group, {8, 16, 32}},
-      {"deliver_blocks", &deliver_blocks_req, {148, 296, 592, 1184, 2368, base}},
-      {"rk5_budget", &rk5_budget, {0, 1, 2, 4, 8}},
+      single("update_threads", &update_threads, {64, 128, 256}),
+      single("update_occupancy", &update_occupancy, {0, 1}),
+      deliver,
+      single("rk5_budget", &rk5_budget, {0, 1, 2, 4, 8}),
   };
-  if (persistent_eligible()) knobs.insert(knobs.begin(), Knob{"persistent", &persistent, {0, 1}});
+  if (persistent_eligible()) knobs.insert(knobs.begin(), single("persistent", &persistent, {0, 1}));
   if (deliver_blocks_req <= 0) deliver_blocks_req = base;
   const float t = (float)steps * dt;
   auto trial = [&]() {
@@ -1067,24 +1079,41 @@ int Engine::autotune(int steps, std::vector<std::pair<std::string, double>> *log
   };
   int n_trials = 0;
   try {
+    // A network started from rest goes through a transient in which its activity, and so
+    // the cost of a step, changes from one trial to the next: run through it first.  Then
+    // each knob's candidates are timed twice, in forward and in reverse order (a slow drift
+    // of the activity then favours none of them), and the better time of each counts.
+    simulate(4.0f * t);
     for (int pass = 0; pass < 2; pass++) {
       for (auto &k : knobs) {
-        int best = *k.var;
-        double best_ms = trial();
-        n_trials++;
-        if (log) log->push_back({std::string(k.name) + "=" + std::to_string(best), best_ms});
-        for (int c : k.cand) {
-          if (c == best) continue;
-          *k.var = c;
-          const double ms = trial();
-          n_trials++;
-          if (log) log->push_back({std::string(k.name) + "=" + std::to_string(c), ms});
-          if (ms < best_ms) {
-            best_ms = ms;
-            best = c;
+        auto set = [&](const std::vector<int> &v) {
+          for (size_t j = 0; j < k.vars.size(); j++) *k.vars[j] = v[j];
+        };
+        std::vector<std::vector<int>> cand;
+        std::vector<int> cur;
+        for (int *p : k.vars) cur.push_back(*p);
+        cand.push_back(cur);
+        for (auto &c : k.cand)
+          if (c != cur) cand.push_back(c);
+        std::vector<double> best_ms(cand.size(), 1e300);
+        for (int rep = 0; rep < 2; rep++) {
+          for (size_t u = 0; u < cand.size(); u++) {
+            const size_t ci = rep == 0 ? u : cand.size() - 1 - u;
+            set(cand[ci]);
+            const double ms = trial();
+            n_trials++;
+            if (log) {
+              std::string s = std::string(k.name) + "=";
+              for (size_t j = 0; j < cand[ci].size(); j++) s += (j ? "," : "") + std::to_string(cand[ci][j]);
+              log->push_back({s, ms});
+            }
+            best_ms[ci] = std::min(best_ms[ci], ms);
           }
         }
-        *k.var = best;
+        size_t bi = 0;
+        for (size_t ci = 1; ci < cand.size(); ci++)
+          if (best_ms[ci] < best_ms[bi]) bi = ci;
+        set(cand[bi]);
       }
     }
   } catch (...) {

@@ -171,6 +171,7 @@ if is_b200_engine:
     _c["NGPU_SetPersistent"] = _bind("NGPU_SetPersistent", _I, [_I])
     _c["NGPU_TestBarrierTimeout"] = _bind("NGPU_TestBarrierTimeout", _I, [_I])
     _c["NGPU_Autotune"] = _bind("NGPU_Autotune", _I, [_I] + [ctypes.POINTER(_I)] * 4)
+    _c["NGPU_GetLaunchMapping"] = _bind("NGPU_GetLaunchMapping", _I, [ctypes.POINTER(_I), _I])
     _c["NGPU_GetSimDeviceMs"] = _bind("NGPU_GetSimDeviceMs", ctypes.c_double, [])
     _c["NGPU_GetLaunchCount"] = _bind("NGPU_GetLaunchCount", ctypes.c_longlong, [])
     _c["NGPU_ProfileSteps"] = _bind("NGPU_ProfileSteps", _I, [_I, ctypes.POINTER(ctypes.c_double)])
@@ -1358,8 +1359,21 @@ def Autotune(steps=200):
     a, b, c, d = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     n = _c["NGPU_Autotune"](steps, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d))
     _check()
-    return {"update_threads": a.value, "deliver_group": b.value, "deliver_blocks": c.value,
-            "rk5_budget": d.value, "trials": n}
+    m = GetLaunchMapping()
+    m["trials"] = n
+    return m
+
+
+def GetLaunchMapping():
+    """The current launch mapping (engine extension): update block size and variant, delivery
+    lane group and grid, RK5 step budget and persistent loop."""
+    _need_b200("GetLaunchMapping")
+    v = (ctypes.c_int * 6)()
+    _c["NGPU_GetLaunchMapping"](v, 6)
+    _check()
+    keys = ["update_threads", "update_occupancy", "deliver_group", "deliver_blocks", "rk5_budget",
+            "persistent"]
+    return dict(zip(keys, [int(x) for x in v]))
 
 
 def SetGraphSteps(n):

@@ -58,6 +58,7 @@ def test_autotuner_picks_valid_mapping_and_keeps_results():
     assert chosen["update_threads"] in (64, 128, 256)
     assert chosen["deliver_group"] in (8, 16, 32)
     assert chosen["rk5_budget"] in (0, 1, 2, 4, 8)
+    assert chosen["update_occupancy"] in (0, 1)
     assert chosen["trials"] > 10
     t_tuned = ngpu.GetStats()["steps"] * 0.1
     c_tuned = {m: np.asarray(ngpu.GetStatus(g, "spike_count")).ravel() for m, g in groups.items()}
