@@ -62,6 +62,9 @@ def parse():
     p.add_argument("--scale", type=float, default=1.0, help="fraction of the 1M-neuron network (tests)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="keep the default launch mappings")
+    p.add_argument("--mapping", default="",
+                   help="fixed launch mapping instead of the autotuner: update threads, register-capped "
+                        "variant (0/1), delivery lane group, delivery blocks, RK5 budget, e.g. 64,1,32,592,1")
     p.add_argument("--batch-max", type=int, default=0, help="upper bound of the time-batch length")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the learned-step and ensemble measurements")
@@ -213,7 +216,16 @@ def engine_arm(args):
     build_s = time.time() - t_build0
     # launch mappings picked on this network (the trial steps are part of the transient)
     t_tune0 = time.time()
-    mapping = ngpu.Autotune(400) if not args.no_autotune else None
+    if args.mapping:
+        th, occ, grp, blk, bud = (int(x) for x in args.mapping.split(","))
+        ngpu.SetUpdateThreads(th)
+        ngpu.SetUpdateOccupancy(occ)
+        ngpu.SetDeliverGroup(grp)
+        ngpu.SetDeliverBlocks(blk)
+        ngpu.SetRk5Budget(bud)
+        mapping = ngpu.GetLaunchMapping()
+    else:
+        mapping = ngpu.Autotune(400) if not args.no_autotune else None
     tune_s = time.time() - t_tune0
     n_neurons = len(neuron)
 

@@ -368,44 +368,60 @@ __device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmi
   for (;;) {
     if (h > hmax) h = hmax;
     if (h < hmin) h = hmin;
-    const float b21 = __fmul_rn(h, ck::a21), b31 = __fmul_rn(h, ck::a31), b32 = __fmul_rn(h, ck::a32),
-                b41 = __fmul_rn(h, ck::a41), b42 = __fmul_rn(h, ck::a42), b43 = __fmul_rn(h, ck::a43),
-                b51 = __fmul_rn(h, ck::a51), b52 = __fmul_rn(h, ck::a52), b53 = __fmul_rn(h, ck::a53),
-                b54 = __fmul_rn(h, ck::a54), b61 = __fmul_rn(h, ck::a61), b62 = __fmul_rn(h, ck::a62),
-                b63 = __fmul_rn(h, ck::a63), b64 = __fmul_rn(h, ck::a64), b65 = __fmul_rn(h, ck::a65),
-                b71 = __fmul_rn(h, ck::a71), b73 = __fmul_rn(h, ck::a73), b74 = __fmul_rn(h, ck::a74),
-                b76 = __fmul_rn(h, ck::a76), f1 = __fmul_rn(h, ck::e1), f3 = __fmul_rn(h, ck::e3),
-                f4 = __fmul_rn(h, ck::e4), f5 = __fmul_rn(h, ck::e5), f6 = __fmul_rn(h, ck::e6);
+    // each stage's coefficients h * a_ij are formed just before the stage (short live ranges)
+    {
+      const float b21 = __fmul_rn(h, ck::a21);
 #pragma unroll
-    for (int i = 0; i < NVM; i++)
-      if (i < NV) yn[i] = __fmaf_rn(b21, k1[i], y[i]);
+      for (int i = 0; i < NVM; i++)
+        if (i < NV) yn[i] = __fmaf_rn(b21, k1[i], y[i]);
+    }
     aeif_derivs(yn, k2, q, refr);
+    {
+      const float b31 = __fmul_rn(h, ck::a31), b32 = __fmul_rn(h, ck::a32);
 #pragma unroll
-    for (int i = 0; i < NVM; i++)
-      if (i < NV) yn[i] = __fmaf_rn(b32, k2[i], __fmaf_rn(b31, k1[i], y[i]));
+      for (int i = 0; i < NVM; i++)
+        if (i < NV) yn[i] = __fmaf_rn(b32, k2[i], __fmaf_rn(b31, k1[i], y[i]));
+    }
     aeif_derivs(yn, k3, q, refr);
+    {
+      const float b41 = __fmul_rn(h, ck::a41), b42 = __fmul_rn(h, ck::a42), b43 = __fmul_rn(h, ck::a43);
 #pragma unroll
-    for (int i = 0; i < NVM; i++)
-      if (i < NV) yn[i] = __fmaf_rn(b43, k3[i], __fmaf_rn(b42, k2[i], __fmaf_rn(b41, k1[i], y[i])));
+      for (int i = 0; i < NVM; i++)
+        if (i < NV) yn[i] = __fmaf_rn(b43, k3[i], __fmaf_rn(b42, k2[i], __fmaf_rn(b41, k1[i], y[i])));
+    }
     aeif_derivs(yn, k4, q, refr);
+    {
+      const float b51 = __fmul_rn(h, ck::a51), b52 = __fmul_rn(h, ck::a52), b53 = __fmul_rn(h, ck::a53),
+                  b54 = __fmul_rn(h, ck::a54);
 #pragma unroll
-    for (int i = 0; i < NVM; i++)
-      if (i < NV)
-        yn[i] = __fmaf_rn(b54, k4[i],
-                          __fmaf_rn(b53, k3[i], __fmaf_rn(b52, k2[i], __fmaf_rn(b51, k1[i], y[i]))));
+      for (int i = 0; i < NVM; i++)
+        if (i < NV)
+          yn[i] = __fmaf_rn(b54, k4[i],
+                            __fmaf_rn(b53, k3[i], __fmaf_rn(b52, k2[i], __fmaf_rn(b51, k1[i], y[i]))));
+    }
     aeif_derivs(yn, k5, q, refr);
+    {
+      const float b61 = __fmul_rn(h, ck::a61), b62 = __fmul_rn(h, ck::a62), b63 = __fmul_rn(h, ck::a63),
+                  b64 = __fmul_rn(h, ck::a64), b65 = __fmul_rn(h, ck::a65);
 #pragma unroll
-    for (int i = 0; i < NVM; i++)
-      if (i < NV)
-        yn[i] = __fmaf_rn(b65, k5[i],
-                          __fmaf_rn(b64, k4[i], __fmaf_rn(b63, k3[i],
-                                                          __fmaf_rn(b62, k2[i], __fmaf_rn(b61, k1[i], y[i])))));
+      for (int i = 0; i < NVM; i++)
+        if (i < NV)
+          yn[i] = __fmaf_rn(b65, k5[i],
+                            __fmaf_rn(b64, k4[i], __fmaf_rn(b63, k3[i],
+                                                            __fmaf_rn(b62, k2[i], __fmaf_rn(b61, k1[i], y[i])))));
+    }
     aeif_derivs(yn, k6, q, refr);
+    {
+      const float b71 = __fmul_rn(h, ck::a71), b73 = __fmul_rn(h, ck::a73), b74 = __fmul_rn(h, ck::a74),
+                  b76 = __fmul_rn(h, ck::a76);
 #pragma unroll
-    for (int i = 0; i < NVM; i++)
-      if (i < NV)
-        yn[i] = __fmaf_rn(b76, k6[i],
-                          __fmaf_rn(b74, k4[i], __fmaf_rn(b73, k3[i], __fmaf_rn(b71, k1[i], y[i]))));
+      for (int i = 0; i < NVM; i++)
+        if (i < NV)
+          yn[i] = __fmaf_rn(b76, k6[i],
+                            __fmaf_rn(b74, k4[i], __fmaf_rn(b73, k3[i], __fmaf_rn(b71, k1[i], y[i]))));
+    }
+    const float f1 = __fmul_rn(h, ck::e1), f3 = __fmul_rn(h, ck::e3), f4 = __fmul_rn(h, ck::e4),
+                f5 = __fmul_rn(h, ck::e5), f6 = __fmul_rn(h, ck::e6);
     err = 0.0f;
 #pragma unroll
     for (int i = 0; i < NVM; i++) {

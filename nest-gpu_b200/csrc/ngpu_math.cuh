@@ -26,10 +26,11 @@ namespace ngpu {
 // |x log2 e| < 2^22; the scale 2^n is applied as 2^(n>>1) * 2^(n - (n>>1)), the first
 // factor keeping the intermediate normal, so the result is the rounding of p * 2^n.
 __device__ __forceinline__ float exp_m(float x) {
-  const float xc = fminf(fmaxf(x, -103.972084045410156f), 88.72283935546875f);   // NaN -> a bound
-  const float t = __fadd_rn(__fmul_rn(xc, 1.44269502162933349609f), 12582912.0f);
+  // inputs outside [-103.97, 88.72] (and NaN) give meaningless bits on the main path, which
+  // the selects at the end replace
+  const float t = __fadd_rn(__fmul_rn(x, 1.44269502162933349609f), 12582912.0f);
   const float n = __fsub_rn(t, 12582912.0f);
-  float r = __fmaf_rn(n, -0.693145751953125f, xc);
+  float r = __fmaf_rn(n, -0.693145751953125f, x);
   r = __fmaf_rn(n, -1.428606765330187045e-06f, r);
   float p = 1.98412701e-04f;
   p = __fmaf_rn(p, r, 1.38888892e-03f);
@@ -39,11 +40,11 @@ __device__ __forceinline__ float exp_m(float x) {
   p = __fmaf_rn(p, r, 0.5f);
   p = __fmaf_rn(p, r, 1.0f);
   p = __fmaf_rn(p, r, 1.0f);
-  const int ni = __float_as_int(t) - 0x4B400000;
+  const int ni = (int)(__float_as_uint(t) - 0x4B400000u);
   const int n1 = ni >> 1;
   const int n2 = ni - n1;
-  p = __fmul_rn(p, __int_as_float((n1 + 127) << 23));
-  p = __fmul_rn(p, __int_as_float((n2 + 127) << 23));
+  p = __fmul_rn(p, __uint_as_float((unsigned)(n1 + 127) << 23));
+  p = __fmul_rn(p, __uint_as_float((unsigned)(n2 + 127) << 23));
   p = (x > 88.72283935546875f) ? __int_as_float(0x7f800000) : p;
   p = (x < -103.972084045410156f) ? 0.0f : p;
   return (x == x) ? p : x;
