@@ -21,6 +21,9 @@
 //                                         src/connect_rules.cpp:274-322
 //   RandomInt / RandomNormal(Clipped)     src/random.cu:8-76, src/nestgpu.cu:1135-1188
 //   step order                            src/nestgpu.cu:294-635
+//   synapse groups and STDP               src/syn_model.cu:43-56,136-152, src/stdp.cu:36-80,
+//                                         src/test_syn_model.cu:35-50, src/get_spike.cu:85-95,
+//                                         src/rev_spike.cu:46-130, src/nestgpu.cu:490-498,606-616
 //
 // Two arithmetic modes:
 //   fp64 = 0  "FP32 mirror": float state, explicit fused multiply-adds, the
@@ -349,7 +352,41 @@ static double mlp_grad_d(const float *M, const float *feat, const float *target,
 
 struct Queued { int age; int cursor; float height; };
 
-struct Edge { int tgt; unsigned char port; float w; };
+// syn: synapse group (0: static, k: syn_groups[k-1]); stamp: low 16 bits of the time index
+// of the last spike that arrived through the edge (plastic edges), 0x8000 initially
+// (src/rev_spike.cu:150-155)
+struct Edge { int tgt; unsigned char port; float w; unsigned char syn = 0; unsigned short stamp = 0x8000; };
+
+// Synapse models (src/syn_model.h, src/stdp.h:70-94, src/test_syn_model.h)
+enum SynType { SYN_TEST = 0, SYN_STDP = 1 };
+struct SynGroupDef { int type; std::vector<float> par; };
+static const char *const kStdpPar[] = {"tau_plus", "tau_minus", "lambda", "alpha", "mu_plus", "mu_minus", "Wmax"};
+static const char *const kTestPar[] = {"fact", "offset"};
+constexpr int kMaxSynDt = 16384;                 // MAX_SYN_DT, src/syn_model.h:33
+constexpr long long kLastSpikeGuard = 0x70000000LL;   // src/spike_buffer.cu:42
+
+// SynapseUpdate (src/syn_model.cu:43-56): STDPUpdate (src/stdp.cu:36-64) in FP64, or the
+// test model's linear rule (src/test_syn_model.cu:35-40).
+static float synapse_update(const SynGroupDef &g, float w, float Dt) {
+  if (g.type == SYN_TEST) {
+    const float fact = g.par[0], offset = g.par[1];
+    return w + std::fma(fact, Dt, offset);
+  }
+  const double tau_plus = g.par[0], tau_minus = g.par[1], lambda = g.par[2], alpha = g.par[3];
+  const double mu_plus = g.par[4], mu_minus = g.par[5], Wmax = g.par[6];
+  const double wd = w;
+  double w1;
+  if (Dt >= 0) {
+    const double fact = lambda * std::exp(-(double)Dt / tau_plus);
+    w1 = wd + fact * Wmax * std::pow(1.0 - wd / Wmax, mu_plus);
+  } else {
+    const double fact = -alpha * lambda * std::exp((double)Dt / tau_minus);
+    w1 = wd + fact * Wmax * std::pow(wd / Wmax, mu_minus);
+  }
+  w1 = w1 > 0.0 ? w1 : 0.0;
+  w1 = w1 < Wmax ? w1 : Wmax;
+  return (float)w1;
+}
 struct DelayGroup { int delay; std::vector<Edge> tg; };
 
 struct Rec { int node; std::string var; int port; };
@@ -364,6 +401,10 @@ struct Net {
   std::vector<Group> groups;
   std::vector<int> node_group;
   std::vector<std::vector<DelayGroup>> conn;     // per source, delays ascending
+  std::vector<SynGroupDef> syn_groups;
+  bool any_plastic = false;
+  std::vector<long long> last_rev;                // per node: time index of the last spike
+  std::vector<std::vector<Edge *>> rev_in;        // per node: incoming plastic edges
   // simulation state
   bool calibrated = false;
   bool first_sim = true;
@@ -586,8 +627,10 @@ struct Net {
   }
 
   // src/connect.cu:38-74
-  void connect1(int src, int tgt, int port, float w, float delay) {
+  void connect1(int src, int tgt, int port, float w, float delay, int syn = 0) {
     if (delay < dt) throw std::runtime_error("Delay must be >= time resolution");
+    if (syn < 0 || syn > (int)syn_groups.size()) throw std::runtime_error("Unrecognized synapse group");
+    if (syn > 0) any_plastic = true;
     int d_int = (int)std::round(delay / dt) - 1;
     std::vector<DelayGroup> &c = conn[src];
     size_t id = 0;
@@ -595,16 +638,20 @@ struct Net {
     if (id == c.size() || d_int != c[id].delay) {
       DelayGroup ng;
       ng.delay = d_int;
-      ng.tg.push_back({tgt, (unsigned char)port, w});
+      Edge e{tgt, (unsigned char)port, w};
+      e.syn = (unsigned char)syn;
+      ng.tg.push_back(e);
       c.insert(c.begin() + id, ng);
     } else {
-      c[id].tg.push_back({tgt, (unsigned char)port, w});
+      Edge e{tgt, (unsigned char)port, w};
+      e.syn = (unsigned char)syn;
+      c[id].tg.push_back(e);
     }
   }
 
   // src/connect_rules.h:161-338 (one host thread: THREAD_MAXNUM == 1)
   void connect_rule(int rule, const int *src_arr, int src0, int ns, const int *tgt_arr, int tgt0,
-                    int nt, int degree, int port, float weight, float delay,
+                    int nt, int degree, int port, int syn, float weight, float delay,
                     const float *warr, const float *darr) {
     if (calibrated) throw std::runtime_error("Connections cannot be created after calibration");
     auto S = [&](int i) { return src_arr ? src_arr[i] : src0 + i; };
@@ -612,7 +659,7 @@ struct Net {
     auto one = [&](int is, int it_, size_t ia) {
       float w = warr ? warr[ia] : weight;
       float d = darr ? darr[ia] : delay;
-      connect1(S(is), T(it_), port, w, d);
+      connect1(S(is), T(it_), port, w, d, syn);
     };
     enum { ONE_TO_ONE = 0, ALL_TO_ALL, FIXED_TOTAL_NUMBER, FIXED_INDEGREE, FIXED_OUTDEGREE };
     const int thresh = 5;
@@ -777,6 +824,20 @@ struct Net {
           Group &tg = groups[node_group[e.tgt]];
           if (e.port >= tg.nport) throw std::runtime_error("receptor port out of range for target node");
         }
+    // plastic edges: per target the incoming ones (src/spike_buffer.cu:430-520), and the
+    // last spike time index of every node (src/spike_buffer.cu:319-328)
+    last_rev.assign(node_group.size(), kLastSpikeGuard);
+    rev_in.assign(node_group.size(), {});
+    if (any_plastic)
+      for (size_t s = 0; s < conn.size(); s++) {
+        if (groups[node_group[s]].model == POISS_GEN)
+          for (auto &dg : conn[s])
+            for (auto &e : dg.tg)
+              if (e.syn) throw std::runtime_error("poiss_gen connections cannot be plastic");
+        for (auto &dg : conn[s])
+          for (auto &e : dg.tg)
+            if (e.syn) rev_in[e.tgt].push_back(&e);
+      }
   }
 
   // ---------------------------------------------------------------- stepping
@@ -1050,7 +1111,7 @@ struct Net {
     if (g.max_rec > 0) {
       if ((int)g.rec_times[i].size() < g.max_rec - 1) g.rec_times[i].push_back((float)neural_time);
     }
-    (void)tidx;
+    last_rev[node] = tidx;   // den_delay 0: the spike reaches the dendrites at once
     if (!conn[node].empty()) {
       std::vector<Queued> &q = queue[node];
       if ((int)q.size() >= max_spike_buffer) return;   // reference prints and drops
@@ -1208,6 +1269,18 @@ struct Net {
     // 2. time
     neural_time = neur_t0 + (double)dt * (double)(it + 1);
     long long tidx = (long long)(int)std::round(neur_t0 / (double)dt) + it + 1;
+    // 2b. keep the 16-bit arrival stamps of plastic edges unambiguous
+    //     (src/nestgpu.cu:490-498, src/rev_spike.cu:93-118)
+    if (any_plastic && ((tidx & 0xffff) == 0x8000 || (tidx & 0xffff) == 0)) {
+      const bool up = (tidx & 0xffff) == 0x8000;
+      for (auto &v : conn)
+        for (auto &dg : v)
+          for (auto &e : dg.tg) {
+            if (!e.syn) continue;
+            if (up && e.stamp >= 0x8000) e.stamp = 0;
+            if (!up && e.stamp < 0x8000) e.stamp = 0x8000;
+          }
+    }
     // 3. update
     for (auto &g : groups) {
       if (is_aeif(g.model)) {
@@ -1241,6 +1314,13 @@ struct Net {
 #pragma omp atomic
         a += v;
         nev++;
+        if (e.syn) {
+          // src/get_spike.cu:85-95: arrival stamp, depression against the target's last spike
+          e.stamp = (unsigned short)(tidx & 0xffff);
+          const long long Dt_int = tidx - last_rev[e.tgt];
+          if (Dt_int > 0 && Dt_int < kMaxSynDt)
+            e.w = synapse_update(syn_groups[e.syn - 1], e.w, -dt * (float)Dt_int);
+        }
       }
     }
     n_events += nev;
@@ -1288,6 +1368,19 @@ struct Net {
           else (*pi)[i] = (double)(float)std::fma(a, pw, (double)(float)cur);
         }
     }
+    // 8. reverse spikes (src/rev_spike.cu:46-92, src/nestgpu.cu:606-616): the plastic
+    //    in-edges of every node that spiked in this step are potentiated
+    if (any_plastic) {
+      const unsigned short t16 = (unsigned short)(tidx & 0xffff);
+#pragma omp parallel for schedule(dynamic, 64)
+      for (size_t nd = 0; nd < rev_in.size(); nd++) {
+        if (rev_in[nd].empty() || last_rev[nd] != tidx) continue;
+        for (Edge *e : rev_in[nd]) {
+          const unsigned short Dt_int = (unsigned short)(t16 - e->stamp);
+          if (Dt_int < kMaxSynDt) e->w = synapse_update(syn_groups[e->syn - 1], e->w, dt * (float)Dt_int);
+        }
+      }
+    }
     it++;
   }
 
@@ -1304,6 +1397,11 @@ struct Net {
 // C ABI for the Python test harness (oracle/oracle.py)
 // ---------------------------------------------------------------------------
 using orc::Net;
+using orc::SynGroupDef;
+using orc::SYN_STDP;
+using orc::SYN_TEST;
+using orc::kStdpPar;
+using orc::kTestPar;
 
 static thread_local std::string g_err;
 
@@ -1401,14 +1499,43 @@ int orc_random_normal_clipped(void *p, size_t n, float mean, float sd, float vmi
 }
 
 int orc_connect(void *p, int rule, const int *src, int src0, int ns, const int *tgt, int tgt0, int nt,
-                int degree, int port, float w, float d, const float *warr, const float *darr) {
+                int degree, int port, int syn, float w, float d, const float *warr, const float *darr) {
   OR_TRY
-  ((Net *)p)->connect_rule(rule, src, src0, ns, tgt, tgt0, nt, degree, port, w, d, warr, darr);
+  ((Net *)p)->connect_rule(rule, src, src0, ns, tgt, tgt0, nt, degree, port, syn, w, d, warr, darr);
   return 0;
   OR_CATCH(-1)
 }
 int orc_connect1(void *p, int src, int tgt, int port, float w, float d) {
   OR_TRY((Net *)p)->connect1(src, tgt, port, w, d); return 0; OR_CATCH(-1)
+}
+
+// Synapse groups (src/syn_model.cu:136-238): 1-based indices, 0 is the static synapse.
+int orc_create_syn_group(void *p, const char *model) {
+  OR_TRY
+  Net *n = (Net *)p;
+  if (n->calibrated) throw std::runtime_error("Nodes cannot be created after calibration");
+  const std::string m = model;
+  SynGroupDef g;
+  if (m == "test_syn_model") { g.type = SYN_TEST; g.par = {0.1f, 0.0f}; }
+  else if (m == "stdp") { g.type = SYN_STDP; g.par = {20.0f, 20.0f, 1.0e-4f, 1.0f, 1.0f, 1.0f, 100.0f}; }
+  else throw std::runtime_error("Unknown synapse model name: " + m);
+  n->syn_groups.push_back(g);
+  return (int)n->syn_groups.size();
+  OR_CATCH(-1)
+}
+static int syn_par_idx(Net *n, int g, const char *name) {
+  if (g < 1 || g > (int)n->syn_groups.size()) throw std::runtime_error("Unrecognized synapse group");
+  const SynGroupDef &d = n->syn_groups[g - 1];
+  const char *const *names = d.type == SYN_STDP ? kStdpPar : kTestPar;
+  for (size_t i = 0; i < d.par.size(); i++)
+    if (std::string(name) == names[i]) return (int)i;
+  throw std::runtime_error(std::string("Unrecognized synapse parameter ") + name);
+}
+int orc_set_syn_param(void *p, int g, const char *name, float v) {
+  OR_TRY Net *n = (Net *)p; n->syn_groups[g - 1].par[syn_par_idx(n, g, name)] = v; return 0; OR_CATCH(-1)
+}
+int orc_get_syn_param(void *p, int g, const char *name, float *v) {
+  OR_TRY Net *n = (Net *)p; *v = n->syn_groups[g - 1].par[syn_par_idx(n, g, name)]; return 0; OR_CATCH(-1)
 }
 
 int orc_connect_arrays(void *p, size_t n, const int *src, const int *tgt, const int *port,
@@ -1484,7 +1611,7 @@ long long orc_n_conn(void *p) {
 }
 // Connections in reference order: source ascending, delay group ascending, insertion order.
 // Columns: source, group index, index in group, target, port, delay (ms), weight.
-int orc_get_conns(void *p, int *src, int *grp, int *idx, int *tgt, int *port, float *delay, float *w) {
+int orc_get_conns(void *p, int *src, int *grp, int *idx, int *tgt, int *port, int *syn, float *delay, float *w) {
   Net *n = (Net *)p;
   long long c = 0;
   for (size_t s = 0; s < n->conn.size(); s++)
@@ -1492,7 +1619,8 @@ int orc_get_conns(void *p, int *src, int *grp, int *idx, int *tgt, int *port, fl
       const auto &dg = n->conn[s][g];
       for (size_t k = 0; k < dg.tg.size(); k++) {
         src[c] = (int)s; grp[c] = (int)g; idx[c] = (int)k; tgt[c] = dg.tg[k].tgt;
-        port[c] = dg.tg[k].port; delay[c] = n->dt * (float)(dg.delay + 1); w[c] = dg.tg[k].w;
+        port[c] = dg.tg[k].port; syn[c] = dg.tg[k].syn; delay[c] = n->dt * (float)(dg.delay + 1);
+        w[c] = dg.tg[k].w;
         c++;
       }
     }

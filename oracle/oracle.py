@@ -61,12 +61,15 @@ def lib():
             "orc_random_normal_clipped": (c_int, [c_void, ctypes.c_size_t, c_float, c_float, c_float,
                                                   c_float, c_float, fp]),
             "orc_connect": (c_int, [c_void, c_int, ip, c_int, c_int, ip, c_int, c_int, c_int, c_int,
-                                    c_float, c_float, fp, fp]),
+                                    c_int, c_float, c_float, fp, fp]),
+            "orc_create_syn_group": (c_int, [c_void, ctypes.c_char_p]),
+            "orc_set_syn_param": (c_int, [c_void, c_int, ctypes.c_char_p, c_float]),
+            "orc_get_syn_param": (c_int, [c_void, c_int, ctypes.c_char_p, fp]),
             "orc_connect1": (c_int, [c_void, c_int, c_int, c_int, c_float, c_float]),
             "orc_n_conn": (ctypes.c_longlong, [c_void]),
             "orc_connect_arrays": (c_int, [c_void, ctypes.c_size_t, ip, ip, ip, fp, fp]),
             "orc_threads": (c_int, []),
-            "orc_get_conns": (c_int, [c_void, ip, ip, ip, ip, ip, fp, fp]),
+            "orc_get_conns": (c_int, [c_void, ip, ip, ip, ip, ip, ip, fp, fp]),
             "orc_record": (c_int, [c_void, c_int, ctypes.c_char_p, c_int]),
             "orc_record_rows": (c_int, [c_void]),
             "orc_record_data": (c_int, [c_void, fp]),
@@ -283,6 +286,11 @@ class Oracle(object):
             self._chk(self.L.orc_set_list(self.h, _iptr(ni), ni.size, name.encode(), 0, _fptr(v), 0))
 
     def SetStatus(self, nodes, params, val=None):
+        if isinstance(nodes, SynGroup):
+            items = {params: val} if val is not None else params
+            for k, v in items.items():
+                self._chk(self.L.orc_set_syn_param(self.h, nodes.i_syn_group, k.encode(), float(v)))
+            return
         if val is not None:
             self._set1(nodes, params, val)
         elif isinstance(params, dict):
@@ -302,6 +310,10 @@ class Oracle(object):
             raise ValueError("Wrong argument in SetStatus")
 
     def GetStatus(self, nodes, var):
+        if isinstance(nodes, SynGroup):
+            out = np.zeros(1, dtype=np.float32)
+            self._chk(self.L.orc_get_syn_param(self.h, nodes.i_syn_group, var.encode(), _fptr(out)))
+            return float(out[0])
         nodes = _nodes(nodes)
         out = np.zeros(1, dtype=np.float32)
         res = []
@@ -325,6 +337,13 @@ class Oracle(object):
                 res.append(float(out[0]))
         return res
 
+    # -- synapse groups (src/syn_model.cu:136-238)
+    def CreateSynGroup(self, model_name, status_dict=None):
+        g = SynGroup(self._chk(self.L.orc_create_syn_group(self.h, model_name.encode())))
+        if status_dict:
+            self.SetStatus(g, status_dict)
+        return g
+
     # -- connections
     def Connect(self, source, target, conn_dict, syn_dict):
         rule = conn_dict["rule"]
@@ -343,13 +362,12 @@ class Oracle(object):
         nt = len(target)
         size = {"one_to_one": ns, "all_to_all": ns * nt, "fixed_total_number": degree,
                 "fixed_indegree": nt * degree, "fixed_outdegree": ns * degree}[rule]
-        port, w, d, warr, darr = 0, 0.0, 0.0, None, None
+        port, syn, w, d, warr, darr = 0, 0, 0.0, 0.0, None, None
         for k, v in syn_dict.items():
             if k == "receptor":
                 port = v
             elif k == "synapse_group":
-                if v != 0:
-                    raise ValueError("synapse groups (plasticity) are not supported")
+                syn = v.i_syn_group if isinstance(v, SynGroup) else int(v)
             elif k == "weight":
                 if isinstance(v, dict):
                     warr = self._dict_to_array(v, size)
@@ -370,7 +388,7 @@ class Oracle(object):
         tarr = np.ascontiguousarray(target, dtype=np.int32) if tgt_list else None
         self._chk(self.L.orc_connect(
             self.h, ir, _iptr(sarr) if src_list else None, 0 if src_list else source.i0, ns,
-            _iptr(tarr) if tgt_list else None, 0 if tgt_list else target.i0, nt, degree, port, w, d,
+            _iptr(tarr) if tgt_list else None, 0 if tgt_list else target.i0, nt, degree, port, syn, w, d,
             _fptr(warr) if warr is not None else None, _fptr(darr) if darr is not None else None))
 
     def ConnectArrays(self, source, target, port, weight, delay):
@@ -388,11 +406,12 @@ class Oracle(object):
     def ConnectionArrays(self):
         """All connections in reference order as a dict of numpy arrays."""
         n = self.L.orc_n_conn(self.h)
-        a = {k: np.zeros(n, dtype=np.int32) for k in ("source", "group", "index", "target", "port")}
+        a = {k: np.zeros(n, dtype=np.int32) for k in ("source", "group", "index", "target", "port", "syn")}
         a["delay"] = np.zeros(n, dtype=np.float32)
         a["weight"] = np.zeros(n, dtype=np.float32)
         self.L.orc_get_conns(self.h, _iptr(a["source"]), _iptr(a["group"]), _iptr(a["index"]),
-                             _iptr(a["target"]), _iptr(a["port"]), _fptr(a["delay"]), _fptr(a["weight"]))
+                             _iptr(a["target"]), _iptr(a["port"]), _iptr(a["syn"]), _fptr(a["delay"]),
+                             _fptr(a["weight"]))
         return a
 
     # -- recording
@@ -531,6 +550,11 @@ def philox(c, k):
     return list(out)
 
 
+class SynGroup(object):
+    def __init__(self, i_syn_group):
+        self.i_syn_group = i_syn_group
+
+
 class ConnectionId(object):
     def __init__(self, i_source, i_group, i_conn):
         self.i_source = i_source
@@ -562,7 +586,7 @@ def _conn_status(self, conn_ids, var_key=None):
     for c in conn_ids:
         i = key[(c.i_source, c.i_group, c.i_conn)]
         d = {"source": int(a["source"][i]), "target": int(a["target"][i]), "port": int(a["port"][i]),
-             "syn": 0, "delay": float(a["delay"][i]), "weight": float(a["weight"][i])}
+             "syn": int(a["syn"][i]), "delay": float(a["delay"][i]), "weight": float(a["weight"][i])}
         if var_key is None:
             res.append(d)
         elif isinstance(var_key, (list, tuple)):

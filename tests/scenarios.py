@@ -181,3 +181,93 @@ def poisson_network(api, n=200, rate=12000.0, t_sim=200.0, seed=3, model="aeif_c
 
 
 from workloads import c4_network  # noqa: E402,F401  (shared with bench.py)
+
+
+def _conn_status(api, ids, key):
+    status = getattr(api, "GetConnStatusList", None)
+    return status(ids, key) if status is not None else api.GetStatus(ids, key)
+
+
+def stdp_expected(w, Dt, tau_plus, tau_minus, lambd, alpha, mu_plus, mu_minus, Wmax):
+    """The weight after one pre/post pair at Dt = t_post - t_pre (ms), as the reference's
+    python/test/test_stdp.py states it (Guetig et al. 2003, step size lambda * Wmax)."""
+    if Dt >= 0:
+        w1 = w + lambd * Wmax * np.exp(-Dt / tau_plus) * (1.0 - w / Wmax) ** mu_plus
+        return min(w1, Wmax)
+    w1 = w - alpha * lambd * Wmax * np.exp(Dt / tau_minus) * (w / Wmax) ** mu_minus
+    return max(w1, 0.0)
+
+
+STDP_PAR = {"tau_plus": 20.0, "tau_minus": 20.0, "lambda": 1.0, "alpha": 1.0, "mu_plus": 1.0,
+            "mu_minus": 1.0, "Wmax": 0.001}
+
+
+def stdp_pair_scenario(api, n=50, dt_step=5.0, par=None, model="aeif_cond_beta_multisynapse"):
+    """python/test/test_stdp.py: n presynaptic/postsynaptic pairs, each neuron driven once by a
+    strong spike_generator input so that it spikes once; the plastic edge pre[i] -> post[i] has
+    a delay making the post spike follow the pre spike's arrival by Dt_i = dt_step*(i-(n-1)/2)
+    ms (negative: depression, positive: potentiation).  Returns (Dt list, simulated weights,
+    expected weights)."""
+    par = dict(STDP_PAR if par is None else par)
+    syn = api.CreateSynGroup("stdp", par)
+    sg = api.Create("spike_generator", n)
+    neuron = api.Create(model, 2 * n)
+    api.SetStatus(neuron, {"t_ref": 1000.0})
+    pre, post = neuron[0:n], neuron[n:2 * n]
+    dts = [dt_step * (i - 0.5 * (n - 1)) for i in range(n)]
+    api.SetStatus(sg, {"spike_times": [50.0], "spike_heights": [1.0]})
+    time_diff, delay0, w_sg = 400.0, 1.0, 17.9
+    w0 = par["Wmax"] / 2
+    api.Connect(sg, pre, {"rule": "one_to_one"}, {"weight": w_sg, "delay": delay0})
+    api.Connect(sg, post, {"rule": "one_to_one"}, {"weight": w_sg, "delay": delay0 + time_diff})
+    for i in range(n):
+        api.Connect([pre[i]], [post[i]], {"rule": "one_to_one"},
+                    {"weight": w0, "delay": time_diff - dts[i], "synapse_group": syn})
+    api.Simulate(1000.0)
+    ids = api.GetConnections(pre, post)
+    w = np.asarray(_conn_status(api, ids, "weight"), dtype=np.float64)
+    exp = [stdp_expected(w0, d, par["tau_plus"], par["tau_minus"], par["lambda"], par["alpha"],
+                         par["mu_plus"], par["mu_minus"], par["Wmax"]) for d in dts]
+    return dts, w, np.asarray(exp)
+
+
+def plastic_network(api, n=80, n_in=20, seed=11, t_sim=400.0, model="aeif_cond_beta_multisynapse"):
+    """A recurrent network with plastic excitatory edges (STDP group) and static inhibitory
+    ones, driven by fixed spike_generator trains (no Poisson): spike counts and the final
+    plastic weights are deterministic.  Returns (spike counts, plastic weights in connection
+    order)."""
+    rng = np.random.RandomState(seed)
+    api.SetKernelStatus("rnd_seed", 2000 + seed)
+    syn = api.CreateSynGroup("stdp", {"tau_plus": 20.0, "tau_minus": 25.0, "lambda": 0.05,
+                                      "alpha": 1.1, "mu_plus": 0.5, "mu_minus": 0.8, "Wmax": 6.0})
+    if model == "iaf_psc_exp":
+        neuron = api.Create("iaf_psc_exp", n)
+        api.SetStatus(neuron, {"I_e": 370.0})
+        w_exc, w_inh, w_in = 35.0, -60.0, 90.0
+        syn = api.CreateSynGroup("stdp", {"tau_plus": 20.0, "tau_minus": 25.0, "lambda": 0.05,
+                                          "alpha": 1.1, "mu_plus": 0.5, "mu_minus": 0.8, "Wmax": 80.0})
+    else:
+        neuron = api.Create(model, n, 2)
+        api.SetStatus(neuron, {"E_rev": [0.0, -85.0], "I_e": 500.0})
+        w_exc, w_inh, w_in = 3.0, 4.0, 6.0
+    n_exc = int(0.8 * n)
+    exc, inh = neuron[0:n_exc], neuron[n_exc:n]
+    gens = api.Create("spike_generator", n_in)
+    for i in range(n_in):
+        t = np.cumsum(rng.exponential(6.0, size=96)) + 1.0
+        t = np.unique(np.round(t[t < t_sim - 1.0], 1))
+        api.SetStatus([gens[i]], {"spike_times": [float(x) for x in t]})
+    api.Connect(exc, neuron, {"rule": "fixed_indegree", "indegree": 10},
+                {"weight": w_exc, "receptor": 0, "synapse_group": syn,
+                 "delay": {"distribution": "normal_clipped", "mu": 1.5, "low": 0.5, "high": 3.0,
+                           "sigma": 0.6}})
+    api.Connect(inh, neuron, {"rule": "fixed_total_number", "total_num": 4 * n},
+                {"weight": w_inh, "receptor": 1, "delay": 0.8})
+    api.Connect(gens, neuron, {"rule": "fixed_indegree", "indegree": 3},
+                {"weight": w_in, "receptor": 0, "delay": 1.0})
+    api.ActivateSpikeCount(neuron)
+    api.Simulate(t_sim)
+    counts = np.asarray(api.GetStatus(neuron, "spike_count")).ravel()
+    ids = api.GetConnections(exc, neuron)
+    w = np.asarray(_conn_status(api, ids, "weight"), dtype=np.float32)
+    return counts, w

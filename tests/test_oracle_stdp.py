@@ -1,0 +1,42 @@
+"""The oracle's synapse groups and STDP pinned against the reference's known-answer test
+(python/test/test_stdp.py: one pre/post pair per time difference, weights against the
+closed-form Guetig rule within the reference's 1e-5).  CPU only."""
+import numpy as np
+import pytest
+
+import oracle as orc
+from scenarios import STDP_PAR, plastic_network, stdp_pair_scenario
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_stdp_pairs_match_closed_form(fp64):
+    dts, w, exp = stdp_pair_scenario(orc.Oracle(fp64=fp64))
+    assert np.max(np.abs(w - exp)) < 1e-5
+    # both branches are exercised and the weights moved
+    assert np.sum(np.asarray(dts) < 0) > 10 and np.sum(np.asarray(dts) > 0) > 10
+    w0 = STDP_PAR["Wmax"] / 2
+    assert np.all(w[np.asarray(dts) < 0] < w0) and np.all(w[np.asarray(dts) > 0] > w0)
+
+
+def test_stdp_weight_dependence_exponents():
+    par = dict(STDP_PAR, mu_plus=0.4, mu_minus=1.7, alpha=0.6, tau_minus=35.0)
+    _, w, exp = stdp_pair_scenario(orc.Oracle(), par=par)
+    assert np.max(np.abs(w - exp)) < 1e-5
+
+
+def test_synapse_group_parameters():
+    o = orc.Oracle()
+    g = o.CreateSynGroup("stdp")
+    assert abs(o.GetStatus(g, "Wmax") - 100.0) < 1e-6 and abs(o.GetStatus(g, "lambda") - 1e-4) < 1e-10
+    o.SetStatus(g, {"Wmax": 3.0})
+    assert o.GetStatus(g, "Wmax") == 3.0
+    with pytest.raises(ValueError):
+        o.CreateSynGroup("no_such_model")
+    with pytest.raises(ValueError):
+        o.GetStatus(g, "no_such_param")
+
+
+def test_plastic_network_moves_weights():
+    counts, w = plastic_network(orc.Oracle())
+    assert counts.sum() > 50
+    assert np.std(w) > 0.05 and np.all(w >= 0.0) and np.all(w <= 6.0)
