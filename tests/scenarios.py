@@ -238,18 +238,18 @@ def plastic_network(api, n=80, n_in=20, seed=11, t_sim=400.0, model="aeif_cond_b
     order)."""
     rng = np.random.RandomState(seed)
     api.SetKernelStatus("rnd_seed", 2000 + seed)
-    syn = api.CreateSynGroup("stdp", {"tau_plus": 20.0, "tau_minus": 25.0, "lambda": 0.05,
-                                      "alpha": 1.1, "mu_plus": 0.5, "mu_minus": 0.8, "Wmax": 6.0})
+    stdp = {"tau_plus": 20.0, "tau_minus": 25.0, "lambda": 0.05, "alpha": 1.1, "mu_plus": 0.5,
+            "mu_minus": 0.8}
     if model == "iaf_psc_exp":
+        syn = api.CreateSynGroup("stdp", dict(stdp, Wmax=80.0))
         neuron = api.Create("iaf_psc_exp", n)
         api.SetStatus(neuron, {"I_e": 370.0})
         w_exc, w_inh, w_in = 35.0, -60.0, 90.0
-        syn = api.CreateSynGroup("stdp", {"tau_plus": 20.0, "tau_minus": 25.0, "lambda": 0.05,
-                                          "alpha": 1.1, "mu_plus": 0.5, "mu_minus": 0.8, "Wmax": 80.0})
     else:
+        syn = api.CreateSynGroup("stdp", dict(stdp, Wmax=3.0))
         neuron = api.Create(model, n, 2)
-        api.SetStatus(neuron, {"E_rev": [0.0, -85.0], "I_e": 500.0})
-        w_exc, w_inh, w_in = 3.0, 4.0, 6.0
+        api.SetStatus(neuron, {"E_rev": [0.0, -85.0], "t_ref": 2.0})
+        w_exc, w_inh, w_in = 1.5, 8.0, 2.0
     n_exc = int(0.8 * n)
     exc, inh = neuron[0:n_exc], neuron[n_exc:n]
     gens = api.Create("spike_generator", n_in)

@@ -36,7 +36,8 @@ def test_synapse_group_parameters():
         o.GetStatus(g, "no_such_param")
 
 
-def test_plastic_network_moves_weights():
-    counts, w = plastic_network(orc.Oracle())
-    assert counts.sum() > 50
-    assert np.std(w) > 0.05 and np.all(w >= 0.0) and np.all(w <= 6.0)
+@pytest.mark.parametrize("model,wmax", [("aeif_cond_beta_multisynapse", 3.0), ("iaf_psc_exp", 80.0)])
+def test_plastic_network_moves_weights(model, wmax):
+    counts, w = plastic_network(orc.Oracle(), model=model)
+    assert 5.0 < counts.sum() / counts.size / 0.4 < 200.0
+    assert np.std(w) > 0.05 * wmax / 3 and np.all(w >= 0.0) and np.all(w <= wmax)
