@@ -162,7 +162,10 @@ int NESTGPU_GetConnectionStatus(int i_source, int i_group, int i_conn, int *i_ta
                                 unsigned char *port, unsigned char *syn_group, float *delay,
                                 float *weight);
 
-/* synapse groups (plasticity; not supported, error 2): src/nestgpu_C.h:275-287 */
+/* synapse groups: src/nestgpu_C.h:275-287.  Models "stdp" (tau_plus, tau_minus, lambda, alpha,
+   mu_plus, mu_minus, Wmax; src/stdp.h:70-94) and "test_syn_model" (fact, offset); indices are
+   1-based, 0 being the static synapse.  A network with plastic connections advances one time
+   step per kernel batch (the weight changes of a step see that step's spikes). */
 int NESTGPU_CreateSynGroup(char *model_name);
 int NESTGPU_GetSynGroupNParam(int i_syn_group);
 char **NESTGPU_GetSynGroupParamNames(int i_syn_group);

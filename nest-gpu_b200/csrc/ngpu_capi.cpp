@@ -2,6 +2,7 @@
 // Error convention of the reference (src/propagate_error.h:4-30): clear the error
 // state, run, map an engine error to code 2, bad_alloc to 1, anything else to 255;
 // exit with that code unless SetOnException(1) asked to return to the caller.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -430,32 +431,33 @@ char **NESTGPU_GetArrayVarNames(int i_node) {
 int NESTGPU_GetNArrayVar(int i_node) { return guard([&] { E().group_of(i_node); return 0; }, 0); }
 
 // ---- connection queries (n <= 0 for a sequence means every node)
-static int *conn_ids(const int *src, int s0, int ns, const int *tgt, int t0, int nt, int *n_conn) {
+static int *conn_ids(const int *src, int s0, int ns, const int *tgt, int t0, int nt, int syn_group,
+                     int *n_conn) {
   const int N = E().n_nodes();
   if (!src && ns <= 0) { s0 = 0; ns = N; }
   if (!tgt && nt <= 0) { t0 = 0; nt = N; }
-  std::vector<int> ids = E().get_connections(src, s0, ns, tgt, t0, nt);
+  std::vector<int> ids = E().get_connections(src, s0, ns, tgt, t0, nt, syn_group);
   *n_conn = (int)(ids.size() / 3);
   return malloc_copy(ids);
 }
-int *NESTGPU_GetSeqSeqConnections(int i_source, int n_source, int i_target, int n_target, int,
+int *NESTGPU_GetSeqSeqConnections(int i_source, int n_source, int i_target, int n_target, int syn_group,
                                   int *n_conn) {
-  return guard([&] { return conn_ids(nullptr, i_source, n_source, nullptr, i_target, n_target, n_conn); },
+  return guard([&] { return conn_ids(nullptr, i_source, n_source, nullptr, i_target, n_target, syn_group, n_conn); },
                (int *)nullptr);
 }
-int *NESTGPU_GetSeqGroupConnections(int i_source, int n_source, int *i_target, int n_target, int,
+int *NESTGPU_GetSeqGroupConnections(int i_source, int n_source, int *i_target, int n_target, int syn_group,
                                     int *n_conn) {
-  return guard([&] { return conn_ids(nullptr, i_source, n_source, i_target, 0, n_target, n_conn); },
+  return guard([&] { return conn_ids(nullptr, i_source, n_source, i_target, 0, n_target, syn_group, n_conn); },
                (int *)nullptr);
 }
-int *NESTGPU_GetGroupSeqConnections(int *i_source, int n_source, int i_target, int n_target, int,
+int *NESTGPU_GetGroupSeqConnections(int *i_source, int n_source, int i_target, int n_target, int syn_group,
                                     int *n_conn) {
-  return guard([&] { return conn_ids(i_source, 0, n_source, nullptr, i_target, n_target, n_conn); },
+  return guard([&] { return conn_ids(i_source, 0, n_source, nullptr, i_target, n_target, syn_group, n_conn); },
                (int *)nullptr);
 }
-int *NESTGPU_GetGroupGroupConnections(int *i_source, int n_source, int *i_target, int n_target, int,
+int *NESTGPU_GetGroupGroupConnections(int *i_source, int n_source, int *i_target, int n_target, int syn_group,
                                       int *n_conn) {
-  return guard([&] { return conn_ids(i_source, 0, n_source, i_target, 0, n_target, n_conn); },
+  return guard([&] { return conn_ids(i_source, 0, n_source, i_target, 0, n_target, syn_group, n_conn); },
                (int *)nullptr);
 }
 int NESTGPU_GetConnectionStatus(int i_source, int i_group, int i_conn, int *i_target,
@@ -467,17 +469,31 @@ int NESTGPU_GetConnectionStatus(int i_source, int i_group, int i_conn, int *i_ta
   }, 0);
 }
 
-// ---- synapse groups: plasticity is outside this engine
-static int no_syn() {
-  return guard([&]() -> int { throw NgpuError("synapse groups (plasticity) are not supported by this engine"); }, 0);
+// ---- synapse groups (src/nestgpu_C.cpp:874-960, src/syn_model.cu:136-238)
+int NESTGPU_CreateSynGroup(char *model_name) {
+  return guard([&] { return E().create_syn_group(model_name); }, 0);
 }
-int NESTGPU_CreateSynGroup(char *) { return no_syn(); }
-int NESTGPU_GetSynGroupNParam(int) { return no_syn(); }
-char **NESTGPU_GetSynGroupParamNames(int) { no_syn(); return nullptr; }
-int NESTGPU_IsSynGroupParam(int, char *) { return no_syn(); }
-int NESTGPU_GetSynGroupParamIdx(int, char *) { return no_syn(); }
-float NESTGPU_GetSynGroupParam(int, char *) { no_syn(); return 0.0f; }
-int NESTGPU_SetSynGroupParam(int, char *, float) { return no_syn(); }
+int NESTGPU_GetSynGroupNParam(int g) {
+  return guard([&] { return (int)E().syn_group_param_names(g).size(); }, 0);
+}
+char **NESTGPU_GetSynGroupParamNames(int g) {
+  return guard([&] { return name_list(E().syn_group_param_names(g)); }, (char **)nullptr);
+}
+int NESTGPU_IsSynGroupParam(int g, char *name) {
+  return guard([&] {
+    const std::vector<std::string> names = E().syn_group_param_names(g);
+    return std::find(names.begin(), names.end(), std::string(name)) != names.end() ? 1 : 0;
+  }, 0);
+}
+int NESTGPU_GetSynGroupParamIdx(int g, char *name) {
+  return guard([&] { return E().syn_group_param_idx(g, name); }, 0);
+}
+float NESTGPU_GetSynGroupParam(int g, char *name) {
+  return guard([&] { return E().get_syn_group_param(g, name); }, 0.0f);
+}
+int NESTGPU_SetSynGroupParam(int g, char *name, float val) {
+  return guard([&] { E().set_syn_group_param(g, name, val); return 0; }, 0);
+}
 
 // ---- spike counting and recording
 int NESTGPU_ActivateSpikeCount(int i_node, int n) {

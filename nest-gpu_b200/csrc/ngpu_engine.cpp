@@ -499,14 +499,65 @@ float Engine::get_group_param(int node, const std::string &name) {
 }
 
 // ---------------------------------------------------------------------------
+// Synapse groups (src/syn_model.cu:136-238, src/stdp.cu:66-80, src/test_syn_model.cu:42-50)
+// ---------------------------------------------------------------------------
+static const char *const kStdpParNames[] = {"tau_plus", "tau_minus", "lambda", "alpha", "mu_plus", "mu_minus",
+                                            "Wmax"};
+static const char *const kTestParNames[] = {"fact", "offset"};
+
+int Engine::create_syn_group(const std::string &model) {
+  if (calibrated_) throw NgpuError("Nodes cannot be created after calibration");
+  SynGroupDef g;
+  if (model == "test_syn_model") {
+    g.type = SYN_TEST;
+    g.par = {0.1f, 0.0f};
+  } else if (model == "stdp") {
+    g.type = SYN_STDP;
+    g.par = {20.0f, 20.0f, 1.0e-4f, 1.0f, 1.0f, 1.0f, 100.0f};
+  } else {
+    throw NgpuError("Unknown synapse model name: " + model);
+  }
+  if (syn_groups_.size() >= 255) throw NgpuError("too many synapse groups");
+  syn_groups_.push_back(g);
+  return (int)syn_groups_.size();
+}
+
+std::vector<std::string> Engine::syn_group_param_names(int g) const {
+  if (g < 1 || g > (int)syn_groups_.size()) throw NgpuError("Unrecognized synapse group");
+  const SynGroupDef &d = syn_groups_[g - 1];
+  const char *const *names = d.type == SYN_STDP ? kStdpParNames : kTestParNames;
+  return std::vector<std::string>(names, names + d.par.size());
+}
+
+int Engine::syn_group_param_idx(int g, const std::string &name) const {
+  const std::vector<std::string> names = syn_group_param_names(g);
+  for (size_t i = 0; i < names.size(); i++)
+    if (names[i] == name) return (int)i;
+  throw NgpuError("Unrecognized parameter " + name);
+}
+
+float Engine::get_syn_group_param(int g, const std::string &name) const {
+  return syn_groups_[g - 1].par[syn_group_param_idx(g, name)];
+}
+
+void Engine::set_syn_group_param(int g, const std::string &name, float v) {
+  syn_groups_[g - 1].par[syn_group_param_idx(g, name)] = v;
+  if (calibrated_ && plastic_) upload_syn_groups();
+}
+
+// ---------------------------------------------------------------------------
 // Connections (src/connect.cu:38-74, src/connect_rules.h:161-338)
 // ---------------------------------------------------------------------------
 void Engine::connect1(int src, int tgt, int port, int syn_group, float w, float d) {
   if (calibrated_) throw NgpuError("Connections cannot be created after calibration");
   if (d < dt) throw NgpuError("Delay must be >= time resolution");
-  if (syn_group != 0) throw NgpuError("synapse groups (plasticity) are not supported by this engine");
+  if (syn_group < 0 || syn_group > (int)syn_groups_.size()) throw NgpuError("Unrecognized synapse group");
   if (port < 0 || port > 255) throw NgpuError("Port index must be >=0");
   if (src < 0 || src >= n_nodes() || tgt < 0 || tgt >= n_nodes()) throw NgpuError("Unrecognized node in connection");
+  if (syn_group != 0 || !c_syn_.empty()) {   // the group store exists once a plastic edge does
+    c_syn_.resize(c_src_.size(), 0);
+    c_syn_.push_back((unsigned char)syn_group);
+  }
   c_src_.push_back(src);
   c_tgt_.push_back(tgt);
   c_port_.push_back((unsigned char)port);
@@ -616,6 +667,7 @@ void Engine::connect_arrays(size_t n, const int *src, const int *tgt, const unsi
   c_port_.resize(base + n);
   c_w_.resize(base + n);
   c_d_.resize(base + n);
+  if (!c_syn_.empty()) c_syn_.resize(base + n, 0);
   const int N = n_nodes();
   for (size_t i = 0; i < n; i++) {
     if (src[i] < 0 || src[i] >= N || tgt[i] < 0 || tgt[i] >= N) throw NgpuError("Unrecognized node in connection");
@@ -660,7 +712,7 @@ void Engine::build_order() {
 }
 
 std::vector<int> Engine::get_connections(const int *src_arr, int src0, int ns, const int *tgt_arr,
-                                         int tgt0, int nt) {
+                                         int tgt0, int nt, int syn_group) {
   build_order();
   std::vector<int> tsorted;
   if (tgt_arr) {
@@ -679,7 +731,7 @@ std::vector<int> Engine::get_connections(const int *src_arr, int src0, int ns, c
     int s = ns < 0 ? is : (src_arr ? src_arr[is] : src0 + is);
     if (s < 0 || s >= N) throw NgpuError("Unrecognized source node");
     for (long long p = src_first_[s]; p < src_first_[s + 1]; p++) {
-      if (want_t(c_tgt_[ord_[p]])) {
+      if (want_t(c_tgt_[ord_[p]]) && (syn_group < 0 || syn_of(ord_[p]) == syn_group)) {
         out.push_back(s);
         out.push_back(ord_grp_[p]);
         out.push_back(ord_idx_[p]);
@@ -698,9 +750,10 @@ void Engine::connection_status(int src, int grp, int idx, int *tgt, unsigned cha
       long long e = ord_[p];
       *tgt = c_tgt_[e];
       *port = c_port_[e];
-      *syn = 0;
+      *syn = syn_of(e);
       *delay = dt * (float)(c_d_[e] + 1);
       *w = c_w_[e];
+      if (*syn && calibrated_) *w = plastic_weight((size_t)e, *w);   // it lives on the device
       return;
     }
   }

@@ -161,15 +161,22 @@ class Engine {
   std::vector<float> random_normal_clipped(size_t n, float mean, float sd, float vmin, float vmax,
                                            float vstep);
 
+  // ---- synapse groups (src/syn_model.cu:136-238): 1-based, 0 is the static synapse
+  int create_syn_group(const std::string &model);
+  std::vector<std::string> syn_group_param_names(int g) const;
+  int syn_group_param_idx(int g, const std::string &name) const;
+  float get_syn_group_param(int g, const std::string &name) const;
+  void set_syn_group_param(int g, const std::string &name, float v);
+
   // ---- connections
   void connect1(int src, int tgt, int port, int syn_group, float w, float d);
   void connect_rule(int rule, const int *src_arr, int src0, int ns, const int *tgt_arr, int tgt0,
                     int nt, int degree, int port, int syn_group, float w, float d,
                     const float *warr, const float *darr);
   size_t n_connections() const { return c_src_.size() + n_generated_; }
-  // ids (source, group, index) in reference order, filtered
+  // ids (source, group, index) in reference order, filtered (syn_group < 0: any group)
   std::vector<int> get_connections(const int *src_arr, int src0, int ns, const int *tgt_arr,
-                                   int tgt0, int nt);
+                                   int tgt0, int nt, int syn_group = -1);
   void connection_status(int src, int grp, int idx, int *tgt, unsigned char *port,
                          unsigned char *syn, float *delay, float *w);
   // Bulk import of a prebuilt edge list (engine extension, used by the large benchmarks).
@@ -240,6 +247,13 @@ class Engine {
   std::vector<unsigned char> c_port_;
   std::vector<float> c_w_;
   std::vector<int> c_d_;
+  std::vector<unsigned char> c_syn_;   // synapse group per edge; empty while all are static
+  unsigned char syn_of(size_t e) const { return c_syn_.empty() ? 0 : c_syn_[e]; }
+  struct SynGroupDef {
+    int type;                 // SynType
+    std::vector<float> par;
+  };
+  std::vector<SynGroupDef> syn_groups_;
   // generated blocks (connect_fixed_indegree_per_target)
   struct GenBlock {
     int src0, nsrc, tgt0, ntgt, k, port;
@@ -271,6 +285,15 @@ class Engine {
   // device
   cudaStream_t stream_ = nullptr;
   cudaStream_t stream2_ = nullptr;      // second stream for non-aeif groups (fork / join per batch)
+  // plastic edges (synapse groups): forward index by (source, delay), reverse by target
+  bool plastic_ = false;
+  StdpArgs stdp_{};
+  std::vector<unsigned long long> pl_pos_;               // per plastic entry: CSR position
+  std::vector<std::pair<size_t, int>> pl_of_edge_;       // (host edge, plastic entry), sorted
+  void build_plastic(const std::vector<size_t> &pl_edge, const std::vector<long long> &pl_key,
+                     const std::vector<int> &pl_rank);
+  void upload_syn_groups();
+  float plastic_weight(size_t e, float fallback);
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   Clock *d_clk_ = nullptr;
   double *d_acc_ = nullptr;
@@ -359,6 +382,10 @@ int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk
 int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *clk, int k0, int M,
                    cudaStream_t st);
 int launch_clock_advance(Clock *clk, int K, cudaStream_t st);
+// STDP (ngpu_stdp.cu)
+int launch_stdp_reset(const StdpArgs &A, const Clock *clk, int k0, cudaStream_t st);
+int launch_stdp_forward(const StdpArgs &A, const Clock *clk, int k0, cudaStream_t st);
+int launch_stdp_reverse(const StdpArgs &A, const Clock *clk, int k0, cudaStream_t st);
 int launch_persistent_iaf(const DeliverArgs &D, int group, const IafArgs *tab, const int *first, int ngroups,
                           const SpikeOut &so, const Clock *clk, int steps, int M, GridBarrier *bar, int max_blocks,
                           int barrier_extra, cudaStream_t st);

@@ -70,6 +70,10 @@ void Engine::free_device() {
   if (ev_fork_) cudaEventDestroy(ev_fork_);
   if (ev_join_) cudaEventDestroy(ev_join_);
   ev_fork_ = ev_join_ = nullptr;
+  plastic_ = false;
+  stdp_ = StdpArgs{};
+  pl_pos_.clear();
+  pl_of_edge_.clear();
 }
 
 void Engine::invalidate_graphs() {
@@ -173,8 +177,12 @@ void Engine::calibrate() {
     if (c_port_[e] >= tg.nport)
       throw NgpuError("receptor port " + std::to_string(c_port_[e]) + " out of range for target node " +
                       std::to_string(c_tgt_[e]));
-    if (is_pg[c_src_[e]]) continue;
+    if (is_pg[c_src_[e]]) {
+      if (syn_of(e)) throw NgpuError("poiss_gen connections cannot be plastic");
+      continue;
+    }
     n_rec_edges++;
+    if (syn_of(e)) plastic_ = true;
     dmin = std::min(dmin, c_d_[e]);
     dmax = std::max(dmax, c_d_[e]);
   }
@@ -205,6 +213,9 @@ void Engine::calibrate() {
   if (dspan_ > deliver_max_pairs())
     throw NgpuError("delay range exceeds " + std::to_string(deliver_max_pairs()) + " time steps");
   d_has_out_ = dalloc<unsigned char>(N);
+  std::vector<size_t> pl_edge;       // plastic host edges with their (source, delay) key and rank
+  std::vector<long long> pl_key;
+  std::vector<int> pl_rank;
   {
     // host edges: per-key counts and each edge's rank inside its (source, delay) segment,
     // in insertion order; the device does the scan, placement and generated blocks
@@ -213,6 +224,9 @@ void Engine::calibrate() {
     std::vector<long long> hkey;
     std::vector<int> hrank;
     std::vector<EdgeW> hew;
+    pl_edge.clear();
+    pl_key.clear();
+    pl_rank.clear();
     if (n_rec_edges) {
       cnt.assign(nkey, 0);
       hkey.reserve(n_rec_edges);
@@ -222,6 +236,11 @@ void Engine::calibrate() {
         if (is_pg[c_src_[e]]) continue;
         const Group &tg = groups_[node_group_[c_tgt_[e]]];
         long long key = (long long)c_src_[e] * dspan_ + (c_d_[e] - dmin);
+        if (syn_of(e)) {
+          pl_edge.push_back(e);
+          pl_key.push_back(key);
+          pl_rank.push_back(cnt[key]);
+        }
         hkey.push_back(key);
         hrank.push_back(cnt[key]++);
         EdgeW x;
@@ -298,6 +317,9 @@ void Engine::calibrate() {
   //      a batch arrive after it); one accumulator slot per step of a batch
   batch_ = (n_rec_edges || !gblocks.empty()) ? std::min(dmin_ + 1, MAX_BATCH) : MAX_BATCH;
   batch_ = std::max(1, std::min(batch_, batch_max));
+  // plastic edges: one step per batch, so that each step's weight changes see the post-
+  // synaptic spikes of the same step (src/nestgpu.cu:469-635 order)
+  if (plastic_) batch_ = 1;
   if (dspan_ * batch_ > deliver_max_pairs()) batch_ = std::max(1, deliver_max_pairs() / dspan_);
   d_acc_ = dalloc<double>(n_acc_ * batch_);
   cuda_check(cudaMemset(d_acc_, 0, std::max<size_t>(n_acc_ * batch_, 1) * sizeof(double)), "memset");
@@ -319,6 +341,7 @@ void Engine::calibrate() {
   d_clk_ = dalloc<Clock>(1);
   cuda_check(cudaMemset(d_clk_, 0, sizeof(Clock)), "clock");
   deliver_blocks_ = std::max(1, std::min(148 * 8, (n_src_out + 63) / 64));
+  if (plastic_) build_plastic(pl_edge, pl_key, pl_rank);
 
   // ---- per-group device state
   for (auto &g : groups_) {
@@ -680,12 +703,128 @@ DeliverArgs Engine::deliver_args() {
 }
 
 // ---------------------------------------------------------------------------
+// Plastic edges: forward index over the delivery CSR's (source, delay) segments, reverse
+// index by target (src/spike_buffer.cu:430-520), 16-bit arrival stamps starting at 0x8000
+// (src/rev_spike.cu:150-155), synapse-group parameter table (src/syn_model.cu:170-238).
+// ---------------------------------------------------------------------------
+// Current weight of plastic host edge e (its device copy).
+float Engine::plastic_weight(size_t e, float fallback) {
+  auto it = std::lower_bound(pl_of_edge_.begin(), pl_of_edge_.end(), std::make_pair(e, INT32_MIN));
+  if (it == pl_of_edge_.end() || it->first != e) return fallback;
+  cuda_check(cudaStreamSynchronize(stream_), "sync");
+  EdgeW x;
+  cuda_check(cudaMemcpy(&x, d_edge_ + pl_pos_[it->second], sizeof(EdgeW), cudaMemcpyDeviceToHost),
+             "plastic weight");
+  return x.w;
+}
+
+void Engine::upload_syn_groups() {
+  const int ng = (int)syn_groups_.size();
+  std::vector<int> type(ng);
+  std::vector<float> par((size_t)ng * SYN_NPAR, 0.0f);
+  for (int g = 0; g < ng; g++) {
+    type[g] = syn_groups_[g].type;
+    for (size_t k = 0; k < syn_groups_[g].par.size(); k++) par[(size_t)g * SYN_NPAR + k] = syn_groups_[g].par[k];
+  }
+  cuda_check(cudaStreamSynchronize(stream_), "sync");
+  cuda_check(cudaMemcpy((void *)stdp_.syn_type, type.data(), ng * sizeof(int), cudaMemcpyHostToDevice), "syn groups");
+  cuda_check(cudaMemcpy((void *)stdp_.syn_par, par.data(), par.size() * sizeof(float), cudaMemcpyHostToDevice),
+             "syn groups");
+}
+
+void Engine::build_plastic(const std::vector<size_t> &pl_edge, const std::vector<long long> &pl_key,
+                           const std::vector<int> &pl_rank) {
+  const int N = n_nodes();
+  const size_t nkey = (size_t)N * dspan_;
+  const size_t P = pl_edge.size();
+  if (P >= (size_t)INT32_MAX) throw NgpuError("too many plastic connections");
+  // a host edge sits at its segment's start plus its rank in the segment
+  std::vector<unsigned long long> off(nkey + 1);
+  cuda_check(cudaMemcpy(off.data(), d_ev_off_, (nkey + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+             "segment offsets");
+  std::vector<size_t> ord(P);
+  std::iota(ord.begin(), ord.end(), (size_t)0);
+  std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) {
+    return pl_key[a] != pl_key[b] ? pl_key[a] < pl_key[b] : pl_rank[a] < pl_rank[b];
+  });
+  std::vector<int> pl_off(nkey + 1, 0);
+  std::vector<PlasticEdge> pl(P);
+  pl_pos_.assign(P, 0);
+  pl_of_edge_.resize(P);
+  std::vector<int> cnt_t(N, 0);
+  for (size_t q = 0; q < P; q++) {
+    const size_t i = ord[q];
+    pl_off[pl_key[i] + 1]++;
+    PlasticEdge x;
+    x.pos = off[pl_key[i]] + (unsigned long long)pl_rank[i];
+    x.target = c_tgt_[pl_edge[i]];
+    x.group = c_syn_[pl_edge[i]];
+    pl[q] = x;
+    pl_pos_[q] = x.pos;
+    pl_of_edge_[q] = {pl_edge[i], (int)q};
+    cnt_t[x.target]++;
+  }
+  for (size_t k = 0; k < nkey; k++) pl_off[k + 1] += pl_off[k];
+  std::sort(pl_of_edge_.begin(), pl_of_edge_.end());
+  // reverse index: targets with plastic in-edges, their entries in forward order
+  std::vector<int> rev_node, rev_off{0}, first(N, -1);
+  for (int t = 0; t < N; t++)
+    if (cnt_t[t]) {
+      first[t] = rev_off.back();
+      rev_node.push_back(t);
+      rev_off.push_back(rev_off.back() + cnt_t[t]);
+    }
+  std::vector<int> rev_id(P);
+  for (size_t q = 0; q < P; q++) rev_id[first[pl[q].target]++] = (int)q;
+  std::vector<unsigned short> stamp(P, 0x8000);
+
+  StdpArgs &A = stdp_;
+  int *d_pl_off = dalloc<int>(nkey + 1);
+  PlasticEdge *d_pl = dalloc<PlasticEdge>(P);
+  unsigned short *d_stamp = dalloc<unsigned short>(P);
+  int *d_rev_off = dalloc<int>(rev_off.size());
+  int *d_rev_id = dalloc<int>(P);
+  int *d_rev_node = dalloc<int>(std::max<size_t>(rev_node.size(), 1));
+  int *d_type = dalloc<int>(syn_groups_.size());
+  float *d_par = dalloc<float>(syn_groups_.size() * SYN_NPAR);
+  cuda_check(cudaMemcpy(d_pl_off, pl_off.data(), pl_off.size() * sizeof(int), cudaMemcpyHostToDevice), "stdp");
+  cuda_check(cudaMemcpy(d_pl, pl.data(), P * sizeof(PlasticEdge), cudaMemcpyHostToDevice), "stdp");
+  cuda_check(cudaMemcpy(d_stamp, stamp.data(), P * sizeof(unsigned short), cudaMemcpyHostToDevice), "stdp");
+  cuda_check(cudaMemcpy(d_rev_off, rev_off.data(), rev_off.size() * sizeof(int), cudaMemcpyHostToDevice), "stdp");
+  cuda_check(cudaMemcpy(d_rev_id, rev_id.data(), P * sizeof(int), cudaMemcpyHostToDevice), "stdp");
+  if (!rev_node.empty())
+    cuda_check(cudaMemcpy(d_rev_node, rev_node.data(), rev_node.size() * sizeof(int), cudaMemcpyHostToDevice),
+               "stdp");
+  A.ring = d_ring_;
+  A.ring_cnt = d_ring_cnt_;
+  A.R = R_;
+  A.cap = cap_;
+  A.dmin = dmin_;
+  A.dspan = dspan_;
+  A.pl_off = d_pl_off;
+  A.pl = d_pl;
+  A.stamp = d_stamp;
+  A.n_pl = (long long)P;
+  A.edge = d_edge_;
+  A.last_tidx = d_last_tidx_;
+  A.syn_type = d_type;
+  A.syn_par = d_par;
+  A.rev_off = d_rev_off;
+  A.rev_id = d_rev_id;
+  A.rev_node = d_rev_node;
+  A.n_rev_nodes = (int)rev_node.size();
+  A.dt = dt;
+  upload_syn_groups();
+}
+
+// ---------------------------------------------------------------------------
 // Step loop
 // ---------------------------------------------------------------------------
 // One batch of M steps starting at graph step k0: delivery, then every group.
 void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   SpikeOut so = spike_out();
   if (ev) cuda_check(cudaEventRecord((*ev)[0], stream_), "event");
+  if (plastic_) count_launch(launch_stdp_reset(stdp_, d_clk_, k0, stream_));
   count_launch(launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_,
                               deliver_group, d_clk_, k0, M, stream_));
   if (ev) cuda_check(cudaEventRecord((*ev)[1], stream_), "event");
@@ -718,6 +857,11 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   if (fork) {
     cuda_check(cudaEventRecord(ev_join_, stream2_), "join");
     cuda_check(cudaStreamWaitEvent(stream_, ev_join_, 0), "join");
+  }
+  // plastic edges (one step per batch): the step's arrivals, then its post-synaptic spikes
+  if (plastic_) {
+    count_launch(launch_stdp_forward(stdp_, d_clk_, k0, stream_));
+    count_launch(launch_stdp_reverse(stdp_, d_clk_, k0, stream_));
   }
   if (ev) cuda_check(cudaEventRecord((*ev)[2], stream_), "event");
 }
@@ -754,6 +898,7 @@ void Engine::prepare_multi() {
 // The persistent step loop serves networks whose only neurons are iaf_psc_exp groups
 // (Poisson generators have no kernel of their own).
 bool Engine::persistent_eligible() const {
+  if (plastic_) return false;
   bool any = false;
   for (auto &g : groups_) {
     if (g.n <= 0 || g.model == M_POISS_GEN) continue;

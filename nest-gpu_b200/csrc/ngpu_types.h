@@ -200,6 +200,40 @@ struct DeliverArgs {
   int n_strag;
 };
 
+// Plastic edge (synapse group > 0): its position in the delivery CSR, its target node and
+// its synapse group (1-based).  Forward order: by (source, delay) segment, insertion order
+// inside a segment.
+struct PlasticEdge {
+  unsigned long long pos;
+  int target;
+  int group;
+};
+
+constexpr int SYN_NPAR = 8;   // parameter slots per synapse group (stdp uses 7)
+enum SynType { SYN_TEST = 0, SYN_STDP = 1 };
+
+// Spike-timing-dependent plasticity, one time step per batch (src/get_spike.cu:85-95,
+// src/rev_spike.cu:46-130).
+struct StdpArgs {
+  const int2 *ring;
+  const int *ring_cnt;
+  int R, cap;
+  int dmin, dspan;
+  const int *pl_off;          // [n_nodes * dspan + 1] plastic entries per (source, delay) segment
+  const PlasticEdge *pl;      // [n_pl]
+  unsigned short *stamp;      // [n_pl] low 16 bits of the time index of the last arrival
+  long long n_pl;
+  EdgeW *edge;                // delivery CSR (weights updated in place)
+  const int *last_tidx;       // per node: time index of its last spike, -1 before the first
+  const int *syn_type;        // [n_groups]
+  const float *syn_par;       // [n_groups][SYN_NPAR]
+  const int *rev_off;         // [n_rev_nodes + 1] into rev_id
+  const int *rev_id;          // plastic entries grouped by target
+  const int *rev_node;        // [n_rev_nodes] targets with plastic in-edges
+  int n_rev_nodes;
+  float dt;
+};
+
 // Generated connection block: fixed in-degree with per-target random sources
 // and uniform delays, drawn on the device (see ngpu_build.cu).
 struct GenBlockDev {

@@ -145,6 +145,12 @@ _sigs = {
     "NESTGPU_GetIntParam": (_I, [ctypes.c_char_p]),
     "NESTGPU_SetIntParam": (_I, [ctypes.c_char_p, _I]),
     "NESTGPU_CreateSynGroup": (_I, [ctypes.c_char_p]),
+    "NESTGPU_GetSynGroupNParam": (_I, [_I]),
+    "NESTGPU_GetSynGroupParamNames": (c_char_pp, [_I]),
+    "NESTGPU_IsSynGroupParam": (_I, [_I, ctypes.c_char_p]),
+    "NESTGPU_GetSynGroupParamIdx": (_I, [_I, ctypes.c_char_p]),
+    "NESTGPU_GetSynGroupParam": (_F, [_I, ctypes.c_char_p]),
+    "NESTGPU_SetSynGroupParam": (_I, [_I, ctypes.c_char_p, _F]),
 }
 for _n in ("IntVar", "ScalVar", "PortVar", "ScalParam", "PortParam", "GroupParam", "ArrayParam",
            "ArrayVar"):
@@ -1024,7 +1030,13 @@ def SetStatus(gen_object, params, val=None):
             SetStatus(gen_object.node_seq, params, val)
         return
     if isinstance(gen_object, SynGroup):
-        raise ValueError("synapse groups (plasticity) are not supported by this engine")
+        if val is not None:
+            return SetSynGroupParam(gen_object, params, val)
+        if not isinstance(params, dict):
+            raise ValueError("Wrong argument in SetStatus")
+        for k, v in params.items():
+            SetSynGroupParam(gen_object, k, v)
+        return None
     gc.disable()
     try:
         nodes = gen_object
@@ -1051,7 +1063,11 @@ def SetStatus(gen_object, params, val=None):
 def GetStatus(gen_object, var_key=None):
     "Get neuron group or connection status"
     if isinstance(gen_object, SynGroup):
-        raise ValueError("synapse groups (plasticity) are not supported by this engine")
+        if var_key is None:
+            return {k: GetSynGroupParam(gen_object, k) for k in GetSynGroupParamNames(gen_object)}
+        if isinstance(var_key, (list, tuple)):
+            return [GetSynGroupParam(gen_object, k) for k in var_key]
+        return GetSynGroupParam(gen_object, var_key)
     if isinstance(gen_object, NodeSeq):
         if isinstance(var_key, str):
             return GetNeuronStatus(gen_object, var_key)
@@ -1082,7 +1098,48 @@ def GetStatus(gen_object, var_key=None):
 
 
 def CreateSynGroup(model_name, status_dict=None):
-    return _check(_c["NESTGPU_CreateSynGroup"](_b(model_name)))
+    "Create a synapse group (models: stdp, test_syn_model)"
+    if status_dict is not None and not isinstance(status_dict, dict):
+        raise ValueError("Wrong argument in CreateSynGroup")
+    syn_group = SynGroup(_check(_c["NESTGPU_CreateSynGroup"](_b(model_name))))
+    if status_dict:
+        SetStatus(syn_group, status_dict)
+    return syn_group
+
+
+def _syn_index(syn_group):
+    if not isinstance(syn_group, SynGroup):
+        raise ValueError("Wrong argument type: a synapse group is expected")
+    return syn_group.i_syn_group
+
+
+def GetSynGroupNParam(syn_group):
+    return _check(_c["NESTGPU_GetSynGroupNParam"](_syn_index(syn_group)))
+
+
+def GetSynGroupParamNames(syn_group):
+    n = GetSynGroupNParam(syn_group)
+    pp = _c["NESTGPU_GetSynGroupParamNames"](_syn_index(syn_group))
+    _check()
+    return [pp[i].decode("utf-8") for i in range(n)]
+
+
+def IsSynGroupParam(syn_group, param_name):
+    return _check(_c["NESTGPU_IsSynGroupParam"](_syn_index(syn_group), _b(param_name))) != 0
+
+
+def GetSynGroupParamIdx(syn_group, param_name):
+    return _check(_c["NESTGPU_GetSynGroupParamIdx"](_syn_index(syn_group), _b(param_name)))
+
+
+def GetSynGroupParam(syn_group, param_name):
+    v = _c["NESTGPU_GetSynGroupParam"](_syn_index(syn_group), _b(param_name))
+    _check()
+    return v
+
+
+def SetSynGroupParam(syn_group, param_name, val):
+    return _check(_c["NESTGPU_SetSynGroupParam"](_syn_index(syn_group), _b(param_name), float(val)))
 
 
 # ---------------------------------------------------------------- spike recording

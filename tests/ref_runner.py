@@ -21,7 +21,7 @@ sys.path.insert(0, os.path.join(os.path.dirname(HERE), "nest-gpu_b200"))
 import numpy as np  # noqa: E402
 
 import nestgpu as ngpu  # noqa: E402
-from scenarios import fixed_train_network, trace_scenario  # noqa: E402
+from scenarios import fixed_train_network, plastic_network, stdp_pair_scenario, trace_scenario  # noqa: E402
 
 
 def conn_arrays():
@@ -86,7 +86,13 @@ def main():
     what = sys.argv[1]
     ngpu.SetVerbosityLevel(0)
     out = {}
-    if what.startswith("fixed_train:"):
+    if what == "stdp_pairs":
+        dts, w, exp = stdp_pair_scenario(ngpu)
+        out = {"dt": list(dts), "weight": [float(x) for x in w], "expected": [float(x) for x in exp]}
+    elif what.startswith("plastic:"):
+        counts, w = plastic_network(ngpu, model=what.split(":")[1])
+        out = {"counts": counts.tolist(), "weight": [float(x) for x in w]}
+    elif what.startswith("fixed_train:"):
         counts, data = fixed_train_network(ngpu, model=what.split(":", 1)[1])
         out = {"counts": counts.tolist(), "record": np.asarray(data).tolist()}
     elif what.startswith("trace:"):

@@ -170,8 +170,10 @@ def test_errors_like_reference():
         ngpu.Create("iaf_psc_exp", 0)
     with pytest.raises(ValueError):
         ngpu.SetStatus(a, "no_such_param", 1.0)
-    with pytest.raises(ValueError, match="not supported"):
+    with pytest.raises(ValueError, match="Unrecognized synapse group"):
         ngpu.Connect(a, a, {"rule": "all_to_all"}, {"weight": 1.0, "delay": 1.0, "synapse_group": 1})
+    with pytest.raises(ValueError, match="Unknown synapse model"):
+        ngpu.CreateSynGroup("no_such_model")
     with pytest.raises(ValueError, match="MPI"):
         ngpu.RemoteConnect(0, a, 1, a, {"rule": "all_to_all"}, {"weight": 1.0, "delay": 1.0})
     assert ngpu.MpiId() == 0 and ngpu.MpiNp() == 1
@@ -186,3 +188,29 @@ def test_calibrate_without_gpu_fails_loudly():
     ngpu.Connect(a, a, {"rule": "all_to_all"}, {"weight": 1.0, "delay": 1.0})
     with pytest.raises(ValueError, match="no CUDA device"):
         ngpu.Simulate(1.0)
+
+
+def test_synapse_groups_and_plastic_connections():
+    """Synapse groups through the C ABI (src/nestgpu_C.h:275-287) and plastic connections in
+    the connection store: defaults, parameter access, the group of each connection and the
+    syn_group filter of GetConnections."""
+    ngpu.Reset()
+    g = ngpu.CreateSynGroup("stdp", {"Wmax": 2.0, "lambda": 0.01})
+    assert ngpu.GetSynGroupNParam(g) == 7
+    assert ngpu.GetSynGroupParamNames(g) == ["tau_plus", "tau_minus", "lambda", "alpha", "mu_plus",
+                                              "mu_minus", "Wmax"]
+    st = ngpu.GetStatus(g)
+    assert st["Wmax"] == 2.0 and abs(st["lambda"] - 0.01) < 1e-9 and st["tau_plus"] == 20.0
+    assert ngpu.GetSynGroupParamIdx(g, "alpha") == 3 and not ngpu.IsSynGroupParam(g, "foo")
+    t = ngpu.CreateSynGroup("test_syn_model")
+    assert abs(ngpu.GetStatus(t, "fact") - 0.1) < 1e-7 and ngpu.GetStatus(t, "offset") == 0.0
+    a = ngpu.Create("aeif_cond_beta_multisynapse", 3, 2)
+    ngpu.Connect(a, a, {"rule": "one_to_one"}, {"weight": 0.5, "delay": 1.0})
+    ngpu.Connect(a, a, {"rule": "all_to_all"}, {"weight": 1.0, "delay": 1.5, "synapse_group": g})
+    c = ngpu.GetConnections(a, a)
+    assert len(c) == 12
+    assert len(ngpu.GetConnections(a, a, syn_group=0)) == 3
+    plastic = ngpu.GetConnections(a, a, syn_group=g.i_syn_group)
+    assert len(plastic) == 9
+    assert all(ngpu.GetStatus(x)["syn"] == g.i_syn_group for x in plastic)
+    ngpu.Reset()

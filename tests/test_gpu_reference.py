@@ -19,7 +19,7 @@ import numpy as np
 import pytest
 
 import nestgpu as ngpu
-from scenarios import fixed_train_network, trace_scenario
+from scenarios import fixed_train_network, plastic_network, stdp_pair_scenario, trace_scenario
 
 pytestmark = pytest.mark.gpu
 
@@ -95,6 +95,52 @@ def test_spike_counts_match_reference(model):
     counts, _ = fixed_train_network(ngpu, model=model)
     assert counts.sum() > 0
     assert counts.tolist() == ref["counts"]
+
+
+@needs_ref
+def test_stdp_pairs_match_reference():
+    """The reference's STDP known-answer scenario (python/test/test_stdp.py) run by the
+    reference build and by this engine.  Both are within the test's 1e-5 of the closed form,
+    and the weights agree bit for bit except where a post-synaptic spike sits on a step
+    boundary: the tiny plastic EPSP then moves it one step in one build and not in the other
+    (the FP32 arithmetic differs: CUDA's expf there, the engine's own exp here), which shows
+    as the closed-form weight for Dt - 0.1 ms."""
+    ref = run_reference("stdp_pairs")
+    dts, w, exp = stdp_pair_scenario(ngpu)
+    w_ref = np.asarray(ref["weight"])
+    assert np.max(np.abs(w_ref - np.asarray(ref["expected"]))) < 1e-5
+    assert np.max(np.abs(w - exp)) < 1e-5
+    same = w == w_ref
+    assert same.sum() >= len(w) - 2
+    for i in np.nonzero(~same)[0]:
+        # each build's weight is the closed form at Dt or at Dt one step (0.1 ms) off
+        cands = [exp[i]] + [stdp_pair_scenario_weight(dts[i] + s) for s in (-0.1, 0.1)]
+        assert all(min(abs(x - c) for c in cands) < 1e-9 for x in (w[i], w_ref[i]))
+
+
+def stdp_pair_scenario_weight(dt_ms):
+    from scenarios import STDP_PAR, stdp_expected
+    p = STDP_PAR
+    return stdp_expected(p["Wmax"] / 2, dt_ms, p["tau_plus"], p["tau_minus"], p["lambda"], p["alpha"],
+                         p["mu_plus"], p["mu_minus"], p["Wmax"])
+
+
+@needs_ref
+@pytest.mark.parametrize("model", ["aeif_cond_beta_multisynapse", "iaf_psc_exp"])
+def test_plastic_network_matches_reference(model):
+    """A recurrent network with plastic excitatory edges under fixed input trains: spike counts
+    equal the reference build's exactly.  iaf_psc_exp (exact propagators, no transcendental
+    functions in the step) gives the same weights; for aeif, whose threshold crossings depend
+    on the FP32 exp, at least 97% of the plastic weights are bit-identical and the others are
+    edges whose pre/post spike pairs ended one step apart in the two builds."""
+    ref = run_reference("plastic:" + model)
+    counts, w = plastic_network(ngpu, model=model)
+    w_ref = np.asarray(ref["weight"], dtype=np.float32)
+    assert counts.tolist() == ref["counts"]
+    if model == "iaf_psc_exp":
+        assert np.allclose(w, w_ref, rtol=1e-6, atol=1e-7)
+    else:
+        assert np.mean(w == w_ref) >= 0.97
 
 
 @needs_ref
