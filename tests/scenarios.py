@@ -271,3 +271,31 @@ def plastic_network(api, n=80, n_in=20, seed=11, t_sim=400.0, model="aeif_cond_b
     ids = api.GetConnections(exc, neuron)
     w = np.asarray(_conn_status(api, ids, "weight"), dtype=np.float32)
     return counts, w
+
+
+def stdp_wrap_network(api, t_sim=7000.0):
+    """Plastic edges driven by regular spike trains for longer than 2^16 steps, so the 16-bit
+    arrival stamps pass both reset points (time index 0x8000 and 0x10000,
+    src/nestgpu.cu:490-498).  Besides four regular presynaptic neurons, one never spikes (its
+    stamps keep the initial 0x8000 until the first reset) and one spikes only in the first
+    200 ms (its stamps are more than 2^16 steps old at the end): without the resets their
+    edges would be potentiated by the later postsynaptic spikes.  Returns the plastic weights
+    in connection order (sources: the four regular neurons, the silent one, the early one)."""
+    syn = api.CreateSynGroup("stdp", {"tau_plus": 20.0, "tau_minus": 20.0, "lambda": 0.002,
+                                      "alpha": 1.0, "mu_plus": 1.0, "mu_minus": 1.0, "Wmax": 2.0})
+    sg = api.Create("spike_generator", 5)
+    pre = api.Create("iaf_psc_exp", 6)     # 0-3 regular, 4 silent, 5 early
+    post = api.Create("iaf_psc_exp", 4)
+    for i in range(4):
+        t = np.arange(20.0 + 3.0 * i, t_sim - 10.0, 47.0 + 6.0 * i)
+        api.SetStatus([sg[i]], {"spike_times": [float(round(x, 1)) for x in t]})
+    api.SetStatus([sg[4]], {"spike_times": [100.0, 150.0]})
+    api.Connect(sg[0:4], pre[0:4], {"rule": "one_to_one"}, {"weight": 5000.0, "delay": 1.0})
+    api.Connect([sg[4]], [pre[5]], {"rule": "one_to_one"}, {"weight": 5000.0, "delay": 1.0})
+    api.Connect(sg[0:4], post, {"rule": "one_to_one"}, {"weight": 5000.0, "delay": 4.0})
+    api.Connect(pre, post, {"rule": "all_to_all"},
+                {"weight": 1.0, "delay": {"distribution": "normal_clipped", "mu": 3.0, "sigma": 1.5,
+                                          "low": 0.5, "high": 8.0}, "synapse_group": syn})
+    api.Simulate(t_sim)
+    ids = api.GetConnections(pre, post)
+    return np.asarray(_conn_status(api, ids, "weight"), dtype=np.float32)

@@ -82,3 +82,13 @@ def test_linear_test_synapse_model_bitexact():
     assert np.array_equal(c_gpu, c_orc)
     assert np.array_equal(w_gpu, w_orc)
     assert np.any(w_gpu != 20.0)
+
+
+def test_stamp_wraparound_matches_oracle():
+    """7 s of plastic edges: the stamp resets at 2^15 and 2^16 steps run on the device as in
+    the oracle; edges without (recent) arrivals stay inert."""
+    from scenarios import stdp_wrap_network
+    w = stdp_wrap_network(ngpu)
+    w_orc = stdp_wrap_network(orc.Oracle())
+    assert np.allclose(w, w_orc, rtol=1e-6, atol=1e-9)
+    assert np.all(w.reshape(6, 4)[4] == 1.0)

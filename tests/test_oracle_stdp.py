@@ -41,3 +41,15 @@ def test_plastic_network_moves_weights(model, wmax):
     counts, w = plastic_network(orc.Oracle(), model=model)
     assert 5.0 < counts.sum() / counts.size / 0.4 < 200.0
     assert np.std(w) > 0.05 * wmax / 3 and np.all(w >= 0.0) and np.all(w <= wmax)
+
+
+def test_stamp_resets_keep_old_and_missing_arrivals_inert():
+    """After 2^15 and 2^16 steps the 16-bit stamps are reset (src/nestgpu.cu:490-498): an edge
+    that never carried a spike and an edge whose last spike is older than 2^16 steps see no
+    potentiation from the later postsynaptic spikes."""
+    from scenarios import stdp_wrap_network
+    w = stdp_wrap_network(orc.Oracle()).reshape(6, 4)
+    w_early = stdp_wrap_network(orc.Oracle(), t_sim=400.0).reshape(6, 4)
+    assert np.all(w[4] == 1.0)
+    assert np.array_equal(w[5], w_early[5]) and np.any(w_early[5] != 1.0)
+    assert np.std(w[0:4]) > 0.01
