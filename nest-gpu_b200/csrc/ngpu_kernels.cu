@@ -75,7 +75,7 @@ __device__ __forceinline__ void iaf_neuron(const IafArgs &A, const SpikeOut &so,
   A.var[3 * (size_t)n + i] = refr;
 }
 
-__global__ void __launch_bounds__(256) iaf_batch_kernel(const IafArgs A, const SpikeOut so,
+__global__ void __launch_bounds__(256, 3) iaf_batch_kernel(const IafArgs A, const SpikeOut so,
                                                         const Clock *clk, int k0, int M) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < A.n) iaf_neuron(A, so, clk, k0, M, i);
@@ -84,7 +84,9 @@ __global__ void __launch_bounds__(256) iaf_batch_kernel(const IafArgs A, const S
 // All iaf_psc_exp groups in one launch (a network of several populations would
 // otherwise pay one launch per population and step): block b serves group g with
 // blk0[g] <= b < blk0[g+1]; the groups' argument blocks are in device memory.
-__global__ void __launch_bounds__(256) iaf_multi_kernel(const IafArgs *tab, const int *blk0, int ngroups,
+// Three 256-thread blocks per SM (80 registers): 113k neurons fit in one wave, which
+// keeps the 77k-neuron microcircuit's 302 blocks from spilling into a second wave.
+__global__ void __launch_bounds__(256, 3) iaf_multi_kernel(const IafArgs *tab, const int *blk0, int ngroups,
                                                         const SpikeOut so, const Clock *clk, int k0, int M) {
   int lo = 0, hi = ngroups;   // largest g with blk0[g] <= blockIdx.x
   while (hi - lo > 1) {
