@@ -304,7 +304,7 @@ def engine_arm(args):
         "vs_baseline": None,
         "dtype": "fp32",
         "data": "synthetic (seeded random network and Poisson drive)",
-        "config": {"workload": "1M AdEx x 1000 syn (config 2)", "neurons": n_neurons,
+        "config": {"workload": "1M aeif_cond_beta_multisynapse x 1000 synapses, Poisson 8 kHz, delays 1-2 ms", "neurons": n_neurons,
                    "synapses": n_neurons * (K_EXC + K_INH), "bio_ms_per_step": STEP_MS,
                    "dt_ms": 0.1, "parallelism": "replicas%d" % WORLD,
                    "l2": "inputs larger than L2 (8 GB edge array)", "scale": args.scale},
@@ -405,7 +405,7 @@ def reference_arm(args):
         "vs_baseline": None,
         "dtype": "fp32",
         "data": "synthetic (seeded random network and Poisson drive)",
-        "config": {"workload": "1M AdEx x 1000 syn (config 2)", "sample_neurons": 20000,
+        "config": {"workload": "1M aeif_cond_beta_multisynapse x 1000 synapses, Poisson 8 kHz, delays 1-2 ms", "sample_neurons": 20000,
                    "bio_ms_per_step": STEP_MS, "dt_ms": 0.1},
         "rtf_extrapolated_1M": r["rtf_extrapolated_1M"],
         "cpu_baseline": dict(r["cpu_baseline"]),

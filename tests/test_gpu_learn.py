@@ -104,7 +104,7 @@ def test_trained_proposal_on_held_out_seed(drive_w):
     training seed, evaluate on a held-out seed: the proposal must not cost evaluations and
     must keep the firing rate, in the quiet network (0.1 nS drive) and the firing one."""
     r = learned_vs_plain(ngpu, drive_w)
-    print("\nC4 drive %.2f nS: %s" % (drive_w, r))
+    print("\nfour-receptor network, drive %.2f nS: %s" % (drive_w, r))
     assert abs(r["learned_rate_hz"] - r["plain_rate_hz"]) <= 0.02 * max(r["plain_rate_hz"], 1.0)
     assert r["logged_steps"] > 0 and r["trained_on"] > 0
     assert r["learned_evals_per_neuron_ms"] <= r["plain_evals_per_neuron_ms"]
