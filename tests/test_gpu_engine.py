@@ -315,3 +315,36 @@ def test_persistent_barrier_timeout_is_reported():
     c_g = np.concatenate([np.asarray(ngpu.GetStatus(p, "spike_count")).ravel() for p in pops_g])
     c_o = np.concatenate([np.asarray(o.GetStatus(p, "spike_count")).ravel() for p in pops_o])
     assert np.array_equal(c_g, c_o)
+
+
+def test_mapping_change_between_calls_keeps_results():
+    """Launch-mapping knobs set between Simulate calls take effect (the captured graphs are
+    dropped) and change nothing in the results: 60 + 90 ms under two mappings equal the same
+    two calls under the default mapping, and GetLaunchMapping reports the new mapping."""
+    ref = _continuation(ngpu, [60.0, 90.0])
+    ngpu.Reset()
+    ngpu.SetVerbosityLevel(0)
+
+    class Switch(object):
+        """Forwards to the engine; from the second Simulate call on, under another mapping."""
+        calls = 0
+
+        def __getattr__(self, name):
+            return getattr(ngpu, name)
+
+        def Simulate(self, t):
+            if self.calls:
+                ngpu.SetUpdateThreads(256)
+                ngpu.SetDeliverGroup(8)
+                ngpu.SetUpdateOccupancy(1)
+                ngpu.SetRk5Budget(2)
+            self.calls += 1
+            ngpu.Simulate(t)
+
+    out = _continuation(Switch(), [60.0, 90.0])
+    m = ngpu.GetLaunchMapping()
+    assert m["update_threads"] == 256 and m["deliver_group"] == 8 and m["update_occupancy"] == 1
+    assert m["rk5_budget"] == 2
+    assert ref[0].sum() > 0
+    for a, b in zip(ref, out):
+        assert np.array_equal(a, b)
