@@ -269,6 +269,11 @@ def engine_arm(args):
     fp32_peak = (148 * 128 * 2 * (clocks["sm_mhz"] or 1965.0) * 1e6) / 1e12
     rk5_tflops = p_derivs * FLOPS_PER_DERIV / (upd_ms / 1e3) / 1e12
     deliver_gbs = (p_events * DELIVERY_BYTES_PER_EVENT + p_spikes * DELIVERY_BYTES_PER_SPIKE) / (del_ms / 1e3) / 1e9
+    # each synaptic event is one FP64 reduction into a random entry of one accumulator slot
+    # (n_neurons x 2 receptor ports x 8 B): its measured random-reduction rate is the second
+    # denominator of the delivery kernel
+    red_gops = p_events / (del_ms / 1e3) / 1e9
+    red_peak = ngpu.MeasureReductionRate(n_neurons * 2 * 8, 1 << 26)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
@@ -329,7 +334,11 @@ def engine_arm(args):
                               "traffic": DELIVERY_TRAFFIC_PER_EVENT * p_events * M,
                               "bytes_per_launch": (p_events * DELIVERY_BYTES_PER_EVENT +
                                                    p_spikes * DELIVERY_BYTES_PER_SPIKE) * M, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
-                              "ms_per_step": del_ms},
+                              "ms_per_step": del_ms,
+                              "reductions": {"achieved": red_gops, "peak": red_peak, "unit": "1e9 FP64 red/s",
+                                             "frac": red_gops / red_peak,
+                                             "peak_source": "measured in this run: random FP64 reductions into a "
+                                                            "buffer of one accumulator slot's size"}},
         "clocks": clocks,
     }
     if WORLD == 1 and not args.no_extras:

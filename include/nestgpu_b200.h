@@ -335,6 +335,11 @@ int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliv
    variant, delivery lane group, delivery grid (0: automatic), RK5 step budget, persistent loop}
    and returns 6 (-1 on error).  No counterpart in the reference. */
 int NGPU_GetLaunchMapping(int *vals, int n);
+/* Measured rate (1e9 per second) of FP64 reductions to uniformly random addresses of a
+   `bytes`-byte device buffer, `n_ops` in total: the access pattern of the spike delivery's
+   accumulator updates, used as that kernel's roofline denominator.  -1 on error.  No
+   counterpart in the reference. */
+double NGPU_MeasureReductionRate(size_t bytes, long long n_ops);
 
 /* 1: draw connection random numbers with cuRAND's host generator instead of the device
    generator the reference uses (integer streams are identical, normal streams are not);

@@ -807,6 +807,10 @@ int NGPU_GetLaunchMapping(int *vals, int n) {
   }, -1);
 }
 
+double NGPU_MeasureReductionRate(size_t bytes, long long n_ops) {
+  return guard([&] { return measure_random_reduction_rate(bytes, n_ops); }, -1.0);
+}
+
 int NGPU_GetBatchLength() {
   return guard([&] {
     if (!E().calibrated()) throw NgpuError("the batch length is known after calibration");

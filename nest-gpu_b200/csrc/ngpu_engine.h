@@ -382,6 +382,8 @@ int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk
 int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *clk, int k0, int M,
                    cudaStream_t st);
 int launch_clock_advance(Clock *clk, int K, cudaStream_t st);
+// reduction-rate probe (ngpu_probe.cu): 1e9 random FP64 reductions per second
+double measure_random_reduction_rate(size_t bytes, long long n_ops);
 // STDP (ngpu_stdp.cu)
 int launch_stdp_reset(const StdpArgs &A, const Clock *clk, int k0, cudaStream_t st);
 int launch_stdp_forward(const StdpArgs &A, const Clock *clk, int k0, cudaStream_t st);

@@ -178,6 +178,8 @@ if is_b200_engine:
     _c["NGPU_TestBarrierTimeout"] = _bind("NGPU_TestBarrierTimeout", _I, [_I])
     _c["NGPU_Autotune"] = _bind("NGPU_Autotune", _I, [_I] + [ctypes.POINTER(_I)] * 4)
     _c["NGPU_GetLaunchMapping"] = _bind("NGPU_GetLaunchMapping", _I, [ctypes.POINTER(_I), _I])
+    _c["NGPU_MeasureReductionRate"] = _bind("NGPU_MeasureReductionRate", ctypes.c_double,
+                                            [ctypes.c_size_t, ctypes.c_longlong])
     _c["NGPU_GetSimDeviceMs"] = _bind("NGPU_GetSimDeviceMs", ctypes.c_double, [])
     _c["NGPU_GetLaunchCount"] = _bind("NGPU_GetLaunchCount", ctypes.c_longlong, [])
     _c["NGPU_ProfileSteps"] = _bind("NGPU_ProfileSteps", _I, [_I, ctypes.POINTER(ctypes.c_double)])
@@ -1419,6 +1421,15 @@ def Autotune(steps=200):
     m = GetLaunchMapping()
     m["trials"] = n
     return m
+
+
+def MeasureReductionRate(nbytes, n_ops):
+    """1e9 FP64 reductions per second to random addresses of an `nbytes` device buffer (the
+    delivery kernel's access pattern; engine extension)."""
+    _need_b200("MeasureReductionRate")
+    v = _c["NGPU_MeasureReductionRate"](nbytes, n_ops)
+    _check()
+    return v
 
 
 def GetLaunchMapping():
