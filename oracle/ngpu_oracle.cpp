@@ -21,6 +21,8 @@
 //                                         src/connect_rules.cpp:274-322
 //   RandomInt / RandomNormal(Clipped)     src/random.cu:8-76, src/nestgpu.cu:1135-1188
 //   step order                            src/nestgpu.cu:294-635
+//   parrot_neuron                         src/parrot_neuron.cu:60-130
+//   dendritic delay of reverse spikes     src/spike_buffer.cu:162-190,247-317
 //   synapse groups and STDP               src/syn_model.cu:43-56,136-152, src/stdp.cu:36-80,
 //                                         src/test_syn_model.cu:35-50, src/get_spike.cu:85-95,
 //                                         src/rev_spike.cu:46-130, src/nestgpu.cu:490-498,606-616
@@ -45,6 +47,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -177,12 +180,19 @@ static int poisson_draw(float lam, uint64_t seed, uint64_t edge, int64_t tidx) {
 // Models
 // --------------------------------------------------------------------------
 enum Model { AEIF_COND_BETA = 0, AEIF_COND_ALPHA, AEIF_PSC_EXP, AEIF_PSC_ALPHA,
-             IAF_PSC_EXP, SPIKE_GEN, POISS_GEN, N_MODEL };
+             IAF_PSC_EXP, SPIKE_GEN, POISS_GEN, PARROT, N_MODEL };
 
 static const char *model_name[N_MODEL] = {
   "aeif_cond_beta_multisynapse", "aeif_cond_alpha_multisynapse",
   "aeif_psc_exp_multisynapse", "aeif_psc_alpha_multisynapse",
-  "iaf_psc_exp", "spike_generator", "poisson_generator"};
+  "iaf_psc_exp", "spike_generator", "poisson_generator", "parrot_neuron"};
+
+// parrot_neuron (src/parrot_neuron.cu:40-52): port 0 input (weight 1) repeated as a spike in
+// the next step, port 1 input weighted 0 (it only reaches plastic synapses)
+enum { PR_input_spike_height = 0, PR_dummy_input, PR_V, PR_NVAR };
+static const char *parrot_var_name[PR_NVAR] = {"input_spike_height", "dummy_input", "V"};
+enum { PR_hold_spike_height = 0, PR_den_delay, PR_NPAR };
+static const char *parrot_par_name[PR_NPAR] = {"hold_spike_height", "den_delay"};
 
 static bool is_aeif(Model m) { return m <= AEIF_PSC_ALPHA; }
 
@@ -404,6 +414,9 @@ struct Net {
   std::vector<SynGroupDef> syn_groups;
   bool any_plastic = false;
   std::vector<long long> last_rev;                // per node: time index of the last spike
+                                                  // to reach the node's synapses
+  std::vector<int> den_steps;                     // per node: dendritic delay in steps
+  std::map<long long, std::vector<int>> rev_pending;   // time index -> nodes whose spike arrives
   std::vector<std::vector<Edge *>> rev_in;        // per node: incoming plastic edges
   // simulation state
   bool calibrated = false;
@@ -548,6 +561,10 @@ struct Net {
       g.nport = 0;
       g.par.assign(PG_NPAR, std::vector<double>(n, 0.0));
       std::fill(g.par[PG_stop].begin(), g.par[PG_stop].end(), (double)1.0e30f);
+    } else if (g.model == PARROT) {
+      g.nport = 2;
+      g.var.assign(PR_NVAR, std::vector<double>(n, 0.0));
+      g.par.assign(PR_NPAR, std::vector<double>(n, 0.0));
     }
     g.acc.assign((size_t)g.nport * n, 0.0);
     groups.push_back(g);
@@ -573,6 +590,9 @@ struct Net {
       for (int k = 0; k < I_NPAR; k++) if (name == iaf_par_name[k]) { kind = 2; return k; }
     } else if (g.model == POISS_GEN) {
       for (int k = 0; k < PG_NPAR; k++) if (name == pg_par_name[k]) { kind = 2; return k; }
+    } else if (g.model == PARROT) {
+      for (int k = 0; k < PR_NVAR; k++) if (name == parrot_var_name[k]) { kind = 0; return k; }
+      for (int k = 0; k < PR_NPAR; k++) if (name == parrot_par_name[k]) { kind = 2; return k; }
     } else if (g.model == SPIKE_GEN) {
       if (name == "spike_times") { kind = 5; return 0; }
       if (name == "spike_heights") { kind = 5; return 1; }
@@ -828,6 +848,16 @@ struct Net {
     // last spike time index of every node (src/spike_buffer.cu:319-328)
     last_rev.assign(node_group.size(), kLastSpikeGuard);
     rev_in.assign(node_group.size(), {});
+    // dendritic delay in steps, round(den_delay / dt) in float (src/spike_buffer.cu:175-177)
+    den_steps.assign(node_group.size(), 0);
+    for (auto &g : groups) {
+      const std::vector<double> *dd = nullptr;
+      if (is_aeif(g.model)) dd = &g.par[A_den_delay];
+      else if (g.model == IAF_PSC_EXP) dd = &g.par[I_den_delay];
+      else if (g.model == PARROT) dd = &g.par[PR_den_delay];
+      if (dd)
+        for (int i = 0; i < g.n; i++) den_steps[g.i0 + i] = (int)std::round((float)(*dd)[i] / dt);
+    }
     if (any_plastic)
       for (size_t s = 0; s < conn.size(); s++) {
         if (groups[node_group[s]].model == POISS_GEN)
@@ -1111,7 +1141,14 @@ struct Net {
     if (g.max_rec > 0) {
       if ((int)g.rec_times[i].size() < g.max_rec - 1) g.rec_times[i].push_back((float)neural_time);
     }
-    last_rev[node] = tidx;   // den_delay 0: the spike reaches the dendrites at once
+    // the spike reaches the node's own synapses at once, or den_delay steps later
+    // (src/spike_buffer.cu:183-186, 279-281, 314-316)
+    if (den_steps[node] == 0) {
+      last_rev[node] = tidx;
+    } else {
+#pragma omp critical(rev_pending)
+      rev_pending[tidx + den_steps[node]].push_back(node);
+    }
     if (!conn[node].empty()) {
       std::vector<Queued> &q = queue[node];
       if ((int)q.size() >= max_spike_buffer) return;   // reference prints and drops
@@ -1289,6 +1326,17 @@ struct Net {
       } else if (g.model == IAF_PSC_EXP) {
         if (fp64) update_iaf<double>(g, tidx);
         else update_iaf<float>(g, tidx);
+      } else if (g.model == PARROT) {
+        // src/parrot_neuron.cu:60-82
+        for (int i = 0; i < g.n; i++) {
+          const float sh = (float)g.var[PR_input_spike_height][i];
+          g.var[PR_V][i] = sh;
+          if (sh != 0.0f) {
+            const float height = g.par[PR_hold_spike_height][i] == 0.0 ? 1.0f : sh;
+            g.var[PR_input_spike_height][i] = 0.0;
+            push_spike(g.i0 + i, height, tidx);
+          }
+        }
       } else if (g.model == SPIKE_GEN) {
         for (int i = 0; i < g.n; i++) {
           int k = g.sg_next[i];
@@ -1301,6 +1349,15 @@ struct Net {
     }
     // 4. records
     write_records((float)neural_time);
+    // 4b. reverse spikes whose dendritic delay ends in this step (set at the start of the
+    //     step in the reference, src/spike_buffer.cu:314-316; only the plasticity below reads it)
+    if (!rev_pending.empty()) {
+      auto it = rev_pending.find(tidx);
+      if (it != rev_pending.end()) {
+        for (int nd : it->second) last_rev[nd] = tidx;
+        rev_pending.erase(it);
+      }
+    }
     // 5. collect spikes (src/get_spike.cu:60-108); FP64 sums, order-independent for
     //    weights whose partial sums are exact
     long long nev = 0;
@@ -1359,6 +1416,10 @@ struct Net {
           if (is_aeif(g.model)) {
             pw = s.weight_par >= 0 ? (double)(float)g.par[A_NSCAL + s.n_port_par * p + s.weight_par][i] : 1.0;
             pi = &g.var[2 + s.n_port_var * p + s.input_var];
+          } else if (g.model == PARROT) {
+            // port weights {1, 0}: port p feeds variable p (src/parrot_neuron.cu:110-122)
+            pw = p == 0 ? 1.0 : 0.0;
+            pi = &g.var[p];
           } else {
             pw = 1.0;
             pi = &g.var[p == 0 ? I_I_syn_ex : I_I_syn_in];

@@ -299,3 +299,66 @@ def stdp_wrap_network(api, t_sim=7000.0):
     api.Simulate(t_sim)
     ids = api.GetConnections(pre, post)
     return np.asarray(_conn_status(api, ids, "weight"), dtype=np.float32)
+
+
+# The reference's STDP cases (python/test/test_stdp/cases/case1-10.py): one presynaptic and
+# one postsynaptic parrot_neuron, each driven by a spike_generator (weight 1, delay 1 ms); the
+# plastic edge enters the postsynaptic parrot on receptor 1 (weight 0 there, so it does not
+# make it fire).  (pre spike times, post spike times, postsynaptic den_delay, plastic delay).
+STDP_CASES = {
+    1: ([2.0], [1.0, 3.0], 3.0, 1.0),
+    2: ([4.0], [1.0, 5.0], 3.0, 1.0),
+    3: ([4.0, 6.5], [1.0, 5.0, 6.0], 3.0, 1.0),
+    4: ([2.0, 6.5], [1.0, 5.0, 6.0], 3.0, 1.0),
+    5: ([1.0], [1.0], 3.0, 1.0),
+    6: ([1.0, 3.0], [2.0], 1.0, 3.0),
+    7: ([1.0, 5.0], [4.0], 1.0, 3.0),
+    8: ([1.0, 5.0, 6.0], [4.0, 6.5], 1.0, 3.0),
+    9: ([1.0, 5.0, 6.0], [2.0, 6.5], 1.0, 3.0),
+    10: ([1.0], [1.0], 1.0, 3.0),
+}
+STDP_CASE_PAR = {"tau_plus": 20.0, "tau_minus": 20.0, "lambda": 0.01, "alpha": 1.0, "mu_plus": 1.0,
+                 "mu_minus": 1.0, "Wmax": 10.0}
+
+
+def stdp_case_expected(case, w0=1.0):
+    """The weight after the case's spikes: a presynaptic spike reaches the synapse `delay`
+    after it is emitted and is depressed against the last postsynaptic spike that reached
+    the synapse before it; a postsynaptic spike reaches it `den_delay` after it is emitted
+    and potentiates against the last presynaptic arrival at or before it (the pairing that
+    the cases' closed forms follow)."""
+    pre, post, den, delay = STDP_CASES[case]
+    p = STDP_CASE_PAR
+    ev = sorted([(t + delay, 0) for t in pre] + [(t + den, 1) for t in post], key=lambda e: (e[0], -e[1]))
+    w, last_pre, last_post = w0, None, None
+    for t, kind in ev:
+        if kind == 0:
+            if last_post is not None and t - last_post > 0:
+                w = stdp_expected(w, last_post - t, p["tau_plus"], p["tau_minus"], p["lambda"], p["alpha"],
+                                  p["mu_plus"], p["mu_minus"], p["Wmax"])
+            last_pre = t
+        else:
+            if last_pre is not None:
+                w = stdp_expected(w, t - last_pre, p["tau_plus"], p["tau_minus"], p["lambda"], p["alpha"],
+                                  p["mu_plus"], p["mu_minus"], p["Wmax"])
+            last_post = t
+    return w
+
+
+def stdp_case(api, case, w0=1.0, sim_time=20.0):
+    """Runs one reference STDP case; returns the simulated weight of the plastic edge."""
+    pre_t, post_t, den, delay = STDP_CASES[case]
+    pre = api.Create("parrot_neuron")
+    post = api.Create("parrot_neuron")
+    sg_pre = api.Create("spike_generator")
+    sg_post = api.Create("spike_generator")
+    api.SetStatus(sg_pre, {"spike_times": pre_t})
+    api.SetStatus(sg_post, {"spike_times": post_t})
+    api.Connect(sg_pre, pre, {"rule": "one_to_one"}, {"weight": 1.0, "delay": 1.0})
+    api.Connect(sg_post, post, {"rule": "one_to_one"}, {"weight": 1.0, "delay": 1.0})
+    syn = api.CreateSynGroup("stdp", STDP_CASE_PAR)
+    api.SetStatus(post, {"den_delay": den})
+    api.Connect(pre, post, {"rule": "one_to_one"},
+                {"weight": w0, "delay": delay, "synapse_group": syn, "receptor": 1})
+    api.Simulate(sim_time)
+    return float(_conn_status(api, api.GetConnections(pre, post), "weight")[0])

@@ -53,3 +53,32 @@ def test_stamp_resets_keep_old_and_missing_arrivals_inert():
     assert np.all(w[4] == 1.0)
     assert np.array_equal(w[5], w_early[5]) and np.any(w_early[5] != 1.0)
     assert np.std(w[0:4]) > 0.01
+
+
+@pytest.mark.parametrize("case", list(range(1, 11)))
+def test_reference_stdp_cases(case):
+    """python/test/test_stdp/cases/case<N>.py: parrot neurons, dendritic delays of 1 and 3 ms,
+    depression and potentiation sequences; the weight against the cases' closed form."""
+    from scenarios import stdp_case, stdp_case_expected
+    assert abs(stdp_case(orc.Oracle(), case) - stdp_case_expected(case)) < 1e-5
+
+
+def test_parrot_neuron_repeats_port0_only():
+    """src/parrot_neuron.cu:60-82: a spike arriving on port 0 is repeated one step after the
+    step it arrives in (height 1 unless hold_spike_height); port 1 input is weighted 0."""
+    o = orc.Oracle()
+    sg = o.Create("spike_generator")
+    p = o.Create("parrot_neuron", 3)
+    o.SetStatus(sg, {"spike_times": [2.0, 5.0], "spike_heights": [2.0, 3.0]})
+    o.Connect(sg, p[0:1], {"rule": "all_to_all"}, {"weight": 1.0, "delay": 1.0})
+    o.Connect(sg, p[1:2], {"rule": "all_to_all"}, {"weight": 1.0, "delay": 1.0, "receptor": 1})
+    o.Connect(sg, p[2:3], {"rule": "all_to_all"}, {"weight": 1.0, "delay": 1.0})
+    o.SetStatus(p[2:3], {"hold_spike_height": 1.0})
+    o.ActivateSpikeCount(p)
+    rec = o.CreateRecord("", ["V", "V", "V"], [p[0], p[1], p[2]], [0, 0, 0])
+    o.Simulate(10.0)
+    assert o.GetStatus(p, "spike_count") == [2, 0, 2]
+    v = np.asarray(o.GetRecordData(rec))
+    # the V column holds the repeated input in the step where the parrot fires
+    assert sorted(set(np.round(v[:, 1], 3))) == [0.0, 2.0, 3.0]
+    assert np.all(v[:, 2] == 0.0)
