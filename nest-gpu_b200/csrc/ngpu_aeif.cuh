@@ -70,6 +70,19 @@ __device__ __forceinline__ void push_spike(const SpikeOut &so, const GroupSpikeR
       atomicOr(so.status, ST_REC_TIMES_FULL);
     }
   }
+  if (so.last_rev) {
+    // the spike reaches the node's own synapses (STDP) now or den_delay steps later
+    // (src/spike_buffer.cu:183-186, 279-281, 314-316)
+    const int D = so.den_steps ? so.den_steps[node] : 0;
+    if (D == 0) {
+      so.last_rev[node] = (int)tidx;
+    } else {
+      const int rs = (int)((tidx + D) % so.rev_R);
+      const int pos = atomicAdd(&so.rev_cnt[rs], 1);
+      if (pos < so.rev_cap) so.rev_ring[(size_t)rs * so.rev_cap + pos] = node;
+      else atomicOr(so.status, ST_RING_OVERFLOW);
+    }
+  }
   if (so.has_out[node]) {
     int slot = (int)(tidx % so.R);
     int pos = atomicAdd(&so.ring_cnt[slot], 1);

@@ -11,7 +11,8 @@ namespace ngpu {
 
 static const char *kModelName[M_NMODEL] = {
     "aeif_cond_beta_multisynapse", "aeif_cond_alpha_multisynapse", "aeif_psc_exp_multisynapse",
-    "aeif_psc_alpha_multisynapse", "iaf_psc_exp", "spike_generator", "poisson_generator"};
+    "aeif_psc_alpha_multisynapse", "iaf_psc_exp", "spike_generator", "poisson_generator",
+    "parrot_neuron"};
 
 static bool is_aeif(int m) { return m <= M_AEIF_PSC_ALPHA; }
 
@@ -47,6 +48,11 @@ static const char *kIafPar[I_NPAR] = {"tau_m", "C_m", "E_L", "I_e", "Theta_rel",
                                       "P11in", "P21ex", "P21in", "P22"};
 enum { PG_rate = 0, PG_origin, PG_start, PG_stop, PG_NPAR };
 static const char *kPgPar[PG_NPAR] = {"rate", "origin", "start", "stop"};
+// parrot_neuron (src/parrot_neuron.cu:40-52)
+enum { PR_input_spike_height = 0, PR_dummy_input, PR_V, PR_NVAR };
+static const char *kParrotVar[PR_NVAR] = {"input_spike_height", "dummy_input", "V"};
+enum { PR_hold_spike_height = 0, PR_den_delay, PR_NPAR };
+static const char *kParrotPar[PR_NPAR] = {"hold_spike_height", "den_delay"};
 
 static Engine *g_engine = nullptr;
 
@@ -210,6 +216,10 @@ int Engine::create(const std::string &name, int n, int nport) {
     g.nport = 0;
     g.sg_times.assign(n, {});
     g.sg_heights.assign(n, {});
+  } else if (m == M_PARROT) {
+    g.nport = 2;
+    g.var.assign(PR_NVAR, std::vector<float>(n, 0.0f));
+    g.par.assign(PR_NPAR, std::vector<float>(n, 0.0f));
   } else {
     g.nport = 0;
     g.par.assign(PG_NPAR, std::vector<float>(n, 0.0f));
@@ -256,6 +266,9 @@ Kind Engine::locate(int node, const std::string &name, int *idx) {
     for (int j = 0; j < I_NPAR && k == K_NONE; j++) if (name == kIafPar[j]) { k = K_SCAL_PARAM; i = j; }
   } else if (g.model == M_POISS_GEN) {
     for (int j = 0; j < PG_NPAR && k == K_NONE; j++) if (name == kPgPar[j]) { k = K_SCAL_PARAM; i = j; }
+  } else if (g.model == M_PARROT) {
+    for (int j = 0; j < PR_NVAR && k == K_NONE; j++) if (name == kParrotVar[j]) { k = K_SCAL_VAR; i = j; }
+    for (int j = 0; j < PR_NPAR && k == K_NONE; j++) if (name == kParrotPar[j]) { k = K_SCAL_PARAM; i = j; }
   } else if (g.model == M_SPIKE_GEN) {
     if (name == "spike_times") { k = K_ARRAY_PARAM; i = 0; }
     else if (name == "spike_heights") { k = K_ARRAY_PARAM; i = 1; }
@@ -284,6 +297,9 @@ std::vector<std::string> Engine::names(int node, Kind kind) {
     if (kind == K_SCAL_PARAM) for (int j = 0; j < I_NPAR; j++) r.push_back(kIafPar[j]);
   } else if (g.model == M_POISS_GEN) {
     if (kind == K_SCAL_PARAM) for (int j = 0; j < PG_NPAR; j++) r.push_back(kPgPar[j]);
+  } else if (g.model == M_PARROT) {
+    if (kind == K_SCAL_VAR) for (int j = 0; j < PR_NVAR; j++) r.push_back(kParrotVar[j]);
+    if (kind == K_SCAL_PARAM) for (int j = 0; j < PR_NPAR; j++) r.push_back(kParrotPar[j]);
   } else if (g.model == M_SPIKE_GEN) {
     if (kind == K_ARRAY_PARAM) r = {"spike_times", "spike_heights"};
   }
@@ -320,7 +336,7 @@ static float *dev_row(Group &g, Kind k, int idx, int port) {
     if (k == K_SCAL_PARAM && idx == A_refractory_step) return g.d_refr;
     return nullptr;
   }
-  if (g.model == M_IAF_PSC_EXP && k == K_SCAL_VAR) return g.d_var + (size_t)idx * g.n;
+  if ((g.model == M_IAF_PSC_EXP || g.model == M_PARROT) && k == K_SCAL_VAR) return g.d_var + (size_t)idx * g.n;
   return nullptr;
 }
 
@@ -383,9 +399,8 @@ void Engine::set_scalar(const std::vector<int> &nodes, const std::string &name, 
   }
   if (k != K_SCAL_PARAM && k != K_SCAL_VAR)
     throw NgpuError("Unrecognized scalar parameter or variable " + name);
-  if (g.model != M_POISS_GEN && calibrated_ && k == K_SCAL_PARAM && is_aeif(g.model) &&
-      idx == A_den_delay && v != 0.0f)
-    throw NgpuError("dendritic delay is not supported");
+  if (calibrated_ && k == K_SCAL_PARAM && name == "den_delay")
+    throw NgpuError("dendritic delays are fixed at calibration");
   write_row(g, k, idx, 0, nodes, std::vector<float>(nodes.size(), v), stream_);
 }
 

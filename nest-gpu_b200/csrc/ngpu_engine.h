@@ -64,6 +64,7 @@ struct Group {
   std::vector<float *> rec_ptr_host;             // exported row pointers
   // device state
   float *d_var = nullptr;        // [nvar][n]
+  float *d_hold = nullptr;       // parrot_neuron: hold_spike_height [n]
   float *d_refr = nullptr;       // aeif refractory counter
   double *d_x = nullptr;
   float *d_h = nullptr;
@@ -288,6 +289,10 @@ class Engine {
   // plastic edges (synapse groups): forward index by (source, delay), reverse by target
   bool plastic_ = false;
   StdpArgs stdp_{};
+  int *d_last_rev_ = nullptr;      // plastic networks: last spike arrival at each node's synapses
+  int *d_den_steps_ = nullptr;     // dendritic delays in steps (null when all are 0)
+  int *d_rev_ring_ = nullptr, *d_rev_cnt_ = nullptr;
+  int rev_R_ = 0, rev_cap_ = 0;
   std::vector<unsigned long long> pl_pos_;               // per plastic entry: CSR position
   std::vector<std::pair<size_t, int>> pl_of_edge_;       // (host edge, plastic entry), sorted
   void build_plastic(const std::vector<size_t> &pl_edge, const std::vector<long long> &pl_key,
@@ -364,6 +369,7 @@ class Engine {
   AeifArgs aeif_args(Group &g);
   IafArgs iaf_args(Group &g);
   SpikeGenArgs sg_args(Group &g);
+  ParrotArgs parrot_args(Group &g);
   DeliverArgs deliver_args();
   void check_status();
 };
@@ -379,6 +385,9 @@ int launch_iaf_multi(const IafArgs *tab, const int *blk0, int ngroups, int nbloc
                      const Clock *clk, int k0, int M, cudaStream_t st);
 int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                      cudaStream_t st);
+int launch_parrot(const ParrotArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st);
+int launch_rev_arrivals(int *rev_ring, int *rev_cnt, int rev_R, int rev_cap, int *last_rev, const Clock *clk,
+                        int k0, cudaStream_t st);
 int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *clk, int k0, int M,
                    cudaStream_t st);
 int launch_clock_advance(Clock *clk, int K, cudaStream_t st);

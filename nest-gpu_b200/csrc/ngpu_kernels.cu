@@ -99,6 +99,45 @@ __global__ void __launch_bounds__(256, 3) iaf_multi_kernel(const IafArgs *tab, c
 }
 
 // ---------------------------------------------------------------------------
+// parrot_neuron (src/parrot_neuron.cu:60-82): the input of a step (port 0, weight 1) is
+// repeated as a spike in the next one (height 1, or the input with hold_spike_height);
+// port 1 has weight 0 (its spikes only reach plastic synapses).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) parrot_batch_kernel(const ParrotArgs A, const SpikeOut so, const Clock *clk,
+                                                           int k0, int M) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const int n = A.n;
+  float in0 = A.var[i], dummy = A.var[(size_t)n + i], V = A.var[2 * (size_t)n + i];
+  const bool hold = A.hold[i] != 0.0f;
+  const Clock cl = *clk;
+  const long long rec_it0 = cl.rec_it0;
+  PoissonCache pc;
+  poisson_cache_load(A.in, i, pc);
+  for (int m = 0; m < M; m++) {
+    const StepT t = step_at(cl, k0, m, A.dt);
+    double apf[2];
+    acc_prefetch<2>(apf, 2, n, i, A.in, m);
+    const float sh = in0;
+    V = sh;
+    if (sh != 0.0f) {
+      in0 = 0.0f;
+      push_spike(so, A.srec, A.i0 + i, i, hold ? sh : 1.0f, t.tidx, t.tnow);
+    }
+    if (A.rec.first) {
+      const float yr[3] = {in0, dummy, V};
+      write_records<3>(A.rec, so, A.i0 + i, i, yr, 3, 0.0f, t.it - rec_it0, t.tidx);
+    }
+    double in[2];
+    step_inputs_pf<2>(in, apf, 2, n, i, A.in, pc, m, t.tidx, t.tnow);
+    if (in[0] != 0.0) in0 = (float)__fma_rn(in[0], 1.0, (double)in0);
+  }
+  A.var[i] = in0;
+  A.var[(size_t)n + i] = dummy;
+  A.var[2 * (size_t)n + i] = V;
+}
+
+// ---------------------------------------------------------------------------
 // spike_generator (src/spike_generator.cu:49-67): compares against the per-call
 // step counter, at most one spike per step.
 // ---------------------------------------------------------------------------
@@ -360,6 +399,12 @@ int launch_iaf_multi(const IafArgs *tab, const int *blk0, int ngroups, int nbloc
                      const Clock *clk, int k0, int M, cudaStream_t st) {
   if (nblocks <= 0) return 0;
   iaf_multi_kernel<<<nblocks, 256, 0, st>>>(tab, blk0, ngroups, so, clk, k0, M);
+  return 1;
+}
+
+int launch_parrot(const ParrotArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
+  if (A.n <= 0) return 0;
+  parrot_batch_kernel<<<(A.n + 255) / 256, 256, 0, st>>>(A, so, clk, k0, M);
   return 1;
 }
 

@@ -72,6 +72,11 @@ void Engine::free_device() {
   ev_fork_ = ev_join_ = nullptr;
   plastic_ = false;
   stdp_ = StdpArgs{};
+  d_last_rev_ = nullptr;
+  d_den_steps_ = nullptr;
+  d_rev_ring_ = nullptr;
+  d_rev_cnt_ = nullptr;
+  rev_R_ = rev_cap_ = 0;
   pl_pos_.clear();
   pl_of_edge_.clear();
 }
@@ -118,7 +123,6 @@ void Engine::calibrate() {
     if (is_aeif(g.model)) {
       const int npp = n_port_par(g.model);
       for (int i = 0; i < g.n; i++) {
-        if (g.par[A_den_delay][i] != 0.0f) throw NgpuError("dendritic delay is not supported");
         g.par[A_refractory_step][i] = 0.0f;
         for (int p = 0; p < g.nport; p++) {
           auto P = [&](int k) -> float & { return g.par[A_NSCAL + npp * p + k][i]; };
@@ -143,7 +147,6 @@ void Engine::calibrate() {
       }
     } else if (g.model == M_IAF_PSC_EXP) {
       for (int i = 0; i < g.n; i++) {
-        if (g.par[I_den_delay][i] != 0.0f) throw NgpuError("dendritic delay is not supported");
         // src/iaf_psc_exp.cu:68-82, propagators in double precision
         const double h = dt, tau_m = g.par[I_tau_m][i], C_m = g.par[I_C_m][i];
         const double tau_ex = g.par[I_tau_ex][i], tau_in = g.par[I_tau_in][i];
@@ -342,10 +345,41 @@ void Engine::calibrate() {
   cuda_check(cudaMemset(d_clk_, 0, sizeof(Clock)), "clock");
   deliver_blocks_ = std::max(1, std::min(148 * 8, (n_src_out + 63) / 64));
   if (plastic_) build_plastic(pl_edge, pl_key, pl_rank);
+  // ---- dendritic delays: the reverse ring (plastic networks only; src/spike_buffer.cu:162-317)
+  if (plastic_) {
+    std::vector<int> den(N, 0);
+    int dmax_den = 0;
+    for (auto &g : groups_) {
+      int pi = -1;
+      if (is_aeif(g.model)) pi = A_den_delay;
+      else if (g.model == M_IAF_PSC_EXP) pi = I_den_delay;
+      else if (g.model == M_PARROT) pi = 1;
+      if (pi < 0) continue;
+      for (int i = 0; i < g.n; i++) {
+        // round(den_delay / dt) in float, as src/spike_buffer.cu:175-177
+        const int d = (int)std::round(g.par[pi][i] / dt);
+        if (d < 0) throw NgpuError("dendritic delay must be >= 0");
+        den[g.i0 + i] = d;
+        dmax_den = std::max(dmax_den, d);
+      }
+    }
+    d_last_rev_ = dalloc<int>(N);
+    cuda_check(cudaMemset(d_last_rev_, 0xff, (size_t)N * sizeof(int)), "last_rev");
+    stdp_.last_tidx = d_last_rev_;
+    if (dmax_den > 0) {
+      d_den_steps_ = dalloc<int>(N);
+      cuda_check(cudaMemcpy(d_den_steps_, den.data(), N * sizeof(int), cudaMemcpyHostToDevice), "den_delay");
+      rev_R_ = dmax_den + 2;
+      rev_cap_ = N;
+      d_rev_ring_ = dalloc<int>((size_t)rev_R_ * rev_cap_);
+      d_rev_cnt_ = dalloc<int>(rev_R_);
+      cuda_check(cudaMemset(d_rev_cnt_, 0, rev_R_ * sizeof(int)), "rev_cnt");
+    }
+  }
 
   // ---- per-group device state
   for (auto &g : groups_) {
-    if (is_aeif(g.model) || g.model == M_IAF_PSC_EXP) {
+    if (is_aeif(g.model) || g.model == M_IAF_PSC_EXP || g.model == M_PARROT) {
       const int nvar = (int)g.var.size();
       g.d_var = dalloc<float>((size_t)nvar * g.n);
       for (int v = 0; v < nvar; v++)
@@ -364,6 +398,10 @@ void Engine::calibrate() {
       g.d_h = dalloc<float>(g.n);
       cuda_check(cudaMemcpy(g.d_x, x.data(), g.n * sizeof(double), cudaMemcpyHostToDevice), "x");
       cuda_check(cudaMemcpy(g.d_h, h.data(), g.n * sizeof(float), cudaMemcpyHostToDevice), "h");
+    }
+    if (g.model == M_PARROT) {
+      g.d_hold = dalloc<float>(g.n);
+      cuda_check(cudaMemcpy(g.d_hold, g.par[0].data(), g.n * sizeof(float), cudaMemcpyHostToDevice), "hold");
     }
     if (g.spike_count_on) {
       g.d_spike_count = dalloc<int>(g.n);
@@ -437,6 +475,8 @@ void Engine::upload_params() {
     g.dirty = false;
     const int n = g.n;
     std::vector<float> v(n);
+    if (g.model == M_PARROT && g.d_hold)
+      cuda_check(cudaMemcpy(g.d_hold, g.par[0].data(), n * sizeof(float), cudaMemcpyHostToDevice), "hold");
     if (is_aeif(g.model)) {
       g.der_val.assign(AEIF_NPAR, 0.0f);
       g.d_der.assign(AEIF_NPAR, nullptr);
@@ -580,6 +620,12 @@ SpikeOut Engine::spike_out() const {
   so.last_height = d_last_h_;
   so.status = d_status_;
   so.n_spikes = d_counters_ + 2;
+  so.last_rev = d_last_rev_;
+  so.den_steps = d_den_steps_;
+  so.rev_ring = d_rev_ring_;
+  so.rev_cnt = d_rev_cnt_;
+  so.rev_R = rev_R_;
+  so.rev_cap = rev_cap_;
   return so;
 }
 
@@ -666,6 +712,19 @@ IafArgs Engine::iaf_args(Group &g) {
     A.pval[j] = g.der_val[j];
     A.parr[j] = g.d_der[j];
   }
+  return A;
+}
+
+ParrotArgs Engine::parrot_args(Group &g) {
+  ParrotArgs A;
+  A.n = g.n;
+  A.i0 = g.i0;
+  A.var = g.d_var;
+  A.hold = g.d_hold;
+  A.in = group_input(g);
+  A.rec = group_record(g);
+  A.dt = dt;
+  A.srec = spike_rec(g);
   return A;
 }
 
@@ -836,7 +895,7 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   for (auto &g : groups_) {
     if (g.n <= 0) continue;
     if (is_aeif(g.model)) has_aeif = true;
-    else if (g.model == M_IAF_PSC_EXP || g.model == M_SPIKE_GEN) has_other = true;
+    else if (g.model == M_IAF_PSC_EXP || g.model == M_SPIKE_GEN || g.model == M_PARROT) has_other = true;
   }
   const bool fork = has_aeif && has_other;
   cudaStream_t s2 = stream_;
@@ -851,6 +910,7 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
     if (g.model == M_IAF_PSC_EXP && n_iaf_multi_ < 2)
       count_launch(launch_iaf(iaf_args(g), so, d_clk_, k0, M, s2));
     else if (g.model == M_SPIKE_GEN) count_launch(launch_spike_gen(sg_args(g), so, d_clk_, k0, M, s2));
+    else if (g.model == M_PARROT) count_launch(launch_parrot(parrot_args(g), so, d_clk_, k0, M, s2));
   }
   for (auto &g : groups_)
     if (is_aeif(g.model)) count_launch(launch_aeif(g.model, aeif_args(g), so, d_clk_, k0, M, stream_));
@@ -860,6 +920,8 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   }
   // plastic edges (one step per batch): the step's arrivals, then its post-synaptic spikes
   if (plastic_) {
+    if (d_rev_ring_)
+      count_launch(launch_rev_arrivals(d_rev_ring_, d_rev_cnt_, rev_R_, rev_cap_, d_last_rev_, d_clk_, k0, stream_));
     count_launch(launch_stdp_forward(stdp_, d_clk_, k0, stream_));
     count_launch(launch_stdp_reverse(stdp_, d_clk_, k0, stream_));
   }

@@ -104,6 +104,27 @@ __global__ void stdp_reverse_kernel(const StdpArgs A, const Clock *clk, int k0) 
   }
 }
 
+// Spikes whose dendritic delay ends in step T reach their neuron's synapses: the reverse
+// ring slot of T gives last_rev = T (set at the start of step T in the reference,
+// src/spike_buffer.cu:314-316; only the plasticity passes after the update read it), and the
+// slot is emptied for T + rev_R.
+__global__ void rev_arrival_kernel(int *rev_ring, int *rev_cnt, int rev_R, int rev_cap, int *last_rev,
+                                   const Clock *clk, int k0) {
+  const long long T = step_tidx(clk, k0);
+  const int rs = (int)(T % rev_R);
+  int cnt = rev_cnt[rs];
+  cnt = cnt < rev_cap ? cnt : rev_cap;
+  for (int j = threadIdx.x; j < cnt; j += blockDim.x) last_rev[rev_ring[(size_t)rs * rev_cap + j]] = (int)T;
+  __syncthreads();
+  if (threadIdx.x == 0) rev_cnt[rs] = 0;
+}
+
+int launch_rev_arrivals(int *rev_ring, int *rev_cnt, int rev_R, int rev_cap, int *last_rev, const Clock *clk,
+                        int k0, cudaStream_t st) {
+  rev_arrival_kernel<<<1, 256, 0, st>>>(rev_ring, rev_cnt, rev_R, rev_cap, last_rev, clk, k0);
+  return 1;
+}
+
 int launch_stdp_reset(const StdpArgs &A, const Clock *clk, int k0, cudaStream_t st) {
   const long long nb = (A.n_pl + 255) / 256;
   stdp_stamp_reset_kernel<<<(int)(nb < 148 * 8 ? (nb > 0 ? nb : 1) : 148 * 8), 256, 0, st>>>(A, clk, k0);

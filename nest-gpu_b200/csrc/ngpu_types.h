@@ -16,6 +16,7 @@ enum Model {
   M_IAF_PSC_EXP,
   M_SPIKE_GEN,
   M_POISS_GEN,
+  M_PARROT,
   M_NMODEL
 };
 
@@ -58,6 +59,14 @@ struct SpikeOut {
   float *last_height;    // per node: height of the most recent spike
   unsigned *status;
   unsigned long long *n_spikes;
+  // plastic networks only (else last_rev is null): per node the time index at which its
+  // last spike reached its own synapses, set at once (no dendritic delay) or through the
+  // reverse ring den_steps[node] steps later
+  int *last_rev;
+  const int *den_steps;  // [n_nodes] or null (no dendritic delays)
+  int *rev_ring;         // [rev_R][rev_cap] nodes whose spike reaches their synapses then
+  int *rev_cnt;          // [rev_R]
+  int rev_R, rev_cap;
 };
 
 // Per-group spike bookkeeping (optional outputs).
@@ -165,6 +174,18 @@ struct IafArgs {
   GroupSpikeRec srec;
   float pval[IP_NPAR];
   const float *parr[IP_NPAR];
+};
+
+// parrot_neuron (src/parrot_neuron.cu:40-130): vars input_spike_height, dummy_input, V.
+struct ParrotArgs {
+  int n;
+  int i0;
+  float *var;            // SoA [3][n]
+  const float *hold;     // [n] hold_spike_height
+  GroupInput in;
+  GroupRecord rec;
+  float dt;
+  GroupSpikeRec srec;
 };
 
 struct SpikeGenArgs {

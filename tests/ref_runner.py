@@ -86,7 +86,10 @@ def main():
     what = sys.argv[1]
     ngpu.SetVerbosityLevel(0)
     out = {}
-    if what == "stdp_pairs":
+    if what.startswith("stdp_case:"):
+        from scenarios import stdp_case
+        out = {"weight": stdp_case(ngpu, int(what.split(":")[1]))}
+    elif what == "stdp_pairs":
         dts, w, exp = stdp_pair_scenario(ngpu)
         out = {"dt": list(dts), "weight": [float(x) for x in w], "expected": [float(x) for x in exp]}
     elif what.startswith("plastic:"):

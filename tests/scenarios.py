@@ -362,3 +362,38 @@ def stdp_case(api, case, w0=1.0, sim_time=20.0):
                 {"weight": w0, "delay": delay, "synapse_group": syn, "receptor": 1})
     api.Simulate(sim_time)
     return float(_conn_status(api, api.GetConnections(pre, post), "weight")[0])
+
+
+def parrot_scenario(api):
+    """Parrot neurons repeating spike-generator trains on port 0 (port 1 weighted 0), one with
+    hold_spike_height; returns (spike counts, recorded V columns)."""
+    sg = api.Create("spike_generator", 2)
+    p = api.Create("parrot_neuron", 3)
+    api.SetStatus([sg[0]], {"spike_times": [2.0, 5.0, 5.3, 9.9], "spike_heights": [2.0, 3.0, 1.0, 4.0]})
+    api.SetStatus([sg[1]], {"spike_times": [1.0, 4.0, 6.0]})
+    api.Connect(sg, p[0:1], {"rule": "all_to_all"}, {"weight": 1.0, "delay": 1.0})
+    api.Connect(sg, p[1:2], {"rule": "all_to_all"}, {"weight": 1.0, "delay": 1.0, "receptor": 1})
+    api.Connect(sg, p[2:3], {"rule": "all_to_all"}, {"weight": 0.5, "delay": 2.0})
+    api.SetStatus(p[2:3], {"hold_spike_height": 1.0})
+    api.ActivateSpikeCount(p)
+    rec = api.CreateRecord("", ["V", "V", "V", "input_spike_height"], [p[0], p[1], p[2], p[2]], [0, 0, 0, 0])
+    api.Simulate(15.0)
+    return np.asarray(api.GetStatus(p, "spike_count")).ravel(), np.asarray(api.GetRecordData(rec))
+
+
+def plastic_den_delay_network(api):
+    """plastic_network's aeif variant with dendritic delays of 0, 0.5 and 2 ms on the targets."""
+    orig_create = api.Create
+
+    class WithDen(object):
+        def __getattr__(self, name):
+            return getattr(api, name)
+
+        def Create(self, model, n=1, n_port=1, *args, **kw):
+            nodes = orig_create(model, n, n_port, *args, **kw)
+            if model == "aeif_cond_beta_multisynapse":
+                for i in range(n):
+                    api.SetStatus([nodes[i]], {"den_delay": [0.0, 0.5, 2.0][i % 3]})
+            return nodes
+
+    return plastic_network(WithDen())

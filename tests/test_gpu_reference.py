@@ -126,6 +126,17 @@ def stdp_pair_scenario_weight(dt_ms):
 
 
 @needs_ref
+@pytest.mark.parametrize("case", [1, 3, 5, 6, 8, 10])
+def test_stdp_cases_match_reference(case):
+    """The reference's STDP cases (parrot neurons, dendritic delays of 1 and 3 ms) run by the
+    reference build and by this engine: the same weight to 1e-6."""
+    from scenarios import stdp_case
+    ref = run_reference("stdp_case:%d" % case)
+    w = stdp_case(ngpu, case)
+    assert abs(w - ref["weight"]) <= 1e-6 * abs(ref["weight"])
+
+
+@needs_ref
 @pytest.mark.parametrize("model", ["aeif_cond_beta_multisynapse", "iaf_psc_exp"])
 def test_plastic_network_matches_reference(model):
     """A recurrent network with plastic excitatory edges under fixed input trains: spike counts

@@ -92,3 +92,32 @@ def test_stamp_wraparound_matches_oracle():
     w_orc = stdp_wrap_network(orc.Oracle())
     assert np.allclose(w, w_orc, rtol=1e-6, atol=1e-9)
     assert np.all(w.reshape(6, 4)[4] == 1.0)
+
+
+@pytest.mark.parametrize("case", list(range(1, 11)))
+def test_reference_stdp_cases(case):
+    """The reference's STDP cases (parrot neurons, dendritic delays): the closed form and the
+    oracle."""
+    from scenarios import stdp_case, stdp_case_expected
+    w = stdp_case(ngpu, case)
+    assert abs(w - stdp_case_expected(case)) < 1e-5
+    ngpu.Reset()
+    ngpu.SetVerbosityLevel(0)
+    assert abs(w - stdp_case(orc.Oracle(), case)) <= 1e-6 * abs(w)
+
+
+def test_parrot_neuron_matches_oracle():
+    from scenarios import parrot_scenario
+    c_gpu, r_gpu = parrot_scenario(ngpu)
+    c_orc, r_orc = parrot_scenario(orc.Oracle())
+    assert c_gpu.tolist() == c_orc.tolist() and c_gpu[1] == 0 and c_gpu[0] > 0
+    assert np.array_equal(np.float32(r_gpu), np.float32(r_orc))
+
+
+def test_plastic_network_with_dendritic_delays_matches_oracle():
+    from scenarios import plastic_den_delay_network
+    c_gpu, w_gpu = plastic_den_delay_network(ngpu)
+    c_orc, w_orc = plastic_den_delay_network(orc.Oracle())
+    assert c_gpu.sum() > 100
+    assert np.array_equal(c_gpu, c_orc)
+    assert np.allclose(w_gpu, w_orc, rtol=1e-6, atol=1e-9)
