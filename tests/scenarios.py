@@ -397,3 +397,26 @@ def plastic_den_delay_network(api):
             return nodes
 
     return plastic_network(WithDen())
+
+
+def syn_model_scenario(api, n=5, fact=0.2, offset=0.03):
+    """python/test/test_syn_model.py: pairs of neurons each firing once, the second dt_i after
+    the first's spike arrives through an edge of the linear test synapse model (weight 0, so
+    it changes nothing in the dynamics); the weight afterwards is dt_i * fact + offset."""
+    g = api.CreateSynGroup("test_syn_model", {"fact": fact, "offset": offset})
+    sg = api.Create("spike_generator", n)
+    neuron = api.Create("aeif_cond_beta_multisynapse", 2 * n)
+    api.SetStatus(neuron, {"t_ref": 10.0})
+    n0, n1 = neuron[0:n], neuron[n:2 * n]
+    dts = [0.1 * (i - 0.5 * (n - 1)) for i in range(n)]
+    api.SetStatus(sg, {"spike_times": [50.0], "spike_heights": [1.0]})
+    api.Connect(sg, n0, {"rule": "one_to_one"}, {"weight": 17.9, "delay": 1.0, "receptor": 0,
+                                                  "synapse_group": 0})
+    api.Connect(sg, n1, {"rule": "one_to_one"}, {"weight": 17.9, "delay": 11.0, "receptor": 0,
+                                                  "synapse_group": 0})
+    for i in range(n):
+        api.Connect([n0[i]], [n1[i]], {"rule": "one_to_one"},
+                    {"weight": 0.0, "delay": 10.0 - dts[i], "receptor": 0, "synapse_group": g})
+    api.Simulate(200.0)
+    w = np.asarray(_conn_status(api, api.GetConnections(n0, n1), "weight"), dtype=np.float64)
+    return w, np.asarray([d * fact + offset for d in dts])

@@ -214,3 +214,21 @@ def test_synapse_groups_and_plastic_connections():
     assert len(plastic) == 9
     assert all(ngpu.GetStatus(x)["syn"] == g.i_syn_group for x in plastic)
     ngpu.Reset()
+
+
+def test_syn_group_status_like_reference_log():
+    """python/test/test_syn_group.py against its log python/test/logp3_syn_group.txt: synapse
+    group parameters through CreateSynGroup / SetStatus / GetStatus / GetSynGroupParam."""
+    ngpu.Reset()
+    g = ngpu.CreateSynGroup("test_syn_model", {"fact": 1.0, "offset": 2.0})
+    assert ngpu.GetStatus(g) == {"fact": 1.0, "offset": 2.0}
+    ngpu.SetStatus(g, "fact", 3.0)
+    ngpu.SetStatus(g, "offset", 4.0)
+    assert ngpu.GetStatus(g) == {"fact": 3.0, "offset": 4.0}
+    ngpu.SetStatus(g, {"fact": 5.0, "offset": 6.0})
+    assert ngpu.GetStatus(g) == {"fact": 5.0, "offset": 6.0}
+    assert ngpu.GetSynGroupParam(g, "fact") == 5.0 and ngpu.GetSynGroupParam(g, "offset") == 6.0
+    assert ngpu.GetStatus(g, "fact") == 5.0 and ngpu.GetStatus(g, "offset") == 6.0
+    assert ngpu.GetStatus(g, ["fact", "offset"]) == [5.0, 6.0]
+    assert ngpu.GetStatus(g, ["offset", "fact"]) == [6.0, 5.0]
+    ngpu.Reset()

@@ -121,3 +121,10 @@ def test_plastic_network_with_dendritic_delays_matches_oracle():
     assert c_gpu.sum() > 100
     assert np.array_equal(c_gpu, c_orc)
     assert np.allclose(w_gpu, w_orc, rtol=1e-6, atol=1e-9)
+
+
+def test_linear_test_synapse_like_reference():
+    """python/test/test_syn_model.py on the GPU: w = dt * fact + offset within its 1e-6."""
+    from scenarios import syn_model_scenario
+    w, exp = syn_model_scenario(ngpu)
+    assert np.max(np.abs(w - exp)) < 1e-6

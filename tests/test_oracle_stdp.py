@@ -82,3 +82,10 @@ def test_parrot_neuron_repeats_port0_only():
     # the V column holds the repeated input in the step where the parrot fires
     assert sorted(set(np.round(v[:, 1], 3))) == [0.0, 2.0, 3.0]
     assert np.all(v[:, 2] == 0.0)
+
+
+def test_linear_test_synapse_like_reference():
+    """python/test/test_syn_model.py: w = dt * fact + offset within its 1e-6."""
+    from scenarios import syn_model_scenario
+    w, exp = syn_model_scenario(orc.Oracle())
+    assert np.max(np.abs(w - exp)) < 1e-6
