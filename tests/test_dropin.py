@@ -29,3 +29,27 @@ def test_reference_binding_drives_engine():
     assert ref == own
     assert ref["n_conn_nm"] == 15 * 4 and ref["n_conn_mn"] == 40
     assert ref["E_rev"][0] == [0.0, -85.0]
+
+
+REF_TEST = os.path.join(os.environ.get("NESTGPU_REF", "/root/reference"), "python", "test")
+
+
+def _clean(text):
+    banner = ("-- NEST GPU --", "Copyright", "This program is provided", "NO WARRANTY", "Homepage")
+    return [l.rstrip() for l in text.splitlines() if l.strip() and not any(b in l for b in banner)]
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_PY, "nestgpu.py")), reason="reference tree absent")
+@pytest.mark.parametrize("name", ["getarr", "setvar2", "syn_group"])
+def test_reference_api_scripts_reproduce_their_logs(name, tmp_path):
+    """The reference's own API test scripts (python/test/test_<name>.py), run unchanged through
+    its unchanged pythonlib/nestgpu.py on this library, print what their logs
+    (python/test/logp3_<name>.txt) hold.  No GPU is needed: none of them calibrates.
+    (logp3_setvar3.txt comes from an older library version, without den_delay among the
+    scalar parameters; test_group_param.py needs iaf_psc_exp_g, outside this engine.)"""
+    env = dict(os.environ, NESTGPU_LIB=LIB, PYTHONPATH=REF_PY)
+    p = subprocess.run([sys.executable, os.path.join(REF_TEST, "test_%s.py" % name)], env=env,
+                       capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
+    assert p.returncode == 0, p.stderr[-2000:]
+    with open(os.path.join(REF_TEST, "logp3_%s.txt" % name)) as f:
+        assert _clean(p.stdout) == _clean(f.read())
