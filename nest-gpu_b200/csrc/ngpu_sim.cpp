@@ -471,7 +471,9 @@ void Engine::upload_params() {
   bool gen_dirty = false;
   for (auto &g : groups_) {
     if (!g.dirty) continue;
-    any = true;
+    // aeif and iaf parameters can travel as kernel arguments, baked into the captured graphs;
+    // poiss_gen and parrot parameters live in device tables that the kernels read each step
+    if (is_aeif(g.model) || g.model == M_IAF_PSC_EXP) any = true;
     g.dirty = false;
     const int n = g.n;
     std::vector<float> v(n);
