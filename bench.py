@@ -289,7 +289,7 @@ def engine_arm(args):
     for _ in range(e2e_steps):
         ngpu.SetStatus(pg, "rate", PG_RATE)
         ngpu.Simulate(STEP_MS)
-        counts = ngpu.GetStatus(neuron, "spike_count")
+        counts = ngpu.GetSpikeCountArray(neuron)   # 4 MB device-to-host, as a NumPy array
     e2e_wall = time.time() - wall_e0
     e2e_events = ngpu.GetStats()["n_events"] - ev_e0
     e2e_t = max_over_ranks(e2e_wall)

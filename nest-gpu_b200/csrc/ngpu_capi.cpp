@@ -257,7 +257,17 @@ float *NESTGPU_GetArrayParam(int i_node, char *name) {
   return guard([&] { return malloc_copy(E().get_array_param(i_node, name)); }, (float *)nullptr);
 }
 int *NESTGPU_GetNeuronIntVar(int i_node, int n, char *name) {
-  return guard([&] { return malloc_copy(E().get_int_values(seq(i_node, n), name)); }, (int *)nullptr);
+  return guard([&] {
+    int *p = (int *)std::malloc(std::max<size_t>(n > 0 ? (size_t)n : 0, 1) * sizeof(int));
+    if (!p) throw std::bad_alloc();
+    try {
+      E().get_int_values_seq(i_node, n, name, p);
+    } catch (...) {
+      std::free(p);
+      throw;
+    }
+    return p;
+  }, (int *)nullptr);
 }
 int *NESTGPU_GetNeuronPtIntVar(int *i_node, int n, char *name) {
   return guard([&] {

@@ -486,6 +486,26 @@ std::vector<int> Engine::get_int_values(const std::vector<int> &nodes, const std
   return out;
 }
 
+void Engine::get_int_values_seq(int i0, int n, const std::string &name, int *out) {
+  if (n <= 0) throw NgpuError("Empty node list");
+  Group &g = group_of(i0);
+  if (group_index(i0 + n - 1) != group_index(i0))
+    throw NgpuError("Nodes belong to different node groups in setting parameter");
+  int idx;
+  Kind k = locate(i0, name, &idx);
+  if (k != K_INT_VAR) throw NgpuError("Unrecognized integer variable " + name);
+  int *d = idx == 0 ? g.d_spike_count : g.d_n_rec;
+  if (d) {
+    cudaStreamSynchronize(stream_);
+    if (cudaMemcpy(out, d + (i0 - g.i0), (size_t)n * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      throw NgpuError("CUDA error");
+  } else {
+    std::memset(out, 0, (size_t)n * sizeof(int));
+  }
+  if (idx == 1)
+    for (int i = 0; i < n; i++) out[i] += (int)g.rec_times_host[i0 - g.i0 + i].size();
+}
+
 std::vector<float> Engine::get_array_param(int node, const std::string &name) {
   Group &g = group_of(node);
   int idx;

@@ -151,6 +151,8 @@ class Engine {
   void set_int_var(const std::vector<int> &nodes, const std::string &name, int v);
   std::vector<float> get_values(const std::vector<int> &nodes, const std::string &name);   // node-major
   std::vector<int> get_int_values(const std::vector<int> &nodes, const std::string &name);
+  // nodes i0 .. i0+n-1 of one group, copied straight into out (n ints)
+  void get_int_values_seq(int i0, int n, const std::string &name, int *out);
   std::vector<float> get_array_param(int node, const std::string &name);
   void set_group_param(const std::vector<int> &nodes, const std::string &name, float v);
   float get_group_param(int node, const std::string &name);

@@ -533,6 +533,19 @@ def GetNeuronVar(i_node, n_node, var_name):
     return _rows(pt, n_node, GetNeuronVarSize(i_node, var_name))
 
 
+def GetSpikeCountArray(nodes):
+    """Spike counts of a node sequence as a NumPy int32 array (engine extension): the same
+    device-to-host copy as GetStatus(nodes, "spike_count"), without building a Python list,
+    for callers that read the counts of many neurons every call."""
+    import numpy as np
+    i0, n = _seq_args(nodes)
+    pt = _c["NESTGPU_GetNeuronIntVar"](i0, n, _b("spike_count"))
+    _check()
+    out = np.ctypeslib.as_array(pt, shape=(n,)).copy() if n > 0 else np.zeros(0, dtype=np.int32)
+    _free(pt)
+    return out
+
+
 def GetNeuronPtIntVar(nodes, var_name):
     pt_n, n = _int_arr(nodes)
     pt = _c["NESTGPU_GetNeuronPtIntVar"](pt_n, n, _b(var_name))

@@ -375,3 +375,10 @@ def test_generator_rate_change_between_calls():
     for a, b in zip(c_gpu, c_orc):
         assert np.array_equal(a, b)
     assert c_gpu[1].sum() - c_gpu[0].sum() > c_gpu[0].sum()   # the higher rate shows
+
+
+def test_spike_count_array_equals_status_list():
+    ngpu.SetHostRng(True)
+    c_list, _ = fixed_train_network(ngpu, model="aeif_cond_beta_multisynapse", t_sim=100.0, record=False)
+    arr = ngpu.GetSpikeCountArray(ngpu.NodeSeq(0, c_list.size))   # the network's neurons come first
+    assert arr.dtype == np.int32 and np.array_equal(arr, c_list) and arr.sum() > 0
