@@ -347,6 +347,41 @@ __device__ __forceinline__ float mlp_propose(const float *M, const float *f) {
   return __fmul_rn(M[SM_SAFETY], exp_m(__fmaf_rn(o, M[SM_LSIG], M[SM_LMU])));
 }
 
+// Stage combination r[i] = y[i] + b1 k1[i] + ... + bK kK[i] as the FMA chain innermost-first,
+// two state variables per instruction with sm_100's packed FP32 FMA. Each lane of __ffma2_rn
+// is rounded exactly as the scalar __fmaf_rn, so r is bit for bit the scalar chain's. A pair
+// whose upper variable lies past NV (odd variable count) computes an unused upper lane.
+// PAIR = false keeps one variable per instruction (the groups with a runtime port count, whose
+// arrays do not fit in registers either way).
+template <int NVM, int K, bool PAIR>
+__device__ __forceinline__ void stage_comb(float *r, const float *y, int NV, const float *k1, float b1,
+                                           const float *k2 = nullptr, float b2 = 0.0f,
+                                           const float *k3 = nullptr, float b3 = 0.0f,
+                                           const float *k4 = nullptr, float b4 = 0.0f,
+                                           const float *k5 = nullptr, float b5 = 0.0f) {
+#pragma unroll
+  for (int i = 0; i < NVM; i += (PAIR ? 2 : 1)) {
+    if (i < NV) {
+      if (PAIR && i + 1 < NVM) {
+        float2 a = __ffma2_rn(make_float2(b1, b1), make_float2(k1[i], k1[i + 1]), make_float2(y[i], y[i + 1]));
+        if (K > 1) a = __ffma2_rn(make_float2(b2, b2), make_float2(k2[i], k2[i + 1]), a);
+        if (K > 2) a = __ffma2_rn(make_float2(b3, b3), make_float2(k3[i], k3[i + 1]), a);
+        if (K > 3) a = __ffma2_rn(make_float2(b4, b4), make_float2(k4[i], k4[i + 1]), a);
+        if (K > 4) a = __ffma2_rn(make_float2(b5, b5), make_float2(k5[i], k5[i + 1]), a);
+        r[i] = a.x;
+        r[i + 1] = a.y;
+      } else {
+        float a = __fmaf_rn(b1, k1[i], y[i]);
+        if (K > 1) a = __fmaf_rn(b2, k2[i], a);
+        if (K > 2) a = __fmaf_rn(b3, k3[i], a);
+        if (K > 3) a = __fmaf_rn(b4, k4[i], a);
+        if (K > 4) a = __fmaf_rn(b5, k5[i], a);
+        r[i] = a;
+      }
+    }
+  }
+}
+
 // One accepted RK5 step (src/rk5.h:69-159); returns the number of derivative evaluations.
 // The error scale y_scal uses the h entering the step (the plain controller's), as in
 // the reference, whatever the learned proposal chooses as the first trial.
@@ -382,67 +417,47 @@ __device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmi
     if (h > hmax) h = hmax;
     if (h < hmin) h = hmin;
     // each stage's coefficients h * a_ij are formed just before the stage (short live ranges)
-    {
-      const float b21 = __fmul_rn(h, ck::a21);
-#pragma unroll
-      for (int i = 0; i < NVM; i++)
-        if (i < NV) yn[i] = __fmaf_rn(b21, k1[i], y[i]);
-    }
+    stage_comb<NVM, 1, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a21));
     aeif_derivs(yn, k2, q, refr);
-    {
-      const float b31 = __fmul_rn(h, ck::a31), b32 = __fmul_rn(h, ck::a32);
-#pragma unroll
-      for (int i = 0; i < NVM; i++)
-        if (i < NV) yn[i] = __fmaf_rn(b32, k2[i], __fmaf_rn(b31, k1[i], y[i]));
-    }
+    stage_comb<NVM, 2, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a31), k2, __fmul_rn(h, ck::a32));
     aeif_derivs(yn, k3, q, refr);
-    {
-      const float b41 = __fmul_rn(h, ck::a41), b42 = __fmul_rn(h, ck::a42), b43 = __fmul_rn(h, ck::a43);
-#pragma unroll
-      for (int i = 0; i < NVM; i++)
-        if (i < NV) yn[i] = __fmaf_rn(b43, k3[i], __fmaf_rn(b42, k2[i], __fmaf_rn(b41, k1[i], y[i])));
-    }
+    stage_comb<NVM, 3, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a41), k2, __fmul_rn(h, ck::a42), k3,
+                       __fmul_rn(h, ck::a43));
     aeif_derivs(yn, k4, q, refr);
-    {
-      const float b51 = __fmul_rn(h, ck::a51), b52 = __fmul_rn(h, ck::a52), b53 = __fmul_rn(h, ck::a53),
-                  b54 = __fmul_rn(h, ck::a54);
-#pragma unroll
-      for (int i = 0; i < NVM; i++)
-        if (i < NV)
-          yn[i] = __fmaf_rn(b54, k4[i],
-                            __fmaf_rn(b53, k3[i], __fmaf_rn(b52, k2[i], __fmaf_rn(b51, k1[i], y[i]))));
-    }
+    stage_comb<NVM, 4, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a51), k2, __fmul_rn(h, ck::a52), k3,
+                       __fmul_rn(h, ck::a53), k4, __fmul_rn(h, ck::a54));
     aeif_derivs(yn, k5, q, refr);
-    {
-      const float b61 = __fmul_rn(h, ck::a61), b62 = __fmul_rn(h, ck::a62), b63 = __fmul_rn(h, ck::a63),
-                  b64 = __fmul_rn(h, ck::a64), b65 = __fmul_rn(h, ck::a65);
-#pragma unroll
-      for (int i = 0; i < NVM; i++)
-        if (i < NV)
-          yn[i] = __fmaf_rn(b65, k5[i],
-                            __fmaf_rn(b64, k4[i], __fmaf_rn(b63, k3[i],
-                                                            __fmaf_rn(b62, k2[i], __fmaf_rn(b61, k1[i], y[i])))));
-    }
+    stage_comb<NVM, 5, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a61), k2, __fmul_rn(h, ck::a62), k3,
+                       __fmul_rn(h, ck::a63), k4, __fmul_rn(h, ck::a64), k5, __fmul_rn(h, ck::a65));
     aeif_derivs(yn, k6, q, refr);
-    {
-      const float b71 = __fmul_rn(h, ck::a71), b73 = __fmul_rn(h, ck::a73), b74 = __fmul_rn(h, ck::a74),
-                  b76 = __fmul_rn(h, ck::a76);
-#pragma unroll
-      for (int i = 0; i < NVM; i++)
-        if (i < NV)
-          yn[i] = __fmaf_rn(b76, k6[i],
-                            __fmaf_rn(b74, k4[i], __fmaf_rn(b73, k3[i], __fmaf_rn(b71, k1[i], y[i]))));
-    }
+    stage_comb<NVM, 4, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a71), k3, __fmul_rn(h, ck::a73), k4,
+                       __fmul_rn(h, ck::a74), k6, __fmul_rn(h, ck::a76));
     const float f1 = __fmul_rn(h, ck::e1), f3 = __fmul_rn(h, ck::e3), f4 = __fmul_rn(h, ck::e4),
                 f5 = __fmul_rn(h, ck::e5), f6 = __fmul_rn(h, ck::e6);
+    // error terms two variables at a time (lane-exact, as in stage_comb)
     err = 0.0f;
 #pragma unroll
-    for (int i = 0; i < NVM; i++) {
+    for (int i = 0; i < NVM; i += (FIXED ? 2 : 1)) {
       if (i < NV) {
-        float v = __fmaf_rn(f6, k6[i], __fmaf_rn(f5, k5[i], __fmaf_rn(f4, k4[i],
-                                                                      __fmaf_rn(f3, k3[i], __fmul_rn(f1, k1[i])))));
-        float av = fabsf(__fmul_rn(v, iys[i]));
-        err = (err > av) ? err : av;
+        if (FIXED && i + 1 < NVM) {
+          float2 v = __fmul2_rn(make_float2(f1, f1), make_float2(k1[i], k1[i + 1]));
+          v = __ffma2_rn(make_float2(f3, f3), make_float2(k3[i], k3[i + 1]), v);
+          v = __ffma2_rn(make_float2(f4, f4), make_float2(k4[i], k4[i + 1]), v);
+          v = __ffma2_rn(make_float2(f5, f5), make_float2(k5[i], k5[i + 1]), v);
+          v = __ffma2_rn(make_float2(f6, f6), make_float2(k6[i], k6[i + 1]), v);
+          v = __fmul2_rn(v, make_float2(iys[i], iys[i + 1]));
+          const float a0 = fabsf(v.x);
+          err = (err > a0) ? err : a0;
+          if (i + 1 < NV) {
+            const float a1 = fabsf(v.y);
+            err = (err > a1) ? err : a1;
+          }
+        } else {
+          float v = __fmaf_rn(f6, k6[i], __fmaf_rn(f5, k5[i], __fmaf_rn(f4, k4[i],
+                                                                        __fmaf_rn(f3, k3[i], __fmul_rn(f1, k1[i])))));
+          float av = fabsf(__fmul_rn(v, iys[i]));
+          err = (err > av) ? err : av;
+        }
       }
     }
     err = __fmul_rn(err, ck::inv_eps);
