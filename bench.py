@@ -64,7 +64,8 @@ def parse():
     p.add_argument("--no-autotune", action="store_true", help="keep the default launch mappings")
     p.add_argument("--mapping", default="",
                    help="fixed launch mapping instead of the autotuner: update threads, register-capped "
-                        "variant (0/1), delivery lane group, delivery blocks, RK5 budget, e.g. 64,1,32,592,1")
+                        "variant (0/1), delivery lane group, delivery blocks, RK5 budget and optionally "
+                        "programmatic launch (0/1), e.g. 64,1,32,592,1")
     p.add_argument("--batch-max", type=int, default=0, help="upper bound of the time-batch length")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the learned-step and ensemble measurements")
@@ -217,7 +218,10 @@ def engine_arm(args):
     # launch mappings picked on this network (the trial steps are part of the transient)
     t_tune0 = time.time()
     if args.mapping:
-        th, occ, grp, blk, bud = (int(x) for x in args.mapping.split(","))
+        vals = [int(x) for x in args.mapping.split(",")]
+        th, occ, grp, blk, bud = vals[:5]
+        if len(vals) > 5:
+            ngpu.SetProgrammaticLaunch(vals[5])
         ngpu.SetUpdateThreads(th)
         ngpu.SetUpdateOccupancy(occ)
         ngpu.SetDeliverGroup(grp)

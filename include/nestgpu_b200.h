@@ -317,6 +317,13 @@ int NGPU_SetDeliverGroup(int g);
    waits); 0 (default): per-batch launches in CUDA graphs.  Results are the same either way; the
    autotuner tries both. */
 int NGPU_SetPersistent(int on);
+/* 1: the kernels of a time batch are launched with programmatic stream serialization, so each
+   kernel's launch and block scheduling overlap the end of the kernel before it (every such
+   kernel first waits for its predecessor's completion and memory, so results are the same);
+   used where the batch is one chain of kernels on one stream (not with plastic synapses or
+   with aeif and other spiking groups together).  0 (default): plain stream order.  The
+   autotuner tries both.  No counterpart in the reference. */
+int NGPU_SetProgrammaticLaunch(int on);
 /* Test hook for the failure path of the persistent loop: with extra > 0 its grid barriers wait
    for more blocks than the launch has, so each wait runs out after its bounded number of polls
    (a second or two); the kernel records the timeout and returns, and the Simulate call fails
@@ -331,9 +338,9 @@ int NGPU_TestBarrierTimeout(int extra);
    values. */
 int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliver_blocks,
                   int *rk5_budget);
-/* The current launch mapping: writes min(n, 6) of {update block size, register-capped update
-   variant, delivery lane group, delivery grid (0: automatic), RK5 step budget, persistent loop}
-   and returns 6 (-1 on error).  No counterpart in the reference. */
+/* The current launch mapping: writes min(n, 7) of {update block size, register-capped update
+   variant, delivery lane group, delivery grid (0: automatic), RK5 step budget, persistent loop,
+   programmatic launch} and returns 7 (-1 on error).  No counterpart in the reference. */
 int NGPU_GetLaunchMapping(int *vals, int n);
 /* Measured rate (1e9 per second) of FP64 reductions to uniformly random addresses of a
    `bytes`-byte device buffer, `n_ops` in total: the access pattern of the spike delivery's

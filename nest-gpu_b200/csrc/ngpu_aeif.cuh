@@ -38,6 +38,39 @@ constexpr int max_trials = 100000;
 constexpr int max_substeps = 1000000;
 }  // namespace ck
 
+// Programmatic dependent launch. A kernel launched with programmatic stream serialization
+// may be scheduled while its predecessor in the stream still runs. Every kernel of the step
+// loop therefore first waits until its predecessor grid has completed and its memory is
+// visible, and only then lets its own successor be scheduled; before the wait it touches no
+// global memory. So the order of memory effects is that of plain stream order, and what
+// overlaps is the launch and block scheduling of the next kernel. Without the launch
+// attribute both instructions do nothing.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Set by the engine around the launches of one time batch (ngpu_kernels.cu).
+extern bool g_launch_pdl;
+
+// kern<<<grid, block, smem, st>>>(args...), with programmatic stream serialization when
+// g_launch_pdl is set.
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                     Args... args) {
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = g_launch_pdl ? at : nullptr;
+  cfg.numAttrs = g_launch_pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 // Step `m` of the batch starting at graph step k0.
 struct StepT {
   long long it, tidx;
@@ -613,6 +646,7 @@ __device__ __forceinline__ void warp_add(unsigned long long *ctr, unsigned long 
 template <int MODEL, int PMAX, bool FIXED, int LM, int OCC = 0, bool UNI = false>
 __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const AeifArgs A, const SpikeOut so,
                                                          const Clock *clk, int k0, int M) {
+  pdl_enter();
   typedef AeifShape<MODEL> S;
   constexpr int NVM = 2 + S::npv * PMAX;
   __shared__ float smodel[LM == LM_PROPOSE ? SM_NPAR : 1];
@@ -671,6 +705,7 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
 template <int MODEL, int PMAX, bool FIXED, int LM, bool UNI = false>
 __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, const SpikeOut so,
                                                              const Clock *clk, int k0, int M) {
+  pdl_enter();
   typedef AeifShape<MODEL> S;
   constexpr int NVM = 2 + S::npv * PMAX;
   __shared__ float smodel[LM == LM_PROPOSE ? SM_NPAR : 1];
@@ -722,27 +757,27 @@ int launch_aeif_p(const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k
   bool done = false;
   if constexpr (LM == LM_PLAIN && FIXED) {
     if (A.occupancy && A.uniform) {
-      aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1, true><<<grid, block, 0, st>>>(A, so, clk, k0, M);
+      launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1, true>, grid, block, 0, st, A, so, clk, k0, M);
       done = true;
     } else if (A.occupancy) {
-      aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1><<<grid, block, 0, st>>>(A, so, clk, k0, M);
+      launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1>, grid, block, 0, st, A, so, clk, k0, M);
       done = true;
     } else if (A.uniform) {
-      aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0, true><<<grid, block, 0, st>>>(A, so, clk, k0, M);
+      launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0, true>, grid, block, 0, st, A, so, clk, k0, M);
       done = true;
     }
   }
-  if (!done) aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0><<<grid, block, 0, st>>>(A, so, clk, k0, M);
+  if (!done) launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0>, grid, block, 0, st, A, so, clk, k0, M);
   if (A.budget <= 0) return 1;
   dim3 sgrid(A.n < 128 * 148 * 4 ? (A.n + 127) / 128 : 148 * 4), sblock(128);
   done = false;
   if constexpr (LM == LM_PLAIN && FIXED) {
     if (A.uniform) {
-      aeif_straggler_kernel<MODEL, PMAX, FIXED, LM, true><<<sgrid, sblock, 0, st>>>(A, so, clk, k0, M);
+      launch_k(aeif_straggler_kernel<MODEL, PMAX, FIXED, LM, true>, sgrid, sblock, 0, st, A, so, clk, k0, M);
       done = true;
     }
   }
-  if (!done) aeif_straggler_kernel<MODEL, PMAX, FIXED, LM><<<sgrid, sblock, 0, st>>>(A, so, clk, k0, M);
+  if (!done) launch_k(aeif_straggler_kernel<MODEL, PMAX, FIXED, LM>, sgrid, sblock, 0, st, A, so, clk, k0, M);
   return 2;
 }
 

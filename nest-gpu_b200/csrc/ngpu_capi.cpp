@@ -797,6 +797,14 @@ int NGPU_SetPersistent(int on) {
   }, -1);
 }
 
+int NGPU_SetProgrammaticLaunch(int on) {
+  return guard([&] {
+    E().launch_pdl = on ? 1 : 0;
+    E().invalidate_graphs();
+    return 0;
+  }, -1);
+}
+
 int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliver_blocks, int *rk5_budget) {
   return guard([&] {
     const int n = E().autotune(steps, nullptr);
@@ -810,10 +818,10 @@ int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliv
 
 int NGPU_GetLaunchMapping(int *vals, int n) {
   return guard([&] {
-    const int v[6] = {E().update_threads, E().update_occupancy, E().deliver_group, E().deliver_blocks_req,
-                      E().rk5_budget, E().persistent};
-    for (int i = 0; i < n && i < 6; i++) vals[i] = v[i];
-    return 6;
+    const int v[7] = {E().update_threads, E().update_occupancy, E().deliver_group, E().deliver_blocks_req,
+                      E().rk5_budget, E().persistent, E().launch_pdl};
+    for (int i = 0; i < n && i < 7; i++) vals[i] = v[i];
+    return 7;
   }, -1);
 }
 

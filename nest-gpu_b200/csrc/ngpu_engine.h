@@ -129,6 +129,7 @@ class Engine {
   int deliver_group = 32;         // lanes per delivery work item (8, 16, 32)
   int update_occupancy = 0;       // 1: register-capped aeif update kernel
   int persistent = 0;             // iaf-only networks: persistent cooperative step loop
+  int launch_pdl = 0;             // programmatic dependent launch of the batch kernels
   int barrier_extra = 0;          // test hook: blocks the persistent loop's barriers wait for in excess
   bool use_device_rng = true;     // cuRAND device generator (as the reference) if a GPU exists
 
@@ -393,6 +394,7 @@ int launch_rev_arrivals(int *rev_ring, int *rev_cnt, int rev_R, int rev_cap, int
 int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *clk, int k0, int M,
                    cudaStream_t st);
 int launch_clock_advance(Clock *clk, int K, cudaStream_t st);
+void set_launch_pdl(bool on);
 // reduction-rate probe (ngpu_probe.cu): 1e9 random FP64 reductions per second
 double measure_random_reduction_rate(size_t bytes, long long n_ops);
 // STDP (ngpu_stdp.cu)

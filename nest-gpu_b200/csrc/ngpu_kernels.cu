@@ -23,6 +23,9 @@
 
 namespace ngpu {
 
+bool g_launch_pdl = false;
+void set_launch_pdl(bool on) { g_launch_pdl = on; }
+
 // ---------------------------------------------------------------------------
 // iaf_psc_exp exact propagator (src/iaf_psc_exp.cu:85-110)
 // ---------------------------------------------------------------------------
@@ -77,6 +80,7 @@ __device__ __forceinline__ void iaf_neuron(const IafArgs &A, const SpikeOut &so,
 
 __global__ void __launch_bounds__(256, 3) iaf_batch_kernel(const IafArgs A, const SpikeOut so,
                                                         const Clock *clk, int k0, int M) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < A.n) iaf_neuron(A, so, clk, k0, M, i);
 }
@@ -88,6 +92,7 @@ __global__ void __launch_bounds__(256, 3) iaf_batch_kernel(const IafArgs A, cons
 // keeps the 77k-neuron microcircuit's 302 blocks from spilling into a second wave.
 __global__ void __launch_bounds__(256, 3) iaf_multi_kernel(const IafArgs *tab, const int *blk0, int ngroups,
                                                         const SpikeOut so, const Clock *clk, int k0, int M) {
+  pdl_enter();
   int lo = 0, hi = ngroups;   // largest g with blk0[g] <= blockIdx.x
   while (hi - lo > 1) {
     const int mid = (lo + hi) >> 1;
@@ -105,6 +110,7 @@ __global__ void __launch_bounds__(256, 3) iaf_multi_kernel(const IafArgs *tab, c
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) parrot_batch_kernel(const ParrotArgs A, const SpikeOut so, const Clock *clk,
                                                            int k0, int M) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
   const int n = A.n;
@@ -143,6 +149,7 @@ __global__ void __launch_bounds__(256) parrot_batch_kernel(const ParrotArgs A, c
 // ---------------------------------------------------------------------------
 __global__ void spike_gen_batch_kernel(const SpikeGenArgs A, const SpikeOut so, const Clock *clk, int k0,
                                        int M) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
   const int e0 = A.off[i], e1 = A.off[i + 1];
@@ -257,12 +264,16 @@ __device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock 
 template <int G>
 __global__ void __launch_bounds__(DELIVER_THREADS) deliver_batch_kernel(const DeliverArgs A,
                                                                         const Clock *clk, int k0, int M) {
+  pdl_enter();
   extern __shared__ int s_pref[];   // npairs + 1 prefix sums over (delay group, arrival step)
   __shared__ typename DeliverScan::TempStorage scan_tmp;
   deliver_batch<G>(A, clk, k0, M, s_pref, scan_tmp, blockIdx.x, gridDim.x);
 }
 
-__global__ void clock_advance_kernel(Clock *clk, int K) { clk->it0 += K; }
+__global__ void clock_advance_kernel(Clock *clk, int K) {
+  pdl_enter();
+  clk->it0 += K;
+}
 
 // ---------------------------------------------------------------------------
 // Persistent step loop for networks whose neurons are all iaf_psc_exp.  One
@@ -391,41 +402,42 @@ int launch_aeif(int model, const AeifArgs &A, const SpikeOut &so, const Clock *c
 
 int launch_iaf(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
   if (A.n <= 0) return 0;
-  iaf_batch_kernel<<<(A.n + 255) / 256, 256, 0, st>>>(A, so, clk, k0, M);
+  launch_k(iaf_batch_kernel, dim3((A.n + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
   return 1;
 }
 
 int launch_iaf_multi(const IafArgs *tab, const int *blk0, int ngroups, int nblocks, const SpikeOut &so,
                      const Clock *clk, int k0, int M, cudaStream_t st) {
   if (nblocks <= 0) return 0;
-  iaf_multi_kernel<<<nblocks, 256, 0, st>>>(tab, blk0, ngroups, so, clk, k0, M);
+  launch_k(iaf_multi_kernel, dim3(nblocks), dim3(256), 0, st, tab, blk0, ngroups, so, clk, k0, M);
   return 1;
 }
 
 int launch_parrot(const ParrotArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
   if (A.n <= 0) return 0;
-  parrot_batch_kernel<<<(A.n + 255) / 256, 256, 0, st>>>(A, so, clk, k0, M);
+  launch_k(parrot_batch_kernel, dim3((A.n + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
   return 1;
 }
 
 int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                      cudaStream_t st) {
   if (A.n <= 0) return 0;
-  spike_gen_batch_kernel<<<(A.n + 255) / 256, 256, 0, st>>>(A, so, clk, k0, M);
+  launch_k(spike_gen_batch_kernel, dim3((A.n + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
   return 1;
 }
 
 int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *clk, int k0, int M,
                    cudaStream_t st) {
   const size_t smem = (size_t)(A.dspan * M + 1) * sizeof(int);
-  if (group == 8) deliver_batch_kernel<8><<<n_blocks, DELIVER_THREADS, smem, st>>>(A, clk, k0, M);
-  else if (group == 16) deliver_batch_kernel<16><<<n_blocks, DELIVER_THREADS, smem, st>>>(A, clk, k0, M);
-  else deliver_batch_kernel<32><<<n_blocks, DELIVER_THREADS, smem, st>>>(A, clk, k0, M);
+  const dim3 g(n_blocks), b(DELIVER_THREADS);
+  if (group == 8) launch_k(deliver_batch_kernel<8>, g, b, smem, st, A, clk, k0, M);
+  else if (group == 16) launch_k(deliver_batch_kernel<16>, g, b, smem, st, A, clk, k0, M);
+  else launch_k(deliver_batch_kernel<32>, g, b, smem, st, A, clk, k0, M);
   return 1;
 }
 
 int launch_clock_advance(Clock *clk, int K, cudaStream_t st) {
-  clock_advance_kernel<<<1, 1, 0, st>>>(clk, K);
+  launch_k(clock_advance_kernel, dim3(1), dim3(1), 0, st, clk, K);
   return 1;
 }
 

@@ -884,11 +884,6 @@ void Engine::build_plastic(const std::vector<size_t> &pl_edge, const std::vector
 // One batch of M steps starting at graph step k0: delivery, then every group.
 void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   SpikeOut so = spike_out();
-  if (ev) cuda_check(cudaEventRecord((*ev)[0], stream_), "event");
-  if (plastic_) count_launch(launch_stdp_reset(stdp_, d_clk_, k0, stream_));
-  count_launch(launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_,
-                              deliver_group, d_clk_, k0, M, stream_));
-  if (ev) cuda_check(cudaEventRecord((*ev)[1], stream_), "event");
   // With aeif groups and other spiking groups in the network, the others run on a second
   // stream next to the aeif kernels: they then fill the SMs that the aeif straggler tail
   // leaves idle.  The groups touch disjoint state (their own accumulator rows, node
@@ -900,6 +895,14 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
     else if (g.model == M_IAF_PSC_EXP || g.model == M_SPIKE_GEN || g.model == M_PARROT) has_other = true;
   }
   const bool fork = has_aeif && has_other;
+  // Programmatic dependent launch where the batch is one chain of kernels on one stream
+  // (no event edges between streams, no plastic-edge kernels, no per-kernel timing events).
+  set_launch_pdl(launch_pdl && !fork && !plastic_ && !ev);
+  if (ev) cuda_check(cudaEventRecord((*ev)[0], stream_), "event");
+  if (plastic_) count_launch(launch_stdp_reset(stdp_, d_clk_, k0, stream_));
+  count_launch(launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_,
+                              deliver_group, d_clk_, k0, M, stream_));
+  if (ev) cuda_check(cudaEventRecord((*ev)[1], stream_), "event");
   cudaStream_t s2 = stream_;
   if (fork) {
     cuda_check(cudaEventRecord(ev_fork_, stream_), "fork");
@@ -928,6 +931,7 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
     count_launch(launch_stdp_reverse(stdp_, d_clk_, k0, stream_));
   }
   if (ev) cuda_check(cudaEventRecord((*ev)[2], stream_), "event");
+  set_launch_pdl(false);
 }
 
 // Argument table of the iaf groups for the single multi-group launch; rebuilt before
@@ -1276,6 +1280,7 @@ int Engine::autotune(int steps, std::vector<std::pair<std::string, double>> *log
       single("update_occupancy", &update_occupancy, {0, 1}),
       deliver,
       single("rk5_budget", &rk5_budget, {0, 1, 2, 4, 8}),
+      single("programmatic_launch", &launch_pdl, {0, 1}),
   };
   if (persistent_eligible()) knobs.insert(knobs.begin(), single("persistent", &persistent, {0, 1}));
   if (deliver_blocks_req <= 0) deliver_blocks_req = base;

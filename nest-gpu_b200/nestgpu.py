@@ -172,6 +172,7 @@ if is_b200_engine:
     _c["NGPU_SetBatchMax"] = _bind("NGPU_SetBatchMax", _I, [_I])
     _c["NGPU_SetUpdateThreads"] = _bind("NGPU_SetUpdateThreads", _I, [_I])
     _c["NGPU_SetDeliverGroup"] = _bind("NGPU_SetDeliverGroup", _I, [_I])
+    _c["NGPU_SetProgrammaticLaunch"] = _bind("NGPU_SetProgrammaticLaunch", _I, [_I])
     _c["NGPU_SetUpdateOccupancy"] = _bind("NGPU_SetUpdateOccupancy", _I, [_I])
     _c["NGPU_GetBatchLength"] = _bind("NGPU_GetBatchLength", _I, [])
     _c["NGPU_SetPersistent"] = _bind("NGPU_SetPersistent", _I, [_I])
@@ -1423,6 +1424,13 @@ def SetDeliverGroup(g):
     return _check(_c["NGPU_SetDeliverGroup"](g))
 
 
+def SetProgrammaticLaunch(on=True):
+    """Programmatic dependent launch of the kernels of a time batch (engine extension;
+    results are the same either way)."""
+    _need_b200("SetProgrammaticLaunch")
+    return _check(_c["NGPU_SetProgrammaticLaunch"](1 if on else 0))
+
+
 def Autotune(steps=200):
     """Pick the update block size, delivery lane group, delivery grid and RK5 step budget
     by timing `steps` simulation steps per candidate on the calibrated network (the network
@@ -1447,13 +1455,13 @@ def MeasureReductionRate(nbytes, n_ops):
 
 def GetLaunchMapping():
     """The current launch mapping (engine extension): update block size and variant, delivery
-    lane group and grid, RK5 step budget and persistent loop."""
+    lane group and grid, RK5 step budget, persistent loop and programmatic launch."""
     _need_b200("GetLaunchMapping")
-    v = (ctypes.c_int * 6)()
-    _c["NGPU_GetLaunchMapping"](v, 6)
+    v = (ctypes.c_int * 7)()
+    _c["NGPU_GetLaunchMapping"](v, 7)
     _check()
     keys = ["update_threads", "update_occupancy", "deliver_group", "deliver_blocks", "rk5_budget",
-            "persistent"]
+            "persistent", "programmatic_launch"]
     return dict(zip(keys, [int(x) for x in v]))
 
 

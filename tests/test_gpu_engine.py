@@ -382,3 +382,43 @@ def test_spike_count_array_equals_status_list():
     c_list, _ = fixed_train_network(ngpu, model="aeif_cond_beta_multisynapse", t_sim=100.0, record=False)
     arr = ngpu.GetSpikeCountArray(ngpu.NodeSeq(0, c_list.size))   # the network's neurons come first
     assert arr.dtype == np.int32 and np.array_equal(arr, c_list) and arr.sum() > 0
+
+
+@pytest.mark.parametrize("net", ["microcircuit", "aeif_poisson"])
+def test_programmatic_launch_keeps_results(net):
+    """Programmatic dependent launch of the batch kernels (default) and plain stream order
+    give the same spikes, recorded traces and event counts: the microcircuit slice (one step
+    per batch, delivery and update alternating) and an aeif network with Poisson drive
+    (batch, straggler and delivery kernels)."""
+    from workloads import microcircuit
+    res = []
+    for pdl in (True, False):
+        ngpu.Reset()
+        ngpu.SetVerbosityLevel(0)
+        ngpu.SetProgrammaticLaunch(pdl)
+        if net == "microcircuit":
+            pops = microcircuit(ngpu, scale=0.03)
+            rec = ngpu.CreateRecord("", ["V_m_rel", "I_syn_ex"], [pops[0][0], pops[2][3]], [0, 0])
+            t = (60.0, 45.0)
+        else:
+            ngpu.SetKernelStatus("rnd_seed", 3)
+            pg = ngpu.Create("poisson_generator")
+            ngpu.SetStatus(pg, "rate", 12000.0)
+            nodes = ngpu.Create("aeif_cond_beta_multisynapse", 200, 2)
+            ngpu.SetStatus(nodes, {"E_rev": [0.0, -85.0]})
+            ngpu.Connect(pg, nodes, {"rule": "all_to_all"}, {"weight": 0.4, "delay": 0.2, "receptor": 0})
+            ngpu.Connect(nodes, nodes, {"rule": "fixed_total_number", "total_num": 1600},
+                         {"weight": 0.2, "delay": 1.3, "receptor": 0})
+            ngpu.ActivateSpikeCount(nodes)
+            pops = [nodes]
+            rec = ngpu.CreateRecord("", ["V_m", "w"], [nodes[0], nodes[7]], [0, 0])
+            t = (40.0, 30.0)
+        for ti in t:
+            ngpu.Simulate(ti)
+        counts = np.concatenate([np.asarray(ngpu.GetStatus(p, "spike_count")).ravel() for p in pops])
+        res.append((counts, np.asarray(ngpu.GetRecordData(rec), dtype=np.float32), ngpu.GetStats()))
+    (c1, r1, s1), (c2, r2, s2) = res
+    assert c1.sum() > 100
+    assert np.array_equal(c1, c2)
+    assert np.array_equal(r1, r2)
+    assert s1["n_events"] == s2["n_events"] and s1["status"] == 0 and s2["status"] == 0
