@@ -50,7 +50,7 @@ DELIVERY_BYTES_PER_SPIKE = 8  # ring entry (source, height)
 # profiles/deliver_batch_kernel_1M_network_at_0.3_scale.md and
 # profiles/aeif_batch_kernel_1M_network_at_0.3_scale.md), scaled to a launch by its units
 DELIVERY_TRAFFIC_PER_EVENT = 95.6e6 / 5.82e6   # bytes per synaptic event
-RK5_TRAFFIC_PER_NEURON_STEP = 76.1e6 / 3.0e6   # bytes per neuron-step
+RK5_TRAFFIC_PER_NEURON_STEP = 74.7e6 / 3.0e6   # bytes per neuron-step
 
 
 def parse():
