@@ -158,6 +158,47 @@ def fixed_train_network(api, n=60, n_in=20, seed=7, t_sim=300.0, model="aeif_con
     return counts, data
 
 
+def many_port_network(api, model, nport, n=40, n_in=12, seed=11, t_sim=150.0):
+    """aeif neurons with `nport` receptors (1 up to the reference's maximum of 20), each port
+    with its own time constants (and reversal potential for the conductance models), driven by
+    fixed spike_generator trains spread over all ports plus recurrent connections onto the
+    last port. Returns spike counts and a record of V_m and the input variable of the first
+    and the last port."""
+    rng = np.random.RandomState(seed)
+    api.SetKernelStatus("rnd_seed", 2000 + seed)
+    neuron = api.Create(model, n, nport)
+    taus = [float(x) for x in np.round(np.linspace(1.0, 12.0, nport), 3)]
+    if model == "aeif_cond_beta_multisynapse":
+        api.SetStatus(neuron, {"E_rev": [-85.0 if p % 3 == 2 else 0.0 for p in range(nport)],
+                               "tau_rise": [0.2 + 0.1 * (p % 5) for p in range(nport)],
+                               "tau_decay": taus, "I_e": 650.0})
+        w, w_rec, var = 3.0, 1.5, "g"
+    elif model == "aeif_cond_alpha_multisynapse":
+        api.SetStatus(neuron, {"E_rev": [-85.0 if p % 3 == 2 else 0.0 for p in range(nport)],
+                               "tau_syn": taus, "I_e": 650.0})
+        w, w_rec, var = 1.0, 0.5, "g"
+    else:
+        api.SetStatus(neuron, {"tau_syn": taus, "I_e": 650.0})
+        w, w_rec, var = (150.0, 80.0, "I_syn") if model == "aeif_psc_exp_multisynapse" else (50.0, 30.0, "I_syn")
+    gens = api.Create("spike_generator", n_in)
+    for i in range(n_in):
+        t = np.cumsum(rng.exponential(6.0, size=48)) + 1.0
+        t = np.unique(np.round(t[t < t_sim - 1.0], 1))
+        api.SetStatus([gens[i]], {"spike_times": [float(x) for x in t]})
+    for p in range(nport):
+        sign = -1.0 if (model not in ("aeif_cond_beta_multisynapse", "aeif_cond_alpha_multisynapse")
+                        and p % 3 == 2) else 1.0
+        api.Connect(gens, neuron, {"rule": "fixed_indegree", "indegree": max(2, n_in // nport)},
+                    {"weight": sign * w, "receptor": p, "delay": 1.0 + 0.1 * (p % 4)})
+    api.Connect(neuron, neuron, {"rule": "fixed_total_number", "total_num": 3 * n},
+                {"weight": w_rec, "receptor": nport - 1, "delay": 1.2})
+    api.ActivateSpikeCount(neuron)
+    rec = api.CreateRecord("", ["V_m", var, var], [neuron[0], neuron[1], neuron[2]], [0, 0, nport - 1])
+    api.Simulate(t_sim)
+    counts = np.asarray(api.GetStatus(neuron, "spike_count")).ravel().astype(np.int64)
+    return counts, np.asarray(api.GetRecordData(rec))
+
+
 def poisson_network(api, n=200, rate=12000.0, t_sim=200.0, seed=3, model="aeif_cond_beta_multisynapse"):
     """Neurons driven only by one poisson_generator (all_to_all) plus sparse recurrent
     coupling; used for bit-exact comparison of the counter-based Poisson drive."""

@@ -422,3 +422,18 @@ def test_programmatic_launch_keeps_results(net):
     assert np.array_equal(c1, c2)
     assert np.array_equal(r1, r2)
     assert s1["n_events"] == s2["n_events"] and s1["status"] == 0 and s2["status"] == 0
+
+
+@pytest.mark.parametrize("nport", [1, 2, 5, 8, 20])
+@pytest.mark.parametrize("model", MODELS[:4])
+def test_many_receptor_ports_bitexact(model, nport):
+    """Receptor counts from 1 up to the reference's maximum of 20 (compile-time port counts up
+    to 4, the runtime-port kernel above): spike counts and the recorded membrane potential and
+    first- and last-port inputs equal the oracle's bit for bit."""
+    from scenarios import many_port_network
+    c_gpu, d_gpu = many_port_network(ngpu, model, nport)
+    c_orc, d_orc = many_port_network(orc.Oracle(), model, nport)
+    assert c_gpu.sum() > 0
+    assert np.array_equal(c_gpu, c_orc)
+    assert np.array_equal(np.float32(d_gpu), np.float32(d_orc))
+    assert ngpu.GetStats()["status"] == 0
