@@ -321,8 +321,9 @@ int NGPU_SetPersistent(int on);
    kernel's launch and block scheduling overlap the end of the kernel before it (every such
    kernel first waits for its predecessor's completion and memory, so results are the same);
    used where the batch is one chain of kernels on one stream (not with plastic synapses or
-   with aeif and other spiking groups together).  0 (default): plain stream order.  The
-   autotuner tries both.  No counterpart in the reference. */
+   with aeif and other spiking groups together).  0: plain stream order.  A negative value
+   (default) uses it for batches of one time step only (a minimum delay of one step), where a
+   step is two short launches.  The autotuner tries both.  No counterpart in the reference. */
 int NGPU_SetProgrammaticLaunch(int on);
 /* Test hook for the failure path of the persistent loop: with extra > 0 its grid barriers wait
    for more blocks than the launch has, so each wait runs out after its bounded number of polls

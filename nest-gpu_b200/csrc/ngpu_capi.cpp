@@ -799,7 +799,7 @@ int NGPU_SetPersistent(int on) {
 
 int NGPU_SetProgrammaticLaunch(int on) {
   return guard([&] {
-    E().launch_pdl = on ? 1 : 0;
+    E().launch_pdl = on < 0 ? -1 : (on ? 1 : 0);
     E().invalidate_graphs();
     return 0;
   }, -1);

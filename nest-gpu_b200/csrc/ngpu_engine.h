@@ -129,7 +129,7 @@ class Engine {
   int deliver_group = 32;         // lanes per delivery work item (8, 16, 32)
   int update_occupancy = 0;       // 1: register-capped aeif update kernel
   int persistent = 0;             // iaf-only networks: persistent cooperative step loop
-  int launch_pdl = 0;             // programmatic dependent launch of the batch kernels
+  int launch_pdl = -1;            // programmatic dependent launch of the batch kernels (-1: one-step batches)
   int barrier_extra = 0;          // test hook: blocks the persistent loop's barriers wait for in excess
   bool use_device_rng = true;     // cuRAND device generator (as the reference) if a GPU exists
 

@@ -897,7 +897,10 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   const bool fork = has_aeif && has_other;
   // Programmatic dependent launch where the batch is one chain of kernels on one stream
   // (no event edges between streams, no plastic-edge kernels, no per-kernel timing events).
-  set_launch_pdl(launch_pdl && !fork && !plastic_ && !ev);
+  // (automatic: for one-step batches, where a step is two short launches and their launch
+  // latency shows; longer batches measured slower with it)
+  const bool pdl = launch_pdl > 0 || (launch_pdl < 0 && M == 1);
+  set_launch_pdl(pdl && !fork && !plastic_ && !ev);
   if (ev) cuda_check(cudaEventRecord((*ev)[0], stream_), "event");
   if (plastic_) count_launch(launch_stdp_reset(stdp_, d_clk_, k0, stream_));
   count_launch(launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_,

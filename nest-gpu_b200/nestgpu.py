@@ -1426,9 +1426,10 @@ def SetDeliverGroup(g):
 
 def SetProgrammaticLaunch(on=True):
     """Programmatic dependent launch of the kernels of a time batch (engine extension;
-    results are the same either way)."""
+    results are the same either way): True, False, or None for the default (batches of one
+    time step only)."""
     _need_b200("SetProgrammaticLaunch")
-    return _check(_c["NGPU_SetProgrammaticLaunch"](1 if on else 0))
+    return _check(_c["NGPU_SetProgrammaticLaunch"](-1 if on is None else (1 if on else 0)))
 
 
 def Autotune(steps=200):
