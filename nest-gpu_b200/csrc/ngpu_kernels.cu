@@ -239,14 +239,16 @@ __device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock 
     const int m = lo / A.dspan, dd = lo - m * A.dspan;
     const int j = item - s_pref[lo];
     const long long te = t_first + m - 1 - (A.dmin + dd);
+    // segment offsets and edges are written by no kernel that delivers (the persistent loop
+    // writes ring entries between its deliveries): read-only path for those two
     const int2 sp = A.ring[(size_t)(te % A.R) * A.cap + j];
     const float height = __int_as_float(sp.y);
     const size_t key = (size_t)sp.x * A.dspan + dd;
-    const long long e0 = A.ev_off[key], e1 = A.ev_off[key + 1];
+    const long long e0 = __ldg(&A.ev_off[key]), e1 = __ldg(&A.ev_off[key + 1]);
     double *acc = A.acc + (size_t)m * A.slot_stride;
     for (long long e = e0 + sub; e < e1; e += G) {
-      const EdgeW ew = A.edge[e];
-      atomicAdd(&acc[ew.acc], (double)__fmul_rn(height, ew.w));
+      const uint2 ew = __ldg(reinterpret_cast<const uint2 *>(A.edge + e));
+      atomicAdd(&acc[ew.x], (double)__fmul_rn(height, __uint_as_float(ew.y)));
     }
     if (sub == 0) nev += (unsigned long long)(e1 - e0);
   }
