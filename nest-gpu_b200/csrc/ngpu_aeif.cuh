@@ -136,15 +136,42 @@ struct PoissonCache {
   U4 r;
 };
 
+// The edge tables and the generator table change only between kernels (calibration, host
+// copies between Simulate calls): they are read through the read-only data path.
+__device__ __forceinline__ PoissonIn ldg_pin(const PoissonIn *p) {
+  static_assert(sizeof(PoissonIn) == 24, "PoissonIn is three 8-byte words");
+  const uint2 *q = reinterpret_cast<const uint2 *>(p);
+  const uint2 a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2);
+  PoissonIn e;
+  e.edge_id = a.x;
+  e.gen = (int)a.y;
+  e.weight = __uint_as_float(b.x);
+  e.delay = __uint_as_float(b.y);
+  e.port = (int)d.x;
+  e.pad = (int)d.y;
+  return e;
+}
+
+__device__ __forceinline__ GenPar ldg_gen(const GenPar *p) {
+  static_assert(sizeof(GenPar) == 16, "GenPar is one 16-byte word");
+  const float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+  GenPar g;
+  g.rate = v.x;
+  g.origin = v.y;
+  g.start = v.z;
+  g.stop = v.w;
+  return g;
+}
+
 __device__ __forceinline__ void poisson_cache_load(const GroupInput &G, int i, PoissonCache &c) {
   c.e0 = c.e1 = 0;
   c.blk = -1;
   if (G.pin_off) {
-    c.e0 = G.pin_off[i];
-    c.e1 = G.pin_off[i + 1];
+    c.e0 = __ldg(G.pin_off + i);
+    c.e1 = __ldg(G.pin_off + i + 1);
     if (c.e1 - c.e0 == 1) {
-      c.pe = G.pin[c.e0];
-      c.g = G.gen[c.pe.gen];
+      c.pe = ldg_pin(G.pin + c.e0);
+      c.g = ldg_gen(G.gen + c.pe.gen);
       c.lam = __fmul_rn(G.lam_scale, c.g.rate);
       c.emlam = exp_m(-c.lam);
     }
