@@ -46,9 +46,10 @@ STEP_MS = 100.0
 FLOPS_PER_DERIV = 110        # FP32 flops per derivative evaluation incl. stage algebra, 2 ports
 DELIVERY_BYTES_PER_EVENT = 8  # 4 B packed target/port + 4 B weight per synaptic event
 DELIVERY_BYTES_PER_SPIKE = 8  # ring entry (source, height)
-# DRAM traffic per unit from the ncu captures of the 3/10-size network (summaries in
-# profiles/deliver_batch_kernel_1M_network_at_0.3_scale.md and
-# profiles/aeif_batch_kernel_1M_network_at_0.3_scale.md), scaled to a launch by its units
+# DRAM traffic per unit (dram__bytes_read.sum + dram__bytes_write.sum per launch divided by
+# the launch's units) from one-kernel ncu captures of the network at 3/10 size:
+#   ncu --set full --clock-control none -k regex:<kernel> -s <n> -c 2 python bench.py --scale 0.3 ...
+# scaled to a full-size launch by its units
 DELIVERY_TRAFFIC_PER_EVENT = 95.6e6 / 5.82e6   # bytes per synaptic event
 RK5_TRAFFIC_PER_NEURON_STEP = 74.7e6 / 3.0e6   # bytes per neuron-step
 
@@ -120,20 +121,9 @@ class ClockSampler(object):
 
 
 def build_engine_network(ngpu, scale, seed):
-    n_exc, n_inh = int(N_EXC * scale), int(N_INH * scale)
+    from workloads import benchmark_network
     ngpu.SetVerbosityLevel(0)
-    ngpu.SetKernelStatus("rnd_seed", seed)
-    neuron = ngpu.Create("aeif_cond_beta_multisynapse", n_exc + n_inh, 2)
-    ngpu.SetStatus(neuron, {"E_rev": [0.0, -85.0]})
-    exc, inh = neuron[0:n_exc], neuron[n_exc:n_exc + n_inh]
-    pg = ngpu.Create("poisson_generator")
-    ngpu.SetStatus(pg, "rate", PG_RATE)
-    ngpu.Connect(pg, neuron, {"rule": "all_to_all"}, {"weight": W_PG, "delay": 1.0, "receptor": 0})
-    ngpu.ConnectFixedIndegreeGPU(exc, neuron, K_EXC, W_EXC, DELAY_MIN, DELAY_MAX, receptor=0, seed=seed)
-    ngpu.ConnectFixedIndegreeGPU(inh, neuron, K_INH, W_INH, DELAY_MIN, DELAY_MAX, receptor=1,
-                                 seed=seed + 7919)
-    ngpu.ActivateSpikeCount(neuron)
-    return neuron, pg
+    return benchmark_network(ngpu, scale, seed)
 
 
 def ensemble_run(ngpu, bio_ms=1000.0):

@@ -249,10 +249,34 @@ int NGPU_ProfileSteps(int n, double *ms_out);
    starting at i_source, with delays uniform on the time grid in [delay_min, delay_max] ms.
    Unlike NESTGPU's fixed_indegree rule (one draw shared by all targets of a call), every
    target draws its own sources.  The edges live only on the device (GetConnections does not
-   list them). */
+   list them).  Edge kk of the block's t-th target draws one Philox4x32-10 block keyed by
+   `seed` with counter (t, kk, 0, 0x9E3779B9): source i_source + floor(x * n_source / 2^32),
+   delay step round(delay_min/dt) - 1 + floor(y * n_steps / 2^32).  The draws depend only on
+   the block's own indices and seed, so blocks meant to differ need different seeds. */
 int NGPU_ConnectFixedIndegreeGPU(int i_source, int n_source, int i_target, int n_target, int indegree,
                                  int port, float weight, float delay_min, float delay_max,
                                  unsigned long long seed);
+
+/* poisson_generator nodes i_node .. i_node+n_node-1 draw from Poisson streams stream ..
+   stream+n_node-1 (before calibration).  A generator's draw for its j-th out-edge (in
+   connection order) at time index t depends only on (kernel seed, stream, j, t); by default
+   the stream is the generator's index among all poisson_generator nodes.  Giving each
+   generator of an independent sub-network its own fixed stream makes that sub-network's
+   input the same wherever it sits in a larger network.  No counterpart in the reference
+   (its generators draw from per-edge cuRAND states). */
+int NGPU_SetPoissonStream(int i_node, int n_node, unsigned int stream);
+
+/* Shape of the recurrent delivery layout after calibration: the number of nodes, the smallest
+   delay step (round(delay/dt) - 1) and the number of delay steps spanned, and the number of
+   edges.  No counterpart in the reference (its layout is the per-source connection groups of
+   src/connect.h:58-70). */
+int NGPU_GetDeliveryShape(int *n_nodes, int *dmin, int *dspan, long long *n_edges);
+
+/* Copy the recurrent delivery layout to host arrays: seg_off[n_nodes*dspan + 1] (segment
+   (source s, delay step dmin + d) holds edges seg_off[s*dspan + d] .. seg_off[s*dspan + d + 1]
+   - 1), and per edge its target node, receptor port and weight (any of the three may be
+   NULL).  The order inside a segment is unspecified. */
+int NGPU_GetDeliveryCsr(long long *seg_off, int *target, unsigned char *port, float *weight);
 
 /* Thread blocks of the spike-delivery kernel (0 = chosen from the number of nodes with
    outgoing connections, at most 8 per SM).  Results do not depend on it. */
@@ -291,8 +315,10 @@ int NGPU_BuildDeliveryCsr(const int *src, const int *dly, const unsigned *target
    loading the library holds until exit.  Same arguments and results as
    NGPU_BuildDeliveryCsr; n_nodes * dspan must not exceed 524288 segments (larger problems
    are rejected with error code 2).  All calls share the array: calls that overlap on the
-   GPU race.  The first call on a device looks up the array's device address, with that
-   device current; make it before any stream capture. */
+   GPU race.  Each call is synchronous: it returns after its work on `stream` has finished
+   and its status word (an out-of-range source or delay index, code 255) has been read
+   back.  The first call on a device looks up the array's device address, with that device
+   current; make it before any stream capture. */
 int NGPU_BuildDeliveryCsrNoAlloc(const int *src, const int *dly, const unsigned *target,
                                  const float *weight, size_t n, int n_nodes, int dspan,
                                  unsigned long long *seg_off, void *edge, void *stream);

@@ -148,8 +148,13 @@ __device__ __forceinline__ PoissonIn ldg_pin(const PoissonIn *p) {
   e.weight = __uint_as_float(b.x);
   e.delay = __uint_as_float(b.y);
   e.port = (int)d.x;
-  e.pad = (int)d.y;
+  e.stream = d.y;
   return e;
+}
+
+// 64-bit Philox counter key of a poiss_gen edge: (generator stream, out-edge index).
+__device__ __forceinline__ uint64_t pin_key(const PoissonIn &pe) {
+  return ((uint64_t)pe.stream << 32) | (uint64_t)pe.edge_id;
 }
 
 __device__ __forceinline__ GenPar ldg_gen(const GenPar *p) {
@@ -198,12 +203,12 @@ __device__ __forceinline__ void poisson_add_cached(double *in, const GroupInput 
     if (c.lam > 0.0f && c.lam <= 10.0f) {
       const long long b = tidx >> 2;
       if (b != c.blk) {
-        c.r = poisson_block(G.seed, c.pe.edge_id, tidx, 0);
+        c.r = poisson_block(G.seed, pin_key(c.pe), tidx, 0);
         c.blk = b;
       }
       k = poisson_small(c.lam, c.emlam, u01(word_of(c.r, (int)(tidx & 3))));
     } else {
-      k = poisson_draw(c.lam, G.seed, c.pe.edge_id, tidx);
+      k = poisson_draw(c.lam, G.seed, pin_key(c.pe), tidx);
     }
     if (k > 0) add_to_port<PMAX>(in, c.pe.port, (double)__fmul_rn(c.pe.weight, (float)k));
   }
@@ -214,7 +219,7 @@ __device__ __forceinline__ void poisson_add(double *in, const GroupInput &G, con
                                             long long tidx, double tnow) {
   const double t_rel = tnow - (double)g.origin - (double)pe.delay;
   if (t_rel >= (double)g.start && t_rel <= (double)g.stop) {
-    int k = poisson_draw(__fmul_rn(G.lam_scale, g.rate), G.seed, pe.edge_id, tidx);
+    int k = poisson_draw(__fmul_rn(G.lam_scale, g.rate), G.seed, pin_key(pe), tidx);
     if (k > 0) add_to_port<PMAX>(in, pe.port, (double)__fmul_rn(pe.weight, (float)k));
   }
 }

@@ -21,10 +21,16 @@
 namespace ngpu {
 
 
+// Edge e = t*k + kk of a block: in-edge kk of the block's target t (0-based inside the
+// block).  One Philox4x32-10 call keyed by the block's seed with counter (t, kk, 0,
+// 0x9E3779B9): source = src0 + floor(x * nsrc / 2^32), delay step = dlo +
+// floor(y * (dhi - dlo + 1) / 2^32).  Everything is relative to the block, so a block
+// draws the same edges wherever its nodes sit in the network; blocks that should differ
+// need different seeds.
 __device__ __forceinline__ void gen_edge(const GenBlockDev &b, long long e, int &src, int &d, int &tgt) {
   const int t = (int)(e / b.k);
   const int kk = (int)(e - (long long)t * b.k);
-  U4 c = {(uint32_t)t, (uint32_t)kk, (uint32_t)b.block_id, 0x9E3779B9u};
+  U4 c = {(uint32_t)t, (uint32_t)kk, 0u, 0x9E3779B9u};
   U4 r = philox(c, (uint32_t)b.seed, (uint32_t)(b.seed >> 32));
   src = b.src0 + (int)(((unsigned long long)r.x * (unsigned)b.nsrc) >> 32);
   d = b.dlo + (int)(((unsigned long long)r.y * (unsigned)(b.dhi - b.dlo + 1)) >> 32);

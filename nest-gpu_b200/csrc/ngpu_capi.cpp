@@ -699,6 +699,18 @@ int NGPU_ConnectFixedIndegreeGPU(int i_source, int n_source, int i_target, int n
   }, 0);
 }
 
+int NGPU_SetPoissonStream(int i_node, int n_node, unsigned int stream) {
+  return guard([&] { E().set_poisson_stream(i_node, n_node, stream); return 0; }, 0);
+}
+
+int NGPU_GetDeliveryShape(int *n_nodes, int *dmin, int *dspan, long long *n_edges) {
+  return guard([&] { E().delivery_shape(n_nodes, dmin, dspan, n_edges); return 0; }, 0);
+}
+
+int NGPU_GetDeliveryCsr(long long *seg_off, int *target, unsigned char *port, float *weight) {
+  return guard([&] { E().delivery_csr(seg_off, target, port, weight); return 0; }, 0);
+}
+
 int NGPU_BuildDeliveryCsr(const int *src, const int *dly, const unsigned *target, const float *weight,
                           size_t n, int n_nodes, int dspan, unsigned long long *seg_off, void *edge,
                           void *stream) {

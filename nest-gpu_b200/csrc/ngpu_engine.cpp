@@ -693,6 +693,20 @@ void Engine::connect_fixed_indegree_per_target(int src0, int ns, int tgt0, int n
   n_generated_ += (size_t)nt * k;
 }
 
+void Engine::set_poisson_stream(int i0, int n, uint32_t stream0) {
+  if (calibrated_) throw NgpuError("Poisson streams must be set before calibration");
+  if (n <= 0) return;
+  Group &g = group_of(i0);
+  if (g.model != M_POISS_GEN) throw NgpuError("Poisson streams apply to poisson_generator nodes only");
+  if (i0 + n > g.i0 + g.n) throw NgpuError("Poisson stream range crosses a node group");
+  if (g.pg_stream.empty()) {
+    // untouched generators keep their default: the index among all generators, known at
+    // calibration; mark them with the default computed there
+    g.pg_stream.assign(g.n, 0xffffffffu);
+  }
+  for (int j = 0; j < n; j++) g.pg_stream[i0 - g.i0 + j] = stream0 + (uint32_t)j;
+}
+
 void Engine::connect_arrays(size_t n, const int *src, const int *tgt, const unsigned char *port,
                             const float *w, const float *d) {
   if (calibrated_) throw NgpuError("Connections cannot be created after calibration");

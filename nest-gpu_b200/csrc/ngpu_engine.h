@@ -83,6 +83,7 @@ struct Group {
   int *d_sg_off = nullptr, *d_sg_tidx = nullptr, *d_sg_next = nullptr;
   float *d_sg_h = nullptr;
   int gen0 = -1;                 // poiss_gen: first row in the generator table
+  std::vector<uint32_t> pg_stream;   // poiss_gen: stream numbers (empty: index among generators)
   bool dirty = true;             // parameters changed since last upload
 };
 
@@ -186,6 +187,8 @@ class Engine {
   // Bulk import of a prebuilt edge list (engine extension, used by the large benchmarks).
   void connect_arrays(size_t n, const int *src, const int *tgt, const unsigned char *port,
                       const float *w, const float *d);
+  // poiss_gen nodes i0 .. i0+n-1 draw from streams stream0 .. stream0+n-1 (engine extension)
+  void set_poisson_stream(int i0, int n, uint32_t stream0);
   void connect_fixed_indegree_per_target(int src0, int ns, int tgt0, int nt, int k, int port,
                                          float w, float dmin_ms, float dmax_ms, uint64_t seed);
 
@@ -212,6 +215,10 @@ class Engine {
   // returns the average device time per step [ms] of: neuron updates (all groups),
   // record gather, spike delivery.  The steps are ordinary simulation steps.
   std::vector<double> profile_steps(int n);
+  // The recurrent delivery layout after calibration: segments by (source node, delay step
+  // - dmin), nodes * dspan + 1 offsets, and per edge its target node, receptor port, weight.
+  void delivery_shape(int *n_nodes, int *dmin, int *dspan, long long *n_edges);
+  void delivery_csr(long long *seg_off, int *target, unsigned char *port, float *weight);
   long long n_launches() const { return n_launch_; }
 
   // Tune update_threads, update_occupancy, deliver_group, deliver_blocks_req and rk5_budget
@@ -360,6 +367,7 @@ class Engine {
   template <class T> T *dalloc(size_t n);
   void free_device();
   void upload_params();
+  void upload_dirty_params();   // upload_params() if any group's parameters changed
   void build_records();
   void launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev);
   void ensure_record_window(long long rows);

@@ -18,6 +18,8 @@
 //   - every call shares the one array and leaves its contents behind; each call
 //     clears the counters it uses before counting, so calls must not overlap on the
 //     GPU (two calls on different streams at the same time race on the scratch).
+//   - each call is synchronous: it waits for its work on the given stream and reads the
+//     bad-index flag back before it returns;
 //   - the device address of the array is looked up once per device, with that device
 //     current, by the first call on it; make that first call before any stream
 //     capture.

@@ -205,7 +205,6 @@ void Engine::calibrate() {
     d.dlo = (int)std::round(b.dmin_ms / dt) - 1;
     d.dhi = (int)std::round(b.dmax_ms / dt) - 1;
     d.seed = b.seed;
-    d.block_id = (int)bi;
     dmin = std::min(dmin, d.dlo);
     dmax = std::max(dmax, d.dhi);
     gblocks.push_back(d);
@@ -276,20 +275,23 @@ void Engine::calibrate() {
   {
     struct DE { int tgt; PoissonIn pe; };
     std::vector<DE> de;
-    uint32_t id = 0;
     for (int s = 0; s < N; s++) {
       if (!is_pg[s]) continue;
       const Group &pg = groups_[node_group_[s]];
+      const int gi = pg.gen0 + (s - pg.i0);
+      const uint32_t set = pg.pg_stream.empty() ? 0xffffffffu : pg.pg_stream[s - pg.i0];
+      const uint32_t stream = set == 0xffffffffu ? (uint32_t)gi : set;
+      uint32_t id = 0;   // out-edges of this generator in connection order
       for (long long p = src_first_[s]; p < src_first_[s + 1]; p++) {
         long long e = ord_[p];
         DE x;
         x.tgt = c_tgt_[e];
         x.pe.edge_id = id++;
-        x.pe.gen = pg.gen0 + (s - pg.i0);
+        x.pe.gen = gi;
         x.pe.weight = c_w_[e];
         x.pe.delay = dt * (float)(c_d_[e] + 1);
         x.pe.port = c_port_[e];
-        x.pe.pad = 0;
+        x.pe.stream = stream;
         de.push_back(x);
       }
     }
@@ -454,6 +456,9 @@ void Engine::calibrate() {
 // Derived parameters: uniform over the group -> kernel argument, else device array.
 void Engine::upload_params() {
   bool any = false;
+  // device arrays of the previous upload, reused when a parameter stays non-uniform (a
+  // step loop that sets parameters between steps allocates nothing after the first change)
+  std::vector<float *> prev;
   auto put = [&](Group &g, int slot, const std::vector<float> &v) {
     bool uni = true;
     for (int i = 1; i < g.n && uni; i++) uni = (std::memcmp(&v[i], &v[0], 4) == 0);
@@ -461,7 +466,7 @@ void Engine::upload_params() {
       g.der_val[slot] = v[0];
       g.d_der[slot] = nullptr;
     } else {
-      float *d = dalloc<float>(g.n);
+      float *d = (slot < (int)prev.size() && prev[slot]) ? prev[slot] : dalloc<float>(g.n);
       cuda_check(cudaMemcpy(d, v.data(), g.n * sizeof(float), cudaMemcpyHostToDevice), "param");
       g.der_val[slot] = 0.0f;
       g.d_der[slot] = d;
@@ -479,6 +484,7 @@ void Engine::upload_params() {
     std::vector<float> v(n);
     if (g.model == M_PARROT && g.d_hold)
       cuda_check(cudaMemcpy(g.d_hold, g.par[0].data(), n * sizeof(float), cudaMemcpyHostToDevice), "hold");
+    prev = g.d_der;
     if (is_aeif(g.model)) {
       g.der_val.assign(AEIF_NPAR, 0.0f);
       g.d_der.assign(AEIF_NPAR, nullptr);
@@ -1118,9 +1124,20 @@ void Engine::check_status() {
   }
 }
 
+void Engine::upload_dirty_params() {
+  for (auto &g : groups_)
+    if (g.dirty) {
+      upload_params();
+      return;
+    }
+}
+
 void Engine::start_simulation() {
   if (!calibrated_) calibrate();
-  if (in_sim_) return;
+  if (in_sim_) {
+    upload_dirty_params();
+    return;
+  }
   upload_params();
   if (first_sim_) {
     // initial record row (src/nestgpu.cu:384-389)
@@ -1169,6 +1186,9 @@ void Engine::end_simulation() {
 
 void Engine::simulation_step() {
   if (!in_sim_) start_simulation();
+  // parameters set between steps apply from the next step, as the reference's setters
+  // write to the device at once (src/base_neuron.cu:219-260)
+  upload_dirty_params();
   // every step ends with its input fold, so state queries between steps see what the
   // reference shows
   run_steps(1);
@@ -1199,6 +1219,42 @@ void Engine::simulate(float t) {
   last_sim_seconds_ = std::chrono::duration<double>(t1 - t0).count();
   total_steps_ += Nt_;
   if (verbosity >= 1) printf("Simulation time: %g\n", last_sim_seconds_);
+}
+
+void Engine::delivery_shape(int *n_nodes_out, int *dmin, int *dspan, long long *n_edges) {
+  if (!calibrated_) throw NgpuError("the delivery layout exists after calibration");
+  if (n_nodes_out) *n_nodes_out = n_nodes();
+  if (dmin) *dmin = dmin_;
+  if (dspan) *dspan = dspan_;
+  if (n_edges) *n_edges = (long long)n_edge_dev_;
+}
+
+void Engine::delivery_csr(long long *seg_off, int *target, unsigned char *port, float *weight) {
+  if (!calibrated_) throw NgpuError("the delivery layout exists after calibration");
+  const size_t nkey = (size_t)n_nodes() * dspan_;
+  cuda_check(cudaStreamSynchronize(stream_), "sync");
+  cuda_check(cudaMemcpy(seg_off, d_ev_off_, (nkey + 1) * sizeof(long long), cudaMemcpyDeviceToHost), "seg_off");
+  std::vector<EdgeW> ew(n_edge_dev_);
+  if (n_edge_dev_)
+    cuda_check(cudaMemcpy(ew.data(), d_edge_, n_edge_dev_ * sizeof(EdgeW), cudaMemcpyDeviceToHost), "edges");
+  // accumulator index -> (target node, receptor port): groups own contiguous ranges
+  std::vector<const Group *> by_off;
+  for (auto &g : groups_)
+    if (g.nport > 0) by_off.push_back(&g);
+  std::sort(by_off.begin(), by_off.end(), [](const Group *a, const Group *b) { return a->acc_off < b->acc_off; });
+  for (size_t e = 0; e < n_edge_dev_; e++) {
+    const size_t a = ew[e].acc;
+    size_t lo = 0, hi = by_off.size();
+    while (hi - lo > 1) {
+      const size_t mid = (lo + hi) / 2;
+      if (by_off[mid]->acc_off <= a) lo = mid; else hi = mid;
+    }
+    const Group &g = *by_off[lo];
+    const size_t r = a - g.acc_off;
+    if (target) target[e] = g.i0 + (int)(r % g.n);
+    if (port) port[e] = (unsigned char)(r / g.n);
+    if (weight) weight[e] = ew[e].w;
+  }
 }
 
 std::vector<double> Engine::profile_steps(int n) {

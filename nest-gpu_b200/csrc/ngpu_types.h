@@ -87,14 +87,18 @@ struct GroupRecord {
   int ncol;
 };
 
-// Incoming poiss_gen edge, target-major, with its canonical direct-edge id.
+// Incoming poiss_gen edge, target-major.  Its Poisson stream is keyed by
+// (stream, edge_id): edge_id numbers the generator's out-edges in connection order
+// (source-major, delay groups ascending, insertion order) from 0, and stream is the
+// generator's stream number (its index among all poiss_gen nodes unless set), so a
+// generator's draws do not depend on what else the network holds.
 struct PoissonIn {
   uint32_t edge_id;
   int gen;               // index into the generator parameter table
   float weight;
   float delay;
   int port;
-  int pad;
+  uint32_t stream;
 };
 
 // Generator parameters: rate [Hz], origin, start, stop [ms].
@@ -265,7 +269,6 @@ struct GenBlockDev {
   float w;
   int dlo, dhi;            // delay indices, inclusive
   uint64_t seed;
-  int block_id;
 };
 
 }  // namespace ngpu

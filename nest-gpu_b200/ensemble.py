@@ -12,7 +12,10 @@ The default specification: 256 networks, sizes lognormal (median 8000, log-sd 0.
 clipped to [1000, 50000], 60% aeif / 40% iaf_psc_exp, 80% excitatory neurons,
 in-degree uniform in [100, 500] per network (80% excitatory sources), Poisson drive
 of 400 inputs per neuron at a per-network rate uniform in [5, 20] Hz, delays 1.5 ms
-(recurrent) and 1.0 ms (drive), per-network connection seeds.
+(recurrent) and 1.0 ms (drive), per-network seeds.  Every random stream of a network
+(its generated connections and its Poisson generator's stream) is keyed by the
+network's own seed and network-local indices, so a network gives the same spikes
+alone as inside the ensemble.
 """
 import numpy as np
 
@@ -67,6 +70,8 @@ def build_ensemble(ngpu, spec, n_inputs=400, delay=1.5, drive_delay=1.0):
         ngpu.ConnectFixedIndegreeGPU(inh, cells, k_inh, w["inh"], delay, delay, receptor=1,
                                      seed=net["seed"] + 7919)
         ngpu.SetStatus([pgs[i]], "rate", n_inputs * net["rate"])
+        # the network's Poisson input is keyed by its own seed, not by its position
+        ngpu.SetPoissonStream(pgs[i:i + 1], net["seed"])
         ngpu.Connect([pgs[i]], cells, {"rule": "all_to_all"}, {"weight": w["drive"], "delay": drive_delay,
                                                                "receptor": 0})
     for g in groups.values():

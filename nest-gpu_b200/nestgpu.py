@@ -200,6 +200,10 @@ if is_b200_engine:
     _c["NGPU_MlpGrad"] = _bind("NGPU_MlpGrad", _I, [c_void_p, c_void_p, c_void_p, _I, c_void_p, c_void_p])
     _c["NGPU_ConnectFixedIndegreeGPU"] = _bind("NGPU_ConnectFixedIndegreeGPU", _I,
                                                [_I, _I, _I, _I, _I, _I, _F, _F, _F, ctypes.c_ulonglong])
+    _c["NGPU_SetPoissonStream"] = _bind("NGPU_SetPoissonStream", _I, [_I, _I, ctypes.c_uint])
+    _c["NGPU_GetDeliveryShape"] = _bind("NGPU_GetDeliveryShape", _I, [ctypes.POINTER(_I)] * 3 +
+                                        [ctypes.POINTER(ctypes.c_longlong)])
+    _c["NGPU_GetDeliveryCsr"] = _bind("NGPU_GetDeliveryCsr", _I, [c_void_p] * 4)
 
 
 def _b(s):
@@ -1365,6 +1369,36 @@ def ConnectFixedIndegreeGPU(source, target, indegree, weight, delay_min, delay_m
     """Per-target fixed in-degree block generated on the GPU (engine extension)."""
     return _check(_c["NGPU_ConnectFixedIndegreeGPU"](source.i0, source.n, target.i0, target.n, indegree,
                                                      receptor, weight, delay_min, delay_max, seed))
+
+
+def SetPoissonStream(nodes, stream):
+    """poisson_generator nodes draw from streams stream, stream+1, ... (engine extension,
+    before calibration): a generator's draws then depend only on (kernel seed, stream,
+    out-edge index, time step), not on where it sits in the network."""
+    _need_b200("SetPoissonStream")
+    if not isinstance(nodes, NodeSeq):
+        nodes = NodeSeq(nodes[0], len(nodes)) if len(nodes) else NodeSeq(0, 0)
+    return _check(_c["NGPU_SetPoissonStream"](nodes.i0, nodes.n, int(stream) & 0xffffffff))
+
+
+def GetDeliveryCsr():
+    """The recurrent delivery layout after calibration (engine extension): a dict with
+    n_nodes, dmin, dspan, seg_off (int64, n_nodes*dspan+1: segment (source s, delay step
+    dmin+d) is seg_off[s*dspan+d] .. seg_off[s*dspan+d+1]) and per edge target, port,
+    weight (order inside a segment unspecified)."""
+    import numpy as np
+    _need_b200("GetDeliveryCsr")
+    nn, dmin, dspan, ne = _I(), _I(), _I(), ctypes.c_longlong()
+    _c["NGPU_GetDeliveryShape"](ctypes.byref(nn), ctypes.byref(dmin), ctypes.byref(dspan), ctypes.byref(ne))
+    _check()
+    off = np.zeros(nn.value * dspan.value + 1, dtype=np.int64)
+    tgt = np.zeros(max(ne.value, 1), dtype=np.int32)
+    port = np.zeros(max(ne.value, 1), dtype=np.uint8)
+    w = np.zeros(max(ne.value, 1), dtype=np.float32)
+    _c["NGPU_GetDeliveryCsr"](off.ctypes.data, tgt.ctypes.data, port.ctypes.data, w.ctypes.data)
+    _check()
+    return {"n_nodes": nn.value, "dmin": dmin.value, "dspan": dspan.value, "seg_off": off,
+            "target": tgt[:ne.value], "port": port[:ne.value], "weight": w[:ne.value]}
 
 
 def SetHostRng(on=True):

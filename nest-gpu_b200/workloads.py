@@ -3,6 +3,81 @@ the same calling conventions, such as the CPU oracle's)."""
 import numpy as np
 
 
+# The 1M-neuron benchmark network: 800k exc + 200k inh aeif_cond_beta_multisynapse neurons
+# with two receptors (E_rev 0 / -85 mV), 800 exc (0.05 nS, receptor 0) + 200 inh (0.35 nS,
+# receptor 1) inputs per neuron drawn per target with replacement, delays uniform on the
+# 0.1 ms grid in [1.0, 2.0] ms, one poisson_generator at 8 kHz into every neuron (0.1 nS,
+# receptor 0, delay 1.0 ms).
+BENCH_N_EXC, BENCH_N_INH = 800_000, 200_000
+BENCH_K_EXC, BENCH_K_INH = 800, 200
+BENCH_W_EXC, BENCH_W_INH, BENCH_W_PG = 0.05, 0.35, 0.1
+BENCH_PG_RATE = 8000.0
+BENCH_DELAY_MIN, BENCH_DELAY_MAX = 1.0, 2.0
+
+
+def benchmark_network(api, scale=1.0, seed=20240):
+    """The benchmark network at `scale` of its 1M neurons (in-degrees unchanged), built with
+    the generated per-target fixed in-degree rule (ConnectFixedIndegreeGPU, seeds seed and
+    seed + 7919).  Returns (neurons, generator)."""
+    n_exc, n_inh = int(BENCH_N_EXC * scale), int(BENCH_N_INH * scale)
+    api.SetKernelStatus("rnd_seed", seed)
+    neuron = api.Create("aeif_cond_beta_multisynapse", n_exc + n_inh, 2)
+    api.SetStatus(neuron, {"E_rev": [0.0, -85.0]})
+    exc, inh = neuron[0:n_exc], neuron[n_exc:n_exc + n_inh]
+    pg = api.Create("poisson_generator")
+    api.SetStatus(pg, "rate", BENCH_PG_RATE)
+    api.Connect(pg, neuron, {"rule": "all_to_all"}, {"weight": BENCH_W_PG, "delay": 1.0, "receptor": 0})
+    api.ConnectFixedIndegreeGPU(exc, neuron, BENCH_K_EXC, BENCH_W_EXC, BENCH_DELAY_MIN, BENCH_DELAY_MAX,
+                                receptor=0, seed=seed)
+    api.ConnectFixedIndegreeGPU(inh, neuron, BENCH_K_INH, BENCH_W_INH, BENCH_DELAY_MIN, BENCH_DELAY_MAX,
+                                receptor=1, seed=seed + 7919)
+    api.ActivateSpikeCount(neuron)
+    return neuron, pg
+
+
+def balanced_network(api, seed=42, n=1000, drive="poisson", n_gen=400, gen_rate=10.0, t_sim=1000.0):
+    """The plain small balanced network as specified: n aeif_cond_beta_multisynapse neurons
+    (80% exc / 20% inh, reference default parameters, receptors E_rev 0 / -85 mV), the
+    reference's fixed_indegree rule (one source draw per call, shared by all targets) with
+    80 exc inputs (0.05 nS, receptor 0) and 20 inh inputs (0.35 nS, receptor 1), delay
+    1.5 ms; drive on receptor 0 (0.1 nS, delay 1.0 ms):
+      "poisson": n_gen poisson_generators at gen_rate Hz, all_to_all (400 x 10 Hz = 4 kHz);
+      "trains":  one spike_generator per neuron, one_to_one, replaying a seeded Poisson
+                 train of the same aggregate rate (n_gen x gen_rate) as spike heights per
+                 0.1 ms step (deterministic input for comparisons across libraries).
+    Returns the neurons."""
+    api.SetKernelStatus("rnd_seed", seed)
+    neuron = api.Create("aeif_cond_beta_multisynapse", n, 2)
+    api.SetStatus(neuron, {"E_rev": [0.0, -85.0]})
+    ne = int(0.8 * n)
+    exc, inh = neuron[0:ne], neuron[ne:n]
+    api.Connect(exc, neuron, {"rule": "fixed_indegree", "indegree": 80},
+                {"weight": 0.05, "delay": 1.5, "receptor": 0})
+    api.Connect(inh, neuron, {"rule": "fixed_indegree", "indegree": 20},
+                {"weight": 0.35, "delay": 1.5, "receptor": 1})
+    if drive == "poisson":
+        pg = api.Create("poisson_generator", n_gen)
+        api.SetStatus(pg, "rate", gen_rate)
+        api.Connect(pg, neuron, {"rule": "all_to_all"}, {"weight": 0.1, "delay": 1.0, "receptor": 0})
+    elif drive == "trains":
+        rng = np.random.RandomState(seed)
+        lam = n_gen * gen_rate * 1e-4            # expected input spikes per 0.1 ms step
+        n_steps = int(round(t_sim / 0.1))
+        sg = api.Create("spike_generator", n)
+        for i in range(n):
+            k = rng.poisson(lam, n_steps)
+            steps = np.nonzero(k)[0]
+            # steps 1 .. n_steps - 1 on the 0.1 ms grid (times strictly increasing)
+            steps = steps[steps > 0]
+            api.SetStatus(sg[i:i + 1], {"spike_times": [round(0.1 * int(s), 1) for s in steps],
+                                        "spike_heights": [float(k[s]) for s in steps]})
+        api.Connect(sg, neuron, {"rule": "one_to_one"}, {"weight": 0.1, "delay": 1.0, "receptor": 0})
+    else:
+        raise ValueError(drive)
+    api.ActivateSpikeCount(neuron)
+    return neuron
+
+
 def c4_network(api, seed=42, n=1000, drive_w=0.1, n_port=4):
     """The small balanced network (800 exc / 200 inh aeif_cond_beta_multisynapse,
     fixed in-degree 80 exc w=0.05 nS / 20 inh w=0.35 nS, delay 1.5 ms, 4 kHz Poisson

@@ -425,8 +425,11 @@ struct Net {
   long long it = 0, Nt = 0;
   std::vector<std::vector<Queued>> queue;         // per source, most recent first
   // direct (poiss_gen) edges in canonical order
-  struct Direct { int gen; int tgt; unsigned char port; float w; float delay; int group; };
+  // Poisson stream of an edge: (stream, out-edge index of its generator in connection
+  // order); stream = the generator's index among all poiss_gen nodes unless set
+  struct Direct { int gen; int tgt; unsigned char port; float w; float delay; int group; uint64_t key; };
   std::vector<Direct> direct;
+  std::map<int, uint32_t> pg_stream;              // poiss_gen node -> stream (set explicitly)
   std::vector<Rec> recs;
   std::vector<std::vector<float>> rec_rows;
   long long n_derivs = 0;
@@ -651,7 +654,12 @@ struct Net {
     if (delay < dt) throw std::runtime_error("Delay must be >= time resolution");
     if (syn < 0 || syn > (int)syn_groups.size()) throw std::runtime_error("Unrecognized synapse group");
     if (syn > 0) any_plastic = true;
-    int d_int = (int)std::round(delay / dt) - 1;
+    connect_step(src, tgt, port, w, (int)std::round(delay / dt) - 1, syn);
+  }
+
+  // insertion into the source's delay group d_int (src/connect.cu:38-74: groups ascending
+  // by delay, targets in insertion order)
+  void connect_step(int src, int tgt, int port, float w, int d_int, int syn = 0) {
     std::vector<DelayGroup> &c = conn[src];
     size_t id = 0;
     while (id < c.size() && d_int > c[id].delay) id++;
@@ -667,6 +675,29 @@ struct Net {
       e.syn = (unsigned char)syn;
       c[id].tg.push_back(e);
     }
+  }
+
+  // The engine's generated fixed in-degree block (ConnectFixedIndegreeGPU; no reference
+  // counterpart: it stands in for src/connect_rules.h:203-269 in the large benchmark
+  // networks, with sources drawn per target and with replacement).  Edge kk of the block's
+  // t-th target: one Philox4x32-10 block keyed by the seed with counter (t, kk, 0,
+  // 0x9E3779B9); source = src0 + floor(x * ns / 2^32), delay step = dlo + floor(y * (dhi -
+  // dlo + 1) / 2^32) with dlo/dhi = round(delay_min/max / dt) - 1.
+  void connect_generated(int src0, int ns, int tgt0, int nt, int k, int port, float w, float dmin_ms,
+                         float dmax_ms, uint64_t seed) {
+    if (calibrated) throw std::runtime_error("Connections cannot be created after calibration");
+    if (ns <= 0 || nt <= 0 || k <= 0) throw std::runtime_error("empty connection block");
+    if (dmin_ms < dt || dmax_ms < dmin_ms) throw std::runtime_error("Delay must be >= time resolution");
+    const int dlo = (int)std::round(dmin_ms / dt) - 1;
+    const int dhi = (int)std::round(dmax_ms / dt) - 1;
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    for (int t = 0; t < nt; t++)
+      for (int kk = 0; kk < k; kk++) {
+        U4 r = philox({(uint32_t)t, (uint32_t)kk, 0u, 0x9E3779B9u}, k0, k1);
+        const int s = src0 + (int)(((uint64_t)r.x * (uint32_t)ns) >> 32);
+        const int d = dlo + (int)(((uint64_t)r.y * (uint32_t)(dhi - dlo + 1)) >> 32);
+        connect_step(s, tgt0 + t, port, w, d, 0);
+      }
   }
 
   // src/connect_rules.h:161-338 (one host thread: THREAD_MAXNUM == 1)
@@ -765,13 +796,19 @@ struct Net {
     queue.assign(node_group.size(), {});
     // direct edges: poiss_gen sources, source-major, delay groups ascending, insertion order
     direct.clear();
+    uint32_t ordinal = 0;
     for (size_t gi = 0; gi < groups.size(); gi++) {
       Group &g = groups[gi];
       if (g.model != POISS_GEN) continue;
-      for (int s = g.i0; s < g.i0 + g.n; s++)
+      for (int s = g.i0; s < g.i0 + g.n; s++, ordinal++) {
+        auto it = pg_stream.find(s);
+        const uint64_t stream = it != pg_stream.end() ? it->second : ordinal;
+        uint32_t local = 0;
         for (auto &dg : conn[s])
           for (auto &e : dg.tg)
-            direct.push_back({s - g.i0, e.tgt, e.port, e.w, dt * (float)(dg.delay + 1), (int)gi});
+            direct.push_back({s - g.i0, e.tgt, e.port, e.w, dt * (float)(dg.delay + 1), (int)gi,
+                              (stream << 32) | (uint64_t)(local++)});
+      }
     }
     for (auto &g : groups) {
       if (is_aeif(g.model)) {
@@ -1391,7 +1428,7 @@ struct Net {
       float start_ = (float)g.par[PG_start][d.gen], stop_ = (float)g.par[PG_stop][d.gen];
       double t_rel = neural_time - (double)origin - (double)d.delay;
       if (t_rel >= (double)start_ && t_rel <= (double)stop_) {
-        int n = poisson_draw(time_step * rate, kernel_seed, (uint64_t)ie, tidx);
+        int n = poisson_draw(time_step * rate, kernel_seed, d.key, tidx);
         if (n > 0) {
           Group &tg = groups[node_group[d.tgt]];
           double &a = tg.acc[(size_t)d.port * tg.n + (d.tgt - tg.i0)];
@@ -1599,6 +1636,21 @@ int orc_get_syn_param(void *p, int g, const char *name, float *v) {
   OR_TRY Net *n = (Net *)p; *v = n->syn_groups[g - 1].par[syn_par_idx(n, g, name)]; return 0; OR_CATCH(-1)
 }
 
+int orc_connect_generated(void *p, int src0, int ns, int tgt0, int nt, int k, int port, float w,
+                          float dmin_ms, float dmax_ms, unsigned long long seed) {
+  OR_TRY ((Net *)p)->connect_generated(src0, ns, tgt0, nt, k, port, w, dmin_ms, dmax_ms, seed); return 0;
+  OR_CATCH(-1)
+}
+int orc_set_poisson_stream(void *p, int i0, int n, unsigned int stream0) {
+  OR_TRY
+  Net *net = (Net *)p;
+  for (int j = 0; j < n; j++) {
+    if (net->group_of(i0 + j).model != orc::POISS_GEN) throw std::runtime_error("not a poisson_generator");
+    net->pg_stream[i0 + j] = stream0 + (uint32_t)j;
+  }
+  return 0;
+  OR_CATCH(-1)
+}
 int orc_connect_arrays(void *p, size_t n, const int *src, const int *tgt, const int *port,
                        const float *w, const float *d) {
   OR_TRY

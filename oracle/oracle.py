@@ -68,6 +68,9 @@ def lib():
             "orc_connect1": (c_int, [c_void, c_int, c_int, c_int, c_float, c_float]),
             "orc_n_conn": (ctypes.c_longlong, [c_void]),
             "orc_connect_arrays": (c_int, [c_void, ctypes.c_size_t, ip, ip, ip, fp, fp]),
+            "orc_connect_generated": (c_int, [c_void, c_int, c_int, c_int, c_int, c_int, c_int, c_float,
+                                              c_float, c_float, c_ull]),
+            "orc_set_poisson_stream": (c_int, [c_void, c_int, c_int, ctypes.c_uint]),
             "orc_threads": (c_int, []),
             "orc_get_conns": (c_int, [c_void, ip, ip, ip, ip, ip, ip, fp, fp]),
             "orc_record": (c_int, [c_void, c_int, ctypes.c_char_p, c_int]),
@@ -399,6 +402,18 @@ class Oracle(object):
         w = np.ascontiguousarray(weight, dtype=np.float32)
         d = np.ascontiguousarray(delay, dtype=np.float32)
         self._chk(self.L.orc_connect_arrays(self.h, s.size, _iptr(s), _iptr(t), _iptr(p), _fptr(w), _fptr(d)))
+
+    def ConnectFixedIndegreeGPU(self, source, target, indegree, weight, delay_min, delay_max, receptor=0,
+                                seed=1):
+        """The engine's per-target generated fixed in-degree block, restated on the host."""
+        self._chk(self.L.orc_connect_generated(self.h, source.i0, source.n, target.i0, target.n, indegree,
+                                               receptor, weight, delay_min, delay_max, seed))
+
+    def SetPoissonStream(self, nodes, stream):
+        """poisson_generator nodes draw from streams stream, stream+1, ..."""
+        if not hasattr(nodes, "i0"):
+            nodes = NodeSeq(nodes[0], len(nodes))
+        self._chk(self.L.orc_set_poisson_stream(self.h, nodes.i0, nodes.n, int(stream) & 0xffffffff))
 
     def Threads(self):
         return self.L.orc_threads()

@@ -29,7 +29,9 @@ MODELS = ["aeif_cond_beta_multisynapse", "aeif_cond_alpha_multisynapse",
 
 
 def main():
-    ref = os.environ.get("NESTGPU_REF", "/root/reference")
+    ref = os.environ.get("NESTGPU_REF")
+    if not ref:
+        sys.exit("set NESTGPU_REF to the reference source tree")
     tdir = os.path.join(ref, "python", "test")
     if not os.path.isdir(tdir):
         sys.exit("reference test directory not found: " + tdir)

@@ -1,6 +1,7 @@
 """Drop-in check: the reference's own pythonlib/nestgpu.py, unchanged, loads
 libnestgpu_b200.so through NESTGPU_LIB and a user script gives the same network through it as
-through this repository's front-end.  Needs the reference tree (skipped where it is absent)."""
+through this repository's front-end.  Needs the reference's binding and scripts as copied
+into oracle/_ref/py by oracle/Makefile.ref (skipped where they are absent)."""
 import json
 import os
 import subprocess
@@ -10,7 +11,9 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB = os.path.join(ROOT, "nest-gpu_b200", "lib", "libnestgpu_b200.so")
-REF_PY = os.path.join(os.environ.get("NESTGPU_REF", "/root/reference"), "pythonlib")
+# the reference's binding and scripts as copied beside the reference library by
+# oracle/Makefile.ref (its `py` target)
+REF_PY = os.path.join(ROOT, "oracle", "_ref", "py")
 SCRIPT = os.path.join(ROOT, "tests", "dropin_script.py")
 
 
@@ -22,7 +25,7 @@ def run(binding_dir):
     return json.loads([x for x in p.stdout.splitlines() if x.startswith("JSON:")][-1][5:])
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REF_PY, "nestgpu.py")), reason="reference tree absent")
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_PY, "nestgpu.py")), reason="reference binding not copied into oracle/_ref/py")
 def test_reference_binding_drives_engine():
     ref = run(REF_PY)
     own = run(os.path.join(ROOT, "nest-gpu_b200"))
@@ -31,7 +34,7 @@ def test_reference_binding_drives_engine():
     assert ref["E_rev"][0] == [0.0, -85.0]
 
 
-REF_TEST = os.path.join(os.environ.get("NESTGPU_REF", "/root/reference"), "python", "test")
+REF_TEST = os.path.join(ROOT, "oracle", "_ref", "py", "test")
 
 
 def _clean(text):
@@ -39,8 +42,8 @@ def _clean(text):
     return [l.rstrip() for l in text.splitlines() if l.strip() and not any(b in l for b in banner)]
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REF_PY, "nestgpu.py")), reason="reference tree absent")
-@pytest.mark.parametrize("name", ["getarr", "setvar2", "syn_group"])
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_PY, "nestgpu.py")), reason="reference binding not copied into oracle/_ref/py")
+@pytest.mark.parametrize("name", ["getarr", "setvar2", "syn_group", "connect"])
 def test_reference_api_scripts_reproduce_their_logs(name, tmp_path):
     """The reference's own API test scripts (python/test/test_<name>.py), run unchanged through
     its unchanged pythonlib/nestgpu.py on this library, print what their logs

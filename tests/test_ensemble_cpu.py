@@ -32,3 +32,23 @@ def test_ensemble_layout_slices_groups():
     for m, g in groups.items():
         assert len(g) == tot[m]
     ngpu.Reset()
+
+
+def test_network_alone_equals_network_in_ensemble_oracle():
+    """Every random stream of an ensemble network is keyed by its own seed and local
+    indices (generated connections, Poisson stream), so on the oracle a network simulated
+    alone gives the same spikes, neuron by neuron, as inside the ensemble."""
+    import oracle as orc
+    spec = ensemble_spec(n_networks=6, seed=11, median=1000, lo=600, hi=1400)
+    o = orc.Oracle()
+    groups, layout = build_ensemble(o, spec)
+    o.Simulate(100.0)
+    counts = {m: np.asarray(o.GetStatus(g, "spike_count")).ravel() for m, g in groups.items()}
+    assert sum(c.sum() for c in counts.values()) > 0
+    for i in (0, 1, 5):
+        model, off, n = layout[i]
+        a = orc.Oracle()
+        g1, l1 = build_ensemble(a, [spec[i]])
+        a.Simulate(100.0)
+        alone = np.asarray(a.GetStatus(g1[model], "spike_count")).ravel()
+        assert np.array_equal(alone, counts[model][off:off + n])

@@ -115,6 +115,54 @@ def test_simulation_step_api_matches_simulate():
     assert max(v) > 0.0
 
 
+def _step_param_changes(api, stepwise):
+    """A Poisson rate and the I_e of an aeif and an iaf group changed between steps of
+    a StartSimulation / SimulationStep loop (stepwise) or between Simulate calls."""
+    api.SetKernelStatus("rnd_seed", 31)
+    pg = api.Create("poisson_generator")
+    api.SetStatus(pg, "rate", 3000.0)
+    a = api.Create("aeif_cond_beta_multisynapse", 40, 2)
+    api.SetStatus(a, {"E_rev": [0.0, -85.0]})
+    b = api.Create("iaf_psc_exp", 20)
+    api.Connect(pg, a, {"rule": "all_to_all"}, {"weight": 0.5, "delay": 1.0, "receptor": 0})
+    api.Connect(pg, b, {"rule": "all_to_all"}, {"weight": 30.0, "delay": 1.0})
+    api.ActivateSpikeCount(a)
+    api.ActivateSpikeCount(b)
+    phases = [(300, None), (300, (9000.0, 400.0, 300.0)), (300, (0.0, 0.0, 0.0))]
+    out = []
+    if stepwise:
+        api.SetSimTime(90.0)
+        api.StartSimulation()
+    for k, change in phases:
+        if change is not None:
+            api.SetStatus(pg, "rate", change[0])
+            api.SetStatus(a, "I_e", change[1])
+            api.SetStatus(b, "I_e", change[2])
+        if stepwise:
+            for _ in range(k):
+                api.SimulationStep()
+        else:
+            api.Simulate(k * 0.1)
+        out.append(np.concatenate([np.asarray(api.GetStatus(a, "spike_count")).ravel(),
+                                   np.asarray(api.GetStatus(b, "spike_count")).ravel()]))
+    if stepwise:
+        api.EndSimulation()
+    return out
+
+
+def test_parameter_changes_between_simulation_steps():
+    """Parameters set between SimulationStep calls apply from the next step, as the
+    reference's setters write to the device at once: the same spikes as setting them
+    between Simulate calls on the oracle."""
+    got = _step_param_changes(ngpu, True)
+    ref = _step_param_changes(orc.Oracle(), False)
+    for x, y in zip(got, ref):
+        assert np.array_equal(x, y)
+    # each change shows: more spikes in phase 2 than in phase 1, none added in phase 3
+    d1, d2, d3 = got[0].sum(), got[1].sum() - got[0].sum(), got[2].sum() - got[1].sum()
+    assert d2 > d1 and d3 < d2
+
+
 def test_status_after_simulate_matches_oracle():
     def run(api):
         api.SetKernelStatus("rnd_seed", 21)
@@ -437,3 +485,57 @@ def test_many_receptor_ports_bitexact(model, nport):
     assert np.array_equal(c_gpu, c_orc)
     assert np.array_equal(np.float32(d_gpu), np.float32(d_orc))
     assert ngpu.GetStats()["status"] == 0
+
+
+def _iaf_singular(api, tau_ex):
+    """iaf_psc_exp neurons whose excitatory synaptic time constant equals (or nearly equals)
+    the membrane time constant: the propagator's singular branch
+    (src/propagator_stability.cu:31-52)."""
+    n = api.Create("iaf_psc_exp", 2)
+    api.SetStatus(n, {"tau_m": 10.0, "tau_ex": tau_ex, "C_m": 250.0})
+    sg = api.Create("spike_generator")
+    api.SetStatus(sg, {"spike_times": [1.0, 4.0, 4.5, 12.0]})
+    api.Connect(sg, n, {"rule": "all_to_all"}, {"weight": 300.0, "delay": 1.0, "receptor": 0})
+    rec = api.CreateRecord("", ["V_m_rel", "V_m_rel"], [n[0], n[1]], [0, 0])
+    api.Simulate(40.0)
+    return np.asarray(api.GetRecordData(rec), dtype=np.float64)[:, 1], n
+
+
+@pytest.mark.parametrize("tau_ex", [10.0, 10.05])
+def test_iaf_propagator_singular_branch(tau_ex):
+    v_gpu, n = _iaf_singular(ngpu, tau_ex)
+    v32, _ = _iaf_singular(orc.Oracle(fp64=False), tau_ex)
+    v64, _ = _iaf_singular(orc.Oracle(fp64=True), tau_ex)
+    assert np.array_equal(np.float32(v_gpu), np.float32(v32))
+    assert np.max(np.abs(v_gpu - v64)) / np.max(np.abs(v64)) < 1e-5
+    assert v_gpu.max() > 1.0
+    if tau_ex == 10.0:
+        # P21ex = h / C_m * exp(-h / tau) in the singular case
+        p21 = ngpu.GetStatus(n[0], "P21ex")[0]
+        assert abs(p21 - 0.1 / 250.0 * math.exp(-0.1 / 10.0)) < 1e-9
+
+
+def _aeif_guard(api):
+    """aeif neurons started outside the ExternalUpdate guard bounds
+    (src/aeif_cond_beta_multisynapse_kernel.h:196-207): V_m < -1e3 mV, w > 1e6 pA, w < -1e6 pA
+    and one neuron inside them.  The guard resets V_m to V_reset and w to 0."""
+    n = api.Create("aeif_cond_beta_multisynapse", 4, 2)
+    api.SetStatus(n, {"E_rev": [0.0, -85.0], "I_e": 300.0})
+    api.SetStatus(n[0:1], {"V_m": -2000.0})
+    api.SetStatus(n[1:2], {"w": 2.0e6})
+    api.SetStatus(n[2:3], {"w": -2.0e6})
+    rec = api.CreateRecord("", ["V_m"] * 4 + ["w"] * 4, [n[i] for i in range(4)] * 2, [0] * 8)
+    api.Simulate(5.0)
+    return np.asarray(api.GetRecordData(rec), dtype=np.float64)
+
+
+def test_aeif_state_guard_resets():
+    d_gpu = _aeif_guard(ngpu)
+    d_orc = _aeif_guard(orc.Oracle(fp64=False))
+    assert np.array_equal(np.float32(d_gpu), np.float32(d_orc))
+    assert ngpu.GetStats()["status"] & 4        # the numeric-guard status bit
+    # after the first step the three guarded neurons sit near V_reset with w near 0
+    row = d_gpu[1]
+    for i in range(3):
+        assert abs(row[1 + i] + 60.0) < 5.0 and abs(row[5 + i]) < 10.0
+    assert abs(row[4] + 70.6) < 5.0

@@ -175,3 +175,12 @@ def test_bound_mode_is_a_floor():
     assert res["bound"][0] < res["plain"][0] and res["bound"][0] < res["const"][0]
     assert res["bound"][2] == 0          # the bound never needs a rejected trial
     assert abs(res["bound"][1] - res["plain"][1]) <= 0.02 * res["plain"][1]
+
+
+def test_step_bound_script_small():
+    """tests/step_bound.py (the floor of RK5 evaluations behind the learned-step
+    comparison) at a short window: the bound never needs more evaluations than plain."""
+    from step_bound import evals
+    p, rp = evals(43, 1.0, False, warm_ms=10.0, t_ms=10.0)
+    b, rb = evals(43, 1.0, True, warm_ms=10.0, t_ms=10.0)
+    assert 60.0 <= b <= p

@@ -92,3 +92,29 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
                  edge.data_ptr(), None)
     assert rc == -1 and ngpu.GetErrorCode() == 2
     assert "segments" in ngpu.GetErrorMessage()
+
+
+def test_noalloc_reports_out_of_range_index_then_recovers():
+    """A source or delay index outside the declared ranges is reported through the shared
+    status word of the scratch array; the next valid call starts from a cleared word and
+    packs like the allocating entry point."""
+    import torch
+    alloc = bind("NGPU_BuildDeliveryCsr")
+    noalloc = bind("NGPU_BuildDeliveryCsrNoAlloc")
+    n_nodes, dspan = 3000, 7
+    for field, bad_value in ((0, n_nodes), (1, dspan)):
+        edges = list(device_edges(20_000, n_nodes, dspan, 4 + field))
+        bad = edges[field].clone()
+        bad[123] = bad_value
+        off = torch.zeros(n_nodes * dspan + 1, dtype=torch.int64, device=bad.device)
+        edge = torch.zeros(2 * 20_000, dtype=torch.int32, device=bad.device)
+        args = [x.data_ptr() for x in (edges[0], edges[1], edges[2], edges[3])]
+        args[field] = bad.data_ptr()
+        torch.cuda.synchronize()
+        rc = noalloc(*args, 20_000, n_nodes, dspan, off.data_ptr(), edge.data_ptr(), None)
+        torch.cuda.synchronize()
+        assert rc == -1 and ngpu.GetErrorCode() != 0
+        assert "out of range" in ngpu.GetErrorMessage()
+        ref = pack(alloc, edges, n_nodes, dspan)
+        again = pack(noalloc, edges, n_nodes, dspan)
+        same_segments(ref, again)
