@@ -66,10 +66,12 @@ def parse():
     p.add_argument("--mapping", default="",
                    help="fixed launch mapping instead of the autotuner: update threads, register-capped "
                         "variant (0/1), delivery lane group, delivery blocks, RK5 budget and optionally "
-                        "programmatic launch (0/1), e.g. 64,1,32,592,1")
+                        "programmatic launch (0/1) and one RK5 trial per iteration (0/1), e.g. 64,1,32,592,1")
     p.add_argument("--batch-max", type=int, default=0, help="upper bound of the time-batch length")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the learned-step and ensemble measurements")
+    p.add_argument("--no-ref-cuda", action="store_true",
+                   help="skip the timing of the reference's own CUDA build (several minutes)")
     return p.parse_args()
 
 
@@ -149,12 +151,69 @@ def ensemble_run(ngpu, bio_ms=1000.0):
     st1, l1 = ngpu.GetStats(), ngpu.GetLaunchCount()
     rates, _ = per_network_rates(ngpu, groups, layout, counts0, bio_ms)
     n_neurons = int(sum(x["n"] for x in spec))
-    return {"networks": len(spec), "neurons": n_neurons, "synapses": ensemble_synapses(spec),
-            "bio_ms": bio_ms, "rtf": dev_s / (bio_ms / 1000.0),
-            "events_per_s": (st1["n_events"] - st0["n_events"]) / dev_s,
-            "launches_per_step": (l1 - l0) / (bio_ms / 0.1),
-            "rate_hz_min_median_max": [float(rates.min()), float(np.median(rates)), float(rates.max())],
-            "mapping": chosen, "build_s": build_s, "autotune_s": tune_s}
+    # kernel time per step (each kernel bracketed by events) against the graph-timed step:
+    # the difference bounds what a persistent launch could save over the captured graphs
+    prof = ngpu.ProfileSteps(300)
+    step_ms = dev_s * 1000.0 / (bio_ms / 0.1)
+    out = {"networks": len(spec), "neurons": n_neurons, "synapses": ensemble_synapses(spec),
+           "bio_ms": bio_ms, "rtf": dev_s / (bio_ms / 1000.0),
+           "events_per_s": (st1["n_events"] - st0["n_events"]) / dev_s,
+           "launches_per_step": (l1 - l0) / (bio_ms / 0.1),
+           "rate_hz_min_median_max": [float(rates.min()), float(np.median(rates)), float(rates.max())],
+           "mapping": chosen, "build_s": build_s, "autotune_s": tune_s,
+           "ms_per_step": step_ms, "kernel_ms_per_step": sum(prof),
+           "launch_gap_frac": max(0.0, 1.0 - sum(prof) / step_ms)}
+    # the same networks one after another, each alone in the engine with its own graphs and
+    # the default launch mapping: what batching them into one ensemble gains
+    seq_ms, seq_bio = 0.0, 200.0
+    t_seq = time.time()
+    for net in spec:
+        ngpu.Reset()
+        ngpu.SetVerbosityLevel(0)
+        build_ensemble(ngpu, [net])
+        ngpu.Calibrate()
+        ngpu.Simulate(20.0)
+        ngpu.Simulate(seq_bio)
+        seq_ms += ngpu.GetSimDeviceMs()
+    out["sequential_rtf"] = (seq_ms / 1000.0) / (seq_bio / 1000.0)
+    out["sequential_bio_ms_per_network"] = seq_bio
+    out["sequential_wall_s"] = time.time() - t_seq
+    out["batching_gain"] = out["sequential_rtf"] / out["rtf"]
+    ngpu.Reset()
+    return out
+
+
+def ref_cuda_leg(args):
+    """The reference's own CUDA build (oracle/_ref/libnestgpukernel.so, compiled from the
+    reference sources) on this GPU, through the same nestgpu.py interface in child processes
+    (tests/ref_runner.py; the reference keeps one network per process):
+      - the benchmark network, identical edges (the generated blocks as edge lists), 500 ms
+        first call, then 1000 ms timed as the reference's own "Simulation time" (wall time of
+        Simulate, src/nestgpu.cu:458-463);
+      - the microcircuit (workloads.microcircuit) through both libraries, same protocol."""
+    lib = os.path.join(HERE, "oracle", "_ref", "libnestgpukernel.so")
+    if not os.path.exists(lib):
+        return {"unavailable": "reference library not built (oracle/Makefile.ref)"}
+    runner = os.path.join(HERE, "tests", "ref_runner.py")
+
+    def child(what, ref, extra_env=None, timeout=1500):
+        env = dict(os.environ)
+        env.pop("NESTGPU_LIB", None)
+        if ref:
+            env["NESTGPU_LIB"] = lib
+        env.update(extra_env or {})
+        p = subprocess.run([sys.executable, runner, what], env=env, capture_output=True, text=True,
+                           timeout=timeout)
+        if p.returncode != 0:
+            return {"error": p.stderr[-500:]}
+        return json.loads([x for x in p.stdout.splitlines() if x.startswith("JSON:")][-1][5:])
+
+    out = {"library": "oracle/_ref/libnestgpukernel.so (reference sources, nvcc 12.9, sm_100, maxrregcount 55)",
+           "protocol": "500 ms first call, then Simulate(1000) wall time, child process per run"}
+    out["network_1M"] = child("timing_gen:%g:500:1000" % args.scale, True)
+    out["microcircuit"] = child("microcircuit:1.0:1000:500", True)
+    out["microcircuit_engine"] = child("microcircuit:1.0:1000:500", False, {"NGPU_AUTOTUNE": "1"})
+    return out
 
 
 def rank_reducers(dist, device):
@@ -212,6 +271,8 @@ def engine_arm(args):
         th, occ, grp, blk, bud = vals[:5]
         if len(vals) > 5:
             ngpu.SetProgrammaticLaunch(vals[5])
+        if len(vals) > 6:
+            ngpu.SetUpdateTrialIter(vals[6])
         ngpu.SetUpdateThreads(th)
         ngpu.SetUpdateOccupancy(occ)
         ngpu.SetDeliverGroup(grp)
@@ -339,6 +400,17 @@ def engine_arm(args):
         from workloads import learned_vs_plain
         result["rk5_learned"] = [learned_vs_plain(ngpu, w) for w in (0.1, 1.0)]
         result["ensemble"] = ensemble_run(ngpu)
+    if WORLD == 1 and not args.no_ref_cuda:
+        rc = ref_cuda_leg(args)
+        net = rc.get("network_1M", {})
+        if "rtf" in net:
+            rc["rtf_ratio"] = net["rtf"] / rtf                  # reference RTF / engine RTF
+            rc["engine_rtf"] = rtf
+            rc["engine_rate_hz"] = rate_hz
+        mc, mce = rc.get("microcircuit", {}), rc.get("microcircuit_engine", {})
+        if "rtf" in mc and "rtf" in mce:
+            rc["rtf_ratio_microcircuit"] = mc["rtf"] / mce["rtf"]
+        result["ref_cuda"] = rc
     if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_sample(steps=1, warmup=0)["cpu_baseline"]
     if RANK == 0:

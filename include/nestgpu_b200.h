@@ -257,6 +257,14 @@ int NGPU_ConnectFixedIndegreeGPU(int i_source, int n_source, int i_target, int n
                                  int port, float weight, float delay_min, float delay_max,
                                  unsigned long long seed);
 
+/* Connect calls with the fixed_total_number, fixed_indegree or fixed_outdegree rule, static
+   synapses and at least n edges (default 65536) keep their random numbers (the same cuRAND
+   draws as otherwise), weights and delays on the device; their edges are expanded into the
+   delivery layout on the device at calibration and reach the host connection store only when
+   a connection query needs them.  Needs a GPU; results and GetConnections do not depend on
+   it.  No counterpart in the reference (src/connect_rules.h:161-338 expands on the host). */
+int NGPU_SetDeviceRuleMinEdges(long long n);
+
 /* poisson_generator nodes i_node .. i_node+n_node-1 draw from Poisson streams stream ..
    stream+n_node-1 (before calibration).  A generator's draw for its j-th out-edge (in
    connection order) at time index t depends only on (kernel seed, stream, j, t); by default
@@ -334,6 +342,10 @@ int NGPU_SetUpdateThreads(int n);
 /* 1: use the register-capped variant of the aeif update kernel (three 256-thread blocks per
    SM, more warps in flight, a few register spills); 0: the unconstrained one (default). */
 int NGPU_SetUpdateOccupancy(int on);
+/* 1: the aeif update kernel advances one RK5 trial per loop iteration (a rejected trial is
+   retried in the next iteration beside the neighbouring lanes' next trials); 0: one whole
+   step, rejected trials included, per iteration (default).  Results do not depend on it. */
+int NGPU_SetUpdateTrialIter(int on);
 /* Lanes per spike-delivery work item (8, 16 or 32; default 32): one item is the out-edge
    segment of one (source, delay) pair; short segments leave fewer lanes idle with small
    groups. */
@@ -365,9 +377,10 @@ int NGPU_TestBarrierTimeout(int extra);
    values. */
 int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliver_blocks,
                   int *rk5_budget);
-/* The current launch mapping: writes min(n, 7) of {update block size, register-capped update
+/* The current launch mapping: writes min(n, 8) of {update block size, register-capped update
    variant, delivery lane group, delivery grid (0: automatic), RK5 step budget, persistent loop,
-   programmatic launch} and returns 7 (-1 on error).  No counterpart in the reference. */
+   programmatic launch, trial-per-iteration update} and returns 8 (-1 on error).  No
+   counterpart in the reference. */
 int NGPU_GetLaunchMapping(int *vals, int n);
 /* Measured rate (1e9 per second) of FP64 reductions to uniformly random addresses of a
    `bytes`-byte device buffer, `n_ops` in total: the access pattern of the spike delivery's

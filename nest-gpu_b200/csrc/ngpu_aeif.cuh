@@ -447,6 +447,100 @@ __device__ __forceinline__ void stage_comb(float *r, const float *y, int NV, con
   }
 }
 
+// The pieces of one RK5 step (src/rk5.h:69-159), shared by the step-at-once form
+// (rk5_step) and the trial-per-iteration form of the plain batch kernel.
+//
+// rk5_begin: k1 = f(y) and the reciprocal error scale 1 / (|y| + |h k1| + scal_min), with the
+// h entering the step (the reference computes y_scal before clamping h).
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ void rk5_begin(const float *y, float h, const AeifQ<MODEL, PMAX, FIXED> &q, float refr,
+                                          float *k1, float *iys) {
+  constexpr int NVM = 2 + AeifShape<MODEL>::npv * PMAX;
+  const int NV = 2 + AeifShape<MODEL>::npv * q.ports();
+  aeif_derivs(y, k1, q, refr);
+#pragma unroll
+  for (int i = 0; i < NVM; i++) {
+    if (i < NV) {
+      float ys = __fadd_rn(__fadd_rn(fabsf(y[i]), fabsf(__fmul_rn(k1[i], h))), ck::scal_min);
+      iys[i] = __fdiv_rn(1.0f, ys);
+    }
+  }
+}
+
+// rk5_trial: one trial with h clamped to [hmin, hmax] (h keeps the clamped value): the
+// 5th-order solution in yn and the scaled error estimate (accept when <= 1).  Five
+// derivative evaluations.
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ float rk5_trial(const float *y, float &h, float hmin, float hmax,
+                                           const AeifQ<MODEL, PMAX, FIXED> &q, float refr, const float *k1,
+                                           const float *iys, float *yn) {
+  constexpr int NVM = 2 + AeifShape<MODEL>::npv * PMAX;
+  const int NV = 2 + AeifShape<MODEL>::npv * q.ports();
+  float k2[NVM], k3[NVM], k4[NVM], k5[NVM], k6[NVM];
+  if (h > hmax) h = hmax;
+  if (h < hmin) h = hmin;
+  // each stage's coefficients h * a_ij are formed just before the stage (short live ranges)
+  stage_comb<NVM, 1, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a21));
+  aeif_derivs(yn, k2, q, refr);
+  stage_comb<NVM, 2, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a31), k2, __fmul_rn(h, ck::a32));
+  aeif_derivs(yn, k3, q, refr);
+  stage_comb<NVM, 3, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a41), k2, __fmul_rn(h, ck::a42), k3,
+                            __fmul_rn(h, ck::a43));
+  aeif_derivs(yn, k4, q, refr);
+  stage_comb<NVM, 4, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a51), k2, __fmul_rn(h, ck::a52), k3,
+                            __fmul_rn(h, ck::a53), k4, __fmul_rn(h, ck::a54));
+  aeif_derivs(yn, k5, q, refr);
+  stage_comb<NVM, 5, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a61), k2, __fmul_rn(h, ck::a62), k3,
+                            __fmul_rn(h, ck::a63), k4, __fmul_rn(h, ck::a64), k5, __fmul_rn(h, ck::a65));
+  aeif_derivs(yn, k6, q, refr);
+  stage_comb<NVM, 4, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a71), k3, __fmul_rn(h, ck::a73), k4,
+                            __fmul_rn(h, ck::a74), k6, __fmul_rn(h, ck::a76));
+  const float f1 = __fmul_rn(h, ck::e1), f3 = __fmul_rn(h, ck::e3), f4 = __fmul_rn(h, ck::e4),
+              f5 = __fmul_rn(h, ck::e5), f6 = __fmul_rn(h, ck::e6);
+  // error terms two variables at a time (lane-exact, as in stage_comb)
+  float err = 0.0f;
+#pragma unroll
+  for (int i = 0; i < NVM; i += (FIXED ? 2 : 1)) {
+    if (i < NV) {
+      if (FIXED && i + 1 < NVM) {
+        float2 v = __fmul2_rn(make_float2(f1, f1), make_float2(k1[i], k1[i + 1]));
+        v = __ffma2_rn(make_float2(f3, f3), make_float2(k3[i], k3[i + 1]), v);
+        v = __ffma2_rn(make_float2(f4, f4), make_float2(k4[i], k4[i + 1]), v);
+        v = __ffma2_rn(make_float2(f5, f5), make_float2(k5[i], k5[i + 1]), v);
+        v = __ffma2_rn(make_float2(f6, f6), make_float2(k6[i], k6[i + 1]), v);
+        v = __fmul2_rn(v, make_float2(iys[i], iys[i + 1]));
+        const float a0 = fabsf(v.x);
+        err = (err > a0) ? err : a0;
+        if (i + 1 < NV) {
+          const float a1 = fabsf(v.y);
+          err = (err > a1) ? err : a1;
+        }
+      } else {
+        float v = __fmaf_rn(f6, k6[i], __fmaf_rn(f5, k5[i], __fmaf_rn(f4, k4[i],
+                                                                      __fmaf_rn(f3, k3[i], __fmul_rn(f1, k1[i])))));
+        float av = fabsf(__fmul_rn(v, iys[i]));
+        err = (err > av) ? err : av;
+      }
+    }
+  }
+  return __fmul_rn(err, ck::inv_eps);
+}
+
+// Step size of the next trial after a rejection: max(0.9 h err^-1/4, 0.1 h).
+__device__ __forceinline__ float rk5_shrink(float h, float err) {
+  float hnew = __fmul_rn(__fmul_rn(h, ck::coeff), __fdiv_rn(1.0f, __fsqrt_rn(__fsqrt_rn(err))));
+  float h01 = __fmul_rn(0.1f, h);
+  return (hnew > h01) ? hnew : h01;
+}
+
+// Step size proposed after an accepted trial: 0.9 h err^-1/5, or 5 h for a tiny error.
+__device__ __forceinline__ float rk5_grow(float h, float err, float hmin) {
+  if (err > ck::err_min) h = __fmul_rn(__fmul_rn(h, ck::coeff), exp_m(__fmul_rn(-0.2f, log_m(err))));
+  else h = __fmul_rn(5.0f, h);
+  if (!(h == h)) h = hmin;
+  return h;
+}
+
 // One accepted RK5 step (src/rk5.h:69-159); returns the number of derivative evaluations.
 // The error scale y_scal uses the h entering the step (the plain controller's), as in
 // the reference, whatever the learned proposal chooses as the first trial.
@@ -456,15 +550,8 @@ __device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmi
                                         unsigned *status, const float *smodel, const LearnCtx &L) {
   constexpr int NVM = 2 + AeifShape<MODEL>::npv * PMAX;
   const int NV = 2 + AeifShape<MODEL>::npv * q.ports();
-  float k1[NVM], k2[NVM], k3[NVM], k4[NVM], k5[NVM], k6[NVM], yn[NVM], iys[NVM];
-  aeif_derivs(y, k1, q, refr);
-#pragma unroll
-  for (int i = 0; i < NVM; i++) {
-    if (i < NV) {
-      float ys = __fadd_rn(__fadd_rn(fabsf(y[i]), fabsf(__fmul_rn(k1[i], h))), ck::scal_min);
-      iys[i] = __fdiv_rn(1.0f, ys);
-    }
-  }
+  float k1[NVM], yn[NVM], iys[NVM];
+  rk5_begin(y, h, q, refr, k1, iys);
   float f[LM == LM_PLAIN ? 1 : SM_NF];
   if (LM == LM_LOG || (LM == LM_PROPOSE && h < hmax)) step_features<MODEL, PMAX>(y, k1, q.ports(), h, hmax, f);
   if (LM == LM_PROPOSE && h < hmax) {
@@ -479,53 +566,7 @@ __device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmi
   int trials = 0;
   float err;
   for (;;) {
-    if (h > hmax) h = hmax;
-    if (h < hmin) h = hmin;
-    // each stage's coefficients h * a_ij are formed just before the stage (short live ranges)
-    stage_comb<NVM, 1, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a21));
-    aeif_derivs(yn, k2, q, refr);
-    stage_comb<NVM, 2, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a31), k2, __fmul_rn(h, ck::a32));
-    aeif_derivs(yn, k3, q, refr);
-    stage_comb<NVM, 3, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a41), k2, __fmul_rn(h, ck::a42), k3,
-                       __fmul_rn(h, ck::a43));
-    aeif_derivs(yn, k4, q, refr);
-    stage_comb<NVM, 4, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a51), k2, __fmul_rn(h, ck::a52), k3,
-                       __fmul_rn(h, ck::a53), k4, __fmul_rn(h, ck::a54));
-    aeif_derivs(yn, k5, q, refr);
-    stage_comb<NVM, 5, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a61), k2, __fmul_rn(h, ck::a62), k3,
-                       __fmul_rn(h, ck::a63), k4, __fmul_rn(h, ck::a64), k5, __fmul_rn(h, ck::a65));
-    aeif_derivs(yn, k6, q, refr);
-    stage_comb<NVM, 4, FIXED>(yn, y, NV, k1, __fmul_rn(h, ck::a71), k3, __fmul_rn(h, ck::a73), k4,
-                       __fmul_rn(h, ck::a74), k6, __fmul_rn(h, ck::a76));
-    const float f1 = __fmul_rn(h, ck::e1), f3 = __fmul_rn(h, ck::e3), f4 = __fmul_rn(h, ck::e4),
-                f5 = __fmul_rn(h, ck::e5), f6 = __fmul_rn(h, ck::e6);
-    // error terms two variables at a time (lane-exact, as in stage_comb)
-    err = 0.0f;
-#pragma unroll
-    for (int i = 0; i < NVM; i += (FIXED ? 2 : 1)) {
-      if (i < NV) {
-        if (FIXED && i + 1 < NVM) {
-          float2 v = __fmul2_rn(make_float2(f1, f1), make_float2(k1[i], k1[i + 1]));
-          v = __ffma2_rn(make_float2(f3, f3), make_float2(k3[i], k3[i + 1]), v);
-          v = __ffma2_rn(make_float2(f4, f4), make_float2(k4[i], k4[i + 1]), v);
-          v = __ffma2_rn(make_float2(f5, f5), make_float2(k5[i], k5[i + 1]), v);
-          v = __ffma2_rn(make_float2(f6, f6), make_float2(k6[i], k6[i + 1]), v);
-          v = __fmul2_rn(v, make_float2(iys[i], iys[i + 1]));
-          const float a0 = fabsf(v.x);
-          err = (err > a0) ? err : a0;
-          if (i + 1 < NV) {
-            const float a1 = fabsf(v.y);
-            err = (err > a1) ? err : a1;
-          }
-        } else {
-          float v = __fmaf_rn(f6, k6[i], __fmaf_rn(f5, k5[i], __fmaf_rn(f4, k4[i],
-                                                                        __fmaf_rn(f3, k3[i], __fmul_rn(f1, k1[i])))));
-          float av = fabsf(__fmul_rn(v, iys[i]));
-          err = (err > av) ? err : av;
-        }
-      }
-    }
-    err = __fmul_rn(err, ck::inv_eps);
+    err = rk5_trial(y, h, hmin, hmax, q, refr, k1, iys, yn);
     nd += 5;
     trials++;
     if (err <= 1.0f || h <= hmin_acc) break;
@@ -533,9 +574,7 @@ __device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmi
       atomicOr(status, ST_RK5_TRIALS);
       break;
     }
-    float hnew = __fmul_rn(__fmul_rn(h, ck::coeff), __fdiv_rn(1.0f, __fsqrt_rn(__fsqrt_rn(err))));
-    float h01 = __fmul_rn(0.1f, h);
-    h = (hnew > h01) ? hnew : h01;
+    h = rk5_shrink(h, err);
   }
   if (LM == LM_LOG) {
     const unsigned long long pos = atomicAdd(L.log_cursor, 1ULL);
@@ -548,14 +587,17 @@ __device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmi
     }
   }
   x += (double)h;
-  if (err > ck::err_min) h = __fmul_rn(__fmul_rn(h, ck::coeff), exp_m(__fmul_rn(-0.2f, log_m(err))));
-  else h = __fmul_rn(5.0f, h);
-  if (!(h == h)) h = hmin;
+  h = rk5_grow(h, err, hmin);
 #pragma unroll
   for (int i = 0; i < NVM; i++)
     if (i < NV) y[i] = yn[i];
   return nd;
 }
+
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ bool aeif_external(const AeifArgs &A, const SpikeOut &so, int i,
+                                              const AeifQ<MODEL, PMAX, FIXED> &q, float *y, float &refr,
+                                              double x, long long tidx, double tnow, int &guard);
 
 // One RK5 sub-step of neuron i from x towards the end of the time step tnow
 // (src/rk5.h:161-174), followed by the model's ExternalUpdate
@@ -570,6 +612,17 @@ __device__ __forceinline__ bool aeif_substep(const AeifArgs &A, const SpikeOut &
   const float hmax = (float)(x1 - x);
   nd += rk5_step<MODEL, PMAX, FIXED, LM>(x, y, h, A.hmin, A.hmin_acc, hmax, q, refr, so.status, smodel,
                                          A.learn);
+  return aeif_external(A, so, i, q, y, refr, x, tidx, tnow, guard);
+}
+
+// After an accepted RK5 sub-step: whether the time step is complete, then the model's
+// ExternalUpdate (src/aeif_cond_beta_multisynapse_kernel.h:190-226): state guards,
+// refractoriness, spike and reset.
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ bool aeif_external(const AeifArgs &A, const SpikeOut &so, int i,
+                                              const AeifQ<MODEL, PMAX, FIXED> &q, float *y, float &refr,
+                                              double x, long long tidx, double tnow, int &guard) {
+  const double x1 = tnow;
   const bool end = (x >= x1 - (double)A.hmin);
   if (++guard > ck::max_substeps) {
     atomicOr(so.status, ST_RK5_TRIALS);
@@ -675,7 +728,14 @@ __device__ __forceinline__ void warp_add(unsigned long long *ctr, unsigned long 
 // Main aeif kernel: one thread per neuron, steps m = 0..M-1 of the batch.
 // OCC = 1 caps the registers so that three 256-thread blocks fit on an SM (more warps
 // in flight to hide the dependent FP32 latency, at the price of a few spills).
-template <int MODEL, int PMAX, bool FIXED, int LM, int OCC = 0, bool UNI = false>
+// TPI = true (plain controller only): one RK5 trial per loop iteration.  A lane whose
+// trial is rejected retries in the next iteration, beside its neighbours' next trials,
+// instead of holding its whole warp in a second trial (with ~4% of the trials rejected,
+// most warps have a rejecting lane at most steps).  k1 and the error scale of the open
+// step stay in registers across iterations; a lane is handed to the straggler kernel
+// only between accepted steps, so every lane runs the same sequence of operations as
+// in the step-at-once form and results are identical.
+template <int MODEL, int PMAX, bool FIXED, int LM, int OCC = 0, bool UNI = false, bool TPI = false>
 __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const AeifArgs A, const SpikeOut so,
                                                          const Clock *clk, int k0, int M) {
   pdl_enter();
@@ -708,18 +768,63 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
     StepT t = step_at(cl, k0, 0, A.dt);
     double apf[PMAX];
     acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, 0);
-    while (m < M) {
-      if (budget == 0) {
-        deferred = true;
-        break;
+    if constexpr (TPI) {
+      static_assert(LM == LM_PLAIN, "one trial per iteration is a form of the plain controller");
+      float k1[NVM], iys[NVM];
+      bool open = false;     // a step has begun (k1, iys valid) and no trial was accepted yet
+      int trials = 0;
+      while (m < M) {
+        if (!open) {
+          if (budget == 0) {
+            deferred = true;
+            break;
+          }
+          rk5_begin(y, h, q, refr, k1, iys);
+          nd += 1;
+          trials = 0;
+          open = true;
+        }
+        if (budget > 0) budget--;
+        float yn[NVM];
+        const float err = rk5_trial(y, h, A.hmin, (float)(t.tnow - x), q, refr, k1, iys, yn);
+        nd += 5;
+        if (!(err <= 1.0f || h <= A.hmin_acc)) {
+          if (++trials < ck::max_trials) {
+            h = rk5_shrink(h, err);
+            continue;
+          }
+          atomicOr(so.status, ST_RK5_TRIALS);
+        }
+        open = false;
+        x += (double)h;
+        h = rk5_grow(h, err, A.hmin);
+#pragma unroll
+        for (int v = 0; v < NVM; v++)
+          if (v < NV) y[v] = yn[v];
+        if (aeif_external(A, so, i, q, y, refr, x, t.tidx, t.tnow, guard)) {
+          aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
+          guard = 0;
+          if (++m < M) {
+            t = step_at(cl, k0, m, A.dt);
+            acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
+          }
+        }
       }
-      if (budget > 0) budget--;
-      if (aeif_substep<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, nd, smodel, guard)) {
-        aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
-        guard = 0;
-        if (++m < M) {
-          t = step_at(cl, k0, m, A.dt);
-          acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
+    } else {
+      while (m < M) {
+        if (budget == 0) {
+          deferred = true;
+          break;
+        }
+        if (budget > 0) budget--;
+        if (aeif_substep<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, nd, smodel,
+                                                 guard)) {
+          aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
+          guard = 0;
+          if (++m < M) {
+            t = step_at(cl, k0, m, A.dt);
+            acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
+          }
         }
       }
     }
@@ -788,7 +893,19 @@ int launch_aeif_p(const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k
   dim3 grid((A.n + tb - 1) / tb), block(tb);
   bool done = false;
   if constexpr (LM == LM_PLAIN && FIXED) {
-    if (A.occupancy && A.uniform) {
+    if (A.trial_iter && A.occupancy && A.uniform) {
+      launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1, true, true>, grid, block, 0, st, A, so, clk, k0, M);
+      done = true;
+    } else if (A.trial_iter && A.uniform) {
+      launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0, true, true>, grid, block, 0, st, A, so, clk, k0, M);
+      done = true;
+    } else if (A.trial_iter && A.occupancy) {
+      launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1, false, true>, grid, block, 0, st, A, so, clk, k0, M);
+      done = true;
+    } else if (A.trial_iter) {
+      launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0, false, true>, grid, block, 0, st, A, so, clk, k0, M);
+      done = true;
+    } else if (A.occupancy && A.uniform) {
       launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1, true>, grid, block, 0, st, A, so, clk, k0, M);
       done = true;
     } else if (A.occupancy) {

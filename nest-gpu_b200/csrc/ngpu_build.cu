@@ -62,6 +62,58 @@ __global__ void gen_fill_kernel(GenBlockDev b, int dmin, int dspan, unsigned lon
   }
 }
 
+// Edge e of a rule block (see RuleBlockDev): source and target nodes, weight, delay [ms].
+__device__ __forceinline__ void rule_edge(const RuleBlockDev &b, long long e, int &src, int &tgt, float &w,
+                                          float &d) {
+  int is, it;
+  if (b.rule == 2) {
+    is = (int)(b.rnd[2 * e] % (unsigned)b.ns);
+    it = (int)(b.rnd[2 * e + 1] % (unsigned)b.nt);
+  } else {
+    const long long kk = e / b.degree;
+    const int i = (int)(e - kk * b.degree);
+    if (b.rule == 3) {
+      is = b.pick[i];
+      it = (int)kk;
+    } else {
+      is = (int)kk;
+      it = b.pick[i];
+    }
+  }
+  src = b.src_arr ? b.src_arr[is] : b.src0 + is;
+  tgt = b.tgt_arr ? b.tgt_arr[it] : b.tgt0 + it;
+  w = b.warr ? b.warr[e] : b.w;
+  d = b.darr ? b.darr[e] : b.d_ms;
+}
+
+// Delay step of a delay in ms: round(d / dt) - 1 (src/connect.cu:49), float arithmetic.
+__device__ __forceinline__ int delay_step(float d, float dt) { return (int)roundf(__fdiv_rn(d, dt)) - 1; }
+
+__global__ void rule_count_kernel(RuleBlockDev b, int dmin, int dspan, unsigned long long *cnt) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < b.n_edges;
+       e += (long long)gridDim.x * blockDim.x) {
+    int s, t;
+    float w, d;
+    rule_edge(b, e, s, t, w, d);
+    atomicAdd(&cnt[(size_t)s * dspan + (delay_step(d, b.dt) - dmin)], 1ULL);
+  }
+}
+
+__global__ void rule_fill_kernel(RuleBlockDev b, int dmin, int dspan, unsigned long long *cursor, EdgeW *edge,
+                                 const unsigned *node_acc0, const int *node_gn) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < b.n_edges;
+       e += (long long)gridDim.x * blockDim.x) {
+    int s, t;
+    float w, d;
+    rule_edge(b, e, s, t, w, d);
+    const unsigned long long pos = atomicAdd(&cursor[(size_t)s * dspan + (delay_step(d, b.dt) - dmin)], 1ULL);
+    EdgeW x;
+    x.acc = node_acc0[t] + (unsigned)b.port * (unsigned)node_gn[t];
+    x.w = w;
+    edge[pos] = x;
+  }
+}
+
 __global__ void host_edge_scatter_kernel(size_t n, const long long *key, const int *rank,
                                          const EdgeW *ew, const unsigned long long *off, EdgeW *edge) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -88,8 +140,9 @@ static void ck(cudaError_t e, const char *what) {
 void build_csr_device(int n_nodes, int dmin, int dspan, const std::vector<int> &cnt_host,
                       const std::vector<long long> &h_key, const std::vector<int> &h_rank,
                       const std::vector<EdgeW> &h_ew, const std::vector<GenBlockDev> &blocks,
-                      unsigned long long **d_off_out, EdgeW **d_edge_out, size_t *n_edge_out,
-                      unsigned char *d_has_out, cudaStream_t st) {
+                      const std::vector<RuleBlockDev> &rblocks, const unsigned *d_node_acc0,
+                      const int *d_node_gn, unsigned long long **d_off_out, EdgeW **d_edge_out,
+                      size_t *n_edge_out, unsigned char *d_has_out, cudaStream_t st) {
   const size_t nkey = (size_t)n_nodes * dspan;
   unsigned long long *d_cnt = nullptr, *d_off = nullptr, *d_cursor = nullptr;
   int *d_cnt_host = nullptr;
@@ -105,6 +158,7 @@ void build_csr_device(int n_nodes, int dmin, int dspan, const std::vector<int> &
   }
   const int gb = 148 * 8, tb = 256;
   for (const auto &b : blocks) gen_count_kernel<<<gb, tb, 0, st>>>(b, dmin, dspan, d_cnt);
+  for (const auto &b : rblocks) rule_count_kernel<<<gb, tb, 0, st>>>(b, dmin, dspan, d_cnt);
   size_t tmp_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_cnt, d_off, nkey + 1, st);
   void *d_tmp = nullptr;
@@ -132,10 +186,12 @@ void build_csr_device(int n_nodes, int dmin, int dspan, const std::vector<int> &
     cudaFree(d_rank);
     cudaFree(d_hew);
   }
-  if (!blocks.empty()) {
+  if (!blocks.empty() || !rblocks.empty()) {
     ck(cudaMalloc(&d_cursor, nkey * sizeof(unsigned long long)), "cudaMalloc");
     cursor_init_kernel<<<gb, tb, 0, st>>>(nkey, d_off, d_cnt_host, d_cursor);
     for (const auto &b : blocks) gen_fill_kernel<<<gb, tb, 0, st>>>(b, dmin, dspan, d_cursor, d_edge);
+    for (const auto &b : rblocks)
+      rule_fill_kernel<<<gb, tb, 0, st>>>(b, dmin, dspan, d_cursor, d_edge, d_node_acc0, d_node_gn);
   }
   has_out_kernel<<<gb, tb, 0, st>>>(n_nodes, dspan, d_off, d_has_out);
   ck(cudaStreamSynchronize(st), "build");

@@ -792,6 +792,21 @@ int NGPU_SetUpdateOccupancy(int on) {
   }, -1);
 }
 
+int NGPU_SetDeviceRuleMinEdges(long long n) {
+  return guard([&] {
+    E().device_rule_min_edges = n;
+    return 0;
+  }, -1);
+}
+
+int NGPU_SetUpdateTrialIter(int on) {
+  return guard([&] {
+    E().update_trial_iter = on ? 1 : 0;
+    E().invalidate_graphs();
+    return 0;
+  }, -1);
+}
+
 // Test hook: the persistent loop's grid barriers wait for `extra` blocks more than the launch
 // has, so their bounded waits run out (the kernel records a timeout and returns).
 int NGPU_TestBarrierTimeout(int extra) {
@@ -830,10 +845,10 @@ int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliv
 
 int NGPU_GetLaunchMapping(int *vals, int n) {
   return guard([&] {
-    const int v[7] = {E().update_threads, E().update_occupancy, E().deliver_group, E().deliver_blocks_req,
-                      E().rk5_budget, E().persistent, E().launch_pdl};
-    for (int i = 0; i < n && i < 7; i++) vals[i] = v[i];
-    return 7;
+    const int v[8] = {E().update_threads, E().update_occupancy, E().deliver_group, E().deliver_blocks_req,
+                      E().rk5_budget, E().persistent, E().launch_pdl, E().update_trial_iter};
+    for (int i = 0; i < n && i < 8; i++) vals[i] = v[i];
+    return 8;
   }, -1);
 }
 

@@ -601,10 +601,236 @@ void Engine::connect1(int src, int tgt, int port, int syn_group, float w, float 
   order_valid_ = false;
 }
 
+static void cuda_check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw NgpuError(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+template <class T> T *Engine::dcopy(const T *h, size_t n) {
+  T *p = nullptr;
+  if (cudaMalloc((void **)&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    throw NgpuError("CUDA error: out of device memory for a connection call");
+  }
+  allocs_.push_back(p);
+  if (h && n && cudaMemcpy(p, h, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    throw NgpuError("CUDA error in a connection call");
+  return p;
+}
+
+// fixed_total_number / fixed_indegree / fixed_outdegree with static synapses and at least
+// device_rule_min_edges edges, when the connection generator is cuRAND's device generator:
+// the call draws the same random numbers as on the host path (the generator advances the
+// same way), keeps them on the device with its weight and delay arrays, and its edges are
+// expanded into the delivery layout at calibration (RuleBlockDev, ngpu_build.cu).  Returns
+// false (nothing drawn) when the call does not qualify or its arguments need the host path's
+// per-edge error reporting.
+bool Engine::connect_rule_device(int rule, const int *src_arr, int src0, int ns, const int *tgt_arr, int tgt0,
+                                 int nt, int degree, int port, float w, float d, const float *warr,
+                                 const float *darr) {
+  enum { FIXED_TOTAL_NUMBER = 2, FIXED_INDEGREE = 3, FIXED_OUTDEGREE = 4 };
+  if (rule != FIXED_TOTAL_NUMBER && rule != FIXED_INDEGREE && rule != FIXED_OUTDEGREE) return false;
+  if (ns <= 0 || nt <= 0 || degree <= 0 || port < 0 || port > 255) return false;
+  const size_t n_edges = rule == FIXED_TOTAL_NUMBER ? (size_t)degree
+                                                    : (size_t)(rule == FIXED_INDEGREE ? nt : ns) * degree;
+  if ((long long)n_edges < device_rule_min_edges) return false;
+  const int N = n_nodes();
+  for (int i = 0; i < ns; i++) {
+    const int s = src_arr ? src_arr[i] : src0 + i;
+    if (s < 0 || s >= N || groups_[node_group_[s]].model == M_POISS_GEN) return false;
+  }
+  for (int i = 0; i < nt; i++) {
+    const int t = tgt_arr ? tgt_arr[i] : tgt0 + i;
+    if (t < 0 || t >= N) return false;
+  }
+  // delays: all >= dt (else the host path reports the first offending edge), step range
+  int dlo = INT32_MAX, dhi = INT32_MIN;
+  if (darr) {
+    for (size_t e = 0; e < n_edges; e++) {
+      if (!(darr[e] >= dt)) return false;
+      const int st = (int)std::round(darr[e] / dt) - 1;
+      dlo = std::min(dlo, st);
+      dhi = std::max(dhi, st);
+    }
+  } else {
+    if (!(d >= dt)) return false;
+    dlo = dhi = (int)std::round(d / dt) - 1;
+  }
+  make_generator();
+  if (!gen_device_) return false;
+  const int thresh = 5;
+  RuleBlock b;
+  b.host_pos = c_src_.size();
+  b.dlo = dlo;
+  b.dhi = dhi;
+  RuleBlockDev &v = b.dev;
+  std::memset(&v, 0, sizeof(v));
+  v.rule = rule;
+  v.ns = ns;
+  v.nt = nt;
+  v.degree = degree;
+  v.port = port;
+  v.src0 = src0;
+  v.tgt0 = tgt0;
+  v.w = w;
+  v.d_ms = d;
+  v.n_edges = (long long)n_edges;
+  v.dt = dt;
+  if (rule == FIXED_TOTAL_NUMBER) {
+    // the same draw as random_int(2 * degree) on the host path, left on the device
+    unsigned *r = dcopy<unsigned>(nullptr, 2 * (size_t)degree);
+    if (curandGenerate(gen_, r, 2 * (size_t)degree) != CURAND_STATUS_SUCCESS) throw NgpuError("cuRAND error");
+    v.rnd = r;
+  } else {
+    // one pick shared by all targets (sources), as the host path computes it
+    const bool in = rule == FIXED_INDEGREE;
+    const int npool = in ? ns : nt;
+    if (degree > npool)
+      throw NgpuError(in ? "Indegree larger than number of source nodes"
+                         : "Outdegree larger than number of target nodes");
+    size_t n_rnd = degree;
+    if (npool >= thresh * degree) n_rnd *= 5;
+    std::vector<unsigned> rnd = random_int(n_rnd);
+    std::vector<int> pick;
+    if (npool < thresh * degree) {
+      pick.resize(npool);
+      std::iota(pick.begin(), pick.end(), 0);
+      for (int i = 0; i < degree; i++) {
+        int j = i + (int)(rnd[i] % (unsigned)(npool - i));
+        if (j != i) std::swap(pick[i], pick[j]);
+      }
+      pick.resize(degree);
+    } else {
+      std::vector<int> sorted;
+      for (int i = 0; i < degree; i++) {
+        int i1 = 0, j;
+        std::vector<int>::iterator itr;
+        do {
+          size_t ri = (size_t)i1 * degree + i;
+          if (ri >= rnd.size()) throw NgpuError("fixed-degree draw exhausted its random buffer");
+          j = (int)(rnd[ri] % (unsigned)npool);
+          itr = std::lower_bound(sorted.begin(), sorted.end(), j);
+          i1++;
+        } while (itr != sorted.end() && *itr == j);
+        sorted.insert(itr, j);
+        pick.push_back(j);
+      }
+    }
+    v.pick = dcopy<int>(pick.data(), pick.size());
+  }
+  if (src_arr) {
+    b.src_arr.assign(src_arr, src_arr + ns);
+    v.src_arr = dcopy<int>(src_arr, ns);
+  }
+  if (tgt_arr) {
+    b.tgt_arr.assign(tgt_arr, tgt_arr + nt);
+    v.tgt_arr = dcopy<int>(tgt_arr, nt);
+  }
+  if (warr) v.warr = dcopy<float>(warr, n_edges);
+  if (darr) v.darr = dcopy<float>(darr, n_edges);
+  rblocks_.push_back(std::move(b));
+  n_rule_edges_ += n_edges;
+  order_valid_ = false;
+  return true;
+}
+
+// Expand the device rule blocks into the host store, each at its place in call order (as
+// the host path would have inserted them), for the queries that read the host store.
+void Engine::materialize_rule_blocks() {
+  if (rblocks_.empty()) return;
+  cuda_check(cudaDeviceSynchronize(), "connection store");
+  const size_t old_n = c_src_.size();
+  std::vector<int> src, tgt, dly;
+  std::vector<unsigned char> port, syn;
+  std::vector<float> wgt;
+  const size_t total = old_n + n_rule_edges_;
+  src.reserve(total);
+  tgt.reserve(total);
+  dly.reserve(total);
+  port.reserve(total);
+  wgt.reserve(total);
+  if (!c_syn_.empty()) syn.reserve(total);
+  std::vector<std::pair<size_t, size_t>> shift;   // (old position, edges inserted up to it)
+  size_t pos = 0, inserted = 0;
+  auto copy_host = [&](size_t upto) {
+    for (; pos < upto; pos++) {
+      src.push_back(c_src_[pos]);
+      tgt.push_back(c_tgt_[pos]);
+      dly.push_back(c_d_[pos]);
+      port.push_back(c_port_[pos]);
+      wgt.push_back(c_w_[pos]);
+      if (!c_syn_.empty()) syn.push_back(c_syn_[pos]);
+    }
+  };
+  for (auto &b : rblocks_) {
+    copy_host(b.host_pos);
+    const RuleBlockDev &v = b.dev;
+    const size_t n = (size_t)v.n_edges;
+    std::vector<unsigned> rnd;
+    std::vector<int> pick;
+    std::vector<float> wa, da;
+    if (v.rnd) {
+      rnd.resize(2 * (size_t)v.degree);
+      cuda_check(cudaMemcpy(rnd.data(), v.rnd, rnd.size() * sizeof(unsigned), cudaMemcpyDeviceToHost), "rnd");
+    } else {
+      pick.resize(v.degree);
+      cuda_check(cudaMemcpy(pick.data(), v.pick, pick.size() * sizeof(int), cudaMemcpyDeviceToHost), "pick");
+    }
+    if (v.warr) {
+      wa.resize(n);
+      cuda_check(cudaMemcpy(wa.data(), v.warr, n * sizeof(float), cudaMemcpyDeviceToHost), "weights");
+    }
+    if (v.darr) {
+      da.resize(n);
+      cuda_check(cudaMemcpy(da.data(), v.darr, n * sizeof(float), cudaMemcpyDeviceToHost), "delays");
+    }
+    auto S = [&](int i) { return b.src_arr.empty() ? v.src0 + i : b.src_arr[i]; };
+    auto T = [&](int i) { return b.tgt_arr.empty() ? v.tgt0 + i : b.tgt_arr[i]; };
+    for (size_t e = 0; e < n; e++) {
+      int is, it;
+      if (v.rule == 2) {
+        is = (int)(rnd[2 * e] % (unsigned)v.ns);
+        it = (int)(rnd[2 * e + 1] % (unsigned)v.nt);
+      } else {
+        const size_t kk = e / v.degree;
+        const int i = (int)(e - kk * v.degree);
+        if (v.rule == 3) { is = pick[i]; it = (int)kk; } else { is = (int)kk; it = pick[i]; }
+      }
+      src.push_back(S(is));
+      tgt.push_back(T(it));
+      port.push_back((unsigned char)v.port);
+      wgt.push_back(v.warr ? wa[e] : v.w);
+      dly.push_back((int)std::round((v.darr ? da[e] : v.d_ms) / dt) - 1);
+      if (!c_syn_.empty()) syn.push_back(0);
+    }
+    inserted += n;
+    shift.push_back({b.host_pos, inserted});
+  }
+  copy_host(old_n);
+  // host-edge ids held elsewhere (plastic entries) move by the edges inserted before them
+  for (auto &pe : pl_of_edge_) {
+    size_t add = 0;
+    for (auto &sh : shift)
+      if (sh.first <= pe.first) add = sh.second;
+    pe.first += add;
+  }
+  c_src_.swap(src);
+  c_tgt_.swap(tgt);
+  c_d_.swap(dly);
+  c_port_.swap(port);
+  c_w_.swap(wgt);
+  if (!c_syn_.empty()) c_syn_.swap(syn);
+  rblocks_.clear();
+  n_rule_edges_ = 0;
+  order_valid_ = false;
+}
+
 void Engine::connect_rule(int rule, const int *src_arr, int src0, int ns, const int *tgt_arr, int tgt0,
                           int nt, int degree, int port, int syn_group, float w, float d,
                           const float *warr, const float *darr) {
   if (calibrated_) throw NgpuError("Connections cannot be created after calibration");
+  if (syn_group == 0 && connect_rule_device(rule, src_arr, src0, ns, tgt_arr, tgt0, nt, degree, port, w, d,
+                                            warr, darr))
+    return;
   auto S = [&](int i) { return src_arr ? src_arr[i] : src0 + i; };
   auto T = [&](int i) { return tgt_arr ? tgt_arr[i] : tgt0 + i; };
   auto one = [&](int is, int itn, size_t ia) {
@@ -732,6 +958,7 @@ void Engine::connect_arrays(size_t n, const int *src, const int *tgt, const unsi
 
 // Reference order: sources ascending, delay groups ascending, insertion order.
 void Engine::build_order() {
+  materialize_rule_blocks();
   if (order_valid_) return;
   const size_t E = c_src_.size();
   const int N = n_nodes();

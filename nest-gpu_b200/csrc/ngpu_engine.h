@@ -129,6 +129,7 @@ class Engine {
   int update_threads = 128;       // threads per block of the aeif update kernel (64, 128, 256)
   int deliver_group = 32;         // lanes per delivery work item (8, 16, 32)
   int update_occupancy = 0;       // 1: register-capped aeif update kernel
+  int update_trial_iter = 0;      // 1: aeif update kernel advances one RK5 trial per iteration
   int persistent = 0;             // iaf-only networks: persistent cooperative step loop
   int launch_pdl = -1;            // programmatic dependent launch of the batch kernels (-1: one-step batches)
   int barrier_extra = 0;          // test hook: blocks the persistent loop's barriers wait for in excess
@@ -178,7 +179,10 @@ class Engine {
   void connect_rule(int rule, const int *src_arr, int src0, int ns, const int *tgt_arr, int tgt0,
                     int nt, int degree, int port, int syn_group, float w, float d,
                     const float *warr, const float *darr);
-  size_t n_connections() const { return c_src_.size() + n_generated_; }
+  size_t n_connections() const { return c_src_.size() + n_generated_ + n_rule_edges_; }
+  // rule-based calls with at least this many edges are expanded on the device (a device
+  // cuRAND generator is needed); smaller ones go to the host store at once
+  long long device_rule_min_edges = 1LL << 16;
   // ids (source, group, index) in reference order, filtered (syn_group < 0: any group)
   std::vector<int> get_connections(const int *src_arr, int src0, int ns, const int *tgt_arr,
                                    int tgt0, int nt, int syn_group = -1);
@@ -273,6 +277,22 @@ class Engine {
   };
   std::vector<GenBlock> blocks_;
   size_t n_generated_ = 0;
+  // rule-based calls expanded on the device at calibration (RuleBlockDev): their random
+  // numbers and arrays stay on the device; the host store gets their edges only when a
+  // query needs them (materialize_rule_blocks), spliced in at their place in call order
+  struct RuleBlock {
+    size_t host_pos;                 // host-store edges inserted before the call
+    RuleBlockDev dev;                // device pointers (engine allocations)
+    std::vector<int> src_arr, tgt_arr;   // host copies of node arrays (empty: ranges)
+    int dlo, dhi;                    // delay-step range of the call's edges
+  };
+  std::vector<RuleBlock> rblocks_;
+  size_t n_rule_edges_ = 0;
+  bool connect_rule_device(int rule, const int *src_arr, int src0, int ns, const int *tgt_arr, int tgt0,
+                           int nt, int degree, int port, float w, float d, const float *warr,
+                           const float *darr);
+  void materialize_rule_blocks();
+  template <class T> T *dcopy(const T *h, size_t n);
   // reference order cache: permutation, group index and index-in-group per edge
   bool order_valid_ = false;
   std::vector<long long> ord_;          // edge ids in reference order
@@ -422,7 +442,8 @@ void pack_delivery_csr(const int *src, const int *dly, const unsigned *target, c
 void build_csr_device(int n_nodes, int dmin, int dspan, const std::vector<int> &cnt_host,
                       const std::vector<long long> &h_key, const std::vector<int> &h_rank,
                       const std::vector<EdgeW> &h_ew, const std::vector<GenBlockDev> &blocks,
-                      unsigned long long **d_off_out, EdgeW **d_edge_out, size_t *n_edge_out,
-                      unsigned char *d_has_out, cudaStream_t st);
+                      const std::vector<RuleBlockDev> &rblocks, const unsigned *d_node_acc0,
+                      const int *d_node_gn, unsigned long long **d_off_out, EdgeW **d_edge_out,
+                      size_t *n_edge_out, unsigned char *d_has_out, cudaStream_t st);
 
 }  // namespace ngpu

@@ -167,7 +167,6 @@ void Engine::calibrate() {
   n_acc_ = acc_total;
 
   // ---- connections: recurrent edges into CSR by (source, delay); poiss_gen edges apart
-  build_order();   // reference order: the canonical numbering of poiss_gen edges
   const size_t E = c_src_.size();
   std::vector<unsigned char> is_pg(N, 0);
   for (auto &g : groups_)
@@ -209,7 +208,37 @@ void Engine::calibrate() {
     dmax = std::max(dmax, d.dhi);
     gblocks.push_back(d);
   }
-  if (n_rec_edges == 0 && gblocks.empty()) { dmin = 0; dmax = 0; }
+  // rule blocks expanded on the device: their delay steps, and target ports checked here
+  // (the host path checks them edge by edge above)
+  std::vector<RuleBlockDev> rdev;
+  unsigned *d_node_acc0 = nullptr;
+  int *d_node_gn = nullptr;
+  if (!rblocks_.empty()) {
+    for (const auto &b : rblocks_) {
+      const RuleBlockDev &v = b.dev;
+      for (int i = 0; i < v.nt; i++) {
+        const int t = b.tgt_arr.empty() ? v.tgt0 + i : b.tgt_arr[i];
+        if (v.port >= groups_[node_group_[t]].nport)
+          throw NgpuError("receptor port " + std::to_string(v.port) + " out of range for target node " +
+                          std::to_string(t));
+      }
+      dmin = std::min(dmin, b.dlo);
+      dmax = std::max(dmax, b.dhi);
+      rdev.push_back(v);
+    }
+    std::vector<unsigned> acc0(N, 0);
+    std::vector<int> gn(N, 0);
+    for (auto &g : groups_)
+      for (int i = 0; i < g.n; i++) {
+        acc0[g.i0 + i] = (unsigned)(g.acc_off + (size_t)i);
+        gn[g.i0 + i] = g.n;
+      }
+    d_node_acc0 = dalloc<unsigned>(N);
+    d_node_gn = dalloc<int>(N);
+    cuda_check(cudaMemcpy(d_node_acc0, acc0.data(), N * sizeof(unsigned), cudaMemcpyHostToDevice), "node map");
+    cuda_check(cudaMemcpy(d_node_gn, gn.data(), N * sizeof(int), cudaMemcpyHostToDevice), "node map");
+  }
+  if (n_rec_edges == 0 && gblocks.empty() && rdev.empty()) { dmin = 0; dmax = 0; }
   dmin_ = dmin;
   dspan_ = dmax - dmin + 1;
   if (dspan_ > deliver_max_pairs())
@@ -254,8 +283,8 @@ void Engine::calibrate() {
     unsigned long long *d_off = nullptr;
     EdgeW *d_edge = nullptr;
     size_t n_edge = 0;
-    build_csr_device(N, dmin_, dspan_, cnt, hkey, hrank, hew, gblocks, &d_off, &d_edge, &n_edge,
-                     d_has_out_, stream_);
+    build_csr_device(N, dmin_, dspan_, cnt, hkey, hrank, hew, gblocks, rdev, d_node_acc0, d_node_gn, &d_off,
+                     &d_edge, &n_edge, d_has_out_, stream_);
     allocs_.push_back(d_off);
     allocs_.push_back(d_edge);
     d_ev_off_ = (long long *)d_off;
@@ -275,6 +304,15 @@ void Engine::calibrate() {
   {
     struct DE { int tgt; PoissonIn pe; };
     std::vector<DE> de;
+    // the generators' out-edges in reference order: source-major, delay groups ascending,
+    // insertion order (src/connect.cu:38-74)
+    std::vector<long long> pg_edges;
+    for (size_t e = 0; e < E; e++)
+      if (is_pg[c_src_[e]]) pg_edges.push_back((long long)e);
+    std::stable_sort(pg_edges.begin(), pg_edges.end(), [&](long long a, long long b) {
+      return c_src_[a] != c_src_[b] ? c_src_[a] < c_src_[b] : c_d_[a] < c_d_[b];
+    });
+    size_t q = 0;
     for (int s = 0; s < N; s++) {
       if (!is_pg[s]) continue;
       const Group &pg = groups_[node_group_[s]];
@@ -282,8 +320,8 @@ void Engine::calibrate() {
       const uint32_t set = pg.pg_stream.empty() ? 0xffffffffu : pg.pg_stream[s - pg.i0];
       const uint32_t stream = set == 0xffffffffu ? (uint32_t)gi : set;
       uint32_t id = 0;   // out-edges of this generator in connection order
-      for (long long p = src_first_[s]; p < src_first_[s + 1]; p++) {
-        long long e = ord_[p];
+      for (; q < pg_edges.size() && c_src_[pg_edges[q]] == s; q++) {
+        long long e = pg_edges[q];
         DE x;
         x.tgt = c_tgt_[e];
         x.pe.edge_id = id++;
@@ -320,7 +358,7 @@ void Engine::calibrate() {
 
   // ---- time batching: M steps per batch, M <= min delay in steps (spikes emitted inside
   //      a batch arrive after it); one accumulator slot per step of a batch
-  batch_ = (n_rec_edges || !gblocks.empty()) ? std::min(dmin_ + 1, MAX_BATCH) : MAX_BATCH;
+  batch_ = (n_rec_edges || !gblocks.empty() || !rdev.empty()) ? std::min(dmin_ + 1, MAX_BATCH) : MAX_BATCH;
   batch_ = std::max(1, std::min(batch_, batch_max));
   // plastic edges: one step per batch, so that each step's weight changes see the post-
   // synaptic spikes of the same step (src/nestgpu.cu:469-635 order)
@@ -691,6 +729,7 @@ AeifArgs Engine::aeif_args(Group &g) {
   A.srec = spike_rec(g);
   A.threads = update_threads;
   A.occupancy = update_occupancy;
+  A.trial_iter = update_trial_iter;
   A.uniform = 1;
   for (int j = 0; j < AEIF_NSCAL + AEIF_NPORTPAR * g.nport && j < AEIF_NPAR; j++)
     if (g.d_der[j]) A.uniform = 0;
@@ -1337,6 +1376,7 @@ int Engine::autotune(int steps, std::vector<std::pair<std::string, double>> *log
   std::vector<Knob> knobs = {
       single("update_threads", &update_threads, {64, 128, 256}),
       single("update_occupancy", &update_occupancy, {0, 1}),
+      single("update_trial_iter", &update_trial_iter, {0, 1}),
       deliver,
       single("rk5_budget", &rk5_budget, {0, 1, 2, 4, 8}),
       single("programmatic_launch", &launch_pdl, {0, 1}),

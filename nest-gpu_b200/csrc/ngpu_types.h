@@ -155,6 +155,7 @@ struct AeifArgs {
   int threads;           // threads per block of the main kernel (64, 128 or 256)
   int occupancy;         // 1: register-capped variant of the main kernel (more resident warps)
   int uniform;           // 1: every parameter is uniform over the group (no parameter arrays)
+  int trial_iter;        // 1: main kernel advances one RK5 trial per loop iteration
   int2 *strag_list;      // [n] (neuron, step of the batch) left for the straggler kernel
   int *strag_cnt;        // list length
   GroupSpikeRec srec;
@@ -269,6 +270,28 @@ struct GenBlockDev {
   float w;
   int dlo, dhi;            // delay indices, inclusive
   uint64_t seed;
+};
+
+// A rule-based connection call (src/connect_rules.h:161-338) whose edges are expanded on the
+// device at calibration.  The random numbers are the call's cuRAND draws, kept on the device:
+//   rule 2 (fixed_total_number): edge i: source index rnd[2i] % ns, target index rnd[2i+1] % nt,
+//          array index i;
+//   rule 3 (fixed_indegree): edge (kk, i): source index pick[i], target index kk, array index
+//          kk * degree + i;
+//   rule 4 (fixed_outdegree): edge (kk, i): source index kk, target index pick[i], array index
+//          kk * degree + i.
+// An index j maps to node src_arr[j] (or src0 + j), likewise for targets.
+struct RuleBlockDev {
+  int rule;
+  int ns, nt, degree, port;
+  int src0, tgt0;
+  const int *src_arr, *tgt_arr;   // node arrays or null (contiguous ranges)
+  const unsigned *rnd;            // rule 2: 2 * degree draws
+  const int *pick;                // rules 3, 4: degree picks shared by all targets (sources)
+  float w, d_ms;                  // uniform weight and delay [ms] ...
+  const float *warr, *darr;       // ... or per-edge arrays
+  long long n_edges;
+  float dt;
 };
 
 }  // namespace ngpu

@@ -174,6 +174,7 @@ if is_b200_engine:
     _c["NGPU_SetDeliverGroup"] = _bind("NGPU_SetDeliverGroup", _I, [_I])
     _c["NGPU_SetProgrammaticLaunch"] = _bind("NGPU_SetProgrammaticLaunch", _I, [_I])
     _c["NGPU_SetUpdateOccupancy"] = _bind("NGPU_SetUpdateOccupancy", _I, [_I])
+    _c["NGPU_SetUpdateTrialIter"] = _bind("NGPU_SetUpdateTrialIter", _I, [_I])
     _c["NGPU_GetBatchLength"] = _bind("NGPU_GetBatchLength", _I, [])
     _c["NGPU_SetPersistent"] = _bind("NGPU_SetPersistent", _I, [_I])
     _c["NGPU_TestBarrierTimeout"] = _bind("NGPU_TestBarrierTimeout", _I, [_I])
@@ -201,6 +202,7 @@ if is_b200_engine:
     _c["NGPU_ConnectFixedIndegreeGPU"] = _bind("NGPU_ConnectFixedIndegreeGPU", _I,
                                                [_I, _I, _I, _I, _I, _I, _F, _F, _F, ctypes.c_ulonglong])
     _c["NGPU_SetPoissonStream"] = _bind("NGPU_SetPoissonStream", _I, [_I, _I, ctypes.c_uint])
+    _c["NGPU_SetDeviceRuleMinEdges"] = _bind("NGPU_SetDeviceRuleMinEdges", _I, [ctypes.c_longlong])
     _c["NGPU_GetDeliveryShape"] = _bind("NGPU_GetDeliveryShape", _I, [ctypes.POINTER(_I)] * 3 +
                                         [ctypes.POINTER(ctypes.c_longlong)])
     _c["NGPU_GetDeliveryCsr"] = _bind("NGPU_GetDeliveryCsr", _I, [c_void_p] * 4)
@@ -1381,6 +1383,13 @@ def SetPoissonStream(nodes, stream):
     return _check(_c["NGPU_SetPoissonStream"](nodes.i0, nodes.n, int(stream) & 0xffffffff))
 
 
+def SetDeviceRuleMinEdges(n):
+    """Connect calls with the fixed_total_number / fixed_indegree / fixed_outdegree rule and
+    at least n edges are expanded on the device at calibration (engine extension)."""
+    _need_b200("SetDeviceRuleMinEdges")
+    return _check(_c["NGPU_SetDeviceRuleMinEdges"](int(n)))
+
+
 def GetDeliveryCsr():
     """The recurrent delivery layout after calibration (engine extension): a dict with
     n_nodes, dmin, dspan, seg_off (int64, n_nodes*dspan+1: segment (source s, delay step
@@ -1452,6 +1461,13 @@ def SetUpdateOccupancy(on=True):
     return _check(_c["NGPU_SetUpdateOccupancy"](1 if on else 0))
 
 
+def SetUpdateTrialIter(on=True):
+    """aeif update kernel advancing one RK5 trial per loop iteration (engine extension;
+    results are identical either way)."""
+    _need_b200("SetUpdateTrialIter")
+    return _check(_c["NGPU_SetUpdateTrialIter"](1 if on else 0))
+
+
 def SetDeliverGroup(g):
     """Lanes per spike-delivery work item: 8, 16 or 32 (engine extension)."""
     _need_b200("SetDeliverGroup")
@@ -1492,11 +1508,11 @@ def GetLaunchMapping():
     """The current launch mapping (engine extension): update block size and variant, delivery
     lane group and grid, RK5 step budget, persistent loop and programmatic launch."""
     _need_b200("GetLaunchMapping")
-    v = (ctypes.c_int * 7)()
-    _c["NGPU_GetLaunchMapping"](v, 7)
+    v = (ctypes.c_int * 8)()
+    _c["NGPU_GetLaunchMapping"](v, 8)
     _check()
     keys = ["update_threads", "update_occupancy", "deliver_group", "deliver_blocks", "rk5_budget",
-            "persistent", "programmatic_launch"]
+            "persistent", "programmatic_launch", "update_trial_iter"]
     return dict(zip(keys, [int(x) for x in v]))
 
 

@@ -244,14 +244,16 @@ def test_device_rng_matches_reference_generator_for_ints():
     assert np.array_equal(a, o.RandomInt(4096))
 
 
-@pytest.mark.parametrize("batch_max,budget", [(1, 0), (1, 2), (32, 0), (32, 1), (3, 4)])
-def test_time_batching_and_straggler_handoff_keep_results(batch_max, budget):
+@pytest.mark.parametrize("batch_max,budget,tpi", [(1, 0, 0), (1, 2, 0), (32, 0, 0), (32, 1, 0), (3, 4, 0),
+                                                  (1, 2, 1), (32, 1, 1), (32, 0, 1)])
+def test_time_batching_and_straggler_handoff_keep_results(batch_max, budget, tpi):
     """Integrating several steps per kernel (up to the minimum delay) and handing long RK5
     sequences to the straggler kernel are scheduling choices: spike counts and recorded
     traces equal the oracle's for every setting."""
     ngpu.SetHostRng(True)
     ngpu.SetBatchMax(batch_max)
     ngpu.SetRk5Budget(budget)
+    ngpu.SetUpdateTrialIter(tpi)
     c_gpu, d_gpu = fixed_train_network(ngpu, model="aeif_cond_beta_multisynapse", t_sim=150.0)
     c_orc, d_orc = fixed_train_network(orc.Oracle(), model="aeif_cond_beta_multisynapse", t_sim=150.0)
     assert np.array_equal(c_gpu, c_orc)
@@ -268,14 +270,16 @@ def test_profile_and_launch_counters():
     assert ngpu.GetStats()["steps"] == 250
 
 
-@pytest.mark.parametrize("threads,group,occ", [(64, 8, 0), (256, 16, 1), (128, 32, 1)])
-def test_launch_mappings_keep_results(threads, group, occ):
-    """The update block size and kernel variant and the delivery lane group change only
-    the launch mapping."""
+@pytest.mark.parametrize("threads,group,occ,tpi", [(64, 8, 0, 0), (256, 16, 1, 0), (128, 32, 1, 0),
+                                                   (64, 8, 0, 1), (128, 32, 1, 1)])
+def test_launch_mappings_keep_results(threads, group, occ, tpi):
+    """The update block size and kernel variants (register cap, one RK5 trial per loop
+    iteration) and the delivery lane group change only the launch mapping."""
     ngpu.SetHostRng(True)
     ngpu.SetUpdateThreads(threads)
     ngpu.SetDeliverGroup(group)
     ngpu.SetUpdateOccupancy(occ)
+    ngpu.SetUpdateTrialIter(tpi)
     c_gpu, d_gpu = fixed_train_network(ngpu, model="aeif_cond_beta_multisynapse")
     c_orc, d_orc = fixed_train_network(orc.Oracle(), model="aeif_cond_beta_multisynapse")
     assert c_gpu.sum() > 0
@@ -300,12 +304,13 @@ def test_microcircuit_slice_bitexact():
     assert np.array_equal(c_g, c_o)
 
 
-@pytest.mark.parametrize("occ", [0, 1])
-def test_per_neuron_parameters_bitexact(occ):
+@pytest.mark.parametrize("occ,tpi", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_per_neuron_parameters_bitexact(occ, tpi):
     """Receptor time constants drawn per neuron (parameter arrays instead of uniform kernel
     arguments): spike counts and derivative evaluations equal the oracle's."""
     from workloads import c4_network
     ngpu.SetUpdateOccupancy(occ)
+    ngpu.SetUpdateTrialIter(tpi)
     n_g = c4_network(ngpu, 5, n=300, drive_w=1.5)
     o = orc.Oracle()
     n_o = c4_network(o, 5, n=300, drive_w=1.5)
@@ -539,3 +544,47 @@ def test_aeif_state_guard_resets():
     for i in range(3):
         assert abs(row[1 + i] + 60.0) < 5.0 and abs(row[5 + i]) < 10.0
     assert abs(row[4] + 70.6) < 5.0
+
+
+@pytest.mark.parametrize("query_first", [False, True])
+def test_device_rule_expansion_keeps_connections(query_first):
+    """Connect calls expanded on the device (every fixed_total_number / fixed_indegree /
+    fixed_outdegree call, whatever its size) list the same connections, in the reference's
+    order, as the host path: queried after calibration (the device blocks are brought to the
+    host store then) or before it (the calibration then reads the host store)."""
+    from ref_runner import conn_arrays, rules_network
+    ngpu.SetDeviceRuleMinEdges(1 << 62)
+    rules_network(4321)
+    ngpu.Calibrate()
+    host = conn_arrays()
+    ngpu.Reset()
+    ngpu.SetVerbosityLevel(0)
+    ngpu.SetDeviceRuleMinEdges(0)
+    rules_network(4321)
+    if query_first:
+        early = conn_arrays()
+    ngpu.Calibrate()
+    dev = conn_arrays()
+    for k in ("source", "group", "index", "target", "port"):
+        assert dev[k] == host[k], k
+        if query_first:
+            assert early[k] == host[k], k
+    assert np.array_equal(np.float32(dev["weight"]), np.float32(host["weight"]))
+    assert np.array_equal(np.float32(dev["delay"]), np.float32(host["delay"]))
+
+
+def test_microcircuit_slice_device_rules_bitexact():
+    """The microcircuit slice with every projection expanded on the device gives the same
+    spikes as with the host expansion of the same cuRAND draws."""
+    from workloads import microcircuit
+    counts = []
+    for min_edges in (1 << 62, 0):
+        ngpu.Reset()
+        ngpu.SetVerbosityLevel(0)
+        ngpu.SetDeviceRuleMinEdges(min_edges)
+        pops = microcircuit(ngpu, scale=0.03)
+        ngpu.Simulate(150.0)
+        counts.append(np.concatenate([np.asarray(ngpu.GetStatus(p, "spike_count")).ravel() for p in pops]))
+        assert ngpu.GetStats()["status"] == 0
+    assert counts[0].sum() > 1000
+    assert np.array_equal(counts[0], counts[1])
