@@ -423,6 +423,12 @@ int NGPU_StepModelGet(float *params);
    reach the end of the time step; the error test, the rejection shrink and the controller
    update are unchanged, and invalid proposals fall back to the controller's h. */
 int NGPU_StepModelEnable(int on);
+/* 1: analysis mode for the learned proposal's ceiling: every RK5 step of the aeif groups
+   (1 to 4 receptor ports) starts from the largest step size that passes the unchanged error
+   test (a bisection whose trials are not counted), so the evaluation counter shows the floor
+   no step-size proposal can go below; 0: back to the plain controller.  No counterpart in the
+   reference. */
+int NGPU_StepBoundMode(int on);
 /* Network output for n feature rows, and the mean squared error with its gradient over the
    trainable block W1..b3 (1441 floats), computed by the GPU kernels on host buffers. */
 int NGPU_MlpForward(const float *params, const float *feat, int n, float *out);

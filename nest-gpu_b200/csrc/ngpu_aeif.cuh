@@ -541,6 +541,27 @@ __device__ __forceinline__ float rk5_grow(float h, float err, float hmin) {
   return h;
 }
 
+// Largest step in [hmin, hmax] whose trial passes the error test (hmax if it passes, else a
+// bisection in log h with 30 halvings): the first trial a perfect proposal would choose.
+// Analysis only (LM_BOUND); its trials are not counted as evaluations.
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __noinline__ float rk5_largest_passing(const float *y, float hmin, float hmax,
+                                                  const AeifQ<MODEL, PMAX, FIXED> &q, float refr, const float *k1,
+                                                  const float *iys) {
+  constexpr int NVM = 2 + AeifShape<MODEL>::npv * PMAX;
+  float tmp[NVM];
+  float hh = hmax;
+  if (rk5_trial(y, hh, hmin, hmax, q, refr, k1, iys, tmp) <= 1.0f) return hmax;
+  float lo = hmin, hi = hmax;
+  for (int it = 0; it < 30; it++) {
+    const float mid = (float)sqrt((double)lo * (double)hi);
+    hh = mid;
+    if (rk5_trial(y, hh, hmin, hmax, q, refr, k1, iys, tmp) <= 1.0f) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 // One accepted RK5 step (src/rk5.h:69-159); returns the number of derivative evaluations.
 // The error scale y_scal uses the h entering the step (the plain controller's), as in
 // the reference, whatever the learned proposal chooses as the first trial.
@@ -552,7 +573,8 @@ __device__ __forceinline__ int rk5_step(double &x, float *y, float &h, float hmi
   const int NV = 2 + AeifShape<MODEL>::npv * q.ports();
   float k1[NVM], yn[NVM], iys[NVM];
   rk5_begin(y, h, q, refr, k1, iys);
-  float f[LM == LM_PLAIN ? 1 : SM_NF];
+  if constexpr (LM == LM_BOUND) h = rk5_largest_passing(y, hmin, hmax, q, refr, k1, iys);
+  float f[(LM == LM_PLAIN || LM == LM_BOUND) ? 1 : SM_NF];
   if (LM == LM_LOG || (LM == LM_PROPOSE && h < hmax)) step_features<MODEL, PMAX>(y, k1, q.ports(), h, hmax, f);
   if (LM == LM_PROPOSE && h < hmax) {
     // the plain h would not reach the end of the time step: let the network propose

@@ -930,6 +930,10 @@ int NGPU_StepModelGet(float *params) {
   }, -1);
 }
 
+int NGPU_StepBoundMode(int on) {
+  return guard([&] { E().step_bound_mode(on != 0); return 0; }, -1);
+}
+
 int NGPU_StepModelEnable(int on) {
   return guard([&] { E().step_model_enable(on != 0); return 0; }, -1);
 }

@@ -245,6 +245,9 @@ class Engine {
   void step_model_get(float *p) const;
   bool has_step_model() const { return has_model_; }
   void step_model_enable(bool on);
+  // Analysis mode: every RK5 step starts from the largest step that passes the unchanged
+  // error test (the search is not counted), the floor of evaluations for any proposal.
+  void step_bound_mode(bool on);
   int learn_mode() const { return learn_mode_; }
   int batch_length() const { return batch_; }
   // captured graphs hold the launch mappings: drop them when a mapping knob changes

@@ -56,6 +56,7 @@ static int launch_learn_l(int model, const AeifArgs &A, const SpikeOut &so, cons
 int launch_aeif_learn(int model, const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                       cudaStream_t st) {
   if (A.learn.mode == LM_LOG) return launch_learn_l<LM_LOG>(model, A, so, clk, k0, M, st);
+  if (A.learn.mode == LM_BOUND) return launch_learn_l<LM_BOUND>(model, A, so, clk, k0, M, st);
   return launch_learn_l<LM_PROPOSE>(model, A, so, clk, k0, M, st);
 }
 

@@ -1512,6 +1512,8 @@ void Engine::step_model_get(float *p) const {
   std::copy(model_.begin(), model_.end(), p);
 }
 
+void Engine::step_bound_mode(bool on) { set_learn_mode(on ? LM_BOUND : LM_PLAIN); }
+
 void Engine::step_model_enable(bool on) {
   if (on && !has_model_) throw NgpuError("no step model has been trained or set");
   set_learn_mode(on ? LM_PROPOSE : LM_PLAIN);

@@ -47,6 +47,8 @@ constexpr int SM_NTRAIN = SM_B3 + 1 - SM_W1;     // 1441
 // logged tuple: features, accepted h, error of the accepted trial
 constexpr int LOG_W = SM_NF + 2;
 
-enum LearnMode { LM_PLAIN = 0, LM_LOG = 1, LM_PROPOSE = 2 };
+// LM_BOUND: analysis mode, every step starts from the largest step that passes the error
+// test (the floor of evaluations any proposal can reach; the search is not counted)
+enum LearnMode { LM_PLAIN = 0, LM_LOG = 1, LM_PROPOSE = 2, LM_BOUND = 3 };
 
 }  // namespace ngpu

@@ -197,6 +197,7 @@ if is_b200_engine:
     _c["NGPU_StepModelSet"] = _bind("NGPU_StepModelSet", _I, [c_void_p])
     _c["NGPU_StepModelGet"] = _bind("NGPU_StepModelGet", _I, [c_void_p])
     _c["NGPU_StepModelEnable"] = _bind("NGPU_StepModelEnable", _I, [_I])
+    _c["NGPU_StepBoundMode"] = _bind("NGPU_StepBoundMode", _I, [_I])
     _c["NGPU_MlpForward"] = _bind("NGPU_MlpForward", _I, [c_void_p, c_void_p, _I, c_void_p])
     _c["NGPU_MlpGrad"] = _bind("NGPU_MlpGrad", _I, [c_void_p, c_void_p, c_void_p, _I, c_void_p, c_void_p])
     _c["NGPU_ConnectFixedIndegreeGPU"] = _bind("NGPU_ConnectFixedIndegreeGPU", _I,
@@ -1590,6 +1591,13 @@ def StepModelSet(params):
     if p.size != _c["NGPU_StepModelNParams"]():
         raise ValueError("step model parameter vector has the wrong size")
     return _check(_c["NGPU_StepModelSet"](p.ctypes.data))
+
+
+def StepBoundMode(on=True):
+    """Analysis mode: every RK5 step starts from the largest step that passes the error test,
+    so the evaluation counter shows the floor for any step-size proposal (engine extension)."""
+    _need_b200("StepBoundMode")
+    return _check(_c["NGPU_StepBoundMode"](1 if on else 0))
 
 
 def StepModelEnable(on=True):

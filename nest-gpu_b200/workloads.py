@@ -210,18 +210,23 @@ def microcircuit(api, seed=12349, scale=1.0, dt=0.1):
 SAFETY_INDEX = 1463   # position of the safety factor in the step model's parameter vector
 
 
-def learned_vs_plain(ngpu, drive_w, log_ms=2000.0, eval_ms=1000.0):
+def learned_vs_plain(ngpu, drive_w, log_ms=2000.0, eval_ms=1000.0, target_tuples=50_000_000,
+                     max_log_ms=40000.0):
     """RK5 derivative evaluations per neuron-ms with and without the learned step proposal
-    on the four-receptor balanced network: log 2 s of the plain integrator (seed 42), train
+    on the four-receptor balanced network: log the plain integrator on the training seed (42)
+    in chunks of log_ms until target_tuples accepted steps are logged (or max_log_ms), train
     the network on the GPU, pick the safety factor on the training network, evaluate on a
-    held-out seed (43)."""
+    held-out seed (43), and measure there the floor: the evaluations when every step starts
+    from the largest step that passes the error test (no proposal can need fewer)."""
     import time
 
-    def evals(seed, model, t_ms):
+    def evals(seed, model, t_ms, bound=False):
         ngpu.Reset()
         ngpu.SetVerbosityLevel(0)
         n = c4_network(ngpu, seed, drive_w=drive_w)
         ngpu.Simulate(100.0)
+        if bound:
+            ngpu.StepBoundMode(True)
         if model is not None:
             ngpu.StepModelSet(model)
             ngpu.StepModelEnable(True)
@@ -236,11 +241,16 @@ def learned_vs_plain(ngpu, drive_w, log_ms=2000.0, eval_ms=1000.0):
     ngpu.SetVerbosityLevel(0)
     c4_network(ngpu, 42, drive_w=drive_w)
     ngpu.Simulate(100.0)
-    ngpu.Rk5LogStart(60_000_000)
-    ngpu.Simulate(log_ms)
+    ngpu.Rk5LogStart(target_tuples)
+    t_log = 0.0
+    while True:
+        ngpu.Simulate(log_ms)
+        t_log += log_ms
+        n_log, _ = ngpu.Rk5LogCount()
+        if n_log >= target_tuples or t_log >= max_log_ms:
+            break
     ngpu.Rk5LogStop()
-    n_log, _ = ngpu.Rk5LogCount()
-    out = {"drive_nS": drive_w, "logged_steps": n_log}
+    out = {"drive_nS": drive_w, "logged_steps": n_log, "logged_bio_ms": t_log}
     t0 = time.time()
     try:
         used, loss = ngpu.StepModelTrain(iters=3000, batch=4096, lr=2e-3, safety=0.9, floor=0.0, seed=3)
@@ -251,7 +261,9 @@ def learned_vs_plain(ngpu, drive_w, log_ms=2000.0, eval_ms=1000.0):
         used, model, note = 0, None, "not trained: " + str(e)
     train_s = time.time() - t0
     plain, rate_p = evals(43, None, eval_ms)
-    out.update(plain_evals_per_neuron_ms=plain, plain_rate_hz=rate_p)
+    floor, _ = evals(43, None, eval_ms, bound=True)
+    out.update(plain_evals_per_neuron_ms=plain, plain_rate_hz=rate_p, floor_evals_per_neuron_ms=floor,
+               largest_possible_reduction=plain / floor)
     if model is None:
         out.update(trained_on=0, learned_evals_per_neuron_ms=plain, learned_rate_hz=rate_p, ratio=1.0, note=note)
         return out
