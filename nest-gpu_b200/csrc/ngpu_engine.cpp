@@ -12,7 +12,7 @@ namespace ngpu {
 static const char *kModelName[M_NMODEL] = {
     "aeif_cond_beta_multisynapse", "aeif_cond_alpha_multisynapse", "aeif_psc_exp_multisynapse",
     "aeif_psc_alpha_multisynapse", "iaf_psc_exp", "spike_generator", "poisson_generator",
-    "parrot_neuron"};
+    "parrot_neuron", "spike_detector"};
 
 static bool is_aeif(int m) { return m <= M_AEIF_PSC_ALPHA; }
 
@@ -53,6 +53,11 @@ enum { PR_input_spike_height = 0, PR_dummy_input, PR_V, PR_NVAR };
 static const char *kParrotVar[PR_NVAR] = {"input_spike_height", "dummy_input", "V"};
 enum { PR_hold_spike_height = 0, PR_den_delay, PR_NPAR };
 static const char *kParrotPar[PR_NPAR] = {"hold_spike_height", "den_delay"};
+// spike_detector (src/spike_detector.cu:28-70)
+enum { SD_input_spike_height = 0, SD_spike_height, SD_NVAR };
+static const char *kSdetVar[SD_NVAR] = {"input_spike_height", "spike_height"};
+enum { SD_hold_spike_height = 0, SD_NPAR };
+static const char *kSdetPar[SD_NPAR] = {"hold_spike_height"};
 
 static Engine *g_engine = nullptr;
 
@@ -220,6 +225,11 @@ int Engine::create(const std::string &name, int n, int nport) {
     g.nport = 2;
     g.var.assign(PR_NVAR, std::vector<float>(n, 0.0f));
     g.par.assign(PR_NPAR, std::vector<float>(n, 0.0f));
+  } else if (m == M_SPIKE_DET) {
+    // one input port of weight 1; hold_spike_height defaults to 1 (src/spike_detector.cu:57-70)
+    g.nport = 1;
+    g.var.assign(SD_NVAR, std::vector<float>(n, 0.0f));
+    g.par.assign(SD_NPAR, std::vector<float>(n, 1.0f));
   } else {
     g.nport = 0;
     g.par.assign(PG_NPAR, std::vector<float>(n, 0.0f));
@@ -269,6 +279,9 @@ Kind Engine::locate(int node, const std::string &name, int *idx) {
   } else if (g.model == M_PARROT) {
     for (int j = 0; j < PR_NVAR && k == K_NONE; j++) if (name == kParrotVar[j]) { k = K_SCAL_VAR; i = j; }
     for (int j = 0; j < PR_NPAR && k == K_NONE; j++) if (name == kParrotPar[j]) { k = K_SCAL_PARAM; i = j; }
+  } else if (g.model == M_SPIKE_DET) {
+    for (int j = 0; j < SD_NVAR && k == K_NONE; j++) if (name == kSdetVar[j]) { k = K_SCAL_VAR; i = j; }
+    for (int j = 0; j < SD_NPAR && k == K_NONE; j++) if (name == kSdetPar[j]) { k = K_SCAL_PARAM; i = j; }
   } else if (g.model == M_SPIKE_GEN) {
     if (name == "spike_times") { k = K_ARRAY_PARAM; i = 0; }
     else if (name == "spike_heights") { k = K_ARRAY_PARAM; i = 1; }
@@ -300,6 +313,9 @@ std::vector<std::string> Engine::names(int node, Kind kind) {
   } else if (g.model == M_PARROT) {
     if (kind == K_SCAL_VAR) for (int j = 0; j < PR_NVAR; j++) r.push_back(kParrotVar[j]);
     if (kind == K_SCAL_PARAM) for (int j = 0; j < PR_NPAR; j++) r.push_back(kParrotPar[j]);
+  } else if (g.model == M_SPIKE_DET) {
+    if (kind == K_SCAL_VAR) for (int j = 0; j < SD_NVAR; j++) r.push_back(kSdetVar[j]);
+    if (kind == K_SCAL_PARAM) for (int j = 0; j < SD_NPAR; j++) r.push_back(kSdetPar[j]);
   } else if (g.model == M_SPIKE_GEN) {
     if (kind == K_ARRAY_PARAM) r = {"spike_times", "spike_heights"};
   }
@@ -336,7 +352,8 @@ static float *dev_row(Group &g, Kind k, int idx, int port) {
     if (k == K_SCAL_PARAM && idx == A_refractory_step) return g.d_refr;
     return nullptr;
   }
-  if ((g.model == M_IAF_PSC_EXP || g.model == M_PARROT) && k == K_SCAL_VAR) return g.d_var + (size_t)idx * g.n;
+  if ((g.model == M_IAF_PSC_EXP || g.model == M_PARROT || g.model == M_SPIKE_DET) && k == K_SCAL_VAR)
+    return g.d_var + (size_t)idx * g.n;
   return nullptr;
 }
 

@@ -420,6 +420,7 @@ int launch_iaf_multi(const IafArgs *tab, const int *blk0, int ngroups, int nbloc
 int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                      cudaStream_t st);
 int launch_parrot(const ParrotArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st);
+int launch_spike_det(const ParrotArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st);
 int launch_rev_arrivals(int *rev_ring, int *rev_cnt, int rev_R, int rev_cap, int *last_rev, const Clock *clk,
                         int k0, cudaStream_t st);
 int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *clk, int k0, int M,

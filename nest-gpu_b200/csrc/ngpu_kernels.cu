@@ -144,6 +144,44 @@ __global__ void __launch_bounds__(256) parrot_batch_kernel(const ParrotArgs A, c
 }
 
 // ---------------------------------------------------------------------------
+// spike_detector (src/spike_detector.cu:28-50): the input of a step (one port, weight 1)
+// becomes spike_height in the next one (1, or the input itself with hold_spike_height);
+// it emits nothing.  State [2][n]: input_spike_height, spike_height.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) spike_det_batch_kernel(const ParrotArgs A, const SpikeOut so,
+                                                              const Clock *clk, int k0, int M) {
+  pdl_enter();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const int n = A.n;
+  float in0 = A.var[i], sh = A.var[(size_t)n + i];
+  const bool hold = A.hold[i] != 0.0f;
+  const Clock cl = *clk;
+  const long long rec_it0 = cl.rec_it0;
+  PoissonCache pc;
+  poisson_cache_load(A.in, i, pc);
+  for (int m = 0; m < M; m++) {
+    const StepT t = step_at(cl, k0, m, A.dt);
+    double apf[1];
+    acc_prefetch<1>(apf, 1, n, i, A.in, m);
+    sh = in0;
+    if (sh != 0.0f) {
+      if (!hold) sh = 1.0f;
+      in0 = 0.0f;
+    }
+    if (A.rec.first) {
+      const float yr[2] = {in0, sh};
+      write_records<2>(A.rec, so, A.i0 + i, i, yr, 2, 0.0f, t.it - rec_it0, t.tidx);
+    }
+    double in[1];
+    step_inputs_pf<1>(in, apf, 1, n, i, A.in, pc, m, t.tidx, t.tnow);
+    if (in[0] != 0.0) in0 = (float)__fma_rn(in[0], 1.0, (double)in0);
+  }
+  A.var[i] = in0;
+  A.var[(size_t)n + i] = sh;
+}
+
+// ---------------------------------------------------------------------------
 // spike_generator (src/spike_generator.cu:49-67): compares against the per-call
 // step counter, at most one spike per step.
 // ---------------------------------------------------------------------------
@@ -412,6 +450,12 @@ int launch_iaf_multi(const IafArgs *tab, const int *blk0, int ngroups, int nbloc
                      const Clock *clk, int k0, int M, cudaStream_t st) {
   if (nblocks <= 0) return 0;
   launch_k(iaf_multi_kernel, dim3(nblocks), dim3(256), 0, st, tab, blk0, ngroups, so, clk, k0, M);
+  return 1;
+}
+
+int launch_spike_det(const ParrotArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
+  if (A.n <= 0) return 0;
+  launch_k(spike_det_batch_kernel, dim3((A.n + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
   return 1;
 }
 

@@ -419,7 +419,7 @@ void Engine::calibrate() {
 
   // ---- per-group device state
   for (auto &g : groups_) {
-    if (is_aeif(g.model) || g.model == M_IAF_PSC_EXP || g.model == M_PARROT) {
+    if (is_aeif(g.model) || g.model == M_IAF_PSC_EXP || g.model == M_PARROT || g.model == M_SPIKE_DET) {
       const int nvar = (int)g.var.size();
       g.d_var = dalloc<float>((size_t)nvar * g.n);
       for (int v = 0; v < nvar; v++)
@@ -439,7 +439,7 @@ void Engine::calibrate() {
       cuda_check(cudaMemcpy(g.d_x, x.data(), g.n * sizeof(double), cudaMemcpyHostToDevice), "x");
       cuda_check(cudaMemcpy(g.d_h, h.data(), g.n * sizeof(float), cudaMemcpyHostToDevice), "h");
     }
-    if (g.model == M_PARROT) {
+    if (g.model == M_PARROT || g.model == M_SPIKE_DET) {
       g.d_hold = dalloc<float>(g.n);
       cuda_check(cudaMemcpy(g.d_hold, g.par[0].data(), g.n * sizeof(float), cudaMemcpyHostToDevice), "hold");
     }
@@ -520,7 +520,7 @@ void Engine::upload_params() {
     g.dirty = false;
     const int n = g.n;
     std::vector<float> v(n);
-    if (g.model == M_PARROT && g.d_hold)
+    if ((g.model == M_PARROT || g.model == M_SPIKE_DET) && g.d_hold)
       cuda_check(cudaMemcpy(g.d_hold, g.par[0].data(), n * sizeof(float), cudaMemcpyHostToDevice), "hold");
     prev = g.d_der;
     if (is_aeif(g.model)) {
@@ -937,7 +937,9 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   for (auto &g : groups_) {
     if (g.n <= 0) continue;
     if (is_aeif(g.model)) has_aeif = true;
-    else if (g.model == M_IAF_PSC_EXP || g.model == M_SPIKE_GEN || g.model == M_PARROT) has_other = true;
+    else if (g.model == M_IAF_PSC_EXP || g.model == M_SPIKE_GEN || g.model == M_PARROT ||
+             g.model == M_SPIKE_DET)
+      has_other = true;
   }
   const bool fork = has_aeif && has_other;
   // Programmatic dependent launch where the batch is one chain of kernels on one stream
@@ -964,6 +966,7 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
       count_launch(launch_iaf(iaf_args(g), so, d_clk_, k0, M, s2));
     else if (g.model == M_SPIKE_GEN) count_launch(launch_spike_gen(sg_args(g), so, d_clk_, k0, M, s2));
     else if (g.model == M_PARROT) count_launch(launch_parrot(parrot_args(g), so, d_clk_, k0, M, s2));
+    else if (g.model == M_SPIKE_DET) count_launch(launch_spike_det(parrot_args(g), so, d_clk_, k0, M, s2));
   }
   for (auto &g : groups_)
     if (is_aeif(g.model)) count_launch(launch_aeif(g.model, aeif_args(g), so, d_clk_, k0, M, stream_));

@@ -17,6 +17,7 @@ enum Model {
   M_SPIKE_GEN,
   M_POISS_GEN,
   M_PARROT,
+  M_SPIKE_DET,
   M_NMODEL
 };
 

@@ -180,12 +180,12 @@ static int poisson_draw(float lam, uint64_t seed, uint64_t edge, int64_t tidx) {
 // Models
 // --------------------------------------------------------------------------
 enum Model { AEIF_COND_BETA = 0, AEIF_COND_ALPHA, AEIF_PSC_EXP, AEIF_PSC_ALPHA,
-             IAF_PSC_EXP, SPIKE_GEN, POISS_GEN, PARROT, N_MODEL };
+             IAF_PSC_EXP, SPIKE_GEN, POISS_GEN, PARROT, SPIKE_DET, N_MODEL };
 
 static const char *model_name[N_MODEL] = {
   "aeif_cond_beta_multisynapse", "aeif_cond_alpha_multisynapse",
   "aeif_psc_exp_multisynapse", "aeif_psc_alpha_multisynapse",
-  "iaf_psc_exp", "spike_generator", "poisson_generator", "parrot_neuron"};
+  "iaf_psc_exp", "spike_generator", "poisson_generator", "parrot_neuron", "spike_detector"};
 
 // parrot_neuron (src/parrot_neuron.cu:40-52): port 0 input (weight 1) repeated as a spike in
 // the next step, port 1 input weighted 0 (it only reaches plastic synapses)
@@ -193,6 +193,13 @@ enum { PR_input_spike_height = 0, PR_dummy_input, PR_V, PR_NVAR };
 static const char *parrot_var_name[PR_NVAR] = {"input_spike_height", "dummy_input", "V"};
 enum { PR_hold_spike_height = 0, PR_den_delay, PR_NPAR };
 static const char *parrot_par_name[PR_NPAR] = {"hold_spike_height", "den_delay"};
+
+// spike_detector (src/spike_detector.cu:28-70): the input of a step (one port, weight 1)
+// becomes spike_height in the next one (1, or the input with hold_spike_height, default 1)
+enum { SD_input_spike_height = 0, SD_spike_height, SD_NVAR };
+static const char *sdet_var_name[SD_NVAR] = {"input_spike_height", "spike_height"};
+enum { SD_hold_spike_height = 0, SD_NPAR };
+static const char *sdet_par_name[SD_NPAR] = {"hold_spike_height"};
 
 static bool is_aeif(Model m) { return m <= AEIF_PSC_ALPHA; }
 
@@ -568,6 +575,10 @@ struct Net {
       g.nport = 2;
       g.var.assign(PR_NVAR, std::vector<double>(n, 0.0));
       g.par.assign(PR_NPAR, std::vector<double>(n, 0.0));
+    } else if (g.model == SPIKE_DET) {
+      g.nport = 1;
+      g.var.assign(SD_NVAR, std::vector<double>(n, 0.0));
+      g.par.assign(SD_NPAR, std::vector<double>(n, 1.0));
     }
     g.acc.assign((size_t)g.nport * n, 0.0);
     groups.push_back(g);
@@ -596,6 +607,9 @@ struct Net {
     } else if (g.model == PARROT) {
       for (int k = 0; k < PR_NVAR; k++) if (name == parrot_var_name[k]) { kind = 0; return k; }
       for (int k = 0; k < PR_NPAR; k++) if (name == parrot_par_name[k]) { kind = 2; return k; }
+    } else if (g.model == SPIKE_DET) {
+      for (int k = 0; k < SD_NVAR; k++) if (name == sdet_var_name[k]) { kind = 0; return k; }
+      for (int k = 0; k < SD_NPAR; k++) if (name == sdet_par_name[k]) { kind = 2; return k; }
     } else if (g.model == SPIKE_GEN) {
       if (name == "spike_times") { kind = 5; return 0; }
       if (name == "spike_heights") { kind = 5; return 1; }
@@ -1374,6 +1388,16 @@ struct Net {
             push_spike(g.i0 + i, height, tidx);
           }
         }
+      } else if (g.model == SPIKE_DET) {
+        // src/spike_detector.cu:28-50
+        for (int i = 0; i < g.n; i++) {
+          float sh = (float)g.var[SD_input_spike_height][i];
+          if (sh != 0.0f) {
+            if (g.par[SD_hold_spike_height][i] == 0.0) sh = 1.0f;
+            g.var[SD_input_spike_height][i] = 0.0;
+          }
+          g.var[SD_spike_height][i] = sh;
+        }
       } else if (g.model == SPIKE_GEN) {
         for (int i = 0; i < g.n; i++) {
           int k = g.sg_next[i];
@@ -1457,6 +1481,9 @@ struct Net {
             // port weights {1, 0}: port p feeds variable p (src/parrot_neuron.cu:110-122)
             pw = p == 0 ? 1.0 : 0.0;
             pi = &g.var[p];
+          } else if (g.model == SPIKE_DET) {
+            pw = 1.0;
+            pi = &g.var[SD_input_spike_height];
           } else {
             pw = 1.0;
             pi = &g.var[p == 0 ? I_I_syn_ex : I_I_syn_in];

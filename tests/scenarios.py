@@ -461,3 +461,26 @@ def syn_model_scenario(api, n=5, fact=0.2, offset=0.03):
     api.Simulate(200.0)
     w = np.asarray(_conn_status(api, api.GetConnections(n0, n1), "weight"), dtype=np.float64)
     return w, np.asarray([d * fact + offset for d in dts])
+
+
+def spike_detector_scenario(api, n=30, t1=490.0, t2=10.0):
+    """python/test/test_spike_times.py: aeif neurons driven by a Poisson generator, each
+    followed one_to_one by a spike_detector (delay 0.1 ms) whose spike_height is recorded;
+    returns (recorded rows, spike counts, recorded spike times)."""
+    api.SetKernelStatus("rnd_seed", 1234)
+    pg = api.Create("poisson_generator")
+    api.SetStatus(pg, "rate", 500.0)
+    neuron = api.Create("aeif_cond_beta_multisynapse", n)
+    api.ActivateSpikeCount(neuron)
+    api.ActivateRecSpikeTimes(neuron, 500)
+    sd = api.Create("spike_detector", n)
+    api.Connect(pg, neuron, {"rule": "all_to_all"}, {"weight": 4.0, "delay": 0.2})
+    api.Connect(neuron, sd, {"rule": "one_to_one"}, {"weight": 1.0, "delay": 0.1})
+    rec = api.CreateRecord("", ["spike_height"] * n, [sd[i] for i in range(n)], [0] * n)
+    api.Simulate(t1)
+    api.SetStatus(pg, "rate", 0.0)
+    api.Simulate(t2)
+    data = np.asarray(api.GetRecordData(rec), dtype=np.float64)
+    counts = np.asarray(api.GetStatus(neuron, "spike_count")).ravel()
+    times = api.GetRecSpikeTimes(neuron)
+    return data, counts, times

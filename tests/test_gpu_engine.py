@@ -588,3 +588,18 @@ def test_microcircuit_slice_device_rules_bitexact():
         assert ngpu.GetStats()["status"] == 0
     assert counts[0].sum() > 1000
     assert np.array_equal(counts[0], counts[1])
+
+
+def test_spike_detector_matches_oracle():
+    """spike_detector nodes (src/spike_detector.cu) behind Poisson-driven aeif neurons, as in
+    the reference's spike-time test: recorded spike heights, spike counts and recorded spike
+    times equal the oracle's."""
+    from scenarios import spike_detector_scenario
+    d_g, c_g, t_g = spike_detector_scenario(ngpu)
+    d_o, c_o, t_o = spike_detector_scenario(orc.Oracle())
+    assert c_g.sum() > 0
+    assert np.array_equal(c_g, c_o)
+    assert np.array_equal(np.float32(d_g), np.float32(d_o))
+    assert np.array_equal((d_g[:, 1:] > 0.5).sum(axis=0), c_g)
+    for a, b in zip(t_g, t_o):
+        assert np.array_equal(np.float32(a), np.float32(b))

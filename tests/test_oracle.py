@@ -137,3 +137,15 @@ def test_oracle_errors_like_reference():
         o.Connect(a, a, {"rule": "fixed_indegree", "indegree": 4}, {"weight": 1.0, "delay": 1.0})
     with pytest.raises(ValueError, match="one-to-one"):
         o.Connect(a, a[0:2], {"rule": "one_to_one"}, {"weight": 1.0, "delay": 1.0})
+
+
+def test_spike_detector_scenario_consistent():
+    """The reference's spike-time consistency test on the oracle: every detector records
+    exactly its neuron's spikes, one step (its 0.1 ms delay) after each recorded spike time."""
+    from scenarios import spike_detector_scenario
+    data, counts, times = spike_detector_scenario(orc.Oracle())
+    assert counts.sum() > 0
+    assert np.array_equal((data[:, 1:] > 0.5).sum(axis=0), counts)
+    for j in range(len(counts)):
+        t_det = np.round(data[data[:, 1 + j] > 0.5, 0] - 0.2, 4)
+        assert np.allclose(np.round(np.asarray(times[j], dtype=np.float64), 4), t_det, atol=1e-6)
