@@ -799,6 +799,14 @@ int NGPU_SetDeviceRuleMinEdges(long long n) {
   }, -1);
 }
 
+int NGPU_SetDeliverAggregate(int on) {
+  return guard([&] {
+    E().deliver_aggregate = on ? 1 : 0;
+    E().invalidate_graphs();
+    return 0;
+  }, -1);
+}
+
 int NGPU_SetUpdateTrialIter(int on) {
   return guard([&] {
     E().update_trial_iter = on ? 1 : 0;
@@ -845,10 +853,11 @@ int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliv
 
 int NGPU_GetLaunchMapping(int *vals, int n) {
   return guard([&] {
-    const int v[8] = {E().update_threads, E().update_occupancy, E().deliver_group, E().deliver_blocks_req,
-                      E().rk5_budget, E().persistent, E().launch_pdl, E().update_trial_iter};
-    for (int i = 0; i < n && i < 8; i++) vals[i] = v[i];
-    return 8;
+    const int v[9] = {E().update_threads, E().update_occupancy, E().deliver_group, E().deliver_blocks_req,
+                      E().rk5_budget, E().persistent, E().launch_pdl, E().update_trial_iter,
+                      E().deliver_aggregate};
+    for (int i = 0; i < n && i < 9; i++) vals[i] = v[i];
+    return 9;
   }, -1);
 }
 

@@ -221,7 +221,7 @@ constexpr int MAX_PAIRS = 8192;     // dspan * M
 typedef cub::BlockScan<int, DELIVER_THREADS> DeliverScan;
 
 // The delivery of one batch by block `block` of `nblocks`; s_pref holds dspan*M+1 ints.
-template <int G>
+template <int G, bool AGG = false>
 __device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock *clk, int k0, int M, int *s_pref,
                                               typename DeliverScan::TempStorage &scan_tmp, int block,
                                               int nblocks) {
@@ -284,9 +284,35 @@ __device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock 
     const size_t key = (size_t)sp.x * A.dspan + dd;
     const long long e0 = __ldg(&A.ev_off[key]), e1 = __ldg(&A.ev_off[key + 1]);
     double *acc = A.acc + (size_t)m * A.slot_stride;
-    for (long long e = e0 + sub; e < e1; e += G) {
-      const uint2 ew = __ldg(reinterpret_cast<const uint2 *>(A.edge + e));
-      atomicAdd(&acc[ew.x], (double)__fmul_rn(height, __uint_as_float(ew.y)));
+    if constexpr (AGG) {
+      // warp-aggregated reductions (G = 32: the warp is one work group, so this loop is
+      // warp-uniform): lanes whose edges share a target add their products first and the
+      // lowest of them issues one reduction.  FP64 sums of these products are exact, so the
+      // result does not depend on how they are grouped.
+      static_assert(G == 32, "warp aggregation needs one segment per warp");
+      const int lane = threadIdx.x & 31;
+      for (long long base = e0; base < e1; base += 32) {
+        const long long e = base + lane;
+        const bool valid = e < e1;
+        uint2 ew = make_uint2(0xffffffffu, 0u);
+        if (valid) ew = __ldg(reinterpret_cast<const uint2 *>(A.edge + e));
+        double v = valid ? (double)__fmul_rn(height, __uint_as_float(ew.y)) : 0.0;
+        const unsigned peers = __match_any_sync(0xffffffffu, ew.x);
+        if (__any_sync(0xffffffffu, __popc(peers) > 1)) {
+          double sum = 0.0;
+          for (int k = 0; k < 32; k++) {
+            const double o = __shfl_sync(0xffffffffu, v, k);
+            if ((peers >> k) & 1u) sum += o;
+          }
+          v = sum;
+        }
+        if (valid && lane == __ffs(peers) - 1) atomicAdd(&acc[ew.x], v);
+      }
+    } else {
+      for (long long e = e0 + sub; e < e1; e += G) {
+        const uint2 ew = __ldg(reinterpret_cast<const uint2 *>(A.edge + e));
+        atomicAdd(&acc[ew.x], (double)__fmul_rn(height, __uint_as_float(ew.y)));
+      }
     }
     if (sub == 0) nev += (unsigned long long)(e1 - e0);
   }
@@ -301,13 +327,13 @@ __device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock 
   __syncthreads();
 }
 
-template <int G>
+template <int G, bool AGG = false>
 __global__ void __launch_bounds__(DELIVER_THREADS) deliver_batch_kernel(const DeliverArgs A,
                                                                         const Clock *clk, int k0, int M) {
   pdl_enter();
   extern __shared__ int s_pref[];   // npairs + 1 prefix sums over (delay group, arrival step)
   __shared__ typename DeliverScan::TempStorage scan_tmp;
-  deliver_batch<G>(A, clk, k0, M, s_pref, scan_tmp, blockIdx.x, gridDim.x);
+  deliver_batch<G, AGG>(A, clk, k0, M, s_pref, scan_tmp, blockIdx.x, gridDim.x);
 }
 
 __global__ void clock_advance_kernel(Clock *clk, int K) {
@@ -478,6 +504,7 @@ int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *c
   const dim3 g(n_blocks), b(DELIVER_THREADS);
   if (group == 8) launch_k(deliver_batch_kernel<8>, g, b, smem, st, A, clk, k0, M);
   else if (group == 16) launch_k(deliver_batch_kernel<16>, g, b, smem, st, A, clk, k0, M);
+  else if (A.aggregate) launch_k(deliver_batch_kernel<32, true>, g, b, smem, st, A, clk, k0, M);
   else launch_k(deliver_batch_kernel<32>, g, b, smem, st, A, clk, k0, M);
   return 1;
 }

@@ -805,6 +805,7 @@ DeliverArgs Engine::deliver_args() {
   A.n_events = d_counters_ + 1;
   A.strag_cnt = d_strag_cnt_;
   A.n_strag = n_strag_;
+  A.aggregate = deliver_aggregate;
   return A;
 }
 
@@ -1380,6 +1381,7 @@ int Engine::autotune(int steps, std::vector<std::pair<std::string, double>> *log
       single("update_threads", &update_threads, {64, 128, 256}),
       single("update_occupancy", &update_occupancy, {0, 1}),
       single("update_trial_iter", &update_trial_iter, {0, 1}),
+      single("deliver_aggregate", &deliver_aggregate, {0, 1}),
       deliver,
       single("rk5_budget", &rk5_budget, {0, 1, 2, 4, 8}),
       single("programmatic_launch", &launch_pdl, {0, 1}),

@@ -225,6 +225,7 @@ struct DeliverArgs {
   unsigned long long *n_events;
   int *strag_cnt;        // per-group straggler counters, cleared for the batch
   int n_strag;
+  int aggregate;         // 1 (with 32-lane groups): warp-aggregated reductions
 };
 
 // Plastic edge (synapse group > 0): its position in the delivery CSR, its target node and

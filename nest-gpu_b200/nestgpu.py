@@ -175,6 +175,7 @@ if is_b200_engine:
     _c["NGPU_SetProgrammaticLaunch"] = _bind("NGPU_SetProgrammaticLaunch", _I, [_I])
     _c["NGPU_SetUpdateOccupancy"] = _bind("NGPU_SetUpdateOccupancy", _I, [_I])
     _c["NGPU_SetUpdateTrialIter"] = _bind("NGPU_SetUpdateTrialIter", _I, [_I])
+    _c["NGPU_SetDeliverAggregate"] = _bind("NGPU_SetDeliverAggregate", _I, [_I])
     _c["NGPU_GetBatchLength"] = _bind("NGPU_GetBatchLength", _I, [])
     _c["NGPU_SetPersistent"] = _bind("NGPU_SetPersistent", _I, [_I])
     _c["NGPU_TestBarrierTimeout"] = _bind("NGPU_TestBarrierTimeout", _I, [_I])
@@ -1469,6 +1470,13 @@ def SetUpdateTrialIter(on=True):
     return _check(_c["NGPU_SetUpdateTrialIter"](1 if on else 0))
 
 
+def SetDeliverAggregate(on=True):
+    """Warp-aggregated reductions in the delivery kernel with 32-lane work items (engine
+    extension; results are identical either way)."""
+    _need_b200("SetDeliverAggregate")
+    return _check(_c["NGPU_SetDeliverAggregate"](1 if on else 0))
+
+
 def SetDeliverGroup(g):
     """Lanes per spike-delivery work item: 8, 16 or 32 (engine extension)."""
     _need_b200("SetDeliverGroup")
@@ -1509,11 +1517,11 @@ def GetLaunchMapping():
     """The current launch mapping (engine extension): update block size and variant, delivery
     lane group and grid, RK5 step budget, persistent loop and programmatic launch."""
     _need_b200("GetLaunchMapping")
-    v = (ctypes.c_int * 8)()
-    _c["NGPU_GetLaunchMapping"](v, 8)
+    v = (ctypes.c_int * 9)()
+    _c["NGPU_GetLaunchMapping"](v, 9)
     _check()
     keys = ["update_threads", "update_occupancy", "deliver_group", "deliver_blocks", "rk5_budget",
-            "persistent", "programmatic_launch", "update_trial_iter"]
+            "persistent", "programmatic_launch", "update_trial_iter", "deliver_aggregate"]
     return dict(zip(keys, [int(x) for x in v]))
 
 

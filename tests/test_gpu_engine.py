@@ -270,16 +270,18 @@ def test_profile_and_launch_counters():
     assert ngpu.GetStats()["steps"] == 250
 
 
-@pytest.mark.parametrize("threads,group,occ,tpi", [(64, 8, 0, 0), (256, 16, 1, 0), (128, 32, 1, 0),
-                                                   (64, 8, 0, 1), (128, 32, 1, 1)])
-def test_launch_mappings_keep_results(threads, group, occ, tpi):
+@pytest.mark.parametrize("threads,group,occ,tpi,agg", [(64, 8, 0, 0, 0), (256, 16, 1, 0, 0), (128, 32, 1, 0, 0),
+                                                       (64, 8, 0, 1, 0), (128, 32, 1, 1, 1), (64, 32, 0, 0, 1)])
+def test_launch_mappings_keep_results(threads, group, occ, tpi, agg):
     """The update block size and kernel variants (register cap, one RK5 trial per loop
-    iteration) and the delivery lane group change only the launch mapping."""
+    iteration), the delivery lane group and warp-aggregated delivery change only the launch
+    mapping."""
     ngpu.SetHostRng(True)
     ngpu.SetUpdateThreads(threads)
     ngpu.SetDeliverGroup(group)
     ngpu.SetUpdateOccupancy(occ)
     ngpu.SetUpdateTrialIter(tpi)
+    ngpu.SetDeliverAggregate(agg)
     c_gpu, d_gpu = fixed_train_network(ngpu, model="aeif_cond_beta_multisynapse")
     c_orc, d_orc = fixed_train_network(orc.Oracle(), model="aeif_cond_beta_multisynapse")
     assert c_gpu.sum() > 0
@@ -516,7 +518,7 @@ def test_iaf_propagator_singular_branch(tau_ex):
     assert v_gpu.max() > 1.0
     if tau_ex == 10.0:
         # P21ex = h / C_m * exp(-h / tau) in the singular case
-        p21 = ngpu.GetStatus(n[0], "P21ex")[0]
+        p21 = float(np.ravel(ngpu.GetStatus(n[0], "P21ex"))[0])
         assert abs(p21 - 0.1 / 250.0 * math.exp(-0.1 / 10.0)) < 1e-9
 
 
