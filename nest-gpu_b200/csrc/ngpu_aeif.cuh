@@ -116,6 +116,12 @@ __device__ __forceinline__ void push_spike(const SpikeOut &so, const GroupSpikeR
       else atomicOr(so.status, ST_RING_OVERFLOW);
     }
   }
+  if (so.xch && so.has_out_all[node]) {
+    // partitioned network: other processes may deliver this spike
+    const int pos = atomicAdd(&so.xch[0].x, 1);
+    if (pos < so.xch_cap) so.xch[1 + pos] = make_int4(node, __float_as_int(height), (int)tidx, 0);
+    else atomicOr(so.status, ST_EXCHANGE_FULL);
+  }
   if (so.has_out[node]) {
     int slot = (int)(tidx % so.R);
     int pos = atomicAdd(&so.ring_cnt[slot], 1);
@@ -686,7 +692,7 @@ __device__ __forceinline__ void write_records(const GroupRecord &R, const SpikeO
   for (int c = c0; c < c1; c++) {
     const int2 rc = R.col[c];
     float v = 0.0f;
-    if (rc.x < 0) v = (so.has_out[node] && so.last_tidx[node] == (int)tidx) ? so.last_height[node] : 0.0f;
+    if (rc.x < 0) v = (so.has_out_all[node] && so.last_tidx[node] == (int)tidx) ? so.last_height[node] : 0.0f;
     else if (rc.x == nvar) v = refr;
     else {
 #pragma unroll
@@ -747,6 +753,42 @@ __device__ __forceinline__ void warp_add(unsigned long long *ctr, unsigned long 
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr, v);
 }
 
+// One iteration of the trial-per-iteration form: begin a step if none is open (k1 and the
+// error scale), run one trial; after a rejection shrink h and return false (the step stays
+// open); after an acceptance update x, h and y and run the ExternalUpdate.  Returns true
+// when the time step is complete.  The operations of each step are those of rk5_step.
+template <int MODEL, int PMAX, bool FIXED>
+__device__ __forceinline__ bool aeif_tpi_iter(const AeifArgs &A, const SpikeOut &so, int i,
+                                              const AeifQ<MODEL, PMAX, FIXED> &q, float *y, float &refr,
+                                              double &x, float &h, const StepT &t, float *k1, float *iys,
+                                              bool &open, int &trials, unsigned long long &nd, int &guard) {
+  constexpr int NVM = 2 + AeifShape<MODEL>::npv * PMAX;
+  const int NV = 2 + AeifShape<MODEL>::npv * q.ports();
+  if (!open) {
+    rk5_begin(y, h, q, refr, k1, iys);
+    nd += 1;
+    trials = 0;
+    open = true;
+  }
+  float yn[NVM];
+  const float err = rk5_trial(y, h, A.hmin, (float)(t.tnow - x), q, refr, k1, iys, yn);
+  nd += 5;
+  if (!(err <= 1.0f || h <= A.hmin_acc)) {
+    if (++trials < ck::max_trials) {
+      h = rk5_shrink(h, err);
+      return false;
+    }
+    atomicOr(so.status, ST_RK5_TRIALS);
+  }
+  open = false;
+  x += (double)h;
+  h = rk5_grow(h, err, A.hmin);
+#pragma unroll
+  for (int v = 0; v < NVM; v++)
+    if (v < NV) y[v] = yn[v];
+  return aeif_external(A, so, i, q, y, refr, x, t.tidx, t.tnow, guard);
+}
+
 // Main aeif kernel: one thread per neuron, steps m = 0..M-1 of the batch.
 // OCC = 1 caps the registers so that three 256-thread blocks fit on an SM (more warps
 // in flight to hide the dependent FP32 latency, at the price of a few spills).
@@ -768,9 +810,9 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
     for (int j = threadIdx.x; j < SM_NPAR; j += blockDim.x) smodel[j] = A.learn.model[j];
     __syncthreads();
   }
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = A.lo + blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long nd = 0;
-  if (i < A.n) {
+  if (i < A.hi) {
     AeifQ<MODEL, PMAX, FIXED> q;
     load_aeif_par<MODEL, PMAX, FIXED, UNI>(A, i, q);
     const int NV = 2 + S::npv * q.ports();
@@ -796,34 +838,12 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
       bool open = false;     // a step has begun (k1, iys valid) and no trial was accepted yet
       int trials = 0;
       while (m < M) {
-        if (!open) {
-          if (budget == 0) {
-            deferred = true;
-            break;
-          }
-          rk5_begin(y, h, q, refr, k1, iys);
-          nd += 1;
-          trials = 0;
-          open = true;
+        if (!open && budget == 0) {
+          deferred = true;
+          break;
         }
         if (budget > 0) budget--;
-        float yn[NVM];
-        const float err = rk5_trial(y, h, A.hmin, (float)(t.tnow - x), q, refr, k1, iys, yn);
-        nd += 5;
-        if (!(err <= 1.0f || h <= A.hmin_acc)) {
-          if (++trials < ck::max_trials) {
-            h = rk5_shrink(h, err);
-            continue;
-          }
-          atomicOr(so.status, ST_RK5_TRIALS);
-        }
-        open = false;
-        x += (double)h;
-        h = rk5_grow(h, err, A.hmin);
-#pragma unroll
-        for (int v = 0; v < NVM; v++)
-          if (v < NV) y[v] = yn[v];
-        if (aeif_external(A, so, i, q, y, refr, x, t.tidx, t.tnow, guard)) {
+        if (aeif_tpi_iter(A, so, i, q, y, refr, x, h, t, k1, iys, open, trials, nd, guard)) {
           aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
           guard = 0;
           if (++m < M) {
@@ -861,7 +881,7 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
 
 // Neurons the main kernel left unfinished (typically the few that spike in the batch)
 // continue here from the step where they stopped, one per thread.
-template <int MODEL, int PMAX, bool FIXED, int LM, bool UNI = false>
+template <int MODEL, int PMAX, bool FIXED, int LM, bool UNI = false, bool TPI = false>
 __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, const SpikeOut so,
                                                              const Clock *clk, int k0, int M) {
   pdl_enter();
@@ -892,8 +912,15 @@ __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, c
     StepT t = step_at(cl, k0, m, A.dt);
     double apf[PMAX];
     acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
+    float k1[TPI ? NVM : 1], iys[TPI ? NVM : 1];
+    bool open = false;
+    int trials = 0;
     while (m < M) {
-      if (aeif_substep<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, nd, smodel, guard)) {
+      bool done;
+      if constexpr (TPI) done = aeif_tpi_iter(A, so, i, q, y, refr, x, h, t, k1, iys, open, trials, nd, guard);
+      else done = aeif_substep<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, nd, smodel,
+                                                        guard);
+      if (done) {
         aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
         guard = 0;
         if (++m < M) {
@@ -912,7 +939,7 @@ __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, c
 template <int MODEL, int PMAX, bool FIXED, int LM>
 int launch_aeif_p(const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
   const int tb = (A.threads == 64 || A.threads == 256) ? A.threads : 128;
-  dim3 grid((A.n + tb - 1) / tb), block(tb);
+  dim3 grid((A.hi - A.lo + tb - 1) / tb), block(tb);
   bool done = false;
   if constexpr (LM == LM_PLAIN && FIXED) {
     if (A.trial_iter && A.occupancy && A.uniform) {
@@ -940,11 +967,16 @@ int launch_aeif_p(const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k
   }
   if (!done) launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 0>, grid, block, 0, st, A, so, clk, k0, M);
   if (A.budget <= 0) return 1;
-  dim3 sgrid(A.n < 128 * 148 * 4 ? (A.n + 127) / 128 : 148 * 4), sblock(128);
+  const int nl = A.hi - A.lo;
+  dim3 sgrid(nl < 128 * 148 * 4 ? (nl + 127) / 128 : 148 * 4), sblock(128);
   done = false;
   if constexpr (LM == LM_PLAIN && FIXED) {
     if (A.uniform) {
-      launch_k(aeif_straggler_kernel<MODEL, PMAX, FIXED, LM, true>, sgrid, sblock, 0, st, A, so, clk, k0, M);
+      if (A.trial_iter)
+        launch_k(aeif_straggler_kernel<MODEL, PMAX, FIXED, LM, true, true>, sgrid, sblock, 0, st, A, so, clk, k0,
+                 M);
+      else
+        launch_k(aeif_straggler_kernel<MODEL, PMAX, FIXED, LM, true>, sgrid, sblock, 0, st, A, so, clk, k0, M);
       done = true;
     }
   }

@@ -38,8 +38,8 @@ __device__ __forceinline__ void gen_edge(const GenBlockDev &b, long long e, int 
 }
 
 __global__ void gen_count_kernel(GenBlockDev b, int dmin, int dspan, unsigned long long *cnt) {
-  const long long total = (long long)b.ntgt * b.k;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+  const long long total = (long long)b.t_end * b.k;
+  for (long long e = (long long)b.t_begin * b.k + blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     int s, d, t;
     gen_edge(b, e, s, d, t);
@@ -49,8 +49,8 @@ __global__ void gen_count_kernel(GenBlockDev b, int dmin, int dspan, unsigned lo
 
 __global__ void gen_fill_kernel(GenBlockDev b, int dmin, int dspan, unsigned long long *cursor,
                                 EdgeW *edge) {
-  const long long total = (long long)b.ntgt * b.k;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+  const long long total = (long long)b.t_end * b.k;
+  for (long long e = (long long)b.t_begin * b.k + blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     int s, d, t;
     gen_edge(b, e, s, d, t);
@@ -89,12 +89,15 @@ __device__ __forceinline__ void rule_edge(const RuleBlockDev &b, long long e, in
 // Delay step of a delay in ms: round(d / dt) - 1 (src/connect.cu:49), float arithmetic.
 __device__ __forceinline__ int delay_step(float d, float dt) { return (int)roundf(__fdiv_rn(d, dt)) - 1; }
 
-__global__ void rule_count_kernel(RuleBlockDev b, int dmin, int dspan, unsigned long long *cnt) {
+// node_acc0[t] == 0xffffffff marks a target simulated by another process (skipped)
+__global__ void rule_count_kernel(RuleBlockDev b, int dmin, int dspan, unsigned long long *cnt,
+                                  const unsigned *node_acc0) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < b.n_edges;
        e += (long long)gridDim.x * blockDim.x) {
     int s, t;
     float w, d;
     rule_edge(b, e, s, t, w, d);
+    if (node_acc0[t] == 0xffffffffu) continue;
     atomicAdd(&cnt[(size_t)s * dspan + (delay_step(d, b.dt) - dmin)], 1ULL);
   }
 }
@@ -106,12 +109,41 @@ __global__ void rule_fill_kernel(RuleBlockDev b, int dmin, int dspan, unsigned l
     int s, t;
     float w, d;
     rule_edge(b, e, s, t, w, d);
+    if (node_acc0[t] == 0xffffffffu) continue;
     const unsigned long long pos = atomicAdd(&cursor[(size_t)s * dspan + (delay_step(d, b.dt) - dmin)], 1ULL);
     EdgeW x;
     x.acc = node_acc0[t] + (unsigned)b.port * (unsigned)node_gn[t];
     x.w = w;
     edge[pos] = x;
   }
+}
+
+// Partitioned network: mark every source with a recurrent edge anywhere (all targets of the
+// generated and rule blocks, not only those simulated here).
+__global__ void gen_mark_kernel(GenBlockDev b, unsigned char *flag) {
+  const long long total = (long long)b.ntgt * b.k;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    int s, d, t;
+    gen_edge(b, e, s, d, t);
+    flag[s] = 1;
+  }
+}
+
+__global__ void rule_mark_kernel(RuleBlockDev b, unsigned char *flag) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < b.n_edges;
+       e += (long long)gridDim.x * blockDim.x) {
+    int s, t;
+    float w, d;
+    rule_edge(b, e, s, t, w, d);
+    flag[s] = 1;
+  }
+}
+
+void mark_sources_device(const std::vector<GenBlockDev> &blocks, const std::vector<RuleBlockDev> &rblocks,
+                         unsigned char *d_flag, cudaStream_t st) {
+  for (const auto &b : blocks) gen_mark_kernel<<<148 * 8, 256, 0, st>>>(b, d_flag);
+  for (const auto &b : rblocks) rule_mark_kernel<<<148 * 8, 256, 0, st>>>(b, d_flag);
 }
 
 __global__ void host_edge_scatter_kernel(size_t n, const long long *key, const int *rank,
@@ -158,7 +190,7 @@ void build_csr_device(int n_nodes, int dmin, int dspan, const std::vector<int> &
   }
   const int gb = 148 * 8, tb = 256;
   for (const auto &b : blocks) gen_count_kernel<<<gb, tb, 0, st>>>(b, dmin, dspan, d_cnt);
-  for (const auto &b : rblocks) rule_count_kernel<<<gb, tb, 0, st>>>(b, dmin, dspan, d_cnt);
+  for (const auto &b : rblocks) rule_count_kernel<<<gb, tb, 0, st>>>(b, dmin, dspan, d_cnt, d_node_acc0);
   size_t tmp_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_cnt, d_off, nkey + 1, st);
   void *d_tmp = nullptr;

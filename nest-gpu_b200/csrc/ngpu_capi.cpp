@@ -23,7 +23,7 @@ struct ErrState {
   unsigned char code = 0;
   int on_exception = 0;   // 0: exit (reference default for C callers), 1: return
 };
-ErrState g_err;
+thread_local ErrState g_err;
 
 // connection / synapse specification staged by the Set*Spec* calls (src/nestgpu_C.cpp:39-40)
 struct ConnSpecC {
@@ -35,9 +35,9 @@ struct SynSpecC {
   float weight = 0.0f, delay = 0.0f;
   float *weight_array = nullptr, *delay_array = nullptr;
 };
-ConnSpecC g_conn;
-SynSpecC g_syn;
-double g_last_device_ms = 0.0;
+thread_local ConnSpecC g_conn;
+thread_local SynSpecC g_syn;
+thread_local double g_last_device_ms = 0.0;
 
 void fail(unsigned char code, const std::string &msg) {
   g_err.flag = true;
@@ -797,6 +797,14 @@ int NGPU_SetDeviceRuleMinEdges(long long n) {
     E().device_rule_min_edges = n;
     return 0;
   }, -1);
+}
+
+int NGPU_SetPartition(int rank, int world) {
+  return guard([&] { E().set_partition(rank, world); return 0; }, -1);
+}
+
+int NGPU_SetExchange(void *send, void *recv, long long cap, int (*exchange)(void *), void *user) {
+  return guard([&] { E().set_exchange(send, recv, cap, exchange, user); return 0; }, -1);
 }
 
 int NGPU_SetDeliverAggregate(int on) {

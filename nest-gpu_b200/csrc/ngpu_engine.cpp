@@ -59,7 +59,9 @@ static const char *kSdetVar[SD_NVAR] = {"input_spike_height", "spike_height"};
 enum { SD_hold_spike_height = 0, SD_NPAR };
 static const char *kSdetPar[SD_NPAR] = {"hold_spike_height"};
 
-static Engine *g_engine = nullptr;
+// one engine per host thread (one network per process as the reference; a test may run
+// several partitions of a network side by side in threads of one process)
+static thread_local Engine *g_engine = nullptr;
 
 Engine &engine() {
   if (!g_engine) g_engine = new Engine();

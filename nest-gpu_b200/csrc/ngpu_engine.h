@@ -82,6 +82,7 @@ struct Group {
   PoissonIn *d_pin = nullptr;
   int *d_sg_off = nullptr, *d_sg_tidx = nullptr, *d_sg_next = nullptr;
   float *d_sg_h = nullptr;
+  int lo = 0, hi = 0;            // neurons lo .. hi-1 are simulated by this process (calibration)
   int gen0 = -1;                 // poiss_gen: first row in the generator table
   std::vector<uint32_t> pg_stream;   // poiss_gen: stream numbers (empty: index among generators)
   bool dirty = true;             // parameters changed since last upload
@@ -135,6 +136,17 @@ class Engine {
   int launch_pdl = -1;            // programmatic dependent launch of the batch kernels (-1: one-step batches)
   int barrier_extra = 0;          // test hook: blocks the persistent loop's barriers wait for in excess
   bool use_device_rng = true;     // cuRAND device generator (as the reference) if a GPU exists
+
+  // ---- one network over several processes (one GPU each): process `rank` of `world`
+  //      simulates a contiguous share of every node group; after each time batch the spikes
+  //      of its neurons are handed to `exchange` (see set_exchange)
+  void set_partition(int rank, int world);
+  // send / recv: device buffers of int4 records, (cap + 1) per process (recv holds world
+  // blocks, block q = process q's send buffer); exchange(user) must fill recv from every
+  // process's send buffer (an all-gather) and return 0 once recv may be read
+  void set_exchange(void *send, void *recv, long long cap, int (*exchange)(void *), void *user);
+  int part_rank() const { return part_rank_; }
+  int part_world() const { return part_world_; }
 
   void set_seed(unsigned long long s);
   void set_time_resolution(float t);
@@ -398,6 +410,13 @@ class Engine {
   GroupRecord group_record(Group &g);
   GroupInput group_input(Group &g);
   void run_steps(long long n);
+  void run_batches_partitioned(long long n);
+  int part_rank_ = 0, part_world_ = 1;
+  int4 *xch_send_ = nullptr, *xch_recv_ = nullptr;
+  int xch_cap_ = 0;
+  int (*xch_fn_)(void *) = nullptr;
+  void *xch_user_ = nullptr;
+  unsigned char *d_has_out_all_ = nullptr;
   void drain_records(long long rows);
   void drain_rec_spike_times();
   SpikeOut spike_out() const;
@@ -427,6 +446,10 @@ int launch_rev_arrivals(int *rev_ring, int *rev_cnt, int rev_R, int rev_cap, int
 int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *clk, int k0, int M,
                    cudaStream_t st);
 int launch_clock_advance(Clock *clk, int K, cudaStream_t st);
+int launch_exchange_unpack(const SpikeOut &so, const int4 *recv, int xch_cap, int world, int rank,
+                           cudaStream_t st);
+void mark_sources_device(const std::vector<GenBlockDev> &blocks, const std::vector<RuleBlockDev> &rblocks,
+                         unsigned char *d_flag, cudaStream_t st);
 void set_launch_pdl(bool on);
 // reduction-rate probe (ngpu_probe.cu): 1e9 random FP64 reductions per second
 double measure_random_reduction_rate(size_t bytes, long long n_ops);

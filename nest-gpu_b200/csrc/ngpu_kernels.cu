@@ -81,8 +81,8 @@ __device__ __forceinline__ void iaf_neuron(const IafArgs &A, const SpikeOut &so,
 __global__ void __launch_bounds__(256, 3) iaf_batch_kernel(const IafArgs A, const SpikeOut so,
                                                         const Clock *clk, int k0, int M) {
   pdl_enter();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < A.n) iaf_neuron(A, so, clk, k0, M, i);
+  const int i = A.lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < A.hi) iaf_neuron(A, so, clk, k0, M, i);
 }
 
 // All iaf_psc_exp groups in one launch (a network of several populations would
@@ -99,8 +99,8 @@ __global__ void __launch_bounds__(256, 3) iaf_multi_kernel(const IafArgs *tab, c
     if (blk0[mid] <= (int)blockIdx.x) lo = mid; else hi = mid;
   }
   const IafArgs &A = tab[lo];
-  const int i = ((int)blockIdx.x - blk0[lo]) * blockDim.x + threadIdx.x;
-  if (i < A.n) iaf_neuron(A, so, clk, k0, M, i);
+  const int i = A.lo + ((int)blockIdx.x - blk0[lo]) * blockDim.x + threadIdx.x;
+  if (i < A.hi) iaf_neuron(A, so, clk, k0, M, i);
 }
 
 // ---------------------------------------------------------------------------
@@ -111,8 +111,8 @@ __global__ void __launch_bounds__(256, 3) iaf_multi_kernel(const IafArgs *tab, c
 __global__ void __launch_bounds__(256) parrot_batch_kernel(const ParrotArgs A, const SpikeOut so, const Clock *clk,
                                                            int k0, int M) {
   pdl_enter();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
+  const int i = A.lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.hi) return;
   const int n = A.n;
   float in0 = A.var[i], dummy = A.var[(size_t)n + i], V = A.var[2 * (size_t)n + i];
   const bool hold = A.hold[i] != 0.0f;
@@ -151,8 +151,8 @@ __global__ void __launch_bounds__(256) parrot_batch_kernel(const ParrotArgs A, c
 __global__ void __launch_bounds__(256) spike_det_batch_kernel(const ParrotArgs A, const SpikeOut so,
                                                               const Clock *clk, int k0, int M) {
   pdl_enter();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
+  const int i = A.lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.hi) return;
   const int n = A.n;
   float in0 = A.var[i], sh = A.var[(size_t)n + i];
   const bool hold = A.hold[i] != 0.0f;
@@ -188,8 +188,8 @@ __global__ void __launch_bounds__(256) spike_det_batch_kernel(const ParrotArgs A
 __global__ void spike_gen_batch_kernel(const SpikeGenArgs A, const SpikeOut so, const Clock *clk, int k0,
                                        int M) {
   pdl_enter();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
+  const int i = A.lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.hi) return;
   const int e0 = A.off[i], e1 = A.off[i + 1];
   int nx = A.next[i];
   const Clock cl = *clk;
@@ -263,6 +263,7 @@ __device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock 
     // any emission step read here because R >= M + dmax + 3); straggler lists start empty
     for (int m = threadIdx.x; m < M; m += blockDim.x) A.ring_cnt[(int)((t_first + m) % A.R)] = 0;
     for (int g = threadIdx.x; g < A.n_strag; g += blockDim.x) A.strag_cnt[g] = 0;
+    if (A.xch && threadIdx.x == 0) A.xch[0].x = 0;
   }
   const int sub = threadIdx.x & (G - 1);
   const int grp = (block * DELIVER_THREADS + threadIdx.x) / G;
@@ -455,7 +456,7 @@ int launch_aeif_learn(int model, const AeifArgs &A, const SpikeOut &so, const Cl
 
 int launch_aeif(int model, const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                 cudaStream_t st) {
-  if (A.n <= 0) return 0;
+  if (A.hi <= A.lo) return 0;
   if (A.learn.mode != LM_PLAIN) return launch_aeif_learn(model, A, so, clk, k0, M, st);
   switch (model) {
   case M_AEIF_COND_BETA: return launch_aeif_m<M_AEIF_COND_BETA>(A, so, clk, k0, M, st);
@@ -467,8 +468,8 @@ int launch_aeif(int model, const AeifArgs &A, const SpikeOut &so, const Clock *c
 }
 
 int launch_iaf(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
-  if (A.n <= 0) return 0;
-  launch_k(iaf_batch_kernel, dim3((A.n + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
+  if (A.hi <= A.lo) return 0;
+  launch_k(iaf_batch_kernel, dim3((A.hi - A.lo + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
   return 1;
 }
 
@@ -480,21 +481,21 @@ int launch_iaf_multi(const IafArgs *tab, const int *blk0, int ngroups, int nbloc
 }
 
 int launch_spike_det(const ParrotArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
-  if (A.n <= 0) return 0;
-  launch_k(spike_det_batch_kernel, dim3((A.n + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
+  if (A.hi <= A.lo) return 0;
+  launch_k(spike_det_batch_kernel, dim3((A.hi - A.lo + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
   return 1;
 }
 
 int launch_parrot(const ParrotArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
-  if (A.n <= 0) return 0;
-  launch_k(parrot_batch_kernel, dim3((A.n + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
+  if (A.hi <= A.lo) return 0;
+  launch_k(parrot_batch_kernel, dim3((A.hi - A.lo + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
   return 1;
 }
 
 int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                      cudaStream_t st) {
-  if (A.n <= 0) return 0;
-  launch_k(spike_gen_batch_kernel, dim3((A.n + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
+  if (A.hi <= A.lo) return 0;
+  launch_k(spike_gen_batch_kernel, dim3((A.hi - A.lo + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
   return 1;
 }
 
@@ -506,6 +507,30 @@ int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *c
   else if (group == 16) launch_k(deliver_batch_kernel<16>, g, b, smem, st, A, clk, k0, M);
   else if (A.aggregate) launch_k(deliver_batch_kernel<32, true>, g, b, smem, st, A, clk, k0, M);
   else launch_k(deliver_batch_kernel<32>, g, b, smem, st, A, clk, k0, M);
+  return 1;
+}
+
+// Partitioned network: the spikes the other processes' neurons emitted in the batch
+// (recv[q] = their exchange buffers, q = 0 .. world-1, this process's own block skipped) go
+// into this process's ring when their source has out-edges to neurons simulated here.
+__global__ void exchange_unpack_kernel(SpikeOut so, const int4 *recv, int xch_cap, int world, int rank) {
+  const int q = blockIdx.x;
+  if (q == rank || q >= world) return;
+  const int4 *b = recv + (size_t)q * (xch_cap + 1);
+  const int n = min(b[0].x, xch_cap);
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const int4 e = b[1 + j];
+    if (!so.has_out[e.x]) continue;
+    const int slot = (int)((long long)e.z % so.R);
+    const int pos = atomicAdd(&so.ring_cnt[slot], 1);
+    if (pos < so.cap) so.ring[(size_t)slot * so.cap + pos] = make_int2(e.x, e.y);
+    else atomicOr(so.status, ST_RING_OVERFLOW);
+  }
+}
+
+int launch_exchange_unpack(const SpikeOut &so, const int4 *recv, int xch_cap, int world, int rank,
+                           cudaStream_t st) {
+  exchange_unpack_kernel<<<world, 256, 0, st>>>(so, recv, xch_cap, world, rank);
   return 1;
 }
 

@@ -166,6 +166,15 @@ void Engine::calibrate() {
   if (acc_total >= (1ULL << 32)) throw NgpuError("input accumulator exceeds 2^32 entries");
   n_acc_ = acc_total;
 
+  // ---- partition: this process simulates neurons lo .. hi-1 of every group (a contiguous
+  //      share per rank); the delivery layout keeps the in-edges of those neurons only
+  std::vector<unsigned char> local(N, 1);
+  for (auto &g : groups_) {
+    g.lo = (int)((long long)g.n * part_rank_ / part_world_);
+    g.hi = (int)((long long)g.n * (part_rank_ + 1) / part_world_);
+    if (part_world_ > 1)
+      for (int i = 0; i < g.n; i++) local[g.i0 + i] = (i >= g.lo && i < g.hi) ? 1 : 0;
+  }
   // ---- connections: recurrent edges into CSR by (source, delay); poiss_gen edges apart
   const size_t E = c_src_.size();
   std::vector<unsigned char> is_pg(N, 0);
@@ -188,6 +197,7 @@ void Engine::calibrate() {
     dmin = std::min(dmin, c_d_[e]);
     dmax = std::max(dmax, c_d_[e]);
   }
+  if (plastic_ && part_world_ > 1) throw NgpuError("a partitioned network cannot have plastic connections");
   std::vector<GenBlockDev> gblocks;
   for (size_t bi = 0; bi < blocks_.size(); bi++) {
     const GenBlock &b = blocks_[bi];
@@ -204,6 +214,12 @@ void Engine::calibrate() {
     d.dlo = (int)std::round(b.dmin_ms / dt) - 1;
     d.dhi = (int)std::round(b.dmax_ms / dt) - 1;
     d.seed = b.seed;
+    // the block's targets simulated here (block-relative); the draws stay keyed by the
+    // block-relative target, so every rank generates the same edges for a target
+    const int loc_lo = tg.i0 + tg.lo, loc_hi = tg.i0 + tg.hi;
+    d.t_begin = std::max(0, loc_lo - b.tgt0);
+    d.t_end = std::min(b.ntgt, loc_hi - b.tgt0);
+    if (d.t_end < d.t_begin) d.t_end = d.t_begin;
     dmin = std::min(dmin, d.dlo);
     dmax = std::max(dmax, d.dhi);
     gblocks.push_back(d);
@@ -233,6 +249,10 @@ void Engine::calibrate() {
         acc0[g.i0 + i] = (unsigned)(g.acc_off + (size_t)i);
         gn[g.i0 + i] = g.n;
       }
+    // non-local targets get the index 0xffffffff: the expansion skips them
+    if (part_world_ > 1)
+      for (int i = 0; i < N; i++)
+        if (!local[i]) acc0[i] = 0xffffffffu;
     d_node_acc0 = dalloc<unsigned>(N);
     d_node_gn = dalloc<int>(N);
     cuda_check(cudaMemcpy(d_node_acc0, acc0.data(), N * sizeof(unsigned), cudaMemcpyHostToDevice), "node map");
@@ -264,7 +284,7 @@ void Engine::calibrate() {
       hrank.reserve(n_rec_edges);
       hew.reserve(n_rec_edges);
       for (size_t e = 0; e < E; e++) {
-        if (is_pg[c_src_[e]]) continue;
+        if (is_pg[c_src_[e]] || !local[c_tgt_[e]]) continue;
         const Group &tg = groups_[node_group_[c_tgt_[e]]];
         long long key = (long long)c_src_[e] * dspan_ + (c_d_[e] - dmin);
         if (syn_of(e)) {
@@ -295,6 +315,17 @@ void Engine::calibrate() {
   cuda_check(cudaMemcpy(has_out.data(), d_has_out_, N, cudaMemcpyDeviceToHost), "has_out");
   int n_src_out = 0;
   for (int i = 0; i < N; i++) n_src_out += has_out[i];
+  d_has_out_all_ = nullptr;
+  if (part_world_ > 1) {
+    // sources with recurrent edges to any process's neurons: their spikes are exchanged
+    std::vector<unsigned char> all(N, 0);
+    for (size_t e = 0; e < E; e++)
+      if (!is_pg[c_src_[e]]) all[c_src_[e]] = 1;
+    d_has_out_all_ = dalloc<unsigned char>(N);
+    cuda_check(cudaMemcpy(d_has_out_all_, all.data(), N, cudaMemcpyHostToDevice), "has_out_all");
+    mark_sources_device(gblocks, rdev, d_has_out_all_, stream_);
+    cuda_check(cudaStreamSynchronize(stream_), "has_out_all");
+  }
 
   // ---- poiss_gen: generator table and target-major in-edges with canonical ids
   n_gen_ = 0;
@@ -662,6 +693,9 @@ SpikeOut Engine::spike_out() const {
   so.R = R_;
   so.cap = cap_;
   so.has_out = d_has_out_;
+  so.has_out_all = d_has_out_all_ ? d_has_out_all_ : d_has_out_;
+  so.xch = part_world_ > 1 ? xch_send_ : nullptr;
+  so.xch_cap = xch_cap_;
   so.last_tidx = d_last_tidx_;
   so.last_height = d_last_h_;
   so.status = d_status_;
@@ -711,6 +745,8 @@ AeifArgs Engine::aeif_args(Group &g) {
   std::memset(&A, 0, sizeof(A));
   A.n = g.n;
   A.i0 = g.i0;
+  A.lo = g.lo;
+  A.hi = g.hi;
   A.nport = g.nport;
   A.nvar = 2 + n_port_var(g.model) * g.nport;
   A.var = g.d_var;
@@ -750,6 +786,8 @@ IafArgs Engine::iaf_args(Group &g) {
   std::memset(&A, 0, sizeof(A));
   A.n = g.n;
   A.i0 = g.i0;
+  A.lo = g.lo;
+  A.hi = g.hi;
   A.var = g.d_var;
   A.in = group_input(g);
   A.rec = group_record(g);
@@ -766,6 +804,8 @@ ParrotArgs Engine::parrot_args(Group &g) {
   ParrotArgs A;
   A.n = g.n;
   A.i0 = g.i0;
+  A.lo = g.lo;
+  A.hi = g.hi;
   A.var = g.d_var;
   A.hold = g.d_hold;
   A.in = group_input(g);
@@ -779,6 +819,8 @@ SpikeGenArgs Engine::sg_args(Group &g) {
   SpikeGenArgs A;
   A.n = g.n;
   A.i0 = g.i0;
+  A.lo = g.lo;
+  A.hi = g.hi;
   A.off = g.d_sg_off;
   A.tidx = g.d_sg_tidx;
   A.height = g.d_sg_h;
@@ -806,6 +848,7 @@ DeliverArgs Engine::deliver_args() {
   A.strag_cnt = d_strag_cnt_;
   A.n_strag = n_strag_;
   A.aggregate = deliver_aggregate;
+  A.xch = part_world_ > 1 ? xch_send_ : nullptr;
   return A;
 }
 
@@ -996,7 +1039,7 @@ void Engine::prepare_multi() {
     if (g.model != M_IAF_PSC_EXP || g.n <= 0) continue;
     tab.push_back(iaf_args(g));
     blk0.push_back(nb);
-    nb += (g.n + 255) / 256;
+    nb += (g.hi - g.lo + 255) / 256;
     first.push_back(first.back() + g.n);
   }
   n_iaf_multi_ = (int)tab.size();
@@ -1018,7 +1061,7 @@ void Engine::prepare_multi() {
 // The persistent step loop serves networks whose only neurons are iaf_psc_exp groups
 // (Poisson generators have no kernel of their own).
 bool Engine::persistent_eligible() const {
-  if (plastic_) return false;
+  if (plastic_ || part_world_ > 1) return false;
   bool any = false;
   for (auto &g : groups_) {
     if (g.n <= 0 || g.model == M_POISS_GEN) continue;
@@ -1047,7 +1090,60 @@ void Engine::ensure_record_window(long long rows) {
   invalidate_graphs();
 }
 
+void Engine::set_partition(int rank, int world) {
+  if (calibrated_) throw NgpuError("the partition must be set before calibration");
+  if (world < 1 || rank < 0 || rank >= world) throw NgpuError("partition rank out of range");
+  part_rank_ = rank;
+  part_world_ = world;
+}
+
+void Engine::set_exchange(void *send, void *recv, long long cap, int (*exchange)(void *), void *user) {
+  if (cap < 1 || cap > (1LL << 30)) throw NgpuError("exchange capacity out of range");
+  if (!send || !recv || !exchange) throw NgpuError("exchange buffers and function are required");
+  if (((uintptr_t)send | (uintptr_t)recv) & 15) throw NgpuError("exchange buffers must be 16-byte aligned");
+  xch_send_ = (int4 *)send;
+  xch_recv_ = (int4 *)recv;
+  xch_cap_ = (int)cap;
+  xch_fn_ = exchange;
+  xch_user_ = user;
+  invalidate_graphs();
+}
+
+// Partitioned network: batch by batch (no graphs), each followed by the spike exchange:
+// the batch's kernels, a wait for them, the caller's all-gather of the exchange buffers, the
+// other processes' spikes into this process's ring, and the clock advance.  Every process
+// runs the same batches, so the exchange calls pair up.
+void Engine::run_batches_partitioned(long long n) {
+  if (!xch_fn_) throw NgpuError("a partitioned network needs its exchange (NGPU_SetExchange) before simulating");
+  const int M = batch_;
+  long long window = n;
+  const long long REC_WINDOW = 10000;
+  if (rec_ncol_) {
+    window = std::min<long long>(n, REC_WINDOW);
+    ensure_record_window(window);
+  }
+  long long done = 0;
+  while (done < n) {
+    const long long w = std::min(window, n - done);
+    for (long long left = w; left > 0;) {
+      const int mb = (int)std::min<long long>(M, left);
+      launch_batch(0, mb, nullptr);
+      cuda_check(cudaStreamSynchronize(stream_), "batch");
+      if (xch_fn_(xch_user_) != 0) throw NgpuError("the spike exchange failed");
+      count_launch(launch_exchange_unpack(spike_out(), xch_recv_, xch_cap_, part_world_, part_rank_, stream_));
+      count_launch(launch_clock_advance(d_clk_, mb, stream_));
+      left -= mb;
+    }
+    if (rec_ncol_) drain_records(w);
+    done += w;
+  }
+}
+
 void Engine::run_steps(long long n) {
+  if (part_world_ > 1) {
+    run_batches_partitioned(n);
+    return;
+  }
   const int M = batch_;
   const int K = std::max(M, (std::max(1, graph_steps) / M) * M);   // steps per graph
   long long window = n;

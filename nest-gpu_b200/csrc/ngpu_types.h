@@ -32,6 +32,8 @@ enum Status : unsigned {
   ST_NUMERIC = 1u << 2,               // V_m or w left their guard bounds (reset applied)
   ST_REC_TIMES_FULL = 1u << 3,        // a neuron exceeded its recorded-spike-time capacity
   ST_BARRIER_TIMEOUT = 1u << 4,       // a grid barrier of the persistent step loop gave up waiting
+  ST_EXCHANGE_FULL = 1u << 5,         // partitioned network: more local spikes in a batch than the
+                                      // exchange buffer holds (the excess was dropped)
 };
 
 // Barrier state of the persistent step loop (device memory, zero-initialised).
@@ -55,7 +57,12 @@ struct SpikeOut {
   int2 *ring;            // [R][cap] (source node, height bits), slot = time index % R
   int *ring_cnt;         // [R]
   int R, cap;
-  const unsigned char *has_out;   // per node: 1 if it has recurrent out-edges
+  const unsigned char *has_out;   // per node: 1 if it has recurrent out-edges to neurons simulated here
+  const unsigned char *has_out_all;   // per node: 1 if it has recurrent out-edges anywhere
+  // partitioned network: the batch's spikes of the neurons simulated here, for the other
+  // processes; xch[0].x counts them, xch[1 + j] = {node, height bits, time index, 0}
+  int4 *xch;
+  int xch_cap;
   int *last_tidx;        // per node: time index of the most recent spike
   float *last_height;    // per node: height of the most recent spike
   unsigned *status;
@@ -140,6 +147,7 @@ struct LearnCtx {
 struct AeifArgs {
   int n;
   int i0;
+  int lo, hi;            // neurons lo .. hi-1 of the group are simulated here (all: 0, n)
   int nport;
   int nvar;
   float *var;            // SoA [nvar][n]: V_m, w, port vars (port-major)
@@ -173,6 +181,7 @@ enum IafPar {
 struct IafArgs {
   int n;
   int i0;
+  int lo, hi;            // neurons lo .. hi-1 of the group are simulated here (all: 0, n)
   float *var;            // SoA [4][n]: I_syn_ex, I_syn_in, V_m_rel, refractory_step
   GroupInput in;
   GroupRecord rec;
@@ -186,6 +195,7 @@ struct IafArgs {
 struct ParrotArgs {
   int n;
   int i0;
+  int lo, hi;            // neurons lo .. hi-1 of the group are simulated here (all: 0, n)
   float *var;            // SoA [3][n]
   const float *hold;     // [n] hold_spike_height
   GroupInput in;
@@ -197,6 +207,7 @@ struct ParrotArgs {
 struct SpikeGenArgs {
   int n;
   int i0;
+  int lo, hi;            // neurons lo .. hi-1 of the group are simulated here (all: 0, n)
   const int *off;        // [n+1] into tidx/height
   const int *tidx;       // spike step indices (per-call step counter)
   const float *height;
@@ -226,6 +237,7 @@ struct DeliverArgs {
   int *strag_cnt;        // per-group straggler counters, cleared for the batch
   int n_strag;
   int aggregate;         // 1 (with 32-lane groups): warp-aggregated reductions
+  int4 *xch;             // partitioned network: exchange buffer whose count the batch clears
 };
 
 // Plastic edge (synapse group > 0): its position in the delivery CSR, its target node and
@@ -272,6 +284,7 @@ struct GenBlockDev {
   float w;
   int dlo, dhi;            // delay indices, inclusive
   uint64_t seed;
+  int t_begin, t_end;      // block-relative targets whose edges are generated here
 };
 
 // A rule-based connection call (src/connect_rules.h:161-338) whose edges are expanded on the

@@ -176,6 +176,9 @@ if is_b200_engine:
     _c["NGPU_SetUpdateOccupancy"] = _bind("NGPU_SetUpdateOccupancy", _I, [_I])
     _c["NGPU_SetUpdateTrialIter"] = _bind("NGPU_SetUpdateTrialIter", _I, [_I])
     _c["NGPU_SetDeliverAggregate"] = _bind("NGPU_SetDeliverAggregate", _I, [_I])
+    _c["NGPU_SetPartition"] = _bind("NGPU_SetPartition", _I, [_I, _I])
+    _c["NGPU_SetExchange"] = _bind("NGPU_SetExchange", _I, [c_void_p, c_void_p, ctypes.c_longlong, c_void_p,
+                                                             c_void_p])
     _c["NGPU_GetBatchLength"] = _bind("NGPU_GetBatchLength", _I, [])
     _c["NGPU_SetPersistent"] = _bind("NGPU_SetPersistent", _I, [_I])
     _c["NGPU_TestBarrierTimeout"] = _bind("NGPU_TestBarrierTimeout", _I, [_I])
@@ -1475,6 +1478,24 @@ def SetDeliverAggregate(on=True):
     extension; results are identical either way)."""
     _need_b200("SetDeliverAggregate")
     return _check(_c["NGPU_SetDeliverAggregate"](1 if on else 0))
+
+
+def SetPartition(rank, world):
+    """This process simulates share `rank` of `world` of every node group (engine extension,
+    before calibration); see partition.py for the spike exchange."""
+    _need_b200("SetPartition")
+    return _check(_c["NGPU_SetPartition"](int(rank), int(world)))
+
+
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
+
+
+def SetExchange(send_ptr, recv_ptr, cap, fn):
+    """Exchange buffers (device pointers to (cap + 1) int4 records per process) and the
+    all-gather function called after every time batch (an EXCHANGE_FN; keep a reference to
+    it while the engine runs)."""
+    _need_b200("SetExchange")
+    return _check(_c["NGPU_SetExchange"](send_ptr, recv_ptr, int(cap), ctypes.cast(fn, c_void_p), None))
 
 
 def SetDeliverGroup(g):
