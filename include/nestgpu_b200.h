@@ -350,11 +350,6 @@ int NGPU_SetUpdateTrialIter(int on);
    and one lane issues the reduction (warp-aggregated reductions); 0: one reduction per edge
    (default).  Results do not depend on it. */
 int NGPU_SetDeliverAggregate(int on);
-/* 1: a warp of the aeif update kernel whose own neurons are done takes up to 32 entries of the
-   straggler list (neurons that used up their RK5 step budget) and finishes them, beside the
-   blocks still running; the straggler kernel finishes the entries nobody took.  0: the
-   straggler kernel finishes them all (default).  Results do not depend on it. */
-int NGPU_SetStragglerSteal(int on);
 /* Lanes per spike-delivery work item (8, 16 or 32; default 32): one item is the out-edge
    segment of one (source, delay) pair; short segments leave fewer lanes idle with small
    groups. */
@@ -386,10 +381,10 @@ int NGPU_TestBarrierTimeout(int extra);
    values. */
 int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliver_blocks,
                   int *rk5_budget);
-/* The current launch mapping: writes min(n, 10) of {update block size, register-capped update
+/* The current launch mapping: writes min(n, 9) of {update block size, register-capped update
    variant, delivery lane group, delivery grid (0: automatic), RK5 step budget, persistent loop,
-   programmatic launch, trial-per-iteration update, warp-aggregated delivery, straggler taking
-   by the update kernel} and returns 10 (-1 on error).  No counterpart in the reference. */
+   programmatic launch, trial-per-iteration update, warp-aggregated delivery} and returns 9 (-1
+   on error).  No counterpart in the reference. */
 int NGPU_GetLaunchMapping(int *vals, int n);
 /* Measured rate (1e9 per second) of FP64 reductions to uniformly random addresses of a
    `bytes`-byte device buffer, `n_ops` in total: the access pattern of the spike delivery's

@@ -753,46 +753,6 @@ __device__ __forceinline__ void warp_add(unsigned long long *ctr, unsigned long 
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr, v);
 }
 
-// A neuron the main kernel left unfinished (typically one that spikes in the batch),
-// continued from the step where it stopped with the step-at-once form (the
-// trial-per-iteration form measured 2.5% slower here: these lanes are all in long sub-step
-// chains).  Its state is read past L1 (__ldcg): another SM wrote it during this kernel
-// when a lane of the main kernel takes the item.
-template <int MODEL, int PMAX, bool FIXED, int LM, bool UNI>
-__device__ __forceinline__ void aeif_straggler_item(const AeifArgs &A, const SpikeOut &so, const Clock &cl, int k0,
-                                                    int M, int2 e, unsigned long long &nd, const float *smodel) {
-  typedef AeifShape<MODEL> S;
-  constexpr int NVM = 2 + S::npv * PMAX;
-  const long long rec_it0 = cl.rec_it0;
-  const int i = e.x;
-  AeifQ<MODEL, PMAX, FIXED> q;
-  load_aeif_par<MODEL, PMAX, FIXED, UNI>(A, i, q);
-  const int NV = 2 + S::npv * q.ports();
-  float y[NVM];
-#pragma unroll
-  for (int v = 0; v < NVM; v++)
-    if (v < NV) y[v] = __ldcg(&A.var[(size_t)v * A.n + i]);
-  float refr = __ldcg(&A.refr[i]), h = __ldcg(&A.h[i]);
-  double x = __ldcg(&A.x[i]);
-  PoissonCache pc;
-  poisson_cache_load(A.in, i, pc);
-  int m = e.y, guard = 0;
-  StepT t = step_at(cl, k0, m, A.dt);
-  double apf[PMAX];
-  acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
-  while (m < M) {
-    if (aeif_substep<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, nd, smodel, guard)) {
-      aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
-      guard = 0;
-      if (++m < M) {
-        t = step_at(cl, k0, m, A.dt);
-        acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
-      }
-    }
-  }
-  aeif_store<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
-}
-
 // One iteration of the trial-per-iteration form: begin a step if none is open (k1 and the
 // error scale), run one trial; after a rejection shrink h and return false (the step stays
 // open); after an acceptance update x, h and y and run the ExternalUpdate.  Returns true
@@ -912,79 +872,59 @@ __global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const Aeif
     }
     aeif_store<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
     if (deferred) {
-      __threadfence();   // the state is visible before the entry that names it
       const int pos = atomicAdd(A.strag_cnt, 1);
-      // one 8-byte store: a reader sees the whole entry or the empty marker
-      *reinterpret_cast<volatile long long *>(A.strag_list + pos) =
-          (long long)(((unsigned long long)(unsigned)m << 32) | (unsigned)i);
-    }
-  }
-  if constexpr (LM == LM_PLAIN) {
-    if (A.steal) {
-      // A warp whose own neurons are done takes up to 32 entries of the straggler list at a
-      // time and finishes them here, beside the blocks still running, instead of leaving
-      // them to the straggler kernel's low-occupancy tail.  An entry is taken only once it
-      // exists (its producer has counted it); its producer writes it right after counting.
-      const int lane = threadIdx.x & 31;
-      const Clock cl = *clk;
-      for (;;) {
-        int base = 0, nt = 0;
-        if (lane == 0) {
-          for (;;) {
-            const int p = *(volatile int *)A.strag_taken;
-            const int c = *(volatile int *)A.strag_cnt;
-            if (p >= c) break;
-            const int want = (c - p) < 32 ? (c - p) : 32;
-            if (atomicCAS(A.strag_taken, p, p + want) == p) {
-              base = p;
-              nt = want;
-              break;
-            }
-          }
-        }
-        nt = __shfl_sync(0xffffffffu, nt, 0);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (nt == 0) break;
-        if (lane < nt) {
-          volatile long long *slot = reinterpret_cast<volatile long long *>(A.strag_list + base + lane);
-          long long v = *slot;
-          for (int spin = 0; v == -1LL && spin < (1 << 22); spin++) v = *slot;
-          if (v == -1LL) {
-            atomicOr(so.status, ST_STRAGGLER_WAIT);   // the entry never appeared: give up on it
-          } else {
-            __threadfence();   // the neuron's state is read after its entry
-            *slot = -1LL;
-            const int2 e = make_int2((int)(unsigned)((unsigned long long)v & 0xffffffffu),
-                                     (int)(unsigned)((unsigned long long)v >> 32));
-            aeif_straggler_item<MODEL, PMAX, FIXED, LM, UNI>(A, so, cl, k0, M, e, nd, smodel);
-          }
-        }
-        __syncwarp();
-      }
+      A.strag_list[pos] = make_int2(i, m);
     }
   }
   warp_add(A.nderiv, nd);
 }
 
-// The items of the straggler list nobody has taken yet (index >= the taken counter), one per
-// thread.  Every entry read is reset to the empty marker for the next batch.
+// Neurons the main kernel left unfinished (typically the few that spike in the batch)
+// continue here from the step where they stopped, one per thread.
+// (The trial-per-iteration form measured 2.5% slower here than the step-at-once form: the
+// lanes of this kernel are all in long sub-step chains.)
 template <int MODEL, int PMAX, bool FIXED, int LM, bool UNI = false>
 __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, const SpikeOut so,
                                                              const Clock *clk, int k0, int M) {
   pdl_enter();
+  typedef AeifShape<MODEL> S;
+  constexpr int NVM = 2 + S::npv * PMAX;
   __shared__ float smodel[LM == LM_PROPOSE ? SM_NPAR : 1];
   if (LM == LM_PROPOSE) {
     for (int j = threadIdx.x; j < SM_NPAR; j += blockDim.x) smodel[j] = A.learn.model[j];
     __syncthreads();
   }
   const int cnt = *A.strag_cnt;
-  const int first = *A.strag_taken;
   const Clock cl = *clk;
+  const long long rec_it0 = cl.rec_it0;
   unsigned long long nd = 0;
-  for (int j = first + blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
     const int2 e = A.strag_list[j];
-    A.strag_list[j] = make_int2(-1, -1);
-    aeif_straggler_item<MODEL, PMAX, FIXED, LM, UNI>(A, so, cl, k0, M, e, nd, smodel);
+    const int i = e.x;
+    AeifQ<MODEL, PMAX, FIXED> q;
+    load_aeif_par<MODEL, PMAX, FIXED, UNI>(A, i, q);
+    const int NV = 2 + S::npv * q.ports();
+    float y[NVM];
+    float refr, h;
+    double x;
+    aeif_load<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
+    PoissonCache pc;
+    poisson_cache_load(A.in, i, pc);
+    int m = e.y, guard = 0;
+    StepT t = step_at(cl, k0, m, A.dt);
+    double apf[PMAX];
+    acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
+    while (m < M) {
+      if (aeif_substep<MODEL, PMAX, FIXED, LM>(A, so, i, q, y, refr, x, h, t.tidx, t.tnow, nd, smodel, guard)) {
+        aeif_end_step(A, so, i, q, y, refr, m, t, rec_it0, apf, pc);
+        guard = 0;
+        if (++m < M) {
+          t = step_at(cl, k0, m, A.dt);
+          acc_prefetch<PMAX>(apf, q.ports(), A.n, i, A.in, m);
+        }
+      }
+    }
+    aeif_store<MODEL, PMAX, FIXED>(A, i, y, refr, x, h, NV);
   }
   warp_add(A.nderiv, nd);
 }

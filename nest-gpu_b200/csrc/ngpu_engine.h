@@ -132,7 +132,6 @@ class Engine {
   int deliver_aggregate = 0;      // 1: warp-aggregated reductions (with 32-lane work items)
   int update_occupancy = 0;       // 1: register-capped aeif update kernel
   int update_trial_iter = 0;      // 1: aeif update kernel advances one RK5 trial per iteration
-  int straggler_steal = 0;        // 1: warps of the aeif update kernel take straggler entries when done
   int persistent = 0;             // iaf-only networks: persistent cooperative step loop
   int launch_pdl = -1;            // programmatic dependent launch of the batch kernels (-1: one-step batches)
   int barrier_extra = 0;          // test hook: blocks the persistent loop's barriers wait for in excess

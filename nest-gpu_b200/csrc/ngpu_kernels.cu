@@ -262,7 +262,7 @@ __device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock 
     // ring slots of this batch's steps start empty (their previous steps are older than
     // any emission step read here because R >= M + dmax + 3); straggler lists start empty
     for (int m = threadIdx.x; m < M; m += blockDim.x) A.ring_cnt[(int)((t_first + m) % A.R)] = 0;
-    for (int g = threadIdx.x; g < 2 * A.n_strag; g += blockDim.x) A.strag_cnt[g] = 0;   // counts, taken
+    for (int g = threadIdx.x; g < A.n_strag; g += blockDim.x) A.strag_cnt[g] = 0;
     if (A.xch && threadIdx.x == 0) A.xch[0].x = 0;
   }
   const int sub = threadIdx.x & (G - 1);

@@ -459,7 +459,6 @@ void Engine::calibrate() {
     }
     if (is_aeif(g.model)) {
       g.d_strag = dalloc<int2>(g.n);
-      cuda_check(cudaMemset(g.d_strag, 0xff, (size_t)g.n * sizeof(int2)), "strag");   // empty entries
       g.strag_slot = n_strag_++;
       g.d_refr = dalloc<float>(g.n);
       cuda_check(cudaMemcpy(g.d_refr, g.par[A_refractory_step].data(), g.n * sizeof(float),
@@ -517,9 +516,8 @@ void Engine::calibrate() {
       cuda_check(cudaMemset(g.d_sg_next, 0, g.n * sizeof(int)), "sg");
     }
   }
-  // per aeif group: list length at [slot], entries taken at [n_strag + slot]
-  d_strag_cnt_ = dalloc<int>(std::max(1, 2 * n_strag_));
-  cuda_check(cudaMemset(d_strag_cnt_, 0, std::max(1, 2 * n_strag_) * sizeof(int)), "strag");
+  d_strag_cnt_ = dalloc<int>(std::max(1, n_strag_));
+  cuda_check(cudaMemset(d_strag_cnt_, 0, std::max(1, n_strag_) * sizeof(int)), "strag");
   build_records();
   cuda_check(cudaDeviceSynchronize(), "calibrate");
 }
@@ -764,8 +762,6 @@ AeifArgs Engine::aeif_args(Group &g) {
   A.budget = rk5_budget > 0 ? batch_ + rk5_budget : 0;
   A.strag_list = g.d_strag;
   A.strag_cnt = d_strag_cnt_ + g.strag_slot;
-  A.strag_taken = d_strag_cnt_ + n_strag_ + g.strag_slot;
-  A.steal = straggler_steal;
   A.srec = spike_rec(g);
   A.threads = update_threads;
   A.occupancy = update_occupancy;
@@ -1482,7 +1478,6 @@ int Engine::autotune(int steps, std::vector<std::pair<std::string, double>> *log
       single("update_occupancy", &update_occupancy, {0, 1}),
       single("update_trial_iter", &update_trial_iter, {0, 1}),
       single("deliver_aggregate", &deliver_aggregate, {0, 1}),
-      single("straggler_steal", &straggler_steal, {0, 1}),
       deliver,
       single("rk5_budget", &rk5_budget, {0, 1, 2, 4, 8}),
       single("programmatic_launch", &launch_pdl, {0, 1}),

@@ -34,7 +34,6 @@ enum Status : unsigned {
   ST_BARRIER_TIMEOUT = 1u << 4,       // a grid barrier of the persistent step loop gave up waiting
   ST_EXCHANGE_FULL = 1u << 5,         // partitioned network: more local spikes in a batch than the
                                       // exchange buffer holds (the excess was dropped)
-  ST_STRAGGLER_WAIT = 1u << 6,        // a taken straggler entry never appeared (bounded wait ran out)
 };
 
 // Barrier state of the persistent step loop (device memory, zero-initialised).
@@ -166,11 +165,8 @@ struct AeifArgs {
   int occupancy;         // 1: register-capped variant of the main kernel (more resident warps)
   int uniform;           // 1: every parameter is uniform over the group (no parameter arrays)
   int trial_iter;        // 1: main kernel advances one RK5 trial per loop iteration
-  int2 *strag_list;      // [n] (neuron, step of the batch) left for the straggler kernel;
-                         // empty entries hold (-1, -1)
+  int2 *strag_list;      // [n] (neuron, step of the batch) left for the straggler kernel
   int *strag_cnt;        // list length
-  int *strag_taken;      // entries taken so far (by main-kernel warps, then the straggler kernel)
-  int steal;             // 1: warps of the main kernel take straggler entries when done
   GroupSpikeRec srec;
   LearnCtx learn;
   float pval[AEIF_NPAR];
