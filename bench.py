@@ -19,9 +19,11 @@ bounded sample of the workload: 20,000 neurons with the same in-degree, rates
 and delays for 100 ms of biological time per step; events/s and the RTF
 extrapolated per neuron are reported.
 
-Multi-GPU (torchrun): the network does not shard into independent parts, so each
-rank simulates its own replica (different seed); no collective is on the data
-path, only a barrier and a max-reduction of the step time.
+Multi-GPU (torchrun): by default each rank simulates its own replica (different
+seed); no collective is on the data path, only a barrier and a max-reduction of the
+step time (weak scaling).  With --partition the ranks simulate one network together:
+each rank its share of the neurons with their in-edges, the spikes of every time batch
+all-gathered over NCCL (nest-gpu_b200/partition.py; strong scaling).
 """
 import argparse
 import json
@@ -73,6 +75,9 @@ def parse():
                    help="skip the learned-step and ensemble measurements")
     p.add_argument("--no-ref-cuda", action="store_true",
                    help="skip the timing of the reference's own CUDA build (several minutes)")
+    p.add_argument("--partition", action="store_true",
+                   help="with N > 1 GPUs: one 1M-neuron network split over the GPUs (spikes exchanged "
+                        "over NCCL after every time batch, strong scaling) instead of one replica per GPU")
     return p.parse_args()
 
 
@@ -258,11 +263,17 @@ def engine_arm(args):
 
     barrier, max_over_ranks, sum_over_ranks = rank_reducers(dist, "cuda")
 
-    seed = 20240 + 101 * RANK
+    partitioned = args.partition and WORLD > 1
+    seed = 20240 if partitioned else 20240 + 101 * RANK
     t_build0 = time.time()
     if args.batch_max > 0:
         ngpu.SetBatchMax(args.batch_max)
     neuron, pg = build_engine_network(ngpu, args.scale, seed)
+    if partitioned:
+        # every rank built the same network; it simulates its share and exchanges spikes
+        from partition import TorchExchange
+        exchange = TorchExchange(cap=1 << 18)
+        exchange.attach()
     ngpu.Calibrate()
     build_s = time.time() - t_build0
     # launch mappings picked on this network (the trial steps are part of the transient)
@@ -312,6 +323,11 @@ def engine_arm(args):
     events_all = sum_over_ranks(float(events))
     value = events_all / t_max
     rtf = (dev_ms / 1000.0) / bio_s
+    if partitioned:
+        # each rank counted its own neurons' work; the network is the sum
+        derivs = sum_over_ranks(float(derivs))
+        spikes = sum_over_ranks(float(spikes))
+        rtf = t_max / bio_s
     evals_per_neuron_ms = derivs / (n_neurons * args.steps * STEP_MS)
     rate_hz = spikes / (n_neurons * bio_s)
 
@@ -363,13 +379,14 @@ def engine_arm(args):
         "warmup": args.warmup,
         "ms_per_step": t_max * 1000.0 / args.steps,
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong" if partitioned else "weak",
         "vs_baseline": None,
         "dtype": "fp32",
         "data": "synthetic (seeded random network and Poisson drive)",
         "config": {"workload": "1M aeif_cond_beta_multisynapse x 1000 synapses, Poisson 8 kHz, delays 1-2 ms", "neurons": n_neurons,
                    "synapses": n_neurons * (K_EXC + K_INH), "bio_ms_per_step": STEP_MS,
-                   "dt_ms": 0.1, "parallelism": "replicas%d" % WORLD,
+                   "dt_ms": 0.1,
+                   "parallelism": ("partition%d" % WORLD) if partitioned else ("replicas%d" % WORLD),
                    "l2": "inputs larger than L2 (8 GB edge array)", "scale": args.scale},
         "rtf": rtf,
         "rk5_evals_per_neuron_ms": evals_per_neuron_ms,

@@ -1410,6 +1410,12 @@ std::vector<double> Engine::profile_steps(int n) {
   while (done < n) {
     const int mb = std::min(M, n - done);
     launch_batch(0, mb, &ev);
+    if (part_world_ > 1) {
+      // partitioned network: the batch's exchange, as in run_batches_partitioned
+      cuda_check(cudaStreamSynchronize(stream_), "batch");
+      if (!xch_fn_ || xch_fn_(xch_user_) != 0) throw NgpuError("the spike exchange failed");
+      count_launch(launch_exchange_unpack(spike_out(), xch_recv_, xch_cap_, part_world_, part_rank_, stream_));
+    }
     count_launch(launch_clock_advance(d_clk_, mb, stream_));
     cuda_check(cudaEventSynchronize(ev[2]), "event");
     float ms_del = 0.0f, ms_upd = 0.0f;
