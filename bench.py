@@ -68,8 +68,8 @@ def parse():
     p.add_argument("--mapping", default="",
                    help="fixed launch mapping instead of the autotuner: update threads, register-capped "
                         "variant (0/1), delivery lane group, delivery blocks, RK5 budget and optionally "
-                        "programmatic launch (0/1), one RK5 trial per iteration (0/1) and warp-aggregated "
-                        "delivery (0/1), e.g. 64,1,32,592,1")
+                        "programmatic launch (0/1), one RK5 trial per iteration (0/1), warp-aggregated "
+                        "delivery (0/1) and pipelined delivery (0/1), e.g. 64,1,32,592,1")
     p.add_argument("--batch-max", type=int, default=0, help="upper bound of the time-batch length")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the learned-step and ensemble measurements")
@@ -287,6 +287,8 @@ def engine_arm(args):
             ngpu.SetUpdateTrialIter(vals[6])
         if len(vals) > 7:
             ngpu.SetDeliverAggregate(vals[7])
+        if len(vals) > 8:
+            ngpu.SetDeliverPrefetch(vals[8])
         ngpu.SetUpdateThreads(th)
         ngpu.SetUpdateOccupancy(occ)
         ngpu.SetDeliverGroup(grp)

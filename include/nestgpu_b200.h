@@ -350,6 +350,10 @@ int NGPU_SetUpdateTrialIter(int on);
    and one lane issues the reduction (warp-aggregated reductions); 0: one reduction per edge
    (default).  Results do not depend on it. */
 int NGPU_SetDeliverAggregate(int on);
+/* 1: each delivery work group loads its next work item's spike and segment offsets before it
+   streams the current segment (a two-stage software pipeline); 0: one item after the other.
+   Results do not depend on it. */
+int NGPU_SetDeliverPrefetch(int on);
 /* Lanes per spike-delivery work item (8, 16 or 32; default 32): one item is the out-edge
    segment of one (source, delay) pair; short segments leave fewer lanes idle with small
    groups. */
@@ -381,10 +385,10 @@ int NGPU_TestBarrierTimeout(int extra);
    values. */
 int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliver_blocks,
                   int *rk5_budget);
-/* The current launch mapping: writes min(n, 9) of {update block size, register-capped update
+/* The current launch mapping: writes min(n, 10) of {update block size, register-capped update
    variant, delivery lane group, delivery grid (0: automatic), RK5 step budget, persistent loop,
-   programmatic launch, trial-per-iteration update, warp-aggregated delivery} and returns 9 (-1
-   on error).  No counterpart in the reference. */
+   programmatic launch, trial-per-iteration update, warp-aggregated delivery, pipelined delivery}
+   and returns 10 (-1 on error).  No counterpart in the reference. */
 int NGPU_GetLaunchMapping(int *vals, int n);
 /* Measured rate (1e9 per second) of FP64 reductions to uniformly random addresses of a
    `bytes`-byte device buffer, `n_ops` in total: the access pattern of the spike delivery's

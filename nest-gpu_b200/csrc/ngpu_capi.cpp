@@ -807,6 +807,14 @@ int NGPU_SetExchange(void *send, void *recv, long long cap, int (*exchange)(void
   return guard([&] { E().set_exchange(send, recv, cap, exchange, user); return 0; }, -1);
 }
 
+int NGPU_SetDeliverPrefetch(int on) {
+  return guard([&] {
+    E().deliver_prefetch = on ? 1 : 0;
+    E().invalidate_graphs();
+    return 0;
+  }, -1);
+}
+
 int NGPU_SetDeliverAggregate(int on) {
   return guard([&] {
     E().deliver_aggregate = on ? 1 : 0;
@@ -861,11 +869,11 @@ int NGPU_Autotune(int steps, int *update_threads, int *deliver_group, int *deliv
 
 int NGPU_GetLaunchMapping(int *vals, int n) {
   return guard([&] {
-    const int v[9] = {E().update_threads, E().update_occupancy, E().deliver_group, E().deliver_blocks_req,
-                      E().rk5_budget, E().persistent, E().launch_pdl, E().update_trial_iter,
-                      E().deliver_aggregate};
-    for (int i = 0; i < n && i < 9; i++) vals[i] = v[i];
-    return 9;
+    const int v[10] = {E().update_threads, E().update_occupancy, E().deliver_group, E().deliver_blocks_req,
+                       E().rk5_budget, E().persistent, E().launch_pdl, E().update_trial_iter,
+                       E().deliver_aggregate, E().deliver_prefetch};
+    for (int i = 0; i < n && i < 10; i++) vals[i] = v[i];
+    return 10;
   }, -1);
 }
 

@@ -130,6 +130,7 @@ class Engine {
   int update_threads = 128;       // threads per block of the aeif update kernel (64, 128, 256)
   int deliver_group = 32;         // lanes per delivery work item (8, 16, 32)
   int deliver_aggregate = 0;      // 1: warp-aggregated reductions (with 32-lane work items)
+  int deliver_prefetch = 0;       // 1: delivery loads the next work item's segment ahead
   int update_occupancy = 0;       // 1: register-capped aeif update kernel
   int update_trial_iter = 0;      // 1: aeif update kernel advances one RK5 trial per iteration
   int persistent = 0;             // iaf-only networks: persistent cooperative step loop

@@ -221,7 +221,7 @@ constexpr int MAX_PAIRS = 8192;     // dspan * M
 typedef cub::BlockScan<int, DELIVER_THREADS> DeliverScan;
 
 // The delivery of one batch by block `block` of `nblocks`; s_pref holds dspan*M+1 ints.
-template <int G, bool AGG = false>
+template <int G, bool AGG = false, bool PF = false>
 __device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock *clk, int k0, int M, int *s_pref,
                                               typename DeliverScan::TempStorage &scan_tmp, int block,
                                               int nblocks) {
@@ -269,7 +269,13 @@ __device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock 
   const int grp = (block * DELIVER_THREADS + threadIdx.x) / G;
   const int ngrp = (nblocks * DELIVER_THREADS) / G;
   unsigned long long nev = 0;
-  for (int item = grp; item < total; item += ngrp) {
+  // Work item `item`: its (arrival step, delay) pair, the spike's height and the segment.
+  struct Item {
+    int m;
+    float height;
+    long long e0, e1;
+  };
+  auto fetch = [&](int item) {
     int lo = 0, hi = npairs;   // pair with s_pref[pr] <= item < s_pref[pr+1]
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
@@ -281,10 +287,18 @@ __device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock 
     // segment offsets and edges are written by no kernel that delivers (the persistent loop
     // writes ring entries between its deliveries): read-only path for those two
     const int2 sp = A.ring[(size_t)(te % A.R) * A.cap + j];
-    const float height = __int_as_float(sp.y);
     const size_t key = (size_t)sp.x * A.dspan + dd;
-    const long long e0 = __ldg(&A.ev_off[key]), e1 = __ldg(&A.ev_off[key + 1]);
-    double *acc = A.acc + (size_t)m * A.slot_stride;
+    Item it;
+    it.m = m;
+    it.height = __int_as_float(sp.y);
+    it.e0 = __ldg(&A.ev_off[key]);
+    it.e1 = __ldg(&A.ev_off[key + 1]);
+    return it;
+  };
+  auto deliver = [&](const Item &it) {
+    const long long e0 = it.e0, e1 = it.e1;
+    const float height = it.height;
+    double *acc = A.acc + (size_t)it.m * A.slot_stride;
     if constexpr (AGG) {
       // warp-aggregated reductions (G = 32: the warp is one work group, so this loop is
       // warp-uniform): lanes whose edges share a target add their products first and the
@@ -316,6 +330,23 @@ __device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock 
       }
     }
     if (sub == 0) nev += (unsigned long long)(e1 - e0);
+  };
+  if constexpr (PF) {
+    // software pipeline: the next item's ring entry and segment offsets are loaded before
+    // this item's edges, so their dependent latencies overlap this item's traffic
+    int item = grp;
+    Item cur;
+    if (item < total) cur = fetch(item);
+    while (item < total) {
+      const int next = item + ngrp;
+      Item nxt;
+      if (next < total) nxt = fetch(next);
+      deliver(cur);
+      cur = nxt;
+      item = next;
+    }
+  } else {
+    for (int item = grp; item < total; item += ngrp) deliver(fetch(item));
   }
   // one counter update per block
   for (int o = 16; o > 0; o >>= 1) nev += __shfl_down_sync(0xffffffffu, nev, o);
@@ -328,13 +359,13 @@ __device__ __forceinline__ void deliver_batch(const DeliverArgs &A, const Clock 
   __syncthreads();
 }
 
-template <int G, bool AGG = false>
+template <int G, bool AGG = false, bool PF = false>
 __global__ void __launch_bounds__(DELIVER_THREADS) deliver_batch_kernel(const DeliverArgs A,
                                                                         const Clock *clk, int k0, int M) {
   pdl_enter();
   extern __shared__ int s_pref[];   // npairs + 1 prefix sums over (delay group, arrival step)
   __shared__ typename DeliverScan::TempStorage scan_tmp;
-  deliver_batch<G, AGG>(A, clk, k0, M, s_pref, scan_tmp, blockIdx.x, gridDim.x);
+  deliver_batch<G, AGG, PF>(A, clk, k0, M, s_pref, scan_tmp, blockIdx.x, gridDim.x);
 }
 
 __global__ void clock_advance_kernel(Clock *clk, int K) {
@@ -503,10 +534,17 @@ int launch_deliver(const DeliverArgs &A, int n_blocks, int group, const Clock *c
                    cudaStream_t st) {
   const size_t smem = (size_t)(A.dspan * M + 1) * sizeof(int);
   const dim3 g(n_blocks), b(DELIVER_THREADS);
-  if (group == 8) launch_k(deliver_batch_kernel<8>, g, b, smem, st, A, clk, k0, M);
-  else if (group == 16) launch_k(deliver_batch_kernel<16>, g, b, smem, st, A, clk, k0, M);
-  else if (A.aggregate) launch_k(deliver_batch_kernel<32, true>, g, b, smem, st, A, clk, k0, M);
-  else launch_k(deliver_batch_kernel<32>, g, b, smem, st, A, clk, k0, M);
+  if (A.prefetch) {
+    if (group == 8) launch_k(deliver_batch_kernel<8, false, true>, g, b, smem, st, A, clk, k0, M);
+    else if (group == 16) launch_k(deliver_batch_kernel<16, false, true>, g, b, smem, st, A, clk, k0, M);
+    else if (A.aggregate) launch_k(deliver_batch_kernel<32, true, true>, g, b, smem, st, A, clk, k0, M);
+    else launch_k(deliver_batch_kernel<32, false, true>, g, b, smem, st, A, clk, k0, M);
+  } else {
+    if (group == 8) launch_k(deliver_batch_kernel<8>, g, b, smem, st, A, clk, k0, M);
+    else if (group == 16) launch_k(deliver_batch_kernel<16>, g, b, smem, st, A, clk, k0, M);
+    else if (A.aggregate) launch_k(deliver_batch_kernel<32, true>, g, b, smem, st, A, clk, k0, M);
+    else launch_k(deliver_batch_kernel<32>, g, b, smem, st, A, clk, k0, M);
+  }
   return 1;
 }
 

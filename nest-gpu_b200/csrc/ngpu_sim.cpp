@@ -848,6 +848,7 @@ DeliverArgs Engine::deliver_args() {
   A.strag_cnt = d_strag_cnt_;
   A.n_strag = n_strag_;
   A.aggregate = deliver_aggregate;
+  A.prefetch = deliver_prefetch;
   A.xch = part_world_ > 1 ? xch_send_ : nullptr;
   return A;
 }
@@ -1484,6 +1485,7 @@ int Engine::autotune(int steps, std::vector<std::pair<std::string, double>> *log
       single("update_occupancy", &update_occupancy, {0, 1}),
       single("update_trial_iter", &update_trial_iter, {0, 1}),
       single("deliver_aggregate", &deliver_aggregate, {0, 1}),
+      single("deliver_prefetch", &deliver_prefetch, {0, 1}),
       deliver,
       single("rk5_budget", &rk5_budget, {0, 1, 2, 4, 8}),
       single("programmatic_launch", &launch_pdl, {0, 1}),

@@ -237,6 +237,7 @@ struct DeliverArgs {
   int *strag_cnt;        // per-group straggler counters, cleared for the batch
   int n_strag;
   int aggregate;         // 1 (with 32-lane groups): warp-aggregated reductions
+  int prefetch;          // 1: the next work item's ring entry and offsets loaded ahead
   int4 *xch;             // partitioned network: exchange buffer whose count the batch clears
 };
 

@@ -176,6 +176,7 @@ if is_b200_engine:
     _c["NGPU_SetUpdateOccupancy"] = _bind("NGPU_SetUpdateOccupancy", _I, [_I])
     _c["NGPU_SetUpdateTrialIter"] = _bind("NGPU_SetUpdateTrialIter", _I, [_I])
     _c["NGPU_SetDeliverAggregate"] = _bind("NGPU_SetDeliverAggregate", _I, [_I])
+    _c["NGPU_SetDeliverPrefetch"] = _bind("NGPU_SetDeliverPrefetch", _I, [_I])
     _c["NGPU_SetPartition"] = _bind("NGPU_SetPartition", _I, [_I, _I])
     _c["NGPU_SetExchange"] = _bind("NGPU_SetExchange", _I, [c_void_p, c_void_p, ctypes.c_longlong, c_void_p,
                                                              c_void_p])
@@ -1473,6 +1474,13 @@ def SetUpdateTrialIter(on=True):
     return _check(_c["NGPU_SetUpdateTrialIter"](1 if on else 0))
 
 
+def SetDeliverPrefetch(on=True):
+    """Delivery loads the next work item's spike and segment offsets ahead (engine extension;
+    results are identical either way)."""
+    _need_b200("SetDeliverPrefetch")
+    return _check(_c["NGPU_SetDeliverPrefetch"](1 if on else 0))
+
+
 def SetDeliverAggregate(on=True):
     """Warp-aggregated reductions in the delivery kernel with 32-lane work items (engine
     extension; results are identical either way)."""
@@ -1538,11 +1546,11 @@ def GetLaunchMapping():
     """The current launch mapping (engine extension): update block size and variant, delivery
     lane group and grid, RK5 step budget, persistent loop and programmatic launch."""
     _need_b200("GetLaunchMapping")
-    v = (ctypes.c_int * 9)()
-    _c["NGPU_GetLaunchMapping"](v, 9)
+    v = (ctypes.c_int * 10)()
+    _c["NGPU_GetLaunchMapping"](v, 10)
     _check()
     keys = ["update_threads", "update_occupancy", "deliver_group", "deliver_blocks", "rk5_budget",
-            "persistent", "programmatic_launch", "update_trial_iter", "deliver_aggregate"]
+            "persistent", "programmatic_launch", "update_trial_iter", "deliver_aggregate", "deliver_prefetch"]
     return dict(zip(keys, [int(x) for x in v]))
 
 

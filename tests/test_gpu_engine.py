@@ -270,18 +270,20 @@ def test_profile_and_launch_counters():
     assert ngpu.GetStats()["steps"] == 250
 
 
-@pytest.mark.parametrize("threads,group,occ,tpi,agg", [(64, 8, 0, 0, 0), (256, 16, 1, 0, 0), (128, 32, 1, 0, 0),
-                                                       (64, 8, 0, 1, 0), (128, 32, 1, 1, 1), (64, 32, 0, 0, 1)])
-def test_launch_mappings_keep_results(threads, group, occ, tpi, agg):
+@pytest.mark.parametrize("threads,group,occ,tpi,agg,pf", [(64, 8, 0, 0, 0, 0), (256, 16, 1, 0, 0, 1),
+                                                          (128, 32, 1, 0, 0, 0), (64, 8, 0, 1, 0, 1),
+                                                          (128, 32, 1, 1, 1, 1), (64, 32, 0, 0, 1, 0)])
+def test_launch_mappings_keep_results(threads, group, occ, tpi, agg, pf):
     """The update block size and kernel variants (register cap, one RK5 trial per loop
-    iteration), the delivery lane group and warp-aggregated delivery change only the launch
-    mapping."""
+    iteration), the delivery lane group, warp-aggregated and pipelined delivery change only the
+    launch mapping."""
     ngpu.SetHostRng(True)
     ngpu.SetUpdateThreads(threads)
     ngpu.SetDeliverGroup(group)
     ngpu.SetUpdateOccupancy(occ)
     ngpu.SetUpdateTrialIter(tpi)
     ngpu.SetDeliverAggregate(agg)
+    ngpu.SetDeliverPrefetch(pf)
     c_gpu, d_gpu = fixed_train_network(ngpu, model="aeif_cond_beta_multisynapse")
     c_orc, d_orc = fixed_train_network(orc.Oracle(), model="aeif_cond_beta_multisynapse")
     assert c_gpu.sum() > 0

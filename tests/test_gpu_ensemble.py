@@ -36,7 +36,8 @@ def run(settings, t_ms=200.0, autotune=False):
     {"SetUpdateThreads": 256, "SetDeliverGroup": 16, "SetDeliverBlocks": 2368, "SetRk5Budget": 1,
      "SetUpdateOccupancy": 1},
     {"SetUpdateThreads": 64, "SetDeliverGroup": 32, "SetDeliverAggregate": 1, "SetUpdateTrialIter": 1,
-     "SetRk5Budget": 2},
+     "SetRk5Budget": 2, "SetDeliverPrefetch": 1},
+    {"SetDeliverGroup": 8, "SetDeliverPrefetch": 1},
 ])
 def test_ensemble_results_independent_of_mapping(settings):
     ref_counts, ref_rates, st, _ = run({})

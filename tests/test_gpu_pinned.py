@@ -44,10 +44,11 @@ def oracle_segments(conn, dt, skip_sources):
     return src, step, conn["target"][keep], conn["port"][keep], conn["weight"][keep]
 
 
-@pytest.mark.parametrize("tpi", [0, 1])
-def test_benchmark_network_slice_matches_oracle(tpi):
+@pytest.mark.parametrize("tpi,pf", [(0, 0), (1, 1)])
+def test_benchmark_network_slice_matches_oracle(tpi, pf):
     seed = 20240
     ngpu.SetUpdateTrialIter(tpi)
+    ngpu.SetDeliverPrefetch(pf)
     ngpu.SetRk5Budget(1)
     neuron, pg = benchmark_network(ngpu, 0.01, seed)
     ngpu.Calibrate()
