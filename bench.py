@@ -417,6 +417,12 @@ def engine_arm(args):
                                              "peak_source": "measured in this run: random FP64 reductions into a "
                                                             "buffer of one accumulator slot's size"}},
         "clocks": clocks,
+        # the per-kernel times above are CUDA-event brackets around each kernel of ordinary
+        # steps (serialised, outside the graphs); their sum against the graph-timed step
+        "kernel_timing": {"method": "CUDA events around each kernel (ProfileSteps), serialised",
+                          "sum_ms_per_step": upd_ms + rec_ms + del_ms,
+                          "graph_ms_per_step": dev_ms / (args.steps * STEP_MS / 0.1),
+                          "sum_over_graph": (upd_ms + rec_ms + del_ms) / (dev_ms / (args.steps * STEP_MS / 0.1))},
     }
     if WORLD == 1 and not args.no_extras:
         from workloads import learned_vs_plain
