@@ -1,5 +1,9 @@
-"""The multi-GPU bench runs independent replicas whose only cross-rank traffic is a barrier
-and max / sum reductions of the timed scalars.  Checked here with two gloo ranks on CPU."""
+"""Multi-process paths, checked with two gloo ranks on the CPU:
+- the replicas of the multi-GPU bench, whose only cross-rank traffic is a barrier and
+  max / sum reductions of the timed scalars;
+- the spike exchange of a network partitioned over processes (partition.TorchExchange): every
+  rank receives every rank's records of a time batch, in rank order;
+- the partition of a node group into the ranks' contiguous shares."""
 import os
 import sys
 
