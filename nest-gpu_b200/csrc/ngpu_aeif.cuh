@@ -791,7 +791,9 @@ __device__ __forceinline__ bool aeif_tpi_iter(const AeifArgs &A, const SpikeOut 
 
 // Main aeif kernel: one thread per neuron, steps m = 0..M-1 of the batch.
 // OCC = 1 caps the registers so that three 256-thread blocks fit on an SM (more warps
-// in flight to hide the dependent FP32 latency, at the price of a few spills).
+// in flight to hide the dependent FP32 latency, at the price of a few spills); OCC = 2
+// (trial-per-iteration form, blocks of at most 128 threads) caps them at five 128-thread
+// blocks per SM (about 100 registers: 20 warps, fewer spills).
 // TPI = true (plain controller only): one RK5 trial per loop iteration.  A lane whose
 // trial is rejected retries in the next iteration, beside its neighbours' next trials,
 // instead of holding its whole warp in a second trial (with ~4% of the trials rejected,
@@ -800,7 +802,8 @@ __device__ __forceinline__ bool aeif_tpi_iter(const AeifArgs &A, const SpikeOut 
 // only between accepted steps, so every lane runs the same sequence of operations as
 // in the step-at-once form and results are identical.
 template <int MODEL, int PMAX, bool FIXED, int LM, int OCC = 0, bool UNI = false, bool TPI = false>
-__global__ void __launch_bounds__(256, OCC ? 3 : 1) aeif_batch_kernel(const AeifArgs A, const SpikeOut so,
+__global__ void __launch_bounds__(OCC == 2 ? 128 : 256, OCC == 1 ? 3 : (OCC == 2 ? 5 : 1))
+    aeif_batch_kernel(const AeifArgs A, const SpikeOut so,
                                                          const Clock *clk, int k0, int M) {
   pdl_enter();
   typedef AeifShape<MODEL> S;
@@ -933,11 +936,15 @@ __global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, c
 // number of kernels launched.
 template <int MODEL, int PMAX, bool FIXED, int LM>
 int launch_aeif_p(const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
-  const int tb = (A.threads == 64 || A.threads == 256) ? A.threads : 128;
+  int tb = (A.threads == 64 || A.threads == 256) ? A.threads : 128;
+  if (A.occupancy == 2 && tb > 128) tb = 128;   // the OCC = 2 variant is bounded to 128 threads
   dim3 grid((A.hi - A.lo + tb - 1) / tb), block(tb);
   bool done = false;
   if constexpr (LM == LM_PLAIN && FIXED) {
-    if (A.trial_iter && A.occupancy && A.uniform) {
+    if (A.trial_iter && A.occupancy == 2 && A.uniform) {
+      launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 2, true, true>, grid, block, 0, st, A, so, clk, k0, M);
+      done = true;
+    } else if (A.trial_iter && A.occupancy && A.uniform) {
       launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 1, true, true>, grid, block, 0, st, A, so, clk, k0, M);
       done = true;
     } else if (A.trial_iter && A.uniform) {

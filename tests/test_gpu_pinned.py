@@ -44,11 +44,12 @@ def oracle_segments(conn, dt, skip_sources):
     return src, step, conn["target"][keep], conn["port"][keep], conn["weight"][keep]
 
 
-@pytest.mark.parametrize("tpi,pf", [(0, 0), (1, 1)])
-def test_benchmark_network_slice_matches_oracle(tpi, pf):
+@pytest.mark.parametrize("tpi,pf,occ", [(0, 0, 0), (1, 1, 1), (1, 0, 2)])
+def test_benchmark_network_slice_matches_oracle(tpi, pf, occ):
     seed = 20240
     ngpu.SetUpdateTrialIter(tpi)
     ngpu.SetDeliverPrefetch(pf)
+    ngpu.SetUpdateOccupancy(occ)
     ngpu.SetRk5Budget(1)
     neuron, pg = benchmark_network(ngpu, 0.01, seed)
     ngpu.Calibrate()
