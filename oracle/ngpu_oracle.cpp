@@ -243,6 +243,7 @@ static const char *pg_par_name[PG_NPAR] = {"rate", "origin", "start", "stop"};
 struct Group {
   Model model;
   int i0 = 0, n = 0, nport = 0;
+  int lo = 0, hi = -1;                      // neurons simulated by this process (hi < 0: all)
   // aeif: scalar vars V_m,w ; port vars ; scalar params ; port params
   // iaf : vars (4) ; params (16)
   // poiss_gen: params (4)
@@ -437,6 +438,15 @@ struct Net {
   struct Direct { int gen; int tgt; unsigned char port; float w; float delay; int group; uint64_t key; };
   std::vector<Direct> direct;
   std::map<int, uint32_t> pg_stream;              // poiss_gen node -> stream (set explicitly)
+  // partitioned network: this process simulates its share of every group; after the update
+  // phase of each step xch_fn exchanges the step's spikes (orc_step_spikes / orc_inject_spikes)
+  int part_rank = 0, part_world = 1;
+  struct StepSpike { int node; float height; };
+  std::vector<StepSpike> step_spikes;
+  bool injecting = false;
+  int (*xch_fn)(void *) = nullptr;
+  void *xch_user = nullptr;
+  long long cur_tidx = 0;
   std::vector<Rec> recs;
   std::vector<std::vector<float>> rec_rows;
   long long n_derivs = 0;
@@ -806,6 +816,15 @@ struct Net {
   void calibrate() {
     if (calibrated) throw std::runtime_error("Calibration can be made only once");
     calibrated = true;
+    for (auto &g : groups) {
+      if (part_world > 1) {
+        g.lo = (int)((long long)g.n * part_rank / part_world);
+        g.hi = (int)((long long)g.n * (part_rank + 1) / part_world);
+      } else {
+        g.lo = 0;
+        g.hi = -1;
+      }
+    }
     neural_time = 0.0;
     queue.assign(node_group.size(), {});
     // direct edges: poiss_gen sources, source-major, delay groups ascending, insertion order
@@ -1186,6 +1205,10 @@ struct Net {
   void push_spike(int node, float height, long long tidx) {
     Group &g = group_of(node);
     int i = node - g.i0;
+    if (part_world > 1 && !injecting) {
+#pragma omp critical(step_spikes)
+      step_spikes.push_back({node, height});
+    }
 #pragma omp atomic
     n_spikes_total++;
     if (g.spike_count_on) g.spike_count[i]++;
@@ -1215,8 +1238,9 @@ struct Net {
     R hmin = (R)(g.h_min_rel * dt);
     if (fp64) hmin = (R)((double)g.h_min_rel * (double)dt);
     long long nd_total = 0;
+    const int i_lo = g.lo, i_hi = g.hi < 0 ? g.n : g.hi;
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : nd_total)
-    for (int i = 0; i < g.n; i++) {
+    for (int i = i_lo; i < i_hi; i++) {
       Par<R> q;
       auto gp = [&](int j) { return (R)g.par[j][i]; };
       q.V_th = gp(A_V_th); q.Delta_T = gp(A_Delta_T); q.g_L = gp(A_g_L); q.E_L = gp(A_E_L);
@@ -1270,8 +1294,9 @@ struct Net {
   }
 
   template <class R> void update_iaf(Group &g, long long tidx) {
+    const int i_lo = g.lo, i_hi = g.hi < 0 ? g.n : g.hi;
 #pragma omp parallel for schedule(static)
-    for (int i = 0; i < g.n; i++) {
+    for (int i = i_lo; i < i_hi; i++) {
       R Iex = (R)g.var[I_I_syn_ex][i], Iin = (R)g.var[I_I_syn_in][i];
       R V = (R)g.var[I_V_m_rel][i], refr = (R)g.var[I_refractory_step][i];
       auto gp = [&](int j) { return (R)g.par[j][i]; };
@@ -1357,6 +1382,7 @@ struct Net {
     // 2. time
     neural_time = neur_t0 + (double)dt * (double)(it + 1);
     long long tidx = (long long)(int)std::round(neur_t0 / (double)dt) + it + 1;
+    cur_tidx = tidx;
     // 2b. keep the 16-bit arrival stamps of plastic edges unambiguous
     //     (src/nestgpu.cu:490-498, src/rev_spike.cu:93-118)
     if (any_plastic && ((tidx & 0xffff) == 0x8000 || (tidx & 0xffff) == 0)) {
@@ -1379,7 +1405,7 @@ struct Net {
         else update_iaf<float>(g, tidx);
       } else if (g.model == PARROT) {
         // src/parrot_neuron.cu:60-82
-        for (int i = 0; i < g.n; i++) {
+        for (int i = g.lo; i < (g.hi < 0 ? g.n : g.hi); i++) {
           const float sh = (float)g.var[PR_input_spike_height][i];
           g.var[PR_V][i] = sh;
           if (sh != 0.0f) {
@@ -1390,7 +1416,7 @@ struct Net {
         }
       } else if (g.model == SPIKE_DET) {
         // src/spike_detector.cu:28-50
-        for (int i = 0; i < g.n; i++) {
+        for (int i = g.lo; i < (g.hi < 0 ? g.n : g.hi); i++) {
           float sh = (float)g.var[SD_input_spike_height][i];
           if (sh != 0.0f) {
             if (g.par[SD_hold_spike_height][i] == 0.0) sh = 1.0f;
@@ -1399,7 +1425,7 @@ struct Net {
           g.var[SD_spike_height][i] = sh;
         }
       } else if (g.model == SPIKE_GEN) {
-        for (int i = 0; i < g.n; i++) {
+        for (int i = g.lo; i < (g.hi < 0 ? g.n : g.hi); i++) {
           int k = g.sg_next[i];
           if (k < (int)g.sg_tidx[i].size() && g.sg_tidx[i][k] == (int)it) {
             push_spike(g.i0 + i, g.sg_height[i][k], tidx);
@@ -1407,6 +1433,13 @@ struct Net {
           }
         }
       }
+    }
+    // partitioned network: the spikes this process's neurons emitted in the step go to the
+    // other processes, theirs come back and enter the per-source queues at this step, as if
+    // emitted here (the exchange the engine makes once per time batch)
+    if (part_world > 1) {
+      if (!xch_fn || xch_fn(xch_user) != 0) throw std::runtime_error("the spike exchange failed");
+      step_spikes.clear();
     }
     // 4. records
     write_records((float)neural_time);
@@ -1663,6 +1696,42 @@ int orc_get_syn_param(void *p, int g, const char *name, float *v) {
   OR_TRY Net *n = (Net *)p; *v = n->syn_groups[g - 1].par[syn_par_idx(n, g, name)]; return 0; OR_CATCH(-1)
 }
 
+// ---- partitioned network (the engine's process partition, restated step by step)
+int orc_set_partition(void *p, int rank, int world) {
+  OR_TRY
+  Net *n = (Net *)p;
+  if (world < 1 || rank < 0 || rank >= world) throw std::runtime_error("partition rank out of range");
+  n->part_rank = rank;
+  n->part_world = world;
+  return 0;
+  OR_CATCH(-1)
+}
+int orc_set_exchange(void *p, int (*fn)(void *), void *user) {
+  ((Net *)p)->xch_fn = fn;
+  ((Net *)p)->xch_user = user;
+  return 0;
+}
+// the spikes this process's neurons emitted in the current step (nodes / heights may be null
+// to ask for the count)
+int orc_step_spikes(void *p, int *nodes, float *heights) {
+  Net *n = (Net *)p;
+  if (nodes)
+    for (size_t j = 0; j < n->step_spikes.size(); j++) {
+      nodes[j] = n->step_spikes[j].node;
+      heights[j] = n->step_spikes[j].height;
+    }
+  return (int)n->step_spikes.size();
+}
+// the other processes' spikes of the current step, filed as if emitted here
+int orc_inject_spikes(void *p, const int *nodes, const float *heights, int count) {
+  OR_TRY
+  Net *n = (Net *)p;
+  n->injecting = true;
+  for (int j = 0; j < count; j++) n->push_spike(nodes[j], heights[j], n->cur_tidx);
+  n->injecting = false;
+  return 0;
+  OR_CATCH(-1)
+}
 int orc_connect_generated(void *p, int src0, int ns, int tgt0, int nt, int k, int port, float w,
                           float dmin_ms, float dmax_ms, unsigned long long seed) {
   OR_TRY ((Net *)p)->connect_generated(src0, ns, tgt0, nt, k, port, w, dmin_ms, dmax_ms, seed); return 0;

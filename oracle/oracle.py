@@ -71,6 +71,10 @@ def lib():
             "orc_connect_generated": (c_int, [c_void, c_int, c_int, c_int, c_int, c_int, c_int, c_float,
                                               c_float, c_float, c_ull]),
             "orc_set_poisson_stream": (c_int, [c_void, c_int, c_int, ctypes.c_uint]),
+            "orc_set_partition": (c_int, [c_void, c_int, c_int]),
+            "orc_set_exchange": (c_int, [c_void, c_void, c_void]),
+            "orc_step_spikes": (c_int, [c_void, ip, fp]),
+            "orc_inject_spikes": (c_int, [c_void, ip, fp, c_int]),
             "orc_threads": (c_int, []),
             "orc_get_conns": (c_int, [c_void, ip, ip, ip, ip, ip, ip, fp, fp]),
             "orc_record": (c_int, [c_void, c_int, ctypes.c_char_p, c_int]),
@@ -414,6 +418,34 @@ class Oracle(object):
         if not hasattr(nodes, "i0"):
             nodes = NodeSeq(nodes[0], len(nodes))
         self._chk(self.L.orc_set_poisson_stream(self.h, nodes.i0, nodes.n, int(stream) & 0xffffffff))
+
+    # -- partitioned network: this process simulates its share of every group; exchange(self)
+    #    is called after the update phase of every step and must pass the step's spikes
+    #    (StepSpikes) to the other processes and inject theirs (InjectSpikes)
+    def SetPartition(self, rank, world, exchange):
+        self._chk(self.L.orc_set_partition(self.h, rank, world))
+        fn = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
+
+        def cb(user):
+            try:
+                exchange(self)
+                return 0
+            except Exception:
+                return 1
+        self._xch = fn(cb)
+        self.L.orc_set_exchange(self.h, ctypes.cast(self._xch, ctypes.c_void_p), None)
+
+    def StepSpikes(self):
+        n = self.L.orc_step_spikes(self.h, None, None)
+        nodes = np.zeros(max(n, 1), dtype=np.int32)
+        heights = np.zeros(max(n, 1), dtype=np.float32)
+        self.L.orc_step_spikes(self.h, _iptr(nodes), _fptr(heights))
+        return nodes[:n], heights[:n]
+
+    def InjectSpikes(self, nodes, heights):
+        nodes = np.ascontiguousarray(nodes, dtype=np.int32)
+        heights = np.ascontiguousarray(heights, dtype=np.float32)
+        self._chk(self.L.orc_inject_spikes(self.h, _iptr(nodes), _fptr(heights), nodes.size))
 
     def Threads(self):
         return self.L.orc_threads()
