@@ -340,10 +340,9 @@ int NGPU_GetBatchLength(void);
 /* Threads per block of the aeif update kernel (64, 128 or 256; default 128). */
 int NGPU_SetUpdateThreads(int n);
 /* 1: use the register-capped variant of the aeif update kernel (three 256-thread blocks per
-   SM, more warps in flight, a few register spills); 2 and 3: with the trial-per-iteration
-   update and uniform parameters, variants capped at five (96 registers) and four (120
-   registers, no spills) 128-thread blocks per SM, blocks of at most 128 threads; 0: the
-   unconstrained one (default). */
+   SM, more warps in flight, a few register spills); 2: with the trial-per-iteration update
+   and uniform parameters, a variant capped at five 128-thread blocks per SM (96 registers,
+   blocks of at most 128 threads); 0: the unconstrained one (default). */
 int NGPU_SetUpdateOccupancy(int on);
 /* 1: the aeif update kernel advances one RK5 trial per loop iteration (a rejected trial is
    retried in the next iteration beside the neighbouring lanes' next trials); 0: one whole

@@ -793,8 +793,10 @@ __device__ __forceinline__ bool aeif_tpi_iter(const AeifArgs &A, const SpikeOut 
 // OCC = 1 caps the registers so that three 256-thread blocks fit on an SM (more warps
 // in flight to hide the dependent FP32 latency, at the price of a few spills); OCC = 2
 // (trial-per-iteration form, blocks of at most 128 threads) caps them at five 128-thread
-// blocks per SM (96 registers: 20 warps, fewer spills); OCC = 3 at four 128-thread blocks
-// per SM (128 registers, 16 warps).
+// blocks per SM (96 registers: 20 warps, fewer spills).  Measured on the 1M network (RTF,
+// 64-thread blocks): OCC = 0 (145 registers, 14 warps) 0.776, OCC = 1 (80, 24 warps, 204 B of
+// spills) 0.683, OCC = 2 (96, 20 warps, 80 B) 0.649, and a 120-register cap without spills
+// (16 warps) 0.661.
 // TPI = true (plain controller only): one RK5 trial per loop iteration.  A lane whose
 // trial is rejected retries in the next iteration, beside its neighbours' next trials,
 // instead of holding its whole warp in a second trial (with ~4% of the trials rejected,
@@ -803,8 +805,7 @@ __device__ __forceinline__ bool aeif_tpi_iter(const AeifArgs &A, const SpikeOut 
 // only between accepted steps, so every lane runs the same sequence of operations as
 // in the step-at-once form and results are identical.
 template <int MODEL, int PMAX, bool FIXED, int LM, int OCC = 0, bool UNI = false, bool TPI = false>
-__global__ void __launch_bounds__(OCC == 2 || OCC == 3 ? 128 : 256,
-                                  OCC == 1 ? 3 : (OCC == 2 ? 5 : (OCC == 3 ? 4 : 1)))
+__global__ void __launch_bounds__(OCC == 2 ? 128 : 256, OCC == 1 ? 3 : (OCC == 2 ? 5 : 1))
     aeif_batch_kernel(const AeifArgs A, const SpikeOut so,
                                                          const Clock *clk, int k0, int M) {
   pdl_enter();
@@ -940,14 +941,10 @@ template <int MODEL, int PMAX, bool FIXED, int LM>
 int launch_aeif_p(const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
   int tb = (A.threads == 64 || A.threads == 256) ? A.threads : 128;
   if (A.occupancy == 2 && tb > 128) tb = 128;   // the OCC = 2 variant is bounded to 128 threads
-  if (A.occupancy == 3 && tb > 128) tb = 128;   // so is the OCC = 3 variant
   dim3 grid((A.hi - A.lo + tb - 1) / tb), block(tb);
   bool done = false;
   if constexpr (LM == LM_PLAIN && FIXED) {
-    if (A.trial_iter && A.occupancy == 3 && A.uniform) {
-      launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 3, true, true>, grid, block, 0, st, A, so, clk, k0, M);
-      done = true;
-    } else if (A.trial_iter && A.occupancy == 2 && A.uniform) {
+    if (A.trial_iter && A.occupancy == 2 && A.uniform) {
       launch_k(aeif_batch_kernel<MODEL, PMAX, FIXED, LM, 2, true, true>, grid, block, 0, st, A, so, clk, k0, M);
       done = true;
     } else if (A.trial_iter && A.occupancy && A.uniform) {

@@ -786,7 +786,7 @@ int NGPU_SetDeliverGroup(int g) {
 
 int NGPU_SetUpdateOccupancy(int on) {
   return guard([&] {
-    E().update_occupancy = on < 0 ? 0 : (on > 3 ? 3 : on);
+    E().update_occupancy = on < 0 ? 0 : (on > 2 ? 2 : on);
     E().invalidate_graphs();
     return 0;
   }, -1);

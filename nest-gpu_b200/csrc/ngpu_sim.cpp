@@ -1482,7 +1482,7 @@ int Engine::autotune(int steps, std::vector<std::pair<std::string, double>> *log
     for (int b : blocks) deliver.cand.push_back({g, b});
   std::vector<Knob> knobs = {
       single("update_threads", &update_threads, {64, 128, 256}),
-      single("update_occupancy", &update_occupancy, {0, 1, 2, 3}),
+      single("update_occupancy", &update_occupancy, {0, 1, 2}),
       single("update_trial_iter", &update_trial_iter, {0, 1}),
       single("deliver_aggregate", &deliver_aggregate, {0, 1}),
       single("deliver_prefetch", &deliver_prefetch, {0, 1}),

@@ -1463,7 +1463,8 @@ def GetBatchLength():
 
 def SetUpdateOccupancy(on=True):
     """Register-capped variant of the aeif update kernel (engine extension): 1 (or True) three
-    256-thread blocks per SM, 2 five 128-thread blocks (trial-per-iteration update), 0 none."""
+    256-thread blocks per SM, 2 five 128-thread blocks (trial-per-iteration update, uniform
+    parameters), 0 none."""
     _need_b200("SetUpdateOccupancy")
     v = int(on) if not isinstance(on, bool) else (1 if on else 0)
     return _check(_c["NGPU_SetUpdateOccupancy"](v))

@@ -273,8 +273,7 @@ def test_profile_and_launch_counters():
 @pytest.mark.parametrize("threads,group,occ,tpi,agg,pf", [(64, 8, 0, 0, 0, 0), (256, 16, 1, 0, 0, 1),
                                                           (128, 32, 1, 0, 0, 0), (64, 8, 0, 1, 0, 1),
                                                           (128, 32, 1, 1, 1, 1), (64, 32, 0, 0, 1, 0),
-                                                          (128, 32, 2, 1, 0, 0), (256, 16, 2, 1, 0, 1),
-                                                          (64, 32, 3, 1, 0, 1)])
+                                                          (128, 32, 2, 1, 0, 0), (256, 16, 2, 1, 0, 1)])
 def test_launch_mappings_keep_results(threads, group, occ, tpi, agg, pf):
     """The update block size and kernel variants (register cap, one RK5 trial per loop
     iteration), the delivery lane group, warp-aggregated and pipelined delivery change only the
