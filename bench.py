@@ -67,9 +67,9 @@ def parse():
     p.add_argument("--no-autotune", action="store_true", help="keep the default launch mappings")
     p.add_argument("--mapping", default="",
                    help="fixed launch mapping instead of the autotuner: update threads, register-capped "
-                        "variant (0/1), delivery lane group, delivery blocks, RK5 budget and optionally "
+                        "variant (0/1/2), delivery lane group, delivery blocks, RK5 budget and optionally "
                         "programmatic launch (0/1), one RK5 trial per iteration (0/1), warp-aggregated "
-                        "delivery (0/1) and pipelined delivery (0/1), e.g. 64,1,32,592,1")
+                        "delivery (0/1) and pipelined delivery (0/1), e.g. 64,2,32,592,1")
     p.add_argument("--batch-max", type=int, default=0, help="upper bound of the time-batch length")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the learned-step and ensemble measurements")
