@@ -440,7 +440,8 @@ int NGPU_StepModelEnable(int on);
    reference. */
 int NGPU_StepBoundMode(int on);
 /* Network output for n feature rows, and the mean squared error with its gradient over the
-   trainable block W1..b3 (1441 floats), computed by the GPU kernels on host buffers. */
+   trainable block W1..b3 (1441 floats), computed by the GPU kernels on host buffers (the
+   gradient by the training kernel: tensor-core products of BF16 operands, FP32 sums). */
 int NGPU_MlpForward(const float *params, const float *feat, int n, float *out);
 int NGPU_MlpGrad(const float *params, const float *feat, const float *target, int n, float *grad,
                  float *loss);

@@ -2,12 +2,12 @@
 // kernels and the MLP kernels that train the proposal network on the GPU.
 //
 // Training (per iteration, minibatch of B sampled tuples):
-//   mlp_grad_kernel    one 128-sample tile per block: each thread runs the forward
-//                      and backward pass of one sample with the BF16 weights,
-//                      keeping inputs, activations and back-propagated errors in
-//                      shared memory; the block then forms its weight gradients as
-//                      sums over the tile's samples (dW = sum_s delta_s a_s^T), FP32,
-//                      in a fixed order, and writes one partial gradient row;
+//   mlp_grad_kernel    one 128-sample tile per block: the layer products, the
+//                      back-propagated error product and one product for all weight
+//                      and bias gradients (dW = sum_s delta_s a_s^T) on the tensor
+//                      cores (tcgen05, BF16 operands, FP32 accumulators in tensor
+//                      memory); one thread per sample for the elementwise work; one
+//                      partial gradient row per block;
 //   reduce_kernel      sums the partial rows in block order (deterministic);
 //   adam_kernel        Adam update of the FP32 master weights; the weights the
 //                      network runs with are their BF16 roundings.
@@ -173,12 +173,135 @@ __global__ void mlp_forward_kernel(const float *model, const float *feat, int n,
 }
 
 // ---------------------------------------------------------------------------
-// gradient of the mean squared error over one tile of samples per block
+// gradient of the mean squared error over one tile of 128 samples per block, on the
+// tensor cores: tcgen05.mma with BF16 operands in shared memory and FP32 accumulators in
+// tensor memory (TMEM), issued by one thread; the elementwise work between the products
+// (biases, ReLU, the output layer, the loss) runs on the CUDA cores, one thread per sample.
+//
+//   Z1 = X . W1^T       X [128 x 16] . W1^T            -> TMEM columns   0..31
+//   Z2 = A1 . W2^T      A1 [128 x 32] . W2^T           -> TMEM columns  32..63
+//   G1 = D2 . W2        D2 [128 x 32] . (W2^T)^T       -> TMEM columns  64..95
+//   one product for every weight and bias gradient (K = the 128 samples):
+//     GA [128 x 128] = rows D2^T (0..31), D1^T (32..63), d^T (64), zeros
+//     GB [ 96 x 128] = rows A1^T (0..31), A2^T (32..63), X^T (64..73), ones (80), zeros
+//     GA . GB^T -> TMEM columns 96..191: dW2 = rows 0..31 x cols 0..31, dW1 = rows 32..63 x
+//     cols 64..73, dW3 = row 64 x cols 32..63, and the bias gradients in col 80.
+// Operand precision: the inputs, activations and back-propagated errors enter the products
+// as BF16 roundings (the weights are BF16 values already); sums are FP32.
 // ---------------------------------------------------------------------------
-constexpr int GT = 128;                  // samples per tile = threads per block
-constexpr int RS = SM_NH + 1;            // padded row stride of the activation tiles
+constexpr int GT = 128;                  // samples per tile = threads per block = MMA M
 constexpr int PART_W = SM_NTRAIN + 1;    // partial row: gradients, then the loss sum
-constexpr size_t GRAD_SMEM = sizeof(float) * ((size_t)SM_NPAR + GT * SM_NF + 4 * GT * RS + GT);
+
+// Byte offset of element (r, k) of a BF16 operand tile with K columns, in the K-major
+// no-swizzle layout of the tensor core's shared-memory descriptors: 8-row x 16-byte core
+// matrices, the K-chunks of an 8-row group adjacent (128 B apart: the descriptor's leading
+// byte offset), the 8-row groups K/8 x 128 B apart (its stride byte offset).
+__host__ __device__ constexpr int tile_off(int r, int k, int K) {
+  return (r >> 3) * (K / 8) * 128 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+constexpr int TC_X = 0;                          // [128 x 16]
+constexpr int TC_W1 = TC_X + 128 * 16 * 2;       // [ 32 x 16]  W1[j][k]
+constexpr int TC_A1 = TC_W1 + 32 * 16 * 2;       // [128 x 32]
+constexpr int TC_W2 = TC_A1 + 128 * 32 * 2;      // [ 32 x 32]  W2[j][k]
+constexpr int TC_D2 = TC_W2 + 32 * 32 * 2;       // [128 x 32]
+constexpr int TC_W2T = TC_D2 + 128 * 32 * 2;     // [ 32 x 32]  W2[k][j] at (j, k)
+constexpr int TC_GA = TC_W2T + 32 * 32 * 2;      // [128 x 128]
+constexpr int TC_GB = TC_GA + 128 * 128 * 2;     // [ 96 x 128]
+constexpr int TC_M = TC_GB + 96 * 128 * 2;       // model parameters (floats)
+// (the 8 KB tail keeps every address a descriptor can form from these tiles inside the
+// block's shared memory)
+constexpr size_t GRAD_SMEM = TC_M + sizeof(float) * SM_NPAR + 8192;
+constexpr int TC_COLS = 256;                     // TMEM columns allocated (192 used)
+constexpr long long TC_WAIT_POLLS = 1LL << 22;   // bound of each wait for the tensor core
+
+// Shared-memory matrix descriptor of a K-major no-swizzle tile with K columns whose first
+// K-chunk starts at shared address `addr`: start >> 4 (bits 0-13), leading byte offset
+// 128 >> 4 (bits 16-29), stride byte offset (K/8 * 128) >> 4 (bits 32-45), descriptor
+// version 1 (bits 46-47), base offset 0, layout "no swizzle" (bits 61-63 = 0).
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr, int K) {
+  return (uint64_t)((addr >> 4) & 0x3fffu) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)(((K / 8) * 128) >> 4) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), BF16 A and B
+// (bits 7-9 and 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 (bits 17-22), M >> 4
+// (bits 24-28).
+__host__ __device__ constexpr uint32_t tc_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// D[128 x N] (+)= A[128 x K] . B[N x K]^T, K/16 instructions; issued by one thread.
+__device__ __forceinline__ void tc_gemm(uint32_t d_tmem, uint32_t a, uint32_t b, int K, uint32_t idesc) {
+  for (int s = 0; s < K / 16; s++) {
+    const uint64_t ad = tc_desc(a + 256u * s, K), bd = tc_desc(b + 256u * s, K);
+    const uint32_t acc = s > 0 ? 1u : 0u;
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                 ::"r"(d_tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc) : "memory");
+  }
+}
+// The barrier's phase completes when the MMAs this thread issued before are done.
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+// Waits for phase `parity` of the barrier, at most TC_WAIT_POLLS polls; false if it gave up.
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
+  for (long long i = 0; i < TC_WAIT_POLLS; i++) {
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}\n"
+                 : "=r"(done) : "r"(mbar), "r"(parity) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+// Generic-proxy shared-memory writes made visible to the tensor core (async proxy).
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 32 consecutive TMEM columns of this thread's lane (warp w reads lanes 32w .. 32w+31).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+  uint32_t r[32];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]) : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]) : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t bf16_bits(float v) {
+  bool sp;
+  return __float_as_uint(bf16_round_bits(__float_as_uint(v), sp)) >> 16;
+}
+// Row t of a K-major tile from K floats (rounded to BF16), one 16-byte store per 8 values.
+template <int K>
+__device__ __forceinline__ void put_row(unsigned char *tile, int t, const float *v) {
+#pragma unroll
+  for (int c = 0; c < K / 8; c++) {
+    uint4 q;
+    q.x = bf16_bits(v[8 * c + 0]) | (bf16_bits(v[8 * c + 1]) << 16);
+    q.y = bf16_bits(v[8 * c + 2]) | (bf16_bits(v[8 * c + 3]) << 16);
+    q.z = bf16_bits(v[8 * c + 4]) | (bf16_bits(v[8 * c + 5]) << 16);
+    q.w = bf16_bits(v[8 * c + 6]) | (bf16_bits(v[8 * c + 7]) << 16);
+    *reinterpret_cast<uint4 *>(tile + tile_off(t, 8 * c, K)) = q;
+  }
+}
+// Column t (a sample) of rows r0 .. r0+n-1 of a tile with K = 128 columns.
+__device__ __forceinline__ void put_col(unsigned char *tile, int r0, int n, int t, const float *v) {
+  for (int i = 0; i < n; i++)
+    *reinterpret_cast<unsigned short *>(tile + tile_off(r0 + i, t, GT)) = (unsigned short)bf16_bits(v[i]);
+}
 
 __device__ __forceinline__ uint32_t sample_index(uint64_t seed, long long iter, int s, uint32_t n) {
   U4 c{(uint32_t)s, (uint32_t)iter, (uint32_t)((unsigned long long)iter >> 32), 0x51ed2701u};
@@ -187,108 +310,187 @@ __device__ __forceinline__ uint32_t sample_index(uint64_t seed, long long iter, 
 }
 
 // Samples: tile blockIdx.x covers batch positions [GT*blockIdx.x, GT*blockIdx.x+GT) of B;
-// position s uses sample sample_index(seed, iter, s) if sampled, else sample s.
+// position s uses sample sample_index(seed, iter, s) if sampled, else sample s.  Positions
+// past B contribute nothing (their output error is zero).  A wait for the tensor core that
+// gives up sets bit 0 of *status and the block ends after releasing its TMEM.
 __global__ void __launch_bounds__(GT) mlp_grad_kernel(const float *model, const float *feat, const float *target,
                                                       uint32_t n, int B, int sampled, uint64_t seed,
-                                                      const long long *iter_ptr, float *partial) {
-  extern __shared__ float sm[];
-  float *M = sm;                                 // SM_NPAR
-  float *X = M + SM_NPAR;                        // [GT][NF] normalised inputs
-  float *A1 = X + GT * SM_NF;                    // [GT][RS] layer-1 activations
-  float *A2 = A1 + GT * RS;                      // [GT][RS] layer-2 activations
-  float *D1 = A2 + GT * RS;                      // [GT][RS] layer-1 deltas
-  float *D2 = D1 + GT * RS;                      // [GT][RS] layer-2 deltas
-  float *DO = D2 + GT * RS;                      // [GT] output deltas
-  for (int j = threadIdx.x; j < SM_NPAR; j += blockDim.x) M[j] = model[j];
+                                                      const long long *iter_ptr, float *partial,
+                                                      unsigned *status) {
+  extern __shared__ __align__(128) unsigned char tc_sm[];
+  __shared__ __align__(8) unsigned long long s_bar;
+  __shared__ uint32_t s_taddr;
+  __shared__ int s_fail;
+  __shared__ float lred[GT];
+  float *M = reinterpret_cast<float *>(tc_sm + TC_M);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const uint32_t bar = smem_u32(&s_bar);
+  // zero the gradient operands (their padding rows stay zero), load the model
+  {
+    uint4 *z = reinterpret_cast<uint4 *>(tc_sm + TC_GA);
+    const int nz = (TC_M - TC_GA) / 16;
+    for (int i = t; i < nz; i += GT) z[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  for (int j = t; j < SM_NPAR; j += GT) M[j] = model[j];
+  if (t == 0) {
+    s_fail = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_taddr)),
+                 "r"(TC_COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
   __syncthreads();
-  const int t = threadIdx.x;
+  tc_fence_after();
+  const uint32_t tm = s_taddr;
+  const uint32_t my_lanes = tm + ((uint32_t)(warp * 32) << 16);
+  unsigned char *S = tc_sm;
+  // weight operands
+  for (int e = t; e < 32 * 16; e += GT) {
+    const int j = e / 16, k = e % 16;
+    const float w = k < SM_NF ? M[SM_W1 + j * SM_NF + k] : 0.0f;
+    *reinterpret_cast<unsigned short *>(S + TC_W1 + tile_off(j, k, 16)) = (unsigned short)bf16_bits(w);
+  }
+  for (int e = t; e < 32 * 32; e += GT) {
+    const int j = e / 32, k = e % 32;
+    const unsigned short w = (unsigned short)bf16_bits(M[SM_W2 + j * SM_NH + k]);
+    *reinterpret_cast<unsigned short *>(S + TC_W2 + tile_off(j, k, 32)) = w;
+    *reinterpret_cast<unsigned short *>(S + TC_W2T + tile_off(k, j, 32)) = w;
+  }
+  __syncthreads();
+  // layer 1 input
   const int s = blockIdx.x * GT + t;
+  const bool valid = s < B;
   const long long iter = iter_ptr ? *iter_ptr : 0;
-  float loss = 0.0f;
-  if (s < B) {
-    const uint32_t idx = sampled ? sample_index(seed, iter, s, n) : (uint32_t)s;
-    float xn[SM_NF];
+  uint32_t idx = 0;
+  float xn[16];
+#pragma unroll
+  for (int k = 0; k < 16; k++) xn[k] = 0.0f;
+  if (valid) {
+    idx = sampled ? sample_index(seed, iter, s, n) : (uint32_t)s;
 #pragma unroll
     for (int k = 0; k < SM_NF; k++) {
       const float v = __fmul_rn(__fsub_rn(feat[(size_t)idx * SM_NF + k], M[SM_MU + k]), M[SM_ISIG + k]);
       xn[k] = fminf(fmaxf(v, -SM_XCLAMP), SM_XCLAMP);
-      X[t * SM_NF + k] = xn[k];
     }
-    float a1[SM_NH];
-#pragma unroll
-    for (int j = 0; j < SM_NH; j++) {
-      float z = M[SM_B1 + j];
-#pragma unroll
-      for (int k = 0; k < SM_NF; k++) z = __fmaf_rn(M[SM_W1 + j * SM_NF + k], xn[k], z);
-      a1[j] = (z > 0.0f) ? z : 0.0f;
-      A1[t * RS + j] = a1[j];
-    }
-    float out = M[SM_B3];
-    for (int j = 0; j < SM_NH; j++) {
-      float z = M[SM_B2 + j];
-#pragma unroll
-      for (int k = 0; k < SM_NH; k++) z = __fmaf_rn(M[SM_W2 + j * SM_NH + k], a1[k], z);
-      z = (z > 0.0f) ? z : 0.0f;
-      A2[t * RS + j] = z;
-      out = __fmaf_rn(M[SM_W3 + j], z, out);
-    }
-    const float tn = __fdiv_rn(__fsub_rn(target[idx], M[SM_LMU]), M[SM_LSIG]);
-    const float r = __fsub_rn(out, tn);
-    loss = __fmul_rn(r, r);
-    const float d = __fdiv_rn(__fmul_rn(2.0f, r), (float)B);
-    DO[t] = d;
-    float d2[SM_NH];
-#pragma unroll
-    for (int j = 0; j < SM_NH; j++) {
-      d2[j] = (A2[t * RS + j] > 0.0f) ? __fmul_rn(d, M[SM_W3 + j]) : 0.0f;
-      D2[t * RS + j] = d2[j];
-    }
-    for (int k = 0; k < SM_NH; k++) {
-      float g = 0.0f;
-#pragma unroll
-      for (int j = 0; j < SM_NH; j++) g = __fmaf_rn(M[SM_W2 + j * SM_NH + k], d2[j], g);
-      D1[t * RS + k] = (a1[k] > 0.0f) ? g : 0.0f;
-    }
-  } else {
-    for (int k = 0; k < SM_NF; k++) X[t * SM_NF + k] = 0.0f;
-    for (int j = 0; j < SM_NH; j++) A1[t * RS + j] = A2[t * RS + j] = D1[t * RS + j] = D2[t * RS + j] = 0.0f;
-    DO[t] = 0.0f;
   }
-  __syncthreads();
-  // weight gradients: sums over the tile's samples in sample order
-  float *out_row = partial + (size_t)blockIdx.x * PART_W;
-  for (int o = t; o < SM_NTRAIN; o += GT) {
-    const int j = SM_TRAIN0 + o;
-    float g = 0.0f;
-    if (j < SM_B1) {                      // W1[r][c]
-      const int r = (j - SM_W1) / SM_NF, c = (j - SM_W1) % SM_NF;
-      for (int q = 0; q < GT; q++) g = __fmaf_rn(D1[q * RS + r], X[q * SM_NF + c], g);
-    } else if (j < SM_W2) {               // b1[r]
-      const int r = j - SM_B1;
-      for (int q = 0; q < GT; q++) g = __fadd_rn(g, D1[q * RS + r]);
-    } else if (j < SM_B2) {               // W2[r][c]
-      const int r = (j - SM_W2) / SM_NH, c = (j - SM_W2) % SM_NH;
-      for (int q = 0; q < GT; q++) g = __fmaf_rn(D2[q * RS + r], A1[q * RS + c], g);
-    } else if (j < SM_W3) {               // b2[r]
-      const int r = j - SM_B2;
-      for (int q = 0; q < GT; q++) g = __fadd_rn(g, D2[q * RS + r]);
-    } else if (j < SM_B3) {               // W3[c]
-      const int c = j - SM_W3;
-      for (int q = 0; q < GT; q++) g = __fmaf_rn(DO[q], A2[q * RS + c], g);
-    } else {                              // b3
-      for (int q = 0; q < GT; q++) g = __fadd_rn(g, DO[q]);
+  put_row<16>(S + TC_X, t, xn);
+  put_col(S + TC_GB, 64, SM_NF, t, xn);
+  {
+    const float one = 1.0f;
+    put_col(S + TC_GB, 80, 1, t, &one);
+  }
+  float loss = 0.0f;
+  uint32_t phase = 0;
+  // the four products, each followed by its epilogue
+  float a1[SM_NH], z[32];
+  for (int stage = 0; stage < 4; stage++) {
+    proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc_fence_after();
+      if (stage == 0) tc_gemm(tm + 0, smem_u32(S + TC_X), smem_u32(S + TC_W1), 16, tc_idesc(128, 32));
+      else if (stage == 1) tc_gemm(tm + 32, smem_u32(S + TC_A1), smem_u32(S + TC_W2), 32, tc_idesc(128, 32));
+      else if (stage == 2) tc_gemm(tm + 64, smem_u32(S + TC_D2), smem_u32(S + TC_W2T), 32, tc_idesc(128, 32));
+      else tc_gemm(tm + 96, smem_u32(S + TC_GA), smem_u32(S + TC_GB), GT, tc_idesc(128, 96));
+      tc_commit(bar);
     }
-    out_row[o] = g;
+    const bool ok = tc_wait(bar, phase);
+    phase ^= 1u;
+    if (!ok) s_fail = 1;
+    __syncthreads();
+    if (s_fail) break;
+    tc_fence_after();
+    if (stage == 0) {
+      tmem_ld32(my_lanes + 0, z);
+#pragma unroll
+      for (int j = 0; j < SM_NH; j++) {
+        const float v = __fadd_rn(z[j], M[SM_B1 + j]);
+        a1[j] = (valid && v > 0.0f) ? v : 0.0f;
+      }
+      put_row<32>(S + TC_A1, t, a1);
+      put_col(S + TC_GB, 0, SM_NH, t, a1);
+    } else if (stage == 1) {
+      tmem_ld32(my_lanes + 32, z);
+      float a2[SM_NH];
+      float out = M[SM_B3];
+#pragma unroll
+      for (int j = 0; j < SM_NH; j++) {
+        const float v = __fadd_rn(z[j], M[SM_B2 + j]);
+        a2[j] = (valid && v > 0.0f) ? v : 0.0f;
+        out = __fmaf_rn(M[SM_W3 + j], a2[j], out);
+      }
+      put_col(S + TC_GB, 32, SM_NH, t, a2);
+      float d = 0.0f;
+      if (valid) {
+        const float tn = __fdiv_rn(__fsub_rn(target[idx], M[SM_LMU]), M[SM_LSIG]);
+        const float r = __fsub_rn(out, tn);
+        loss = __fmul_rn(r, r);
+        d = __fdiv_rn(__fmul_rn(2.0f, r), (float)B);
+      }
+      float d2[SM_NH];
+#pragma unroll
+      for (int j = 0; j < SM_NH; j++) d2[j] = (a2[j] > 0.0f) ? __fmul_rn(d, M[SM_W3 + j]) : 0.0f;
+      put_row<32>(S + TC_D2, t, d2);
+      put_col(S + TC_GA, 0, SM_NH, t, d2);
+      put_col(S + TC_GA, 64, 1, t, &d);
+    } else if (stage == 2) {
+      tmem_ld32(my_lanes + 64, z);
+      float d1[SM_NH];
+#pragma unroll
+      for (int k = 0; k < SM_NH; k++) d1[k] = (a1[k] > 0.0f) ? z[k] : 0.0f;
+      put_col(S + TC_GA, 32, SM_NH, t, d1);
+    } else {
+      // gradients: warp 0 holds rows 0..31 (W2, b2), warp 1 rows 32..63 (W1, b1), lane 0 of
+      // warp 2 row 64 (W3, b3)
+      float *out_row = partial + (size_t)blockIdx.x * PART_W;
+      float g[32], gb[16];
+      if (warp == 0) {
+        tmem_ld32(my_lanes + 96, g);
+        tmem_ld16(my_lanes + 96 + 80, gb);
+#pragma unroll
+        for (int c = 0; c < SM_NH; c++) out_row[SM_W2 - SM_TRAIN0 + lane * SM_NH + c] = g[c];
+        out_row[SM_B2 - SM_TRAIN0 + lane] = gb[0];
+      } else if (warp == 1) {
+        tmem_ld32(my_lanes + 96 + 64, g);
+#pragma unroll
+        for (int k = 0; k < SM_NF; k++) out_row[SM_W1 - SM_TRAIN0 + lane * SM_NF + k] = g[k];
+        out_row[SM_B1 - SM_TRAIN0 + lane] = g[16];
+      } else if (warp == 2) {
+        tmem_ld32(my_lanes + 96 + 32, g);
+        tmem_ld16(my_lanes + 96 + 80, gb);
+        if (lane == 0) {
+#pragma unroll
+          for (int c = 0; c < SM_NH; c++) out_row[SM_W3 - SM_TRAIN0 + c] = g[c];
+          out_row[SM_B3 - SM_TRAIN0] = gb[0];
+        }
+      }
+    }
+  }
+  if (s_fail) {
+    // a product did not complete in time: record it and wait once more (bounded) for the
+    // tensor core before the TMEM is released
+    if (t == 0) {
+      atomicOr(status, 1u);
+      tc_wait(bar, phase ^ 1u);
+    }
   }
   // loss sum of the tile
-  __shared__ float lred[GT];
   lred[t] = loss;
+  tc_fence_before();
   __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(TC_COLS) : "memory");
   for (int w = GT / 2; w > 0; w >>= 1) {
     if (t < w) lred[t] = __fadd_rn(lred[t], lred[t + w]);
     __syncthreads();
   }
-  if (t == 0) out_row[SM_NTRAIN] = lred[0];
+  if (t == 0 && !s_fail) partial[(size_t)blockIdx.x * PART_W + SM_NTRAIN] = lred[0];
 }
 
 __global__ void reduce_kernel(const float *partial, int nblk, float *grad) {
@@ -368,12 +570,17 @@ void mlp_grad_host(const float *params, const float *feat, const float *target, 
   set_grad_smem();
   const int nblk = (n + GT - 1) / GT;
   DevBuf<float> dm(SM_NPAR), df((size_t)n * SM_NF), dt(n), part((size_t)nblk * PART_W), dg(PART_W);
+  DevBuf<unsigned> st(1);
+  cuda_ok(cudaMemset(st.p, 0, sizeof(unsigned)), "status");
   cuda_ok(cudaMemcpy(dm.p, params, SM_NPAR * sizeof(float), cudaMemcpyHostToDevice), "upload model");
   cuda_ok(cudaMemcpy(df.p, feat, (size_t)n * SM_NF * sizeof(float), cudaMemcpyHostToDevice), "upload features");
   cuda_ok(cudaMemcpy(dt.p, target, n * sizeof(float), cudaMemcpyHostToDevice), "upload targets");
-  mlp_grad_kernel<<<nblk, GT, GRAD_SMEM>>>(dm.p, df.p, dt.p, (uint32_t)n, n, 0, 0, nullptr, part.p);
+  mlp_grad_kernel<<<nblk, GT, GRAD_SMEM>>>(dm.p, df.p, dt.p, (uint32_t)n, n, 0, 0, nullptr, part.p, st.p);
   reduce_kernel<<<(PART_W + 255) / 256, 256>>>(part.p, nblk, dg.p);
   cuda_ok(cudaGetLastError(), "grad");
+  unsigned hst = 0;
+  cuda_ok(cudaMemcpy(&hst, st.p, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
+  if (hst) throw NgpuError("MLP gradient: a tensor-core product did not complete");
   std::vector<float> g(PART_W);
   cuda_ok(cudaMemcpy(g.data(), dg.p, PART_W * sizeof(float), cudaMemcpyDeviceToHost), "download");
   for (int o = 0; o < SM_NTRAIN; o++) grad[o] = g[o];
@@ -467,6 +674,8 @@ TrainResult train_step_model(const float *d_tuples, long long n_tuples, const Tr
   const int hist = 64;
   DevBuf<float> loss_hist(hist);
   DevBuf<long long> iter(1);
+  DevBuf<unsigned> status(1);
+  cuda_ok(cudaMemset(status.p, 0, sizeof(unsigned)), "status");
   cuda_ok(cudaMemcpy(dmodel.p, model.data(), SM_NPAR * sizeof(float), cudaMemcpyHostToDevice), "model");
   cuda_ok(cudaMemcpy(dmaster.p, master.data(), SM_NTRAIN * sizeof(float), cudaMemcpyHostToDevice), "master");
   cuda_ok(cudaMemset(m1.p, 0, SM_NTRAIN * sizeof(float)), "m1");
@@ -490,7 +699,7 @@ TrainResult train_step_model(const float *d_tuples, long long n_tuples, const Tr
         cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
         for (int r = 0; r < len; r++) {
           mlp_grad_kernel<<<nblk, GT, GRAD_SMEM, st>>>(dmodel.p, feat.p, tgt.p, (uint32_t)m, B, 1, cfg.seed,
-                                                         iter.p, part.p);
+                                                         iter.p, part.p, status.p);
           reduce_kernel<<<(PART_W + 255) / 256, 256, 0, st>>>(part.p, nblk, grad.p);
           adam_kernel<<<1, 512, 0, st>>>(dmaster.p, m1.p, m2.p, grad.p, dmodel.p, iter.p, a,
                                                               loss_hist.p, hist);
@@ -511,6 +720,9 @@ TrainResult train_step_model(const float *d_tuples, long long n_tuples, const Tr
   }
   if (exec) cudaGraphExecDestroy(exec);
   cudaStreamDestroy(st);
+  unsigned hst = 0;
+  cuda_ok(cudaMemcpy(&hst, status.p, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
+  if (hst) throw NgpuError("step model training: a tensor-core product did not complete");
   cuda_ok(cudaMemcpy(params, dmodel.p, SM_NPAR * sizeof(float), cudaMemcpyDeviceToHost), "download model");
   std::vector<float> lh(hist);
   cuda_ok(cudaMemcpy(lh.data(), loss_hist.p, hist * sizeof(float), cudaMemcpyDeviceToHost), "loss");

@@ -368,6 +368,69 @@ static double mlp_grad_d(const float *M, const float *feat, const float *target,
   return loss / n;
 }
 
+// Nearest BF16 value of a float, ties to even (finite inputs), as a float.
+static float bf16r(float v) {
+  uint32_t u;
+  std::memcpy(&u, &v, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) u += 0x7fffu + ((u >> 16) & 1u);
+  u &= 0xffff0000u;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+// mlp_grad_d with the operands of the engine's tensor-core training kernel rounded to BF16
+// where they enter a product: the normalised inputs, the layer-1 activations (FP32 first),
+// the layer-2 errors and the output error for the products, the layer-1 errors and the
+// layer-2 activations for the weight gradients; everything else in FP64.
+static double mlp_grad_bf16_d(const float *M, const float *feat, const float *target, int n, double *grad) {
+  using namespace sm;
+  for (int o = 0; o < NTRAIN; o++) grad[o] = 0.0;
+  double loss = 0.0;
+  for (int s = 0; s < n; s++) {
+    double xb[NF], z1[NH], a1b[NH], z2[NH], a2[NH];
+    for (int k = 0; k < NF; k++) {
+      const float v = (feat[s * NF + k] - M[MU + k]) * M[ISIG + k];
+      xb[k] = (double)bf16r(std::fmin(std::fmax(v, -XCLAMP), XCLAMP));
+    }
+    for (int j = 0; j < NH; j++) {
+      double z = 0.0;
+      for (int k = 0; k < NF; k++) z += (double)M[W1 + j * NF + k] * xb[k];
+      z1[j] = z + M[B1 + j];
+      a1b[j] = z1[j] > 0 ? (double)bf16r((float)z1[j]) : 0.0;
+    }
+    double out = M[B3];
+    for (int j = 0; j < NH; j++) {
+      double z = 0.0;
+      for (int k = 0; k < NH; k++) z += (double)M[W2 + j * NH + k] * a1b[k];
+      z2[j] = z + M[B2 + j];
+      a2[j] = z2[j] > 0 ? z2[j] : 0;
+      out += (double)M[W3 + j] * a2[j];
+    }
+    const double tn = ((double)target[s] - M[LMU]) / (double)M[LSIG];
+    const double r = out - tn;
+    loss += r * r;
+    const double d = 2.0 * r / n;
+    const double db = (double)bf16r((float)d);
+    double d2b[NH], d1b[NH];
+    for (int j = 0; j < NH; j++) d2b[j] = z2[j] > 0 ? (double)bf16r((float)(d * M[W3 + j])) : 0.0;
+    for (int k = 0; k < NH; k++) {
+      double g = 0;
+      for (int j = 0; j < NH; j++) g += (double)M[W2 + j * NH + k] * d2b[j];
+      d1b[k] = z1[k] > 0 ? (double)bf16r((float)g) : 0.0;
+    }
+    for (int j = 0; j < NH; j++) {
+      for (int k = 0; k < NF; k++) grad[W1 - W1 + j * NF + k] += d1b[j] * xb[k];
+      grad[B1 - W1 + j] += d1b[j];
+      for (int k = 0; k < NH; k++) grad[W2 - W1 + j * NH + k] += d2b[j] * a1b[k];
+      grad[B2 - W1 + j] += d2b[j];
+      grad[W3 - W1 + j] += db * (double)bf16r((float)a2[j]);
+    }
+    grad[B3 - W1] += db;
+  }
+  return loss / n;
+}
+
 struct Queued { int age; int cursor; float height; };
 
 // syn: synapse group (0: static, k: syn_groups[k-1]); stamp: low 16 bits of the time index
@@ -1808,6 +1871,9 @@ void orc_mlp_propose(const float *params, const float *feat, int n, float *out) 
 }
 double orc_mlp_grad(const float *params, const float *feat, const float *target, int n, double *grad) {
   return orc::mlp_grad_d(params, feat, target, n, grad);
+}
+double orc_mlp_grad_bf16(const float *params, const float *feat, const float *target, int n, double *grad) {
+  return orc::mlp_grad_bf16_d(params, feat, target, n, grad);
 }
 
 int orc_threads() { return omp_get_max_threads(); }

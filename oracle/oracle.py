@@ -107,6 +107,7 @@ def lib():
             "orc_mlp_out": (None, [fp, fp, c_int, fp]),
             "orc_mlp_propose": (None, [fp, fp, c_int, fp]),
             "orc_mlp_grad": (ctypes.c_double, [fp, fp, fp, c_int, ctypes.POINTER(ctypes.c_double)]),
+            "orc_mlp_grad_bf16": (ctypes.c_double, [fp, fp, fp, c_int, ctypes.POINTER(ctypes.c_double)]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -576,6 +577,18 @@ def mlp_grad(params, feat, target):
     g = np.zeros(STEP_MODEL_NTRAIN, dtype=np.float64)
     loss = lib().orc_mlp_grad(_fptr(p), _fptr(f), _fptr(t), f.shape[0],
                               g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return loss, g
+
+
+def mlp_grad_bf16(params, feat, target):
+    """mlp_grad with the operands of the GPU training kernel's tensor-core products
+    rounded to BF16 where they enter a product (FP64 sums)."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    f = np.ascontiguousarray(feat, dtype=np.float32).reshape(-1, 10)
+    t = np.ascontiguousarray(target, dtype=np.float32)
+    g = np.zeros(STEP_MODEL_NTRAIN, dtype=np.float64)
+    loss = lib().orc_mlp_grad_bf16(_fptr(p), _fptr(f), _fptr(t), f.shape[0],
+                                   g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
     return loss, g
 
 

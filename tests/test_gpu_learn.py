@@ -2,8 +2,8 @@
 
 - the inference code (the same device function the RK5 kernels call) is bit-identical
   to the oracle's FP32 statement of the network;
-- the training kernels' gradient (FP32, BF16 weights) agrees with the oracle's FP64
-  gradient;
+- the training kernels' gradient (tensor-core products of BF16 operands, FP32 sums)
+  agrees with the oracle's gradient at the same operand precision;
 - the step log of the plain integrator holds exactly the oracle's tuples;
 - with a network proposing, the simulation is bit-identical to the oracle's;
 - trained on a logged run, the network keeps the firing statistics and does not cost
@@ -35,15 +35,23 @@ def test_mlp_forward_bit_exact():
 
 @pytest.mark.parametrize("n", [1, 127, 128, 1000, 4099])
 def test_mlp_gradient_vs_fp64_oracle(n):
+    """The tensor-core kernel against the oracle with the same BF16 operand roundings (FP64
+    sums; what remains is FP32 accumulation and, rarely, one BF16 rounding step of a value
+    whose FP32 and FP64 forms straddle a rounding boundary), and against the unrounded FP64
+    gradient at BF16 operand precision."""
     p = random_params(7)
     rng = np.random.RandomState(n)
     f = rng.randn(n, 10).astype(np.float32)
     t = rng.uniform(-7, -2, n).astype(np.float32)
     loss, g = ngpu.MlpGrad(p, f, t)
+    loss_b, g_b = orc.mlp_grad_bf16(p, f, t)
     loss64, g64 = orc.mlp_grad(p, f, t)
-    assert abs(loss - loss64) <= 1e-5 * max(1.0, loss64)
-    scale = np.abs(g64).max()
-    assert np.max(np.abs(g.astype(np.float64) - g64)) <= 1e-4 * scale + 1e-8
+    assert abs(loss - loss_b) <= 1e-4 * max(1.0, loss_b)
+    scale = np.abs(g_b).max()
+    assert np.max(np.abs(g.astype(np.float64) - g_b)) <= 5e-3 * scale + 1e-8
+    assert np.median(np.abs(g.astype(np.float64) - g_b)) <= 1e-5 * scale + 1e-9
+    assert abs(loss - loss64) <= 2e-2 * max(1.0, loss64)
+    assert np.max(np.abs(g.astype(np.float64) - g64)) <= 5e-2 * np.abs(g64).max() + 1e-8
 
 
 def sorted_rows(a):

@@ -75,6 +75,34 @@ def test_mlp_gradient_matches_finite_differences():
         assert abs(num - g[j]) <= 1e-6 * max(1.0, np.abs(g).max()), (j, num, g[j])
 
 
+def test_bf16_operand_gradient_restatement():
+    """The oracle's statement of the GPU training kernel's operand precision (BF16 roundings
+    of the values that enter the tensor-core products) stays within BF16 precision of the
+    exact gradient, and equals it where every operand is already a BF16 value."""
+    p = random_params(3)
+    rng = np.random.RandomState(8)
+    f = rng.randn(300, 10).astype(np.float32)
+    t = rng.uniform(-6, -1, 300).astype(np.float32)
+    loss, g = orc.mlp_grad(p, f, t)
+    loss_b, g_b = orc.mlp_grad_bf16(p, f, t)
+    assert abs(loss - loss_b) <= 1e-2 * max(1.0, loss)
+    assert np.max(np.abs(g - g_b)) <= 5e-2 * np.abs(g).max()
+    assert np.max(np.abs(g - g_b)) > 0.0
+    # one sample whose normalised inputs are 0 and whose layer-1 units are all off: only the
+    # output bias and its error remain, and d = 2 r is rounded to BF16 in the restatement
+    q = p.copy()
+    q[T0:T0 + NT] = 0.0
+    q[B3] = 0.5
+    q[B1:W2] = -1.0                                 # every layer-1 unit off
+    f0 = np.zeros((1, 10), np.float32) + p[:10]    # inputs at the mean
+    t0 = np.array([p[LMU]], np.float32)            # normalised target 0
+    l0, g0 = orc.mlp_grad(q, f0, t0)
+    l0b, g0b = orc.mlp_grad_bf16(q, f0, t0)
+    assert l0 == l0b == 0.25
+    assert g0[-1] == g0b[-1] == 1.0
+    assert np.count_nonzero(g0b[:-1]) == 0
+
+
 def test_mlp_fp32_forward_close_to_fp64():
     p = random_params(5)
     f = np.random.RandomState(6).randn(500, 10).astype(np.float32)
