@@ -356,6 +356,16 @@ int NGPU_SetDeliverAggregate(int on);
    streams the current segment (a two-stage software pipeline); 0: one item after the other.
    Results do not depend on it. */
 int NGPU_SetDeliverPrefetch(int on);
+/* 1: in a network whose neurons are all iaf_psc_exp (Poisson generators aside), with no
+   plastic connections and one process, each spike's out-edges are added to the target
+   accumulators by the update kernel's block in the step the spike is emitted, into a ring of
+   accumulator slots indexed by arrival step, and no delivery kernel runs; 0 (default): the
+   delivery kernel.  Takes effect at calibration (call it before the first Simulate); results do not
+   depend on it.  Replaces the delivery path of src/nestgpu.cu:469-635 (SendSpike, then
+   CollectSpikeKernel in the next step); no reference counterpart as a switch. */
+int NGPU_SetDeliverPush(int on);
+/* 1 if delivery at emission is active (after calibration), else 0. */
+int NGPU_DeliverPushActive(void);
 /* Lanes per spike-delivery work item (8, 16 or 32; default 32): one item is the out-edge
    segment of one (source, delay) pair; short segments leave fewer lanes idle with small
    groups. */

@@ -122,7 +122,7 @@ __device__ __forceinline__ void push_spike(const SpikeOut &so, const GroupSpikeR
     if (pos < so.xch_cap) so.xch[1 + pos] = make_int4(node, __float_as_int(height), (int)tidx, 0);
     else atomicOr(so.status, ST_EXCHANGE_FULL);
   }
-  if (so.has_out[node]) {
+  if (so.has_out[node] && !so.push_acc) {
     int slot = (int)(tidx % so.R);
     int pos = atomicAdd(&so.ring_cnt[slot], 1);
     if (pos < so.cap) so.ring[(size_t)slot * so.cap + pos] = make_int2(node, __float_as_int(height));

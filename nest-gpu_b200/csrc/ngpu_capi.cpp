@@ -815,6 +815,19 @@ int NGPU_SetDeliverPrefetch(int on) {
   }, -1);
 }
 
+int NGPU_SetDeliverPush(int on) {
+  return guard([&] {
+    if (E().calibrated())
+      throw NgpuError("SetDeliverPush takes effect at calibration: call it before the first Simulate");
+    E().deliver_push = on ? 1 : 0;
+    return 0;
+  }, -1);
+}
+
+int NGPU_DeliverPushActive(void) {
+  return guard([&] { return E().push_active() ? 1 : 0; }, -1);
+}
+
 int NGPU_SetDeliverAggregate(int on) {
   return guard([&] {
     E().deliver_aggregate = on ? 1 : 0;

@@ -131,6 +131,8 @@ class Engine {
   int deliver_group = 32;         // lanes per delivery work item (8, 16, 32)
   int deliver_aggregate = 0;      // 1: warp-aggregated reductions (with 32-lane work items)
   int deliver_prefetch = 0;       // 1: delivery loads the next work item's segment ahead
+  int deliver_push = 0;           // 1: networks of iaf_psc_exp groups deliver each spike at emission
+                                  // (set before calibration)
   int update_occupancy = 0;       // 1: register-capped aeif update kernel
   int update_trial_iter = 0;      // 1: aeif update kernel advances one RK5 trial per iteration
   int persistent = 0;             // iaf-only networks: persistent cooperative step loop
@@ -227,6 +229,7 @@ class Engine {
   void simulation_step();
   void end_simulation();
   bool calibrated() const { return calibrated_; }
+  bool push_active() const { return push_; }   // delivery at emission (set at calibration)
   double neural_time() const { return neural_time_; }
   EngineStats stats();
   // Run n steps with every kernel bracketed by CUDA events on the engine stream;
@@ -350,6 +353,9 @@ class Engine {
   Clock *d_clk_ = nullptr;
   double *d_acc_ = nullptr;
   size_t n_acc_ = 0;
+  bool push_ = false;             // delivery at emission is active (chosen at calibration)
+  double *d_pacc_ = nullptr;      // its accumulator ring [push_R_][n_acc_]
+  int push_R_ = 0;
   int2 *d_ring_ = nullptr;
   int *d_ring_cnt_ = nullptr;
   int R_ = 0, cap_ = 0;
@@ -399,6 +405,7 @@ class Engine {
   int n_iaf_multi_ = 0, iaf_multi_blocks_ = 0;
   void prepare_multi();
   bool persistent_eligible() const;
+  bool push_eligible() const;
   void run_persistent(int steps);
 
   template <class T> T *dalloc(size_t n);

@@ -34,6 +34,53 @@ __device__ __forceinline__ float iget(const IafArgs &A, int j, int i) {
   return p ? __ldg(p + i) : A.pval[j];
 }
 
+// Delivery at emission: the block adds the out-edges of node `src`, which spiked at time
+// index `tidx`, into the accumulator ring.  The source's edges are contiguous in the CSR,
+// delay group after delay group (group dd reaches the step with time index
+// tidx + 1 + dmin + dd, as in the delivery kernel); thread t takes edges t, t + B, t + 2B, ...
+// (B = block size, so each warp load is coalesced), four loads in flight before their
+// reductions, and walks the delay groups (offsets staged in shared memory when they fit)
+// as its edges advance.  FP64 reductions, so the sums equal those of the delivery kernel
+// whatever the order.  Called by every thread of the block; returns the number of edges.
+constexpr int PUSH_OFF_SMEM = 512;   // staged group offsets (dspan + 1 at most)
+
+__device__ __noinline__ unsigned long long push_out_edges(const SpikeOut &so, int src, long long tidx, float height,
+                                                          long long *s_off) {
+  const long long base = (long long)src * so.dspan;
+  const bool staged = so.dspan + 1 <= PUSH_OFF_SMEM;
+  if (staged)
+    for (int k = threadIdx.x; k <= so.dspan; k += blockDim.x) s_off[k] = __ldg(&so.ev_off[base + k]);
+  __syncthreads();
+  auto off = [&](int k) { return staged ? s_off[k] : __ldg(&so.ev_off[base + k]); };
+  const long long s0 = off(0), s1 = off(so.dspan);
+  const int B = blockDim.x;
+  const uint2 *edge = reinterpret_cast<const uint2 *>(so.edge);
+  int dd = 0;
+  long long next = off(1);
+  int slot = (int)((tidx + 1 + so.dmin) % so.push_R);
+  for (long long e = s0 + threadIdx.x; e < s1; e += 4LL * B) {
+    uint2 ew[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (e + (long long)u * B < s1) ew[u] = __ldg(edge + e + (long long)u * B);
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const long long eu = e + (long long)u * B;
+      if (eu < s1) {
+        while (eu >= next) {           // dd + 1 <= dspan: eu < s1 = off(dspan)
+          dd++;
+          next = off(dd + 1);
+          if (++slot == so.push_R) slot = 0;
+        }
+        atomicAdd(&so.push_acc[(size_t)slot * so.push_stride + ew[u].x],
+                  (double)__fmul_rn(height, __uint_as_float(ew[u].y)));
+      }
+    }
+  }
+  __syncthreads();                     // s_off is reused for the next spike
+  return (unsigned long long)(s1 - s0);
+}
+
 __device__ __forceinline__ void iaf_neuron(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0,
                                            int M, int i) {
   const int n = A.n;
@@ -78,11 +125,99 @@ __device__ __forceinline__ void iaf_neuron(const IafArgs &A, const SpikeOut &so,
   A.var[3 * (size_t)n + i] = refr;
 }
 
+// iaf_neuron with delivery at emission: every thread of the block runs the loop (`valid` false
+// past the group's end) so that after each step the block delivers the out-edges of its
+// neurons that spiked; the input slot of a step is the ring slot of its time index.  The
+// arithmetic of the step is iaf_neuron's.
+__device__ __forceinline__ void iaf_neuron_push(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0,
+                                                int M, int i, bool valid, int *s_src, int *s_n, long long *s_off) {
+  const int n = A.n;
+  float Iex = 0.0f, Iin = 0.0f, V = 0.0f, refr = 0.0f, I_e = 0.0f, P20 = 0.0f, P21ex = 0.0f, P21in = 0.0f,
+        P22 = 0.0f, P11ex = 0.0f, P11in = 0.0f, theta = 0.0f, V_reset = 0.0f, refr_steps = 0.0f;
+  PoissonCache pc;
+  pc.e0 = pc.e1 = 0;
+  if (valid) {
+    Iex = A.var[i];
+    Iin = A.var[(size_t)n + i];
+    V = A.var[2 * (size_t)n + i];
+    refr = A.var[3 * (size_t)n + i];
+    I_e = iget(A, IP_I_e, i);
+    P20 = iget(A, IP_P20, i);
+    P21ex = iget(A, IP_P21ex, i);
+    P21in = iget(A, IP_P21in, i);
+    P22 = iget(A, IP_P22, i);
+    P11ex = iget(A, IP_P11ex, i);
+    P11in = iget(A, IP_P11in, i);
+    theta = iget(A, IP_Theta_rel, i);
+    V_reset = iget(A, IP_V_reset_rel, i);
+    refr_steps = iget(A, IP_refr_steps, i);
+    poisson_cache_load(A.in, i, pc);
+  }
+  const Clock cl = *clk;
+  const long long rec_it0 = cl.rec_it0;
+  unsigned long long nev = 0;
+  for (int m = 0; m < M; m++) {
+    const StepT t = step_at(cl, k0, m, A.dt);
+    const int slot = (int)(t.tidx % A.in.ring_R);
+    double apf[2] = {0.0, 0.0};
+    if (valid) acc_prefetch<2>(apf, 2, n, i, A.in, slot);
+    if (refr > 0.0f) {
+      refr = __fsub_rn(refr, 1.0f);
+    } else {
+      V = __fmaf_rn(I_e, P20, __fmaf_rn(Iin, P21in, __fmaf_rn(Iex, P21ex, __fmul_rn(V, P22))));
+    }
+    Iex = __fmul_rn(Iex, P11ex);
+    Iin = __fmul_rn(Iin, P11in);
+    const bool spike = valid && V >= theta;
+    if (spike) {
+      push_spike(so, A.srec, A.i0 + i, i, 1.0f, t.tidx, t.tnow);
+      V = V_reset;
+      refr = refr_steps;
+    }
+    // the block's spikes of this step, then their out-edges, one spike after the other
+    if (threadIdx.x == 0) *s_n = 0;
+    __syncthreads();
+    if (spike) s_src[atomicAdd(s_n, 1)] = A.i0 + i;
+    __syncthreads();
+    const int ns = *s_n;
+    for (int j = 0; j < ns; j++) nev += push_out_edges(so, s_src[j], t.tidx, 1.0f, s_off);
+    __syncthreads();
+    if (valid && A.rec.first) {
+      const float yr[4] = {Iex, Iin, V, refr};
+      write_records<4>(A.rec, so, A.i0 + i, i, yr, 4, refr, t.it - rec_it0, t.tidx);
+    }
+    if (valid) {
+      double in[2];
+      step_inputs_pf<2>(in, apf, 2, n, i, A.in, pc, slot, t.tidx, t.tnow);
+      if (in[0] != 0.0) Iex = (float)__fma_rn(in[0], 1.0, (double)Iex);
+      if (in[1] != 0.0) Iin = (float)__fma_rn(in[1], 1.0, (double)Iin);
+    }
+  }
+  if (valid) {
+    A.var[i] = Iex;
+    A.var[(size_t)n + i] = Iin;
+    A.var[2 * (size_t)n + i] = V;
+    A.var[3 * (size_t)n + i] = refr;
+  }
+  if (threadIdx.x == 0 && nev) atomicAdd(so.n_events, nev);
+}
+
 __global__ void __launch_bounds__(256, 3) iaf_batch_kernel(const IafArgs A, const SpikeOut so,
                                                         const Clock *clk, int k0, int M) {
   pdl_enter();
   const int i = A.lo + blockIdx.x * blockDim.x + threadIdx.x;
   if (i < A.hi) iaf_neuron(A, so, clk, k0, M, i);
+}
+
+// Delivery at emission (so.push_acc set): every thread of the block runs the step loop.
+__global__ void __launch_bounds__(256, 3) iaf_push_batch_kernel(const IafArgs A, const SpikeOut so,
+                                                             const Clock *clk, int k0, int M) {
+  pdl_enter();
+  const int i = A.lo + blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ int s_src[256];
+  __shared__ int s_n;
+  __shared__ long long s_off[PUSH_OFF_SMEM];
+  iaf_neuron_push(A, so, clk, k0, M, i, i < A.hi, s_src, &s_n, s_off);
 }
 
 // All iaf_psc_exp groups in one launch (a network of several populations would
@@ -101,6 +236,23 @@ __global__ void __launch_bounds__(256, 3) iaf_multi_kernel(const IafArgs *tab, c
   const IafArgs &A = tab[lo];
   const int i = A.lo + ((int)blockIdx.x - blk0[lo]) * blockDim.x + threadIdx.x;
   if (i < A.hi) iaf_neuron(A, so, clk, k0, M, i);
+}
+
+// The multi-group launch with delivery at emission.
+__global__ void __launch_bounds__(256, 3) iaf_push_multi_kernel(const IafArgs *tab, const int *blk0, int ngroups,
+                                                             const SpikeOut so, const Clock *clk, int k0, int M) {
+  pdl_enter();
+  int lo = 0, hi = ngroups;   // largest g with blk0[g] <= blockIdx.x
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (blk0[mid] <= (int)blockIdx.x) lo = mid; else hi = mid;
+  }
+  const IafArgs &A = tab[lo];
+  const int i = A.lo + ((int)blockIdx.x - blk0[lo]) * blockDim.x + threadIdx.x;
+  __shared__ int s_src[256];
+  __shared__ int s_n;
+  __shared__ long long s_off[PUSH_OFF_SMEM];
+  iaf_neuron_push(A, so, clk, k0, M, i, i < A.hi, s_src, &s_n, s_off);
 }
 
 // ---------------------------------------------------------------------------
@@ -500,14 +652,16 @@ int launch_aeif(int model, const AeifArgs &A, const SpikeOut &so, const Clock *c
 
 int launch_iaf(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
   if (A.hi <= A.lo) return 0;
-  launch_k(iaf_batch_kernel, dim3((A.hi - A.lo + 255) / 256), dim3(256), 0, st, A, so, clk, k0, M);
+  launch_k(so.push_acc ? iaf_push_batch_kernel : iaf_batch_kernel, dim3((A.hi - A.lo + 255) / 256), dim3(256), 0,
+           st, A, so, clk, k0, M);
   return 1;
 }
 
 int launch_iaf_multi(const IafArgs *tab, const int *blk0, int ngroups, int nblocks, const SpikeOut &so,
                      const Clock *clk, int k0, int M, cudaStream_t st) {
   if (nblocks <= 0) return 0;
-  launch_k(iaf_multi_kernel, dim3(nblocks), dim3(256), 0, st, tab, blk0, ngroups, so, clk, k0, M);
+  launch_k(so.push_acc ? iaf_push_multi_kernel : iaf_multi_kernel, dim3(nblocks), dim3(256), 0, st, tab, blk0,
+           ngroups, so, clk, k0, M);
   return 1;
 }
 

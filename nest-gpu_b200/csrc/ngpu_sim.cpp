@@ -397,6 +397,17 @@ void Engine::calibrate() {
   if (dspan_ * batch_ > deliver_max_pairs()) batch_ = std::max(1, deliver_max_pairs() / dspan_);
   d_acc_ = dalloc<double>(n_acc_ * batch_);
   cuda_check(cudaMemset(d_acc_, 0, std::max<size_t>(n_acc_ * batch_, 1) * sizeof(double)), "memset");
+  // delivery at emission: a spike of step t reaches steps t + 1 + dmin .. t + dmin + dspan,
+  // all after its batch (batch_ <= dmin + 1); the ring has one slot per step of that reach
+  // and of the batch being read, so a slot being read is never one being written
+  push_ = deliver_push && push_eligible();
+  push_R_ = 0;
+  d_pacc_ = nullptr;
+  if (push_) {
+    push_R_ = batch_ + dmin_ + dspan_;
+    d_pacc_ = dalloc<double>(n_acc_ * (size_t)push_R_);
+    cuda_check(cudaMemset(d_pacc_, 0, std::max<size_t>(n_acc_ * (size_t)push_R_, 1) * sizeof(double)), "memset");
+  }
 
   // ---- spike ring and per-node spike state
   R_ = (dmin_ + dspan_ - 1) + batch_ + 3;
@@ -706,6 +717,14 @@ SpikeOut Engine::spike_out() const {
   so.rev_cnt = d_rev_cnt_;
   so.rev_R = rev_R_;
   so.rev_cap = rev_cap_;
+  so.push_acc = push_ ? d_pacc_ : nullptr;
+  so.push_R = push_R_;
+  so.push_stride = n_acc_;
+  so.ev_off = d_ev_off_;
+  so.edge = d_edge_;
+  so.dmin = dmin_;
+  so.dspan = dspan_;
+  so.n_events = d_counters_ + 1;
   return so;
 }
 
@@ -732,6 +751,11 @@ GroupInput Engine::group_input(Group &g) {
   GroupInput in;
   in.acc = d_acc_ + g.acc_off;
   in.slot_stride = n_acc_;
+  in.ring_R = 0;
+  if (push_ && g.model == M_IAF_PSC_EXP) {
+    in.acc = d_pacc_ + g.acc_off;
+    in.ring_R = push_R_;
+  }
   in.pin_off = g.d_pin_off;
   in.pin = g.d_pin;
   in.gen = d_gen_;
@@ -995,8 +1019,10 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   set_launch_pdl(pdl && !fork && !plastic_ && !ev);
   if (ev) cuda_check(cudaEventRecord((*ev)[0], stream_), "event");
   if (plastic_) count_launch(launch_stdp_reset(stdp_, d_clk_, k0, stream_));
-  count_launch(launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_,
-                              deliver_group, d_clk_, k0, M, stream_));
+  // (delivery at emission: the update kernels deliver; there is no delivery launch)
+  if (!push_)
+    count_launch(launch_deliver(deliver_args(), deliver_blocks_req > 0 ? deliver_blocks_req : deliver_blocks_,
+                                deliver_group, d_clk_, k0, M, stream_));
   if (ev) cuda_check(cudaEventRecord((*ev)[1], stream_), "event");
   cudaStream_t s2 = stream_;
   if (fork) {
@@ -1062,6 +1088,20 @@ void Engine::prepare_multi() {
 // The persistent step loop serves networks whose only neurons are iaf_psc_exp groups
 // (Poisson generators have no kernel of their own).
 bool Engine::persistent_eligible() const {
+  if (plastic_ || part_world_ > 1 || push_) return false;
+  bool any = false;
+  for (auto &g : groups_) {
+    if (g.n <= 0 || g.model == M_POISS_GEN) continue;
+    if (g.model != M_IAF_PSC_EXP) return false;
+    any = true;
+  }
+  return any;
+}
+
+// Delivery at emission serves the same networks as the persistent loop: iaf_psc_exp groups
+// only (their spikes have height 1 and their kernel is the only spike source), no plastic
+// edges, one process.
+bool Engine::push_eligible() const {
   if (plastic_ || part_world_ > 1) return false;
   bool any = false;
   for (auto &g : groups_) {

@@ -53,6 +53,8 @@ struct Clock {
 };
 
 // Spike output context shared by all spiking models.
+struct EdgeW;
+
 struct SpikeOut {
   int2 *ring;            // [R][cap] (source node, height bits), slot = time index % R
   int *ring_cnt;         // [R]
@@ -75,6 +77,17 @@ struct SpikeOut {
   int *rev_ring;         // [rev_R][rev_cap] nodes whose spike reaches their synapses then
   int *rev_cnt;          // [rev_R]
   int rev_R, rev_cap;
+  // Delivery at emission (networks of iaf_psc_exp groups, push_acc non-null): the update
+  // kernel's warp adds each spike's out-edges at once into the accumulator ring
+  // push_acc[push_R][push_stride], slot = arrival time index % push_R; the spike ring is
+  // then not used.
+  double *push_acc;
+  int push_R;
+  size_t push_stride;
+  const long long *ev_off;   // delivery CSR [n_nodes * dspan + 1]
+  const EdgeW *edge;
+  int dmin, dspan;
+  unsigned long long *n_events;
 };
 
 // Per-group spike bookkeeping (optional outputs).
@@ -118,6 +131,8 @@ struct GenPar {
 struct GroupInput {
   double *acc;           // slot 0 row of this group: acc + m*slot_stride + p*n + i
   size_t slot_stride;    // doubles per slot (all groups)
+  int ring_R;            // 0: slot m = step m of the batch; > 0: acc is the delivery-at-emission
+                         // ring, slot = time index % ring_R
   const int *pin_off;    // [n+1] or null
   const PoissonIn *pin;
   const GenPar *gen;

@@ -177,6 +177,8 @@ if is_b200_engine:
     _c["NGPU_SetUpdateTrialIter"] = _bind("NGPU_SetUpdateTrialIter", _I, [_I])
     _c["NGPU_SetDeliverAggregate"] = _bind("NGPU_SetDeliverAggregate", _I, [_I])
     _c["NGPU_SetDeliverPrefetch"] = _bind("NGPU_SetDeliverPrefetch", _I, [_I])
+    _c["NGPU_SetDeliverPush"] = _bind("NGPU_SetDeliverPush", _I, [_I])
+    _c["NGPU_DeliverPushActive"] = _bind("NGPU_DeliverPushActive", _I, [])
     _c["NGPU_SetPartition"] = _bind("NGPU_SetPartition", _I, [_I, _I])
     _c["NGPU_SetExchange"] = _bind("NGPU_SetExchange", _I, [c_void_p, c_void_p, ctypes.c_longlong, c_void_p,
                                                              c_void_p])
@@ -1482,6 +1484,21 @@ def SetDeliverPrefetch(on=True):
     results are identical either way)."""
     _need_b200("SetDeliverPrefetch")
     return _check(_c["NGPU_SetDeliverPrefetch"](1 if on else 0))
+
+
+def SetDeliverPush(on=True):
+    """Delivery at emission for networks of iaf_psc_exp groups (engine extension, default off):
+    each spike's out-edges are added by the update kernel in the step it is emitted, with no
+    delivery kernel; takes effect at calibration (call before the first Simulate); results
+    are identical either way."""
+    _need_b200("SetDeliverPush")
+    return _check(_c["NGPU_SetDeliverPush"](1 if on else 0))
+
+
+def DeliverPushActive():
+    """True if delivery at emission is active (engine extension; after calibration)."""
+    _need_b200("DeliverPushActive")
+    return bool(_check(_c["NGPU_DeliverPushActive"]()))
 
 
 def SetDeliverAggregate(on=True):

@@ -292,12 +292,15 @@ def test_launch_mappings_keep_results(threads, group, occ, tpi, agg, pf):
     assert np.array_equal(np.float32(d_gpu), np.float32(d_orc))
 
 
-def test_microcircuit_slice_bitexact():
+@pytest.mark.parametrize("push", [True, False])
+def test_microcircuit_slice_bitexact(push):
     """The layered microcircuit at 3% size (eight iaf_psc_exp populations served by one
     multi-group launch, fixed_total_number projections with normal_clipped weights and
-    delays, Poisson background): spike counts neuron by neuron equal the oracle's."""
+    delays, Poisson background): spike counts neuron by neuron equal the oracle's, with
+    delivery at emission and with the delivery kernel."""
     from workloads import microcircuit
     ngpu.SetHostRng(True)
+    ngpu.SetDeliverPush(push)
     pops_g = microcircuit(ngpu, scale=0.03)
     o = orc.Oracle()
     pops_o = microcircuit(o, scale=0.03)
@@ -307,6 +310,56 @@ def test_microcircuit_slice_bitexact():
     c_o = np.concatenate([np.asarray(o.GetStatus(p, "spike_count")).ravel() for p in pops_o])
     assert c_g.sum() > 1000
     assert np.array_equal(c_g, c_o)
+    assert ngpu.DeliverPushActive() == push
+
+
+def iaf_two_populations(api, seed=3, delay=1.5):
+    """800 + 200 iaf_psc_exp neurons, fixed in-degree 80 + 20 with one delay, Poisson drive
+    (the minimum delay sets the time batch: 1.5 ms gives 15-step batches)."""
+    api.SetKernelStatus("rnd_seed", seed)
+    n = api.Create("iaf_psc_exp", 1000)
+    exc, inh = n[0:800], n[800:1000]
+    pg = api.Create("poisson_generator")
+    api.SetStatus(pg, "rate", 12000.0)
+    api.Connect(pg, n, {"rule": "all_to_all"}, {"weight": 30.0, "delay": 0.1})
+    api.Connect(exc, n, {"rule": "fixed_indegree", "indegree": 80}, {"weight": 25.0, "delay": delay})
+    api.Connect(inh, n, {"rule": "fixed_indegree", "indegree": 20}, {"weight": -120.0, "delay": delay})
+    api.ActivateSpikeCount(n)
+    return n
+
+
+@pytest.mark.parametrize("delay", [0.1, 1.5])
+def test_delivery_at_emission_equals_delivery_kernel(delay):
+    """Delivery at emission (the update kernel's warps add each spike's out-edges into a ring of
+    accumulator slots) against the delivery kernel, with one-step batches (delay 0.1 ms) and
+    15-step batches (1.5 ms): the same spikes and recorded traces; events are counted when a
+    spike is emitted, so at the end of a run the count also holds those still on their way
+    (at most one delay's worth); the switch is refused after calibration."""
+    res = []
+    for push in (True, False):
+        ngpu.Reset()
+        ngpu.SetVerbosityLevel(0)
+        ngpu.SetHostRng(True)
+        ngpu.SetDeliverPush(push)
+        n = iaf_two_populations(ngpu, delay=delay)
+        rec = ngpu.CreateRecord("", ["V_m_rel", "I_syn_ex", "I_syn_in"], [n[3], n[500], n[900]], [0, 0, 0])
+        ngpu.Simulate(70.0)
+        ngpu.Simulate(33.0)
+        assert ngpu.DeliverPushActive() == push
+        with pytest.raises(ValueError, match="calibration"):
+            ngpu.SetDeliverPush(not push)
+        counts = np.asarray(ngpu.GetStatus(n, "spike_count")).ravel()
+        res.append((counts, np.asarray(ngpu.GetRecordData(rec), dtype=np.float32), ngpu.GetStats()))
+    (c1, r1, s1), (c2, r2, s2) = res
+    assert c1.sum() > 500
+    assert np.array_equal(c1, c2)
+    assert np.array_equal(r1, r2)
+    assert s2["n_events"] > 0 and s1["status"] == s2["status"] == 0
+    assert s2["n_events"] <= s1["n_events"] <= s2["n_events"] * (1.0 + 2.0 * delay / 103.0)
+    o = orc.Oracle()
+    n_o = iaf_two_populations(o, delay=delay)
+    o.Simulate(103.0)
+    assert np.array_equal(c1, np.asarray(o.GetStatus(n_o, "spike_count")).ravel())
 
 
 @pytest.mark.parametrize("occ,tpi", [(0, 0), (1, 0), (0, 1), (1, 1)])
@@ -336,6 +389,7 @@ def test_persistent_step_loop_equals_per_batch_launches():
     for pers in (True, False):
         ngpu.Reset()
         ngpu.SetVerbosityLevel(0)
+        ngpu.SetDeliverPush(False)
         ngpu.SetPersistent(pers)
         pops = microcircuit(ngpu, scale=0.03)
         rec = ngpu.CreateRecord("", ["V_m_rel", "I_syn_ex", "spike"], [pops[0][0], pops[2][3], pops[4][1]],
@@ -356,6 +410,7 @@ def test_persistent_barrier_timeout_is_reported():
     than the launch has run out of polls; Simulate fails with an error instead of hanging,
     and the engine (and its GPU context) keeps working afterwards."""
     from workloads import microcircuit
+    ngpu.SetDeliverPush(False)
     ngpu.SetPersistent(True)
     ngpu._c["NGPU_TestBarrierTimeout"](1)
     microcircuit(ngpu, scale=0.01)
