@@ -388,6 +388,12 @@ int NGPU_SetProgrammaticLaunch(int on);
    (a second or two); the kernel records the timeout and returns, and the Simulate call fails
    with error code 2 while the GPU context stays usable.  0 (default) disables it. */
 int NGPU_TestBarrierTimeout(int extra);
+/* Test hook for the failure path of the step-model training kernel: with on != 0 its
+   tensor-core products are issued but their completion is never signalled on the block's
+   mbarrier, so the bounded wait runs out; the kernel records it, releases its tensor memory
+   and returns, and NGPU_MlpGrad / NGPU_StepModelTrain fail with error code 2 while the GPU
+   context stays usable.  0 (default) disables it.  No counterpart in the reference. */
+int NGPU_TestTensorWaitTimeout(int on);
 /* Autotuner of the launch mappings (no counterpart in the reference): on the calibrated
    network, after 4 x `steps` warm-up steps, times `steps` simulation steps per candidate of the
    update block size, the update kernel variant, the delivery lane group, the delivery grid and

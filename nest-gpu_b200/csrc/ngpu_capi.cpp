@@ -853,6 +853,15 @@ int NGPU_TestBarrierTimeout(int extra) {
   }, -1);
 }
 
+// Test hook: the training kernel's tensor-core products complete unsignalled, so its bounded
+// wait runs out and the call fails.
+int NGPU_TestTensorWaitTimeout(int on) {
+  return guard([&] {
+    set_tensor_wait_test(on);
+    return 0;
+  }, -1);
+}
+
 int NGPU_SetPersistent(int on) {
   return guard([&] {
     E().persistent = on ? 1 : 0;

@@ -39,6 +39,7 @@ struct TrainResult {
 TrainResult train_step_model(const float *d_tuples, long long n_tuples, const TrainConfig &cfg, float *params);
 void mlp_forward_host(const float *params, const float *feat, int n, float *out);
 void mlp_grad_host(const float *params, const float *feat, const float *target, int n, float *grad, float *loss);
+void set_tensor_wait_test(int on);
 
 // Kinds of named quantities of a node group.
 enum Kind { K_NONE = -1, K_SCAL_VAR = 0, K_PORT_VAR, K_SCAL_PARAM, K_PORT_PARAM, K_GROUP_PARAM,

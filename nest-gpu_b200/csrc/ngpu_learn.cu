@@ -246,9 +246,9 @@ __device__ __forceinline__ void tc_commit(uint32_t mbar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                : "memory");
 }
-// Waits for phase `parity` of the barrier, at most TC_WAIT_POLLS polls; false if it gave up.
-__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
-  for (long long i = 0; i < TC_WAIT_POLLS; i++) {
+// Waits for phase `parity` of the barrier, at most `polls` polls; false if it gave up.
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity, long long polls) {
+  for (long long i = 0; i < polls; i++) {
     uint32_t done;
     asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                  "selp.u32 %0, 1, 0, p;\n\t}\n"
@@ -312,11 +312,13 @@ __device__ __forceinline__ uint32_t sample_index(uint64_t seed, long long iter, 
 // Samples: tile blockIdx.x covers batch positions [GT*blockIdx.x, GT*blockIdx.x+GT) of B;
 // position s uses sample sample_index(seed, iter, s) if sampled, else sample s.  Positions
 // past B contribute nothing (their output error is zero).  A wait for the tensor core that
-// gives up sets bit 0 of *status and the block ends after releasing its TMEM.
+// gives up sets bit 0 of *status and the block ends after releasing its TMEM.  test_no_commit
+// (failure-path test only): the products are issued but their completion is never signalled,
+// so the first wait runs out after a short bound.
 __global__ void __launch_bounds__(GT) mlp_grad_kernel(const float *model, const float *feat, const float *target,
                                                       uint32_t n, int B, int sampled, uint64_t seed,
                                                       const long long *iter_ptr, float *partial,
-                                                      unsigned *status) {
+                                                      unsigned *status, int test_no_commit) {
   extern __shared__ __align__(128) unsigned char tc_sm[];
   __shared__ __align__(8) unsigned long long s_bar;
   __shared__ uint32_t s_taddr;
@@ -398,9 +400,9 @@ __global__ void __launch_bounds__(GT) mlp_grad_kernel(const float *model, const 
       else if (stage == 1) tc_gemm(tm + 32, smem_u32(S + TC_A1), smem_u32(S + TC_W2), 32, tc_idesc(128, 32));
       else if (stage == 2) tc_gemm(tm + 64, smem_u32(S + TC_D2), smem_u32(S + TC_W2T), 32, tc_idesc(128, 32));
       else tc_gemm(tm + 96, smem_u32(S + TC_GA), smem_u32(S + TC_GB), GT, tc_idesc(128, 96));
-      tc_commit(bar);
+      if (!test_no_commit) tc_commit(bar);
     }
-    const bool ok = tc_wait(bar, phase);
+    const bool ok = tc_wait(bar, phase, test_no_commit ? (1LL << 12) : TC_WAIT_POLLS);
     phase ^= 1u;
     if (!ok) s_fail = 1;
     __syncthreads();
@@ -477,7 +479,7 @@ __global__ void __launch_bounds__(GT) mlp_grad_kernel(const float *model, const 
     // tensor core before the TMEM is released
     if (t == 0) {
       atomicOr(status, 1u);
-      tc_wait(bar, phase ^ 1u);
+      if (!test_no_commit) tc_wait(bar, phase ^ 1u, TC_WAIT_POLLS);
     }
   }
   // loss sum of the tile
@@ -554,6 +556,10 @@ static void set_grad_smem() {
   }
 }
 
+// Test hook of the training kernel's failure path (mlp_grad_kernel's test_no_commit).
+static int g_test_no_commit = 0;
+void set_tensor_wait_test(int on) { g_test_no_commit = on ? 1 : 0; }
+
 void mlp_forward_host(const float *params, const float *feat, int n, float *out) {
   if (n <= 0) return;
   DevBuf<float> dm(SM_NPAR), df((size_t)n * SM_NF), dout(n);
@@ -575,7 +581,8 @@ void mlp_grad_host(const float *params, const float *feat, const float *target, 
   cuda_ok(cudaMemcpy(dm.p, params, SM_NPAR * sizeof(float), cudaMemcpyHostToDevice), "upload model");
   cuda_ok(cudaMemcpy(df.p, feat, (size_t)n * SM_NF * sizeof(float), cudaMemcpyHostToDevice), "upload features");
   cuda_ok(cudaMemcpy(dt.p, target, n * sizeof(float), cudaMemcpyHostToDevice), "upload targets");
-  mlp_grad_kernel<<<nblk, GT, GRAD_SMEM>>>(dm.p, df.p, dt.p, (uint32_t)n, n, 0, 0, nullptr, part.p, st.p);
+  mlp_grad_kernel<<<nblk, GT, GRAD_SMEM>>>(dm.p, df.p, dt.p, (uint32_t)n, n, 0, 0, nullptr, part.p, st.p,
+                                           g_test_no_commit);
   reduce_kernel<<<(PART_W + 255) / 256, 256>>>(part.p, nblk, dg.p);
   cuda_ok(cudaGetLastError(), "grad");
   unsigned hst = 0;
@@ -699,7 +706,7 @@ TrainResult train_step_model(const float *d_tuples, long long n_tuples, const Tr
         cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
         for (int r = 0; r < len; r++) {
           mlp_grad_kernel<<<nblk, GT, GRAD_SMEM, st>>>(dmodel.p, feat.p, tgt.p, (uint32_t)m, B, 1, cfg.seed,
-                                                         iter.p, part.p, status.p);
+                                                         iter.p, part.p, status.p, g_test_no_commit);
           reduce_kernel<<<(PART_W + 255) / 256, 256, 0, st>>>(part.p, nblk, grad.p);
           adam_kernel<<<1, 512, 0, st>>>(dmaster.p, m1.p, m2.p, grad.p, dmodel.p, iter.p, a,
                                                               loss_hist.p, hist);

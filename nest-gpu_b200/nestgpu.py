@@ -185,6 +185,7 @@ if is_b200_engine:
     _c["NGPU_GetBatchLength"] = _bind("NGPU_GetBatchLength", _I, [])
     _c["NGPU_SetPersistent"] = _bind("NGPU_SetPersistent", _I, [_I])
     _c["NGPU_TestBarrierTimeout"] = _bind("NGPU_TestBarrierTimeout", _I, [_I])
+    _c["NGPU_TestTensorWaitTimeout"] = _bind("NGPU_TestTensorWaitTimeout", _I, [_I])
     _c["NGPU_Autotune"] = _bind("NGPU_Autotune", _I, [_I] + [ctypes.POINTER(_I)] * 4)
     _c["NGPU_GetLaunchMapping"] = _bind("NGPU_GetLaunchMapping", _I, [ctypes.POINTER(_I), _I])
     _c["NGPU_MeasureReductionRate"] = _bind("NGPU_MeasureReductionRate", ctypes.c_double,

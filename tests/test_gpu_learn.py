@@ -54,6 +54,26 @@ def test_mlp_gradient_vs_fp64_oracle(n):
     assert np.max(np.abs(g.astype(np.float64) - g64)) <= 5e-2 * np.abs(g64).max() + 1e-8
 
 
+def test_mlp_gradient_wait_timeout_is_reported():
+    """Failure path of the tensor-core training kernel: with the completion of its products
+    never signalled, the bounded wait runs out, the call fails with an error instead of
+    hanging, and the next call (hook off) is correct."""
+    p = random_params(7)
+    rng = np.random.RandomState(3)
+    f = rng.randn(300, 10).astype(np.float32)
+    t = rng.uniform(-7, -2, 300).astype(np.float32)
+    ngpu._c["NGPU_TestTensorWaitTimeout"](1)
+    try:
+        with pytest.raises(ValueError, match="did not complete"):
+            ngpu.MlpGrad(p, f, t)
+    finally:
+        ngpu._c["NGPU_TestTensorWaitTimeout"](0)
+    loss, g = ngpu.MlpGrad(p, f, t)
+    loss_b, g_b = orc.mlp_grad_bf16(p, f, t)
+    assert abs(loss - loss_b) <= 1e-4 * max(1.0, loss_b)
+    assert np.max(np.abs(g.astype(np.float64) - g_b)) <= 5e-3 * np.abs(g_b).max() + 1e-8
+
+
 def sorted_rows(a):
     return a[np.lexsort(a.T[::-1])]
 
