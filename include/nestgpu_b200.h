@@ -361,7 +361,8 @@ int NGPU_SetDeliverPrefetch(int on);
    accumulators by the update kernel's block in the step the spike is emitted, into a ring of
    accumulator slots indexed by arrival step, and no delivery kernel runs; 0 (default): the
    delivery kernel.  Takes effect at calibration (call it before the first Simulate); results do not
-   depend on it.  Replaces the delivery path of src/nestgpu.cu:469-635 (SendSpike, then
+   depend on it, except that the event counter (NGPU_GetStats) then counts a spike's edges when it
+   is emitted, not when they arrive.  Replaces the delivery path of src/nestgpu.cu:469-635 (SendSpike, then
    CollectSpikeKernel in the next step); no reference counterpart as a switch. */
 int NGPU_SetDeliverPush(int on);
 /* 1 if delivery at emission is active (after calibration), else 0. */
