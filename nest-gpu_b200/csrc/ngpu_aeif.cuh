@@ -87,7 +87,9 @@ __device__ __forceinline__ StepT step_at(const Clock &c, int k0, int m, float dt
   return s;
 }
 
-// PushSpike (src/spike_buffer.cu:162-242) on the ring design.
+// PushSpike (src/spike_buffer.cu:162-242) on the ring design.  RING = false (delivery at
+// emission): the spike goes to no ring, its out-edges are added by the caller.
+template <bool RING = true>
 __device__ __forceinline__ void push_spike(const SpikeOut &so, const GroupSpikeRec &rec, int node,
                                            int rel, float height, long long tidx, double tnow) {
   so.last_tidx[node] = (int)tidx;
@@ -122,7 +124,7 @@ __device__ __forceinline__ void push_spike(const SpikeOut &so, const GroupSpikeR
     if (pos < so.xch_cap) so.xch[1 + pos] = make_int4(node, __float_as_int(height), (int)tidx, 0);
     else atomicOr(so.status, ST_EXCHANGE_FULL);
   }
-  if (so.has_out[node] && !so.push_acc) {
+  if (RING && so.has_out[node]) {
     int slot = (int)(tidx % so.R);
     int pos = atomicAdd(&so.ring_cnt[slot], 1);
     if (pos < so.cap) so.ring[(size_t)slot * so.cap + pos] = make_int2(node, __float_as_int(height));

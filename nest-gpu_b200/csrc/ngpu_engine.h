@@ -429,6 +429,7 @@ class Engine {
   void drain_records(long long rows);
   void drain_rec_spike_times();
   SpikeOut spike_out() const;
+  PushOut push_out() const;
   AeifArgs aeif_args(Group &g);
   IafArgs iaf_args(Group &g);
   SpikeGenArgs sg_args(Group &g);
@@ -443,8 +444,10 @@ void engine_reset();
 // launchers (ngpu_kernels.cu)
 int launch_aeif(int model, const AeifArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                 cudaStream_t st);
-int launch_iaf(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st);
+int launch_iaf(const IafArgs &A, const SpikeOut &so, const PushOut *po, const Clock *clk, int k0, int M,
+               cudaStream_t st);
 int launch_iaf_multi(const IafArgs *tab, const int *blk0, int ngroups, int nblocks, const SpikeOut &so,
+                     const PushOut *po,
                      const Clock *clk, int k0, int M, cudaStream_t st);
 int launch_spike_gen(const SpikeGenArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M,
                      cudaStream_t st);

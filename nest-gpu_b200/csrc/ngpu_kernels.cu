@@ -44,20 +44,20 @@ __device__ __forceinline__ float iget(const IafArgs &A, int j, int i) {
 // whatever the order.  Called by every thread of the block; returns the number of edges.
 constexpr int PUSH_OFF_SMEM = 512;   // staged group offsets (dspan + 1 at most)
 
-__device__ __noinline__ unsigned long long push_out_edges(const SpikeOut &so, int src, long long tidx, float height,
+__device__ __noinline__ unsigned long long push_out_edges(const PushOut &po, int src, long long tidx, float height,
                                                           long long *s_off) {
-  const long long base = (long long)src * so.dspan;
-  const bool staged = so.dspan + 1 <= PUSH_OFF_SMEM;
+  const long long base = (long long)src * po.dspan;
+  const bool staged = po.dspan + 1 <= PUSH_OFF_SMEM;
   if (staged)
-    for (int k = threadIdx.x; k <= so.dspan; k += blockDim.x) s_off[k] = __ldg(&so.ev_off[base + k]);
+    for (int k = threadIdx.x; k <= po.dspan; k += blockDim.x) s_off[k] = __ldg(&po.ev_off[base + k]);
   __syncthreads();
-  auto off = [&](int k) { return staged ? s_off[k] : __ldg(&so.ev_off[base + k]); };
-  const long long s0 = off(0), s1 = off(so.dspan);
+  auto off = [&](int k) { return staged ? s_off[k] : __ldg(&po.ev_off[base + k]); };
+  const long long s0 = off(0), s1 = off(po.dspan);
   const int B = blockDim.x;
-  const uint2 *edge = reinterpret_cast<const uint2 *>(so.edge);
+  const uint2 *edge = reinterpret_cast<const uint2 *>(po.edge);
   int dd = 0;
   long long next = off(1);
-  int slot = (int)((tidx + 1 + so.dmin) % so.push_R);
+  int slot = (int)((tidx + 1 + po.dmin) % po.R);
   for (long long e = s0 + threadIdx.x; e < s1; e += 4LL * B) {
     uint2 ew[4];
 #pragma unroll
@@ -70,9 +70,9 @@ __device__ __noinline__ unsigned long long push_out_edges(const SpikeOut &so, in
         while (eu >= next) {           // dd + 1 <= dspan: eu < s1 = off(dspan)
           dd++;
           next = off(dd + 1);
-          if (++slot == so.push_R) slot = 0;
+          if (++slot == po.R) slot = 0;
         }
-        atomicAdd(&so.push_acc[(size_t)slot * so.push_stride + ew[u].x],
+        atomicAdd(&po.acc[(size_t)slot * po.stride + ew[u].x],
                   (double)__fmul_rn(height, __uint_as_float(ew[u].y)));
       }
     }
@@ -129,8 +129,9 @@ __device__ __forceinline__ void iaf_neuron(const IafArgs &A, const SpikeOut &so,
 // past the group's end) so that after each step the block delivers the out-edges of its
 // neurons that spiked; the input slot of a step is the ring slot of its time index.  The
 // arithmetic of the step is iaf_neuron's.
-__device__ __forceinline__ void iaf_neuron_push(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0,
-                                                int M, int i, bool valid, int *s_src, int *s_n, long long *s_off) {
+__device__ __forceinline__ void iaf_neuron_push(const IafArgs &A, const SpikeOut &so, const PushOut &po,
+                                                const Clock *clk, int k0, int M, int i, bool valid, int *s_src,
+                                                int *s_n, long long *s_off) {
   const int n = A.n;
   float Iex = 0.0f, Iin = 0.0f, V = 0.0f, refr = 0.0f, I_e = 0.0f, P20 = 0.0f, P21ex = 0.0f, P21in = 0.0f,
         P22 = 0.0f, P11ex = 0.0f, P11in = 0.0f, theta = 0.0f, V_reset = 0.0f, refr_steps = 0.0f;
@@ -158,7 +159,7 @@ __device__ __forceinline__ void iaf_neuron_push(const IafArgs &A, const SpikeOut
   unsigned long long nev = 0;
   for (int m = 0; m < M; m++) {
     const StepT t = step_at(cl, k0, m, A.dt);
-    const int slot = (int)(t.tidx % A.in.ring_R);
+    const int slot = (int)(t.tidx % po.R);
     double apf[2] = {0.0, 0.0};
     if (valid) acc_prefetch<2>(apf, 2, n, i, A.in, slot);
     if (refr > 0.0f) {
@@ -170,7 +171,7 @@ __device__ __forceinline__ void iaf_neuron_push(const IafArgs &A, const SpikeOut
     Iin = __fmul_rn(Iin, P11in);
     const bool spike = valid && V >= theta;
     if (spike) {
-      push_spike(so, A.srec, A.i0 + i, i, 1.0f, t.tidx, t.tnow);
+      push_spike<false>(so, A.srec, A.i0 + i, i, 1.0f, t.tidx, t.tnow);
       V = V_reset;
       refr = refr_steps;
     }
@@ -180,7 +181,7 @@ __device__ __forceinline__ void iaf_neuron_push(const IafArgs &A, const SpikeOut
     if (spike) s_src[atomicAdd(s_n, 1)] = A.i0 + i;
     __syncthreads();
     const int ns = *s_n;
-    for (int j = 0; j < ns; j++) nev += push_out_edges(so, s_src[j], t.tidx, 1.0f, s_off);
+    for (int j = 0; j < ns; j++) nev += push_out_edges(po, s_src[j], t.tidx, 1.0f, s_off);
     __syncthreads();
     if (valid && A.rec.first) {
       const float yr[4] = {Iex, Iin, V, refr};
@@ -199,7 +200,7 @@ __device__ __forceinline__ void iaf_neuron_push(const IafArgs &A, const SpikeOut
     A.var[2 * (size_t)n + i] = V;
     A.var[3 * (size_t)n + i] = refr;
   }
-  if (threadIdx.x == 0 && nev) atomicAdd(so.n_events, nev);
+  if (threadIdx.x == 0 && nev) atomicAdd(po.n_events, nev);
 }
 
 __global__ void __launch_bounds__(256, 3) iaf_batch_kernel(const IafArgs A, const SpikeOut so,
@@ -209,15 +210,15 @@ __global__ void __launch_bounds__(256, 3) iaf_batch_kernel(const IafArgs A, cons
   if (i < A.hi) iaf_neuron(A, so, clk, k0, M, i);
 }
 
-// Delivery at emission (so.push_acc set): every thread of the block runs the step loop.
-__global__ void __launch_bounds__(256, 3) iaf_push_batch_kernel(const IafArgs A, const SpikeOut so,
+// Delivery at emission: every thread of the block runs the step loop.
+__global__ void __launch_bounds__(256, 3) iaf_push_batch_kernel(const IafArgs A, const SpikeOut so, const PushOut po,
                                                              const Clock *clk, int k0, int M) {
   pdl_enter();
   const int i = A.lo + blockIdx.x * blockDim.x + threadIdx.x;
   __shared__ int s_src[256];
   __shared__ int s_n;
   __shared__ long long s_off[PUSH_OFF_SMEM];
-  iaf_neuron_push(A, so, clk, k0, M, i, i < A.hi, s_src, &s_n, s_off);
+  iaf_neuron_push(A, so, po, clk, k0, M, i, i < A.hi, s_src, &s_n, s_off);
 }
 
 // All iaf_psc_exp groups in one launch (a network of several populations would
@@ -240,7 +241,8 @@ __global__ void __launch_bounds__(256, 3) iaf_multi_kernel(const IafArgs *tab, c
 
 // The multi-group launch with delivery at emission.
 __global__ void __launch_bounds__(256, 3) iaf_push_multi_kernel(const IafArgs *tab, const int *blk0, int ngroups,
-                                                             const SpikeOut so, const Clock *clk, int k0, int M) {
+                                                             const SpikeOut so, const PushOut po, const Clock *clk,
+                                                             int k0, int M) {
   pdl_enter();
   int lo = 0, hi = ngroups;   // largest g with blk0[g] <= blockIdx.x
   while (hi - lo > 1) {
@@ -252,7 +254,7 @@ __global__ void __launch_bounds__(256, 3) iaf_push_multi_kernel(const IafArgs *t
   __shared__ int s_src[256];
   __shared__ int s_n;
   __shared__ long long s_off[PUSH_OFF_SMEM];
-  iaf_neuron_push(A, so, clk, k0, M, i, i < A.hi, s_src, &s_n, s_off);
+  iaf_neuron_push(A, so, po, clk, k0, M, i, i < A.hi, s_src, &s_n, s_off);
 }
 
 // ---------------------------------------------------------------------------
@@ -650,18 +652,20 @@ int launch_aeif(int model, const AeifArgs &A, const SpikeOut &so, const Clock *c
   return 0;
 }
 
-int launch_iaf(const IafArgs &A, const SpikeOut &so, const Clock *clk, int k0, int M, cudaStream_t st) {
+int launch_iaf(const IafArgs &A, const SpikeOut &so, const PushOut *po, const Clock *clk, int k0, int M,
+               cudaStream_t st) {
   if (A.hi <= A.lo) return 0;
-  launch_k(so.push_acc ? iaf_push_batch_kernel : iaf_batch_kernel, dim3((A.hi - A.lo + 255) / 256), dim3(256), 0,
-           st, A, so, clk, k0, M);
+  const dim3 g((A.hi - A.lo + 255) / 256), b(256);
+  if (po) launch_k(iaf_push_batch_kernel, g, b, 0, st, A, so, *po, clk, k0, M);
+  else launch_k(iaf_batch_kernel, g, b, 0, st, A, so, clk, k0, M);
   return 1;
 }
 
 int launch_iaf_multi(const IafArgs *tab, const int *blk0, int ngroups, int nblocks, const SpikeOut &so,
-                     const Clock *clk, int k0, int M, cudaStream_t st) {
+                     const PushOut *po, const Clock *clk, int k0, int M, cudaStream_t st) {
   if (nblocks <= 0) return 0;
-  launch_k(so.push_acc ? iaf_push_multi_kernel : iaf_multi_kernel, dim3(nblocks), dim3(256), 0, st, tab, blk0,
-           ngroups, so, clk, k0, M);
+  if (po) launch_k(iaf_push_multi_kernel, dim3(nblocks), dim3(256), 0, st, tab, blk0, ngroups, so, *po, clk, k0, M);
+  else launch_k(iaf_multi_kernel, dim3(nblocks), dim3(256), 0, st, tab, blk0, ngroups, so, clk, k0, M);
   return 1;
 }
 

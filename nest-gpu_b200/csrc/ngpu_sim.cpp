@@ -717,15 +717,20 @@ SpikeOut Engine::spike_out() const {
   so.rev_cnt = d_rev_cnt_;
   so.rev_R = rev_R_;
   so.rev_cap = rev_cap_;
-  so.push_acc = push_ ? d_pacc_ : nullptr;
-  so.push_R = push_R_;
-  so.push_stride = n_acc_;
-  so.ev_off = d_ev_off_;
-  so.edge = d_edge_;
-  so.dmin = dmin_;
-  so.dspan = dspan_;
-  so.n_events = d_counters_ + 1;
   return so;
+}
+
+PushOut Engine::push_out() const {
+  PushOut po;
+  po.acc = d_pacc_;
+  po.R = push_R_;
+  po.stride = n_acc_;
+  po.ev_off = d_ev_off_;
+  po.edge = d_edge_;
+  po.dmin = dmin_;
+  po.dspan = dspan_;
+  po.n_events = d_counters_ + 1;
+  return po;
 }
 
 static GroupSpikeRec spike_rec(Group &g) {
@@ -751,11 +756,7 @@ GroupInput Engine::group_input(Group &g) {
   GroupInput in;
   in.acc = d_acc_ + g.acc_off;
   in.slot_stride = n_acc_;
-  in.ring_R = 0;
-  if (push_ && g.model == M_IAF_PSC_EXP) {
-    in.acc = d_pacc_ + g.acc_off;
-    in.ring_R = push_R_;
-  }
+  if (push_ && g.model == M_IAF_PSC_EXP) in.acc = d_pacc_ + g.acc_off;   // the delivery-at-emission ring
   in.pin_off = g.d_pin_off;
   in.pin = g.d_pin;
   in.gen = d_gen_;
@@ -998,6 +999,7 @@ void Engine::build_plastic(const std::vector<size_t> &pl_edge, const std::vector
 // One batch of M steps starting at graph step k0: delivery, then every group.
 void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
   SpikeOut so = spike_out();
+  const PushOut po = push_out();
   // With aeif groups and other spiking groups in the network, the others run on a second
   // stream next to the aeif kernels: they then fill the SMs that the aeif straggler tail
   // leaves idle.  The groups touch disjoint state (their own accumulator rows, node
@@ -1031,10 +1033,11 @@ void Engine::launch_batch(int k0, int M, std::vector<cudaEvent_t> *ev) {
     s2 = stream2_;
   }
   if (n_iaf_multi_ >= 2)
-    count_launch(launch_iaf_multi(d_iaf_tab_, d_iaf_blk0_, n_iaf_multi_, iaf_multi_blocks_, so, d_clk_, k0, M, s2));
+    count_launch(launch_iaf_multi(d_iaf_tab_, d_iaf_blk0_, n_iaf_multi_, iaf_multi_blocks_, so, push_ ? &po : nullptr,
+                                  d_clk_, k0, M, s2));
   for (auto &g : groups_) {
     if (g.model == M_IAF_PSC_EXP && n_iaf_multi_ < 2)
-      count_launch(launch_iaf(iaf_args(g), so, d_clk_, k0, M, s2));
+      count_launch(launch_iaf(iaf_args(g), so, push_ ? &po : nullptr, d_clk_, k0, M, s2));
     else if (g.model == M_SPIKE_GEN) count_launch(launch_spike_gen(sg_args(g), so, d_clk_, k0, M, s2));
     else if (g.model == M_PARROT) count_launch(launch_parrot(parrot_args(g), so, d_clk_, k0, M, s2));
     else if (g.model == M_SPIKE_DET) count_launch(launch_spike_det(parrot_args(g), so, d_clk_, k0, M, s2));

@@ -53,8 +53,6 @@ struct Clock {
 };
 
 // Spike output context shared by all spiking models.
-struct EdgeW;
-
 struct SpikeOut {
   int2 *ring;            // [R][cap] (source node, height bits), slot = time index % R
   int *ring_cnt;         // [R]
@@ -77,17 +75,6 @@ struct SpikeOut {
   int *rev_ring;         // [rev_R][rev_cap] nodes whose spike reaches their synapses then
   int *rev_cnt;          // [rev_R]
   int rev_R, rev_cap;
-  // Delivery at emission (networks of iaf_psc_exp groups, push_acc non-null): the update
-  // kernel's warp adds each spike's out-edges at once into the accumulator ring
-  // push_acc[push_R][push_stride], slot = arrival time index % push_R; the spike ring is
-  // then not used.
-  double *push_acc;
-  int push_R;
-  size_t push_stride;
-  const long long *ev_off;   // delivery CSR [n_nodes * dspan + 1]
-  const EdgeW *edge;
-  int dmin, dspan;
-  unsigned long long *n_events;
 };
 
 // Per-group spike bookkeeping (optional outputs).
@@ -129,10 +116,9 @@ struct GenPar {
 
 // Input side of a group: accumulator slots (one per step of a batch) and poiss_gen edges.
 struct GroupInput {
-  double *acc;           // slot 0 row of this group: acc + m*slot_stride + p*n + i
+  double *acc;           // slot 0 row of this group: acc + m*slot_stride + p*n + i (delivery at
+                         // emission: the ring row, slot = time index % PushOut::R)
   size_t slot_stride;    // doubles per slot (all groups)
-  int ring_R;            // 0: slot m = step m of the batch; > 0: acc is the delivery-at-emission
-                         // ring, slot = time index % ring_R
   const int *pin_off;    // [n+1] or null
   const PoissonIn *pin;
   const GenPar *gen;
@@ -236,6 +222,19 @@ struct SpikeGenArgs {
 struct EdgeW {
   uint32_t acc;
   float w;
+};
+
+// Delivery at emission (networks of iaf_psc_exp groups): the update kernel's block adds each
+// spike's out-edges at once into the accumulator ring acc[R][stride], slot = arrival time
+// index % R; the spike ring is then not used.
+struct PushOut {
+  double *acc;
+  int R;
+  size_t stride;
+  const long long *ev_off;   // delivery CSR [n_nodes * dspan + 1]
+  const EdgeW *edge;
+  int dmin, dspan;
+  unsigned long long *n_events;
 };
 
 struct DeliverArgs {
