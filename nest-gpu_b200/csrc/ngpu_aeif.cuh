@@ -888,11 +888,13 @@ __global__ void __launch_bounds__(OCC == 2 ? 128 : 256, OCC == 1 ? 3 : (OCC == 2
 }
 
 // Neurons the main kernel left unfinished (typically the few that spike in the batch)
-// continue here from the step where they stopped, one per thread.
+// continue here from the step where they stopped, one per thread.  The kernel's length is
+// the longest sub-step chain, so it gets all the registers it wants (151 for the benchmark's
+// model; with 256-thread bounds it was held to 127: RTF 0.6490-0.6509 against 0.6456-0.6471).
 // (The trial-per-iteration form measured 2.5% slower here than the step-at-once form: the
 // lanes of this kernel are all in long sub-step chains.)
 template <int MODEL, int PMAX, bool FIXED, int LM, bool UNI = false>
-__global__ void __launch_bounds__(256) aeif_straggler_kernel(const AeifArgs A, const SpikeOut so,
+__global__ void __launch_bounds__(128, 1) aeif_straggler_kernel(const AeifArgs A, const SpikeOut so,
                                                              const Clock *clk, int k0, int M) {
   pdl_enter();
   typedef AeifShape<MODEL> S;
